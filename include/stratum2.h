@@ -1,0 +1,233 @@
+/*
+ * stratum2.h -- C ABI of the B200 path-tracing hot path (unidirectional path tracing with
+ * next-event estimation and ReSTIR DI), a drop-in for the renderer path of Shmaug/Stratum2.
+ *
+ * Every entry point returns an int status (S2_OK == 0, negative S2_ERR_* on failure), never
+ * throws and never aborts.  s2_last_error() returns a message for the last failing call on a
+ * context.  All structs are plain C: pointers, sizes and fixed-width integers; no C++ or torch
+ * types cross this boundary.
+ *
+ * Reference interfaces replaced (paths relative to the Stratum2 source tree):
+ *   - scene buffers:  Scene::FrameData descriptors bound to SceneParameters
+ *                     (src/App/Scene.cpp:768-790, src/Shaders/common/scene.hlsli:6-41)
+ *   - renderer:       TestRenderer::render(CommandBuffer&, const Image::View&)
+ *                     (src/App/TestRenderer.hpp:20, src/App/TestRenderer.cpp:284-763)
+ *                     VCM::render in kPathTrace mode for minPathLength/maxPathLength
+ *                     (src/App/VCM.cpp:39-40)
+ *   - ray queries:    traceRay / traceVisibilityRay (src/Shaders/common/intersection.hlsli:68-338)
+ *   - exposure:       Tonemapper --exposure (src/App/Tonemapper.cpp:25, kernels/tonemap.slang:154)
+ */
+#ifndef STRATUM2_H_
+#define STRATUM2_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define S2_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define S2_OK               0
+#define S2_ERR_INVALID     -1  /* bad argument (null pointer, size, unknown flag) */
+#define S2_ERR_CUDA        -2  /* a CUDA runtime call failed */
+#define S2_ERR_OOM         -3  /* device allocation failed or allocation budget exceeded */
+#define S2_ERR_NO_SCENE    -4  /* render/trace before s2_scene_upload + s2_build_bvh */
+#define S2_ERR_TIMEOUT     -5  /* a bounded device wait gave up (status word set by a kernel) */
+#define S2_ERR_DEVICE      -6  /* a kernel reported an internal error (stack/queue overflow) */
+#define S2_ERR_UNSUPPORTED -7  /* feature not supported on this device / build */
+
+/* ---- reference-format constants (src/Shaders/compat/scene.h:13-24) ---------------------- */
+#define S2_INVALID_INDEX16       0xFFFFu      /* INVALID_INSTANCE / INVALID_PRIMITIVE */
+#define S2_INVALID_INDEX32       0xFFFFFFFFu
+#define S2_INSTANCE_TYPE_MESH    0u
+#define S2_INSTANCE_TYPE_SPHERE  1u           /* accepted, not rendered (no spheres on this path) */
+#define S2_INSTANCE_TYPE_VOLUME  2u           /* accepted, not rendered (no media on this path) */
+#define S2_NO_BUFFER             0xFFFFu      /* MeshVertexInfo buffer index meaning "absent" */
+#define S2_NO_IMAGE              0xFFFFFFFFu  /* material / environment image index "absent" */
+#define S2_NO_ENVIRONMENT        0xFFFFFFFFu  /* environment material address "absent" */
+#define S2_MATERIAL_RECORD_BYTES 64u          /* Material::store (src/App/Material.hpp:22-38) */
+
+typedef struct S2Context S2Context;
+
+/* A float image: RGBA (channels 4), RG (2) or R (1) texels, row-major, level 0 only. Mip levels
+ * needed by environment importance sampling are built on the device by 2x2 averaging. */
+typedef struct S2Image {
+    uint32_t width, height, channels;
+    const float* texels;           /* host pointer, width*height*channels floats */
+} S2Image;
+
+/* Packed scene, byte-compatible with the reference's frame data:
+ *   instances          InstanceData[n] = {type:4 | materialAddress:28, data}   (compat/scene.h:30-58)
+ *                      mesh data = vertexInfoIndex:16 | primitiveCount:16
+ *   primitive_counts   optional u32[n]: 32-bit primitive counts that override the 16-bit field,
+ *                      so one instance may hold more than 65,535 triangles
+ *   transforms         TransformData[n] = row-major float 3x4 object-to-world (compat/transform.h:7)
+ *   inverse/motion     optional (NULL => computed / identity motion)
+ *   vertex_infos       MeshVertexInfo[] = 8 x u32 each (compat/scene.h:89-132)
+ *   vertex_buffers     ByteAddressBuffer[]: indices (u16/u32), float3 positions/normals, float2 uvs
+ *   material_data      byte-address buffer of 64-B material records plus the 16-B environment
+ *                      record {float3 emission scale, u32 image} (src/App/Scene.hpp:41-45)
+ *   light maps         mLightInstanceMap / mInstanceLightMap (src/App/Scene.cpp:441-491)
+ */
+typedef struct S2SceneDesc {
+    uint32_t instance_count;
+    const uint32_t* instances;            /* 2*instance_count */
+    const uint32_t* primitive_counts;     /* optional, instance_count */
+    const float* transforms;              /* 12*instance_count */
+    const float* inverse_transforms;      /* optional, 12*instance_count */
+    const float* motion_transforms;       /* optional, 12*instance_count */
+
+    uint32_t vertex_info_count;
+    const uint32_t* vertex_infos;         /* 8*vertex_info_count */
+
+    uint32_t vertex_buffer_count;
+    const void* const* vertex_buffers;    /* host pointers */
+    const uint64_t* vertex_buffer_bytes;
+
+    uint32_t material_bytes;
+    const void* material_data;
+
+    uint32_t light_count;
+    const uint32_t* light_instance_map;   /* light_count */
+    const uint32_t* instance_light_map;   /* optional, instance_count */
+
+    uint32_t environment_material_address; /* S2_NO_ENVIRONMENT if none */
+
+    uint32_t image_count;
+    const S2Image* images;
+
+    float scene_sphere[4];                /* center xyz, radius (TestRenderer.cpp:458-461) */
+} S2SceneDesc;
+
+/* BVH8 build parameters (the reference delegates this to vkCmdBuildAccelerationStructuresKHR,
+ * src/App/Scene.cpp:17-55). */
+typedef struct S2BvhParams {
+    uint32_t max_leaf_size;   /* triangles per BVH8 leaf slot, 1..3 (default 3) */
+    uint32_t sah_bins;        /* binned-SAH bins (default 32) */
+    uint32_t threads;         /* host build threads (0 = all) */
+    uint32_t reserved;
+} S2BvhParams;
+
+typedef struct S2BvhStats {
+    uint64_t node_count, triangle_count, leaf_slot_count;
+    uint32_t max_depth, reserved;
+    double build_seconds;
+    double sah_cost;
+} S2BvhStats;
+
+/* Ray and hit for the parity / query entry point s2_trace. */
+typedef struct S2Ray {
+    float origin[3];
+    float tmin;
+    float direction[3];
+    float tmax;
+} S2Ray;                                   /* 32 B */
+
+typedef struct S2Hit {
+    float t;                               /* distance, or tmax when missed */
+    uint32_t instance;                     /* S2_INVALID_INDEX32 when missed */
+    uint32_t primitive;
+    float barycentrics[2];                 /* weights of vertex 1 and vertex 2 */
+} S2Hit;                                   /* 20 B */
+
+/* A pinhole view: ViewData + camera TransformData (compat/scene.h:134-167, transform.h:128-190).
+ * The camera looks down -z of its transform; projection is the reference's reversed-z
+ * perspective (makePerspective, transform.h:181-190). */
+typedef struct S2View {
+    float projection[8];      /* ProjectionData: scale.xy, offset.xy, near, far, sensorArea, vfov */
+    int32_t image_min[2];
+    int32_t image_max[2];
+    float camera_to_world[12];
+    float prev_world_to_camera[12];  /* previous frame's inverse transform (prev-UV AOV) */
+} S2View;
+
+/* Render flags */
+#define S2_FLAG_PIXEL_JITTER        (1u << 0)  /* gPixelJitter (off in the reference) */
+#define S2_FLAG_LAMBERTIAN          (1u << 1)  /* gLambertian: Lambertian instead of Disney */
+#define S2_FLAG_PCG32               (1u << 2)  /* PCG32 per-pixel stream instead of pcg4d */
+#define S2_FLAG_NO_NEE              (1u << 3)  /* disable gSampleDirectIllumination */
+#define S2_FLAG_RESTIR_DI           (1u << 4)  /* gReSTIR_DI: RIS over candidate light samples */
+#define S2_FLAG_REFERENCE_ENV_MIS   (1u << 5)  /* BSDF-hit environment MIS with the disc pdf 1/(pi R^2)
+                                                  as the reference does (testrenderer.slang:1047-1050) */
+#define S2_FLAG_NO_RR               (1u << 6)  /* disable Russian roulette */
+#define S2_FLAG_ACCUMULATE          (1u << 7)  /* add into the previous accumulation (progressive) */
+#define S2_FLAG_SHADING_NORMALS_OFF (1u << 8)  /* ignore vertex normals (gShadingNormals false) */
+
+typedef struct S2RenderParams {
+    uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */
+    uint32_t max_path_length;        /* mMaxDepth / --maxPathLength */
+    float exposure;                  /* radiance *= 2^exposure on output */
+    uint32_t spp;                    /* samples per pixel in this call */
+    uint32_t frame_seed;             /* sample s uses RNG seed frame_seed + s (mRandomSeed) */
+    uint32_t flags;                  /* S2_FLAG_* */
+    float environment_sample_probability; /* default 0.9 (TestRenderer.cpp:41) */
+    uint32_t restir_candidates;      /* mCandidateSamples (default 32) */
+    float restir_max_m;              /* mMaxM (default 3) */
+    uint32_t restir_spatial_count;   /* screen-space spatial neighbours (0 = off) */
+    float restir_spatial_radius;     /* pixels */
+    uint32_t restir_temporal;        /* 1 = reuse the previous call's reservoirs */
+    uint32_t wave_paths;             /* paths in flight per wave (0 = automatic) */
+    uint32_t reserved[7];
+} S2RenderParams;
+
+/* Output AOVs (caller-allocated, device or host pointers per s2_render's `out_on_host`).
+ * Any pointer may be NULL to skip that AOV.  Layouts follow TestRenderer's images
+ * (TestRenderer.cpp:323-347, testrenderer.slang:195-218). */
+typedef struct S2Aovs {
+    float* radiance;        /* float4 per pixel: mean radiance * 2^exposure, w = 1 */
+    float* albedo;          /* float4 per pixel: baseColor at the first hit, 1 on a miss */
+    uint32_t* visibility;   /* uint2 per pixel: {instance:16 | primitive:16, packed shading normal} */
+    float* depth;           /* float4 per pixel: {depth, prevDepth, 1, 1} */
+    float* prev_uv;         /* float2 per pixel */
+    uint32_t* ids32;        /* uint2 per pixel: {instance, primitive} as 32-bit ids */
+} S2Aovs;
+
+/* Per-call statistics (device counters, read back after the call). */
+typedef struct S2RenderStats {
+    uint64_t extension_rays;   /* closest-hit rays traced */
+    uint64_t shadow_rays;      /* any-hit rays traced */
+    uint64_t paths;            /* camera paths (pixels x spp) */
+    uint64_t nan_count;        /* paths dropped for NaN/Inf throughput */
+    double gpu_ms;             /* device time of the call (CUDA events) */
+} S2RenderStats;
+
+/* ---- lifecycle --------------------------------------------------------------------------- */
+int  s2_get_abi_version(void);
+int  s2_create(int device, S2Context** out);
+void s2_destroy(S2Context* ctx);
+const char* s2_last_error(const S2Context* ctx);
+int  s2_sync(S2Context* ctx);
+/* Use `stream` (a cudaStream_t) for all work of this context; NULL = the context's own stream. */
+int  s2_set_stream(S2Context* ctx, void* stream);
+
+/* ---- scene ------------------------------------------------------------------------------- */
+/* Copies the packed scene to the device (inputs are host pointers; the caller keeps ownership). */
+int  s2_scene_upload(S2Context* ctx, const S2SceneDesc* scene);
+/* Builds the BVH8 over all mesh instances (flattened to world space). */
+int  s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStats* stats_out);
+
+/* ---- queries (replace traceRay / traceVisibilityRay) ------------------------------------- */
+/* rays/hits are DEVICE pointers when on_device != 0, else host pointers.
+ * anyhit != 0: first-hit query (RAY_FLAG_ACCEPT_FIRST_HIT_AND_END_SEARCH); hit.t is then the
+ * found hit's distance and only hit.instance != S2_INVALID_INDEX32 is meaningful.
+ * Closest-hit ties (equal t) resolve to the lowest (instance, primitive). */
+int  s2_trace(S2Context* ctx, const S2Ray* rays, uint32_t count, int anyhit, S2Hit* hits, int on_device);
+/* Same query with per-ray node/triangle fetch counts (uint32 pairs, device or host as above). */
+int  s2_trace_counted(S2Context* ctx, const S2Ray* rays, uint32_t count, int anyhit, S2Hit* hits,
+                      uint32_t* fetch_counts, int on_device);
+
+/* ---- rendering (replaces TestRenderer::render) ------------------------------------------- */
+int  s2_render(S2Context* ctx, const S2View* view, const S2RenderParams* params,
+               const S2Aovs* out, int out_on_host, S2RenderStats* stats_out);
+
+/* Defaults as in the reference (TestRenderer.cpp:38-43, VCM.cpp:39-40). */
+void s2_default_render_params(S2RenderParams* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif  /* STRATUM2_H_ */

@@ -1,0 +1,161 @@
+"""ctypes mirror of include/stratum2.h.
+
+Loading fails loudly when the CUDA library is missing: there is no CPU fallback for the product
+path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "libstratum2_b200.so"
+
+S2_OK = 0
+S2_ERR_INVALID = -1
+S2_ERR_CUDA = -2
+S2_ERR_OOM = -3
+S2_ERR_NO_SCENE = -4
+S2_ERR_TIMEOUT = -5
+S2_ERR_DEVICE = -6
+S2_ERR_UNSUPPORTED = -7
+
+INVALID_INDEX16 = 0xFFFF
+INVALID_INDEX32 = 0xFFFFFFFF
+NO_BUFFER = 0xFFFF
+NO_IMAGE = 0xFFFFFFFF
+NO_ENVIRONMENT = 0xFFFFFFFF
+
+FLAG_PIXEL_JITTER = 1 << 0
+FLAG_LAMBERTIAN = 1 << 1
+FLAG_PCG32 = 1 << 2
+FLAG_NO_NEE = 1 << 3
+FLAG_RESTIR_DI = 1 << 4
+FLAG_REFERENCE_ENV_MIS = 1 << 5
+FLAG_NO_RR = 1 << 6
+FLAG_ACCUMULATE = 1 << 7
+FLAG_SHADING_NORMALS_OFF = 1 << 8
+
+# every symbol include/stratum2.h declares
+EXPORTED_SYMBOLS = [
+    "s2_get_abi_version", "s2_create", "s2_destroy", "s2_last_error", "s2_sync", "s2_set_stream",
+    "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
+    "s2_default_render_params",
+]
+
+
+class S2Image(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("channels", C.c_uint32),
+                ("texels", C.POINTER(C.c_float))]
+
+
+class S2SceneDesc(C.Structure):
+    _fields_ = [
+        ("instance_count", C.c_uint32),
+        ("instances", C.POINTER(C.c_uint32)),
+        ("primitive_counts", C.POINTER(C.c_uint32)),
+        ("transforms", C.POINTER(C.c_float)),
+        ("inverse_transforms", C.POINTER(C.c_float)),
+        ("motion_transforms", C.POINTER(C.c_float)),
+        ("vertex_info_count", C.c_uint32),
+        ("vertex_infos", C.POINTER(C.c_uint32)),
+        ("vertex_buffer_count", C.c_uint32),
+        ("vertex_buffers", C.POINTER(C.c_void_p)),
+        ("vertex_buffer_bytes", C.POINTER(C.c_uint64)),
+        ("material_bytes", C.c_uint32),
+        ("material_data", C.c_void_p),
+        ("light_count", C.c_uint32),
+        ("light_instance_map", C.POINTER(C.c_uint32)),
+        ("instance_light_map", C.POINTER(C.c_uint32)),
+        ("environment_material_address", C.c_uint32),
+        ("image_count", C.c_uint32),
+        ("images", C.POINTER(S2Image)),
+        ("scene_sphere", C.c_float * 4),
+    ]
+
+
+class S2BvhParams(C.Structure):
+    _fields_ = [("max_leaf_size", C.c_uint32), ("sah_bins", C.c_uint32), ("threads", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class S2BvhStats(C.Structure):
+    _fields_ = [("node_count", C.c_uint64), ("triangle_count", C.c_uint64), ("leaf_slot_count", C.c_uint64),
+                ("max_depth", C.c_uint32), ("reserved", C.c_uint32), ("build_seconds", C.c_double),
+                ("sah_cost", C.c_double)]
+
+
+class S2Ray(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("tmin", C.c_float), ("direction", C.c_float * 3), ("tmax", C.c_float)]
+
+
+class S2Hit(C.Structure):
+    _fields_ = [("t", C.c_float), ("instance", C.c_uint32), ("primitive", C.c_uint32),
+                ("barycentrics", C.c_float * 2)]
+
+
+class S2View(C.Structure):
+    _fields_ = [("projection", C.c_float * 8), ("image_min", C.c_int32 * 2), ("image_max", C.c_int32 * 2),
+                ("camera_to_world", C.c_float * 12), ("prev_world_to_camera", C.c_float * 12)]
+
+
+class S2RenderParams(C.Structure):
+    _fields_ = [
+        ("min_path_length", C.c_uint32), ("max_path_length", C.c_uint32), ("exposure", C.c_float),
+        ("spp", C.c_uint32), ("frame_seed", C.c_uint32), ("flags", C.c_uint32),
+        ("environment_sample_probability", C.c_float), ("restir_candidates", C.c_uint32),
+        ("restir_max_m", C.c_float), ("restir_spatial_count", C.c_uint32),
+        ("restir_spatial_radius", C.c_float), ("restir_temporal", C.c_uint32),
+        ("wave_paths", C.c_uint32), ("reserved", C.c_uint32 * 7),
+    ]
+
+
+class S2Aovs(C.Structure):
+    _fields_ = [("radiance", C.c_void_p), ("albedo", C.c_void_p), ("visibility", C.c_void_p),
+                ("depth", C.c_void_p), ("prev_uv", C.c_void_p), ("ids32", C.c_void_p)]
+
+
+class S2RenderStats(C.Structure):
+    _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
+                ("nan_count", C.c_uint64), ("gpu_ms", C.c_double)]
+
+
+assert C.sizeof(S2Ray) == 32 and C.sizeof(S2Hit) == 20
+assert C.sizeof(S2RenderParams) == 80
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libstratum2_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise RuntimeError(f"{_LIB_PATH} is missing: build it with `python -m stratum2_b200.build`")
+    L = C.CDLL(str(_LIB_PATH))
+    P = C.POINTER
+    L.s2_get_abi_version.restype = C.c_int
+    L.s2_create.argtypes = [C.c_int, P(C.c_void_p)]
+    L.s2_destroy.argtypes = [C.c_void_p]
+    L.s2_destroy.restype = None
+    L.s2_last_error.argtypes = [C.c_void_p]
+    L.s2_last_error.restype = C.c_char_p
+    L.s2_sync.argtypes = [C.c_void_p]
+    L.s2_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.s2_scene_upload.argtypes = [C.c_void_p, P(S2SceneDesc)]
+    L.s2_build_bvh.argtypes = [C.c_void_p, P(S2BvhParams), P(S2BvhStats)]
+    L.s2_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_int]
+    L.s2_trace_counted.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    L.s2_render.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), C.c_int, P(S2RenderStats)]
+    L.s2_default_render_params.argtypes = [P(S2RenderParams)]
+    L.s2_default_render_params.restype = None
+    for name in EXPORTED_SYMBOLS:
+        getattr(L, name)
+    _lib = L
+    return L
+
+
+class S2Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"stratum2 error {code}: {msg}")
+        self.code = code

@@ -1,0 +1,143 @@
+"""Host-side mirror of the reference's renderer interface over the C ABI.
+
+`Device` owns one S2Context (one CUDA stream).  `Device.render(...)` plays the role of
+TestRenderer::render (src/App/TestRenderer.cpp:284-763) with the VCM path-length arguments
+(--minPathLength / --maxPathLength, src/App/VCM.cpp:39-40) and the tonemapper's --exposure
+(src/App/Tonemapper.cpp:25).  Errors raise S2Error with the library's message, matching the
+reference's host-side exceptions (std::runtime_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import S2Error
+
+
+@dataclass
+class RenderResult:
+    radiance: np.ndarray      # (H, W, 4) float32
+    albedo: np.ndarray        # (H, W, 4) float32
+    visibility: np.ndarray    # (H, W, 2) uint32
+    depth: np.ndarray         # (H, W, 4) float32
+    prev_uv: np.ndarray       # (H, W, 2) float32
+    ids32: np.ndarray         # (H, W, 2) uint32
+    stats: _abi.S2RenderStats
+
+
+def rays_array(origins, directions, tmin=0.0, tmax=np.inf) -> np.ndarray:
+    """Packs rays as S2Ray records (float32 x 8)."""
+    o = np.asarray(origins, np.float32).reshape(-1, 3)
+    d = np.asarray(directions, np.float32).reshape(-1, 3)
+    n = o.shape[0]
+    r = np.empty((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 3] = tmin
+    r[:, 4:7] = d
+    r[:, 7] = tmax
+    return r
+
+
+def hits_from_bytes(buf: np.ndarray) -> dict:
+    rec = np.frombuffer(buf.tobytes(), dtype=np.dtype([("t", "<f4"), ("instance", "<u4"), ("primitive", "<u4"),
+                                                       ("b1", "<f4"), ("b2", "<f4")]))
+    return {k: rec[k].copy() for k in rec.dtype.names}
+
+
+class Device:
+    def __init__(self, device: int = 0):
+        self._lib = _abi.lib()
+        h = C.c_void_p()
+        rc = self._lib.s2_create(device, C.byref(h))
+        if rc != _abi.S2_OK:
+            raise S2Error(rc, "s2_create failed (no CUDA device?)")
+        self._h = h
+        self.bvh_stats = None
+        self.scene = None
+
+    def close(self):
+        if self._h:
+            self._lib.s2_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != _abi.S2_OK:
+            raise S2Error(rc, self._lib.s2_last_error(self._h).decode())
+
+    def upload_scene(self, scene, build: bool = True, max_leaf_size: int = 3):
+        self.scene = scene
+        d = scene.desc()
+        self._check(self._lib.s2_scene_upload(self._h, C.byref(d)))
+        if build:
+            p = _abi.S2BvhParams(max_leaf_size=max_leaf_size, sah_bins=32, threads=0)
+            st = _abi.S2BvhStats()
+            self._check(self._lib.s2_build_bvh(self._h, C.byref(p), C.byref(st)))
+            self.bvh_stats = st
+        return self
+
+    def trace(self, rays: np.ndarray, anyhit: bool = False, counted: bool = False):
+        """Closest-hit (or first-hit) query for host rays (n x 8 float32, S2Ray layout)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        out = np.zeros(n * 5, np.uint32)
+        if counted:
+            cnt = np.zeros(2 * n, np.uint32)
+            self._check(self._lib.s2_trace_counted(self._h, rays.ctypes.data, n, int(anyhit), out.ctypes.data,
+                                                   cnt.ctypes.data, 0))
+            return hits_from_bytes(out), cnt.reshape(n, 2)
+        self._check(self._lib.s2_trace(self._h, rays.ctypes.data, n, int(anyhit), out.ctypes.data, 0))
+        return hits_from_bytes(out)
+
+    def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, anyhit: bool = False):
+        """Same query with device pointers (e.g. torch tensors' data_ptr())."""
+        self._check(self._lib.s2_trace(self._h, C.c_void_p(rays_ptr), n, int(anyhit), C.c_void_p(hits_ptr), 1))
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self._lib.s2_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def sync(self):
+        self._check(self._lib.s2_sync(self._h))
+
+    @staticmethod
+    def default_params() -> _abi.S2RenderParams:
+        p = _abi.S2RenderParams()
+        _abi.lib().s2_default_render_params(C.byref(p))
+        return p
+
+    def render(self, view: _abi.S2View, width: int, height: int, spp: int = 1, min_path_length: int = 0,
+               max_path_length: int = 5, exposure: float = 0.0, frame_seed: int = 0, flags: int = 0,
+               params: _abi.S2RenderParams | None = None) -> RenderResult:
+        p = params if params is not None else self.default_params()
+        if params is None:
+            p.min_path_length = min_path_length
+            p.max_path_length = max_path_length
+            p.exposure = exposure
+            p.spp = spp
+            p.frame_seed = frame_seed
+            p.flags = flags
+        n = width * height
+        rad = np.zeros((height, width, 4), np.float32)
+        alb = np.zeros((height, width, 4), np.float32)
+        vis = np.zeros((height, width, 2), np.uint32)
+        dep = np.zeros((height, width, 4), np.float32)
+        puv = np.zeros((height, width, 2), np.float32)
+        ids = np.zeros((height, width, 2), np.uint32)
+        aov = _abi.S2Aovs(rad.ctypes.data, alb.ctypes.data, vis.ctypes.data, dep.ctypes.data, puv.ctypes.data,
+                          ids.ctypes.data)
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(p), C.byref(aov), 1, C.byref(st)))
+        return RenderResult(rad, alb, vis, dep, puv, ids, st)
+
+    def render_device(self, view, params: _abi.S2RenderParams, aovs: _abi.S2Aovs) -> _abi.S2RenderStats:
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(params), C.byref(aovs), 0, C.byref(st)))
+        return st

@@ -1,0 +1,61 @@
+// Internal context of the C ABI: one device, one stream, device-resident scene and BVH.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/stratum2.h"
+#include "s2_bvh_build.h"
+#include "s2_scene.cuh"
+
+namespace s2 {
+
+// A device allocation owned by the context.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct RenderState;  // wavefront queues and accumulators (s2_render.cu)
+
+struct HostImage {
+    uint32_t w = 0, h = 0;
+    std::vector<float> rgba;  // 4 floats per texel
+};
+
+}  // namespace s2
+
+struct S2Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;       // the stream work is issued on
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string last_error;
+    std::vector<s2::DevBuf> scene_bufs;  // freed on re-upload / destroy
+    std::vector<s2::DevBuf> bvh_bufs;
+    bool has_scene = false, has_bvh = false;
+
+    // host copies needed by the BVH build
+    std::vector<float> tri_v0, tri_v1, tri_v2;
+    std::vector<uint32_t> tri_inst, tri_prim;
+    std::vector<uint32_t> inst_tri_offset;  // flattened triangle base per instance
+
+    // device scene description (pointers into scene_bufs / bvh_bufs)
+    DevScene scene{};
+    std::vector<DevImage> images_host;      // device-side descriptors, host copy
+    DevImage* images_dev = nullptr;
+    uint8_t** vbufs_dev = nullptr;
+    int env_image = -1;
+
+    s2::RenderState* render = nullptr;
+    int* status_dev = nullptr;              // device status word (stack/queue overflow, timeouts)
+};
+
+namespace s2 {
+int set_error(S2Context* ctx, int code, const std::string& msg);
+int check_cuda(S2Context* ctx, cudaError_t e, const char* what);
+void* dev_alloc(S2Context* ctx, std::vector<DevBuf>& owner, size_t bytes);
+void free_bufs(std::vector<DevBuf>& bufs);
+void destroy_render_state(S2Context* ctx);
+}  // namespace s2

@@ -1,0 +1,223 @@
+// BVH8 traversal for closest-hit and first-hit queries.
+//
+// Replaces the hardware RayQuery loop of the reference (src/Shaders/common/intersection.hlsli:
+// 68-193, traceRay; :262-338, traceVisibilityRay without media).  Semantics kept from the
+// reference: a hit is accepted for tmin <= t <= tmax (RayDesc TMin/TMax); a first-hit query
+// (RAY_FLAG_ACCEPT_FIRST_HIT_AND_END_SEARCH) stops at the first accepted triangle.  Added here:
+// closest-hit ties (equal t) resolve to the lowest (instance, primitive) so results do not depend
+// on traversal order.
+//
+// Triangle test: watertight ray/triangle intersection (Woop, Benthin and Wald, JCGT 2013) with
+// the double-precision fallback for zero edge functions.  Every float operation uses an explicit
+// round-to-nearest intrinsic so the compiler cannot contract it into an FMA: the result is then
+// bit-identical to a CPU evaluation of the same operations in IEEE single precision.
+#pragma once
+#include "s2_bvh.h"
+#include "s2_math.cuh"
+
+struct TravRay {
+    float3 o, d;
+    float3 inv_d;
+    float tmin;
+    uint32_t oct;       // bit i set when d[i] < 0
+    int kx, ky, kz;     // watertight axis permutation
+    float Sx, Sy, Sz;   // shear constants
+};
+
+S2D float safe_inv(float d) {
+    // avoid 0*inf = NaN in the slab test for axis-parallel rays
+    const float dd = fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d;
+    return __fdiv_rn(1.f, dd);
+}
+
+S2D float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+S2D TravRay make_trav_ray(float3 o, float3 d, float tmin) {
+    TravRay r;
+    r.o = o; r.d = d; r.tmin = tmin;
+    r.inv_d = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    r.oct = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    if (comp(d, kz) < 0.f) { const int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    const float dz = comp(d, kz);
+    r.Sx = __fdiv_rn(comp(d, kx), dz);
+    r.Sy = __fdiv_rn(comp(d, ky), dz);
+    r.Sz = __fdiv_rn(1.f, dz);
+    return r;
+}
+
+// Watertight triangle test.  Returns true and sets t, b1, b2 when the triangle is hit with
+// tmin <= t <= tmax.
+S2D bool intersect_triangle(const TravRay& r, float3 v0, float3 v1, float3 v2, float tmax, float& t_out, float& b1, float& b2) {
+    const float3 A = f3(__fsub_rn(v0.x, r.o.x), __fsub_rn(v0.y, r.o.y), __fsub_rn(v0.z, r.o.z));
+    const float3 B = f3(__fsub_rn(v1.x, r.o.x), __fsub_rn(v1.y, r.o.y), __fsub_rn(v1.z, r.o.z));
+    const float3 C = f3(__fsub_rn(v2.x, r.o.x), __fsub_rn(v2.y, r.o.y), __fsub_rn(v2.z, r.o.z));
+    const float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+    const float Ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.Sx, Akz));
+    const float Ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.Sy, Akz));
+    const float Bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.Sx, Bkz));
+    const float By = __fsub_rn(comp(B, r.ky), __fmul_rn(r.Sy, Bkz));
+    const float Cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.Sx, Ckz));
+    const float Cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.Sy, Ckz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        U = (float)__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx));
+        V = (float)__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx));
+        W = (float)__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax));
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.f) return false;
+    const float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    const float t = __fdiv_rn(T, det);
+    if (!(t >= r.tmin && t <= tmax)) return false;
+    t_out = t;
+    b1 = __fdiv_rn(V, det);
+    b2 = __fdiv_rn(W, det);
+    return true;
+}
+
+struct TravHit {
+    float t;
+    uint32_t tri;        // triangle record index (BVH order), 0xffffffff when missed
+    uint32_t instance, primitive;
+    float b1, b2;
+};
+
+struct TravCounters { uint32_t nodes, tris; };
+
+S2D uint32_t extract_byte(uint32_t w, uint32_t i) { return (w >> (8 * i)) & 0xffu; }
+
+// Intersect the 8 children of `node` with [tmin, tmax].  Returns the hit mask in bit-position
+// space (bit b = slot b ^ oct) for internal children, and the triangle mask for leaf slots.
+S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint32_t node_idx, float tmax,
+                        uint32_t& child_base, uint32_t& imask, uint32_t& hits, uint32_t& tri_base, uint32_t& trimask) {
+    const uint4* np = nodes4 + (size_t)node_idx * 8;  // 128-byte stride
+    const uint4 n0 = __ldg(np + 0);
+    const uint4 n1 = __ldg(np + 1);
+    const uint4 n2 = __ldg(np + 2);
+    const uint4 n3 = __ldg(np + 3);
+    const uint4 n4 = __ldg(np + 4);
+    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    const uint32_t ex = n0.w & 0xffu, ey = (n0.w >> 8) & 0xffu, ez = (n0.w >> 16) & 0xffu;
+    imask = n0.w >> 24;
+    child_base = n1.x;
+    tri_base = n1.y;
+    const uint32_t meta_lo = n1.z, meta_hi = n1.w;
+    const float sx = __uint_as_float(ex << 23) * r.inv_d.x;
+    const float sy = __uint_as_float(ey << 23) * r.inv_d.y;
+    const float sz = __uint_as_float(ez << 23) * r.inv_d.z;
+    const float ax = (px - r.o.x) * r.inv_d.x;
+    const float ay = (py - r.o.y) * r.inv_d.y;
+    const float az = (pz - r.o.z) * r.inv_d.z;
+    // near/far plane bytes per axis, swapped for negative directions
+    const uint32_t xlo0 = n2.x, xlo1 = n2.y, ylo0 = n2.z, ylo1 = n2.w;
+    const uint32_t zlo0 = n3.x, zlo1 = n3.y, xhi0 = n3.z, xhi1 = n3.w;
+    const uint32_t yhi0 = n4.x, yhi1 = n4.y, zhi0 = n4.z, zhi1 = n4.w;
+    const bool nx = r.inv_d.x < 0, ny = r.inv_d.y < 0, nz = r.inv_d.z < 0;
+    const uint32_t xn0 = nx ? xhi0 : xlo0, xn1 = nx ? xhi1 : xlo1, xf0 = nx ? xlo0 : xhi0, xf1 = nx ? xlo1 : xhi1;
+    const uint32_t yn0 = ny ? yhi0 : ylo0, yn1 = ny ? yhi1 : ylo1, yf0 = ny ? ylo0 : yhi0, yf1 = ny ? ylo1 : yhi1;
+    const uint32_t zn0 = nz ? zhi0 : zlo0, zn1 = nz ? zhi1 : zlo1, zf0 = nz ? zlo0 : zhi0, zf1 = nz ? zlo1 : zhi1;
+    const float tfar_lim = tmax * 1.0000004f;
+    hits = 0; trimask = 0;
+#pragma unroll
+    for (uint32_t s = 0; s < 8; ++s) {
+        const uint32_t w = s < 4 ? 0 : 1, i = s & 3;
+        const float qnx = (float)extract_byte(w ? xn1 : xn0, i), qfx = (float)extract_byte(w ? xf1 : xf0, i);
+        const float qny = (float)extract_byte(w ? yn1 : yn0, i), qfy = (float)extract_byte(w ? yf1 : yf0, i);
+        const float qnz = (float)extract_byte(w ? zn1 : zn0, i), qfz = (float)extract_byte(w ? zf1 : zf0, i);
+        const float tnx = fmaf(qnx, sx, ax), tfx = fmaf(qfx, sx, ax);
+        const float tny = fmaf(qny, sy, ay), tfy = fmaf(qfy, sy, ay);
+        const float tnz = fmaf(qnz, sz, az), tfz = fmaf(qfz, sz, az);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
+        const float tf = fminf(fminf(tfx, tfy), tfz) * 1.0000004f;
+        if (tn <= fminf(tf, tfar_lim)) {
+            if ((imask >> s) & 1u) {
+                hits |= 1u << (s ^ r.oct);
+            } else {
+                const uint32_t meta = extract_byte(w ? meta_hi : meta_lo, i);
+                const uint32_t cnt = meta >> 5, off = meta & 31u;
+                trimask |= ((1u << cnt) - 1u) << off;
+            }
+        }
+    }
+}
+
+// Traverse.  ANYHIT: stop at the first accepted triangle.  COUNT: count node and triangle
+// fetches into `ctr`.  Returns false if the stack overflowed (result may then be incomplete).
+template <bool ANYHIT, bool COUNT>
+S2D bool traverse(const TravRay& r, float tmax, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
+                  uint2* __restrict__ smem_stack, uint32_t lane_stride, TravHit& hit, TravCounters& ctr) {
+    hit.t = tmax; hit.tri = 0xffffffffu; hit.instance = 0xffffffffu; hit.primitive = 0xffffffffu;
+    hit.b1 = hit.b2 = 0.f;
+    uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
+    int sp = 0;
+    bool ok = true;
+    uint32_t node = 0;
+    float best_t = tmax;
+    while (true) {
+        uint32_t child_base, imask, hits, tri_base, trimask;
+        intersect_node(r, nodes4, node, best_t, child_base, imask, hits, tri_base, trimask);
+        if (COUNT) ctr.nodes++;
+        while (trimask) {
+            const uint32_t k = __ffs(trimask) - 1;
+            trimask &= trimask - 1;
+            const uint32_t ti = tri_base + k;
+            const float4 a = __ldg(tris4 + 3 * (size_t)ti + 0);
+            const float4 b = __ldg(tris4 + 3 * (size_t)ti + 1);
+            const float4 c = __ldg(tris4 + 3 * (size_t)ti + 2);
+            if (COUNT) ctr.tris++;
+            float t, b1, b2;
+            if (intersect_triangle(r, ld3(a), ld3(b), ld3(c), best_t, t, b1, b2)) {
+                const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+                if (ANYHIT) {
+                    hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+                    return ok;
+                }
+                if (t < best_t || inst < hit.instance || (inst == hit.instance && prim < hit.primitive)) {
+                    best_t = t;
+                    hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+                }
+            }
+        }
+        if (hits) {
+            const uint32_t b = __ffs(hits) - 1;
+            hits &= hits - 1;
+            const uint32_t s = b ^ r.oct;
+            const uint32_t next = child_base + __popc(imask & ((1u << s) - 1u));
+            if (hits) {
+                const uint2 g = make_uint2(child_base, imask | (hits << 8));
+                if (sp < S2_STACK_SMEM) smem_stack[sp * lane_stride] = g;
+                else if (sp < S2_STACK_DEPTH) lstack[sp - S2_STACK_SMEM] = g;
+                else ok = false;
+                if (sp < S2_STACK_DEPTH) sp++;
+            }
+            node = next;
+            continue;
+        }
+        if (sp == 0) break;
+        // take the nearest remaining child of the top group; pop the group when it empties
+        uint2 g = (sp - 1 < S2_STACK_SMEM) ? smem_stack[(sp - 1) * lane_stride] : lstack[sp - 1 - S2_STACK_SMEM];
+        uint32_t gh = g.y >> 8;
+        const uint32_t b = __ffs(gh) - 1;
+        gh &= gh - 1;
+        const uint32_t gi = g.y & 0xffu;
+        const uint32_t s = b ^ r.oct;
+        node = g.x + __popc(gi & ((1u << s) - 1u));
+        if (gh) {
+            g.y = gi | (gh << 8);
+            if (sp - 1 < S2_STACK_SMEM) smem_stack[(sp - 1) * lane_stride] = g;
+            else lstack[sp - 1 - S2_STACK_SMEM] = g;
+        } else {
+            sp--;
+        }
+    }
+    return ok;
+}

@@ -1,0 +1,148 @@
+"""ctypes access to the oracle (oracle/liboracle.so) and to the reference compat probe
+(oracle/_ref/libref_compat.so).  Test infrastructure only."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE = ROOT / "oracle" / "liboracle.so"
+REF = ROOT / "oracle" / "_ref" / "libref_compat.so"
+
+_o = None
+_r = None
+
+
+def oracle() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not ORACLE.exists():
+            import sys
+            sys.path.insert(0, str(ROOT / "oracle"))
+            from build_oracle import build_oracle  # noqa: E402
+            build_oracle()
+        L = C.CDLL(str(ORACLE))
+        P = C.POINTER
+        L.oracle_scene_create.restype = C.c_void_p
+        L.oracle_scene_create.argtypes = [C.c_void_p, C.c_int]
+        L.oracle_scene_destroy.argtypes = [C.c_void_p]
+        L.oracle_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.oracle_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_int]
+        L.oracle_pcg4d.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        L.oracle_pack_normal.restype = C.c_uint32
+        L.oracle_pack_normal.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.oracle_unpack_normal.argtypes = [C.c_uint32, C.c_void_p]
+        L.oracle_half_round.restype = C.c_float
+        L.oracle_half_round.argtypes = [C.c_float]
+        L.oracle_bsdf_eval.argtypes = [C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_bsdf_sample.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _o = L
+    return _o
+
+
+def ref_compat() -> C.CDLL | None:
+    global _r
+    if _r is None:
+        if not REF.exists():
+            return None
+        L = C.CDLL(str(REF))
+        L.ref_pack_material.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_unpack_material.argtypes = [C.c_void_p, C.c_float, C.c_void_p]
+        L.ref_mesh_instance.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]
+        L.ref_vertex_info.argtypes = [C.c_void_p, C.c_void_p]
+        L.ref_make_perspective.argtypes = [C.c_float, C.c_float, C.c_float, C.c_void_p]
+        L.ref_back_project.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+        L.ref_sizes.argtypes = [C.c_void_p]
+        _r = L
+    return _r
+
+
+class OracleScene:
+    """An oracle copy of a packed scene (precision_mask: 1 = FP64, 2 = FP32-exact, 3 = both)."""
+
+    def __init__(self, scene, precision_mask: int = 3):
+        self._desc = scene.desc()
+        self.h = oracle().oracle_scene_create(C.byref(self._desc), precision_mask)
+        assert self.h
+
+    def __del__(self):
+        try:
+            oracle().oracle_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    def trace(self, rays: np.ndarray, anyhit: bool = False, precision: int = 64, threads: int = 0) -> dict:
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        t = np.zeros(n)
+        inst = np.zeros(n, np.uint32)
+        prim = np.zeros(n, np.uint32)
+        b1 = np.zeros(n)
+        b2 = np.zeros(n)
+        rc = oracle().oracle_trace(self.h, rays.ctypes.data, n, int(anyhit), precision, t.ctypes.data,
+                                   inst.ctypes.data, prim.ctypes.data, b1.ctypes.data, b2.ctypes.data, threads)
+        assert rc == 0
+        return {"t": t, "instance": inst, "primitive": prim, "b1": b1, "b2": b2}
+
+    def render(self, view, params, width: int, height: int, precision: int = 64, rect=None, stride: int = 1,
+               threads: int = 0) -> dict:
+        x0, y0, x1, y1 = rect if rect is not None else (0, 0, width, height)
+        n = width * height
+        out = {
+            "sum": np.zeros((height, width, 3)), "sumsq": np.zeros((height, width, 3)),
+            "albedo": np.zeros((height, width, 4), np.float32), "visibility": np.zeros((height, width, 2), np.uint32),
+            "depth": np.zeros((height, width, 4), np.float32), "prev_uv": np.zeros((height, width, 2), np.float32),
+            "ids32": np.zeros((height, width, 2), np.uint32),
+        }
+        cnt = np.zeros(2, np.uint64)
+        rc = oracle().oracle_render(self.h, C.byref(view), C.byref(params), precision, x0, y0, x1, y1, stride,
+                                    out["sum"].ctypes.data, out["sumsq"].ctypes.data, out["albedo"].ctypes.data,
+                                    out["visibility"].ctypes.data, out["depth"].ctypes.data,
+                                    out["prev_uv"].ctypes.data, out["ids32"].ctypes.data, cnt.ctypes.data, threads)
+        assert rc == 0
+        out["extension_rays"] = int(cnt[0])
+        out["shadow_rays"] = int(cnt[1])
+        spp = max(params.spp, 1)
+        out["mean"] = out["sum"] / spp
+        out["var_of_mean"] = np.maximum(out["sumsq"] / spp - out["mean"] ** 2, 0) / max(spp - 1, 1)
+        return out
+
+
+def camera_rays(view, width: int, height: int) -> np.ndarray:
+    """Pixel-centre camera rays of a view, generated on the host in float64 then rounded
+    (used as seeded query rays, not as the renderer's own rays)."""
+    proj = np.array(view.projection[:], np.float64)
+    cam = np.array(view.camera_to_world[:], np.float64).reshape(3, 4)
+    ys, xs = np.mgrid[0:height, 0:width]
+    cx = 2 * (xs + 0.5) / width - 1
+    cy = -(2 * (ys + 0.5) / height - 1)
+    near = proj[4]
+    sg = np.sign(near)
+    d = np.stack([near * (cx * sg - proj[2]) / proj[0], near * (cy * sg - proj[3]) / proj[1],
+                  np.full_like(cx, near)], -1).reshape(-1, 3)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d @ cam[:, :3].T
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = np.broadcast_to(cam[:, 3], d.shape)
+    r = np.zeros((d.shape[0], 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    return r
+
+
+def random_rays(n: int, seed: int, lo=-1.2, hi=1.2) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo, hi, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    return r
