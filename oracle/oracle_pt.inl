@@ -380,7 +380,10 @@ template <class R> struct Tracer {
     }
 
     // ---------------------------------------------------------------- lights (lights.hlsli)
-    R texel_lum(const Image<R>& im, uint32_t level, int x, int y) const { return im.lum[level][(size_t)y * im.lw[level] + x]; }
+    R texel_lum(const Image<R>& im, uint32_t level, int x, int y) const {
+        if (x < 0 || y < 0 || x >= (int)im.lw[level] || y >= (int)im.lh[level]) return 0;  // outside the level
+        return im.lum[level][(size_t)y * im.lw[level] + x];
+    }
 
     // SampleTexel (lights.hlsli:49-96)
     void sample_texel(const Image<R>& im, R rx, R ry, R& u, R& v, R& pdf) const {

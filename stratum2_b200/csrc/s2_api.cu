@@ -197,6 +197,10 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
         const uint8_t* pbuf = (const uint8_t*)d->vertex_buffers[pb];
         const uint64_t isz = d->vertex_buffer_bytes[ib], psz = d->vertex_buffer_bytes[pb];
         const float* m = d->transforms + 12 * (size_t)i;
+        const uint32_t mat_addr = d->instances[2 * i] >> 4;
+        if ((uint64_t)mat_addr + S2_MATERIAL_RECORD_BYTES > d->material_bytes)
+            return set_error(ctx, S2_ERR_INVALID, "instance " + std::to_string(i) + ": material address out of range");
+        uint32_t max_index = 0;
         for (uint32_t p = 0; p < prim_counts[i]; ++p) {
             bool ok = true;
             uint32_t idx[3];
@@ -210,6 +214,7 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
                 for (int k = 0; k < 3; ++k) idx[k] = rd_u32(ibuf, isz, off + 4 * k, ok);
             }
             float wv[3][3];
+            for (int k = 0; k < 3 && ok; ++k) max_index = std::max(max_index, idx[k]);
             for (int k = 0; k < 3 && ok; ++k) {
                 const uint64_t po = (uint64_t)poff + (uint64_t)pstride * idx[k];
                 const float x = rd_f32(pbuf, psz, po, ok), y = rd_f32(pbuf, psz, po + 4, ok), z = rd_f32(pbuf, psz, po + 8, ok);
@@ -221,6 +226,19 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
             ctx->tri_inst.push_back(i);
             ctx->tri_prim.push_back(p);
         }
+        // optional normal / texcoord streams must cover every referenced vertex
+        const uint32_t nb = w[1] & 0xffffu, tb = w[1] >> 16;
+        const uint64_t need_n = (uint64_t)w[6] + (uint64_t)((w[2] >> 16) & 0xffu) * max_index + 12;
+        const uint64_t need_t = (uint64_t)w[7] + (uint64_t)(w[2] >> 24) * max_index + 8;
+        if (prim_counts[i] && nb < d->vertex_buffer_count && need_n > d->vertex_buffer_bytes[nb])
+            return set_error(ctx, S2_ERR_INVALID, "instance " + std::to_string(i) + ": normal stream out of buffer bounds");
+        if (prim_counts[i] && tb < d->vertex_buffer_count && need_t > d->vertex_buffer_bytes[tb])
+            return set_error(ctx, S2_ERR_INVALID, "instance " + std::to_string(i) + ": texcoord stream out of buffer bounds");
+    }
+    for (uint32_t l = 0; l < d->light_count; ++l) {
+        const uint32_t li = d->light_instance_map[l];
+        if ((d->instances[2 * li] & 0xfu) != S2_INSTANCE_TYPE_MESH || prim_counts[li] == 0)
+            return set_error(ctx, S2_ERR_INVALID, "light " + std::to_string(l) + " is not a non-empty mesh instance");
     }
 
     // ---- device copies of the reference-format buffers
@@ -240,8 +258,14 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     s.motion_transforms = upload(ctx, ctx->scene_bufs, (const float4*)mot.data(), 3 * (size_t)ni);
     s.vertex_infos = upload(ctx, ctx->scene_bufs, d->vertex_infos, 8 * (size_t)d->vertex_info_count);
     std::vector<uint8_t*> vb(d->vertex_buffer_count + 1, nullptr);
-    for (uint32_t i = 0; i < d->vertex_buffer_count; ++i)
-        vb[i] = upload(ctx, ctx->scene_bufs, (const uint8_t*)d->vertex_buffers[i], (size_t)d->vertex_buffer_bytes[i]);
+    for (uint32_t i = 0; i < d->vertex_buffer_count; ++i) {
+        // 16 bytes of zero padding: LoadTriangleIndices reads two aligned words for 16-bit indices
+        const size_t nbytes = (size_t)d->vertex_buffer_bytes[i];
+        vb[i] = (uint8_t*)dev_alloc(ctx, ctx->scene_bufs, nbytes + 16);
+        if (!vb[i]) return S2_ERR_OOM;
+        cudaMemsetAsync(vb[i] + nbytes, 0, 16, ctx->stream);
+        if (nbytes) cudaMemcpyAsync(vb[i], d->vertex_buffers[i], nbytes, cudaMemcpyHostToDevice, ctx->stream);
+    }
     ctx->vbufs_dev = upload(ctx, ctx->scene_bufs, vb.data(), vb.size());
     s.vbufs = ctx->vbufs_dev;
     s.vbuf_count = d->vertex_buffer_count;

@@ -1,0 +1,172 @@
+// Light sampling (src/Shaders/common/lights.hlsli): uniform light instance -> uniform primitive ->
+// uniform area for emissive triangles, and hierarchical importance sampling of the environment map
+// over its luminance mip pyramid.
+#pragma once
+#include "s2_bsdf.cuh"
+
+// Texels outside the level read as 0.  (The reference's descent can address one column or row
+// past a level after skipping an all-black level; those reads are undefined there.)
+S2D float texel_lum(const DevImage& im, uint32_t level, int x, int y) {
+    if (x < 0 || y < 0 || x >= (int)im.lw[level] || y >= (int)im.lh[level]) return 0.f;
+    return im.lum[im.lum_offset[level] + (size_t)y * im.lw[level] + x];
+}
+
+// SampleTexel (lights.hlsli:49-96), at most 10 levels
+S2D float2 sample_texel(const DevImage& im, float rx, float ry, float& pdf) {
+    const uint32_t levels = im.levels;
+    pdf = 1.f;
+    int cx = 0, cy = 0;
+    uint32_t lx = 1, ly = 1;
+    const uint32_t lim = min(11u, levels - 1);
+    for (uint32_t i = 1; i < lim; ++i) {
+        const uint32_t level = levels - 1 - i;
+        const uint32_t ex = im.lw[level], ey = im.lh[level];
+        const float inv_h = 1.f / (float)ey;
+        cx *= (int)(ex / lx);
+        cy *= (int)(ey / ly);
+        float p[4] = {0.f, 0.f, 0.f, 0.f};
+        if ((int)ex - cx > 1) {
+            const float sy = sinf(S2_PI * (cy + 0.5f) * inv_h);
+            p[0] = texel_lum(im, level, cx, cy) * sy;
+            p[1] = texel_lum(im, level, cx + 1, cy) * sy;
+        }
+        if ((int)ey - cy > 1) {
+            const float sy = sinf(S2_PI * (cy + 1.5f) * inv_h);
+            p[2] = texel_lum(im, level, cx, cy + 1) * sy;
+            p[3] = texel_lum(im, level, cx + 1, cy + 1) * sy;
+        }
+        const float sum = p[0] + p[1] + p[2] + p[3];
+        if (sum < 1e-6f) continue;
+        for (int j = 0; j < 4; ++j) p[j] /= sum;
+        for (int j = 0; j < 4; ++j) {
+            if (j == 3 || rx < p[j]) {
+                cx += j % 2; cy += j / 2; pdf *= p[j]; rx /= p[j];
+                break;
+            }
+            rx -= p[j];
+        }
+        lx = ex; ly = ey;
+    }
+    pdf *= (float)(lx * ly);
+    return make_float2(((float)cx + rx) / (float)lx, ((float)cy + ry) / (float)ly);
+}
+
+// SampleTexelPdf (lights.hlsli:97-138)
+S2D float sample_texel_pdf(const DevImage& im, float2 uv) {
+    const uint32_t levels = im.levels;
+    float pdf = 1.f;
+    uint32_t lx = 1, ly = 1;
+    const uint32_t lim = min(11u, levels - 1);
+    for (uint32_t i = 1; i < lim; ++i) {
+        const uint32_t level = levels - 1 - i;
+        const uint32_t ex = im.lw[level], ey = im.lh[level];
+        const float inv_h = 1.f / (float)ey;
+        const int ux = (int)((float)ex * uv.x), uy = (int)((float)ey * uv.y);
+        const int cx = (ux / 2) * 2, cy = (uy / 2) * 2;
+        const int ox = min(ux - cx, 1), oy = min(uy - cy, 1);
+        float p[4] = {0.f, 0.f, 0.f, 0.f};
+        if ((int)ex - cx > 1) {
+            const float sy = sinf(S2_PI * (cy + 0.5f) * inv_h);
+            p[0] = texel_lum(im, level, cx, cy) * sy;
+            p[1] = texel_lum(im, level, cx + 1, cy) * sy;
+        }
+        if ((int)ey - cy > 1) {
+            const float sy = sinf(S2_PI * (cy + 1.5f) * inv_h);
+            p[2] = texel_lum(im, level, cx, cy + 1) * sy;
+            p[3] = texel_lum(im, level, cx + 1, cy + 1) * sy;
+        }
+        const float sum = p[0] + p[1] + p[2] + p[3];
+        if (sum < 1e-6f) continue;
+        pdf *= p[oy * 2 + ox] / sum;
+        lx = ex; ly = ey;
+    }
+    return pdf * (float)(lx * ly);
+}
+
+S2D bool has_env(const DevScene& s) { return s.env_address != 0xffffffffu; }
+
+// EvaluateEnvironment (lights.hlsli:143-164): emission and its solid-angle pdf
+S2D float3 eval_env(const DevScene& s, float3 dir, float& pdfw) {
+    pdfw = 0.f;
+    if (!has_env(s)) return f3(0.f);
+    const float4 rec = *(const float4*)(s.material_data + s.env_address);
+    float3 e = f3(rec.x, rec.y, rec.z);
+    const uint32_t img = __float_as_uint(rec.w);
+    if (img < s.image_count) {
+        const float2 uv = cartesian_to_spherical_uv(dir);
+        const float4 t = sample_image(s.images[img], uv);
+        e = e * f3(t.x, t.y, t.z);
+        pdfw = sample_texel_pdf(s.images[img], uv) / (2.f * S2_PI * S2_PI * sqrtf(1.f - dir.y * dir.y));
+    } else {
+        pdfw = 1.f / (4.f * S2_PI);
+    }
+    if (s.light_count > 0) pdfw *= s.env_sample_prob;
+    return e;
+}
+
+struct Illum {
+    float3 radiance;
+    float pdf;          // area measure for triangle lights, solid angle for the environment
+    float3 dir;         // direction to the light
+    float dist;
+    float cos_light;
+    bool finite;
+};
+
+// SampleEmission + SampleIllumination (lights.hlsli:166-262).  The environment branch returns the
+// sampled direction (the reference leaves mDirectionToLight unset there).
+S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_normals) {
+    Illum r;
+    r.radiance = f3(0.f); r.pdf = 0.f; r.dir = f3(0.f); r.dist = 0.f; r.cos_light = 0.f; r.finite = true;
+    const uint32_t L = s.light_count;
+    const float envp = s.env_sample_prob;
+    if (has_env(s)) {
+        if (L == 0 || rnd.w < envp) {
+            const uint32_t img = ld_u32(s.material_data, s.env_address + 12);
+            float3 dir;
+            float pdf;
+            if (img < s.image_count) {
+                const float2 uv = sample_texel(s.images[img], rnd.x, rnd.y, pdf);
+                dir = spherical_uv_to_cartesian(uv);
+                pdf /= (2.f * S2_PI * S2_PI * sqrtf(1.f - pow2(dir.y)));
+            } else {
+                dir = sample_uniform_sphere(rnd.x, rnd.y);
+                pdf = 1.f / (4.f * S2_PI);
+            }
+            if (L > 0) pdf *= envp;
+            r.pdf = pdf; r.finite = false; r.dist = S2_INF; r.cos_light = 1.f; r.dir = dir;
+            float tmp;
+            r.radiance = eval_env(s, dir, tmp);
+            return r;
+        }
+        if (L > 0) rnd.w = (rnd.w - envp) / (1.f - envp);
+    }
+    if (L == 0) return r;
+    const uint32_t inst = s.light_instance_map[(uint32_t)(rnd.z * L) % L];
+    float pdf = 1.f / (float)L;
+    if (has_env(s)) pdf *= 1.f - envp;
+    if ((s.instances[inst].x & 0xfu) != 0u) return r;
+    const uint32_t pc = s.prim_counts[inst];
+    const uint32_t prim = (uint32_t)(rnd.w * pc) % pc;
+    pdf /= (float)pc;
+    const float2 b = sample_uniform_triangle(rnd.x, rnd.y);
+    const SD sd = make_shading(s, inst, prim, b.x, b.y, shading_normals);
+    pdf /= sd.area;
+    const Mat m = load_material(s, sd.mat, sd.uv);
+    r.radiance = m.emission();
+    r.dir = sd.pos - ref;
+    r.dist = length(r.dir);
+    r.dir = r.dir / r.dist;
+    r.cos_light = -dot(sd.gn, r.dir);
+    r.pdf = pdf;
+    if (r.cos_light <= 0.f) { r.radiance = f3(0.f); r.pdf = 0.f; }  // one-sided lights
+    return r;
+}
+
+// IntersectionResult::LightSamplePdfA (lights.hlsli:264-272)
+S2D float light_pdfa(const DevScene& s, uint32_t inst, float area) {
+    if (s.light_count == 0) return 0.f;
+    float pdf = (1.f / (float)s.prim_counts[inst]) / (area * (float)s.light_count);
+    if (has_env(s)) pdf *= 1.f - s.env_sample_prob;
+    return pdf;
+}

@@ -1,23 +1,241 @@
-// Wavefront path tracer (placeholder until the kernels land).
+// s2_render: host orchestration of the wavefront path tracer (replaces TestRenderer::render,
+// src/App/TestRenderer.cpp:284-763: per-frame dispatch of Render, RenderIteration x (maxDepth-1),
+// ProcessShadowRays and ProcessAtomicOutput).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
 #include "s2_context.h"
+#include "s2_shade_kernel.cuh"
 
 namespace s2 {
-struct RenderState {};
-void destroy_render_state(S2Context* ctx) { delete ctx->render; ctx->render = nullptr; }
+
+struct RenderState {
+    uint32_t capacity = 0;      // paths per wave
+    uint32_t pixels = 0, width = 0, height = 0;
+    std::vector<DevBuf> bufs;   // queues, hits, shadow queue, accumulators
+    std::vector<DevBuf> pixel_bufs;
+    PathQueue q[2]{};
+    float4* hits = nullptr;
+    float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
+    float4* accum = nullptr;
+    float4* total = nullptr;        // per-pixel sum over all samples so far
+    float4* out_radiance = nullptr; // device radiance AOV when the caller's buffers are on the host
+    float4* aov_albedo = nullptr;
+    uint2* aov_vis = nullptr;
+    float4* aov_depth = nullptr;
+    float2* aov_prev_uv = nullptr;
+    uint2* aov_ids = nullptr;
+    uint32_t* counters = nullptr;
+    unsigned long long* stats = nullptr;
+    uint64_t accumulated_spp = 0;
+    int ext_blocks = 0, occ_blocks = 0, shade_blocks = 0;
+};
+
+void destroy_render_state(S2Context* ctx) {
+    if (!ctx->render) return;
+    free_bufs(ctx->render->bufs);
+    free_bufs(ctx->render->pixel_bufs);
+    delete ctx->render;
+    ctx->render = nullptr;
+}
+
+namespace {
+
+template <typename T>
+T* alloc(S2Context* ctx, std::vector<DevBuf>& owner, size_t n) {
+    return (T*)dev_alloc(ctx, owner, n * sizeof(T));
+}
+
+int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capacity) {
+    RenderState* st = ctx->render;
+    if (!st) {
+        st = ctx->render = new (std::nothrow) RenderState();
+        if (!st) return set_error(ctx, S2_ERR_OOM, "render state allocation failed");
+        cudaDeviceProp prop;
+        cudaGetDeviceProperties(&prop, ctx->device);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, kTravBlock, 0);
+        st->ext_blocks = std::max(1, b) * prop.multiProcessorCount;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_occlude, kTravBlock, 0);
+        st->occ_blocks = std::max(1, b) * prop.multiProcessorCount;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, false>, 128, 0);
+        st->shade_blocks = std::max(1, b) * prop.multiProcessorCount;
+    }
+    const uint32_t pixels = width * height;
+    if (st->pixels != pixels || st->width != width) {
+        free_bufs(st->pixel_bufs);
+        st->total = alloc<float4>(ctx, st->pixel_bufs, pixels);
+        st->out_radiance = alloc<float4>(ctx, st->pixel_bufs, pixels);
+        st->aov_albedo = alloc<float4>(ctx, st->pixel_bufs, pixels);
+        st->aov_vis = alloc<uint2>(ctx, st->pixel_bufs, pixels);
+        st->aov_depth = alloc<float4>(ctx, st->pixel_bufs, pixels);
+        st->aov_prev_uv = alloc<float2>(ctx, st->pixel_bufs, pixels);
+        st->aov_ids = alloc<uint2>(ctx, st->pixel_bufs, pixels);
+        st->counters = alloc<uint32_t>(ctx, st->pixel_bufs, C_COUNT);
+        st->stats = alloc<unsigned long long>(ctx, st->pixel_bufs, S_COUNT);
+        if (!st->total || !st->out_radiance || !st->aov_albedo || !st->aov_vis || !st->aov_depth || !st->aov_prev_uv ||
+            !st->aov_ids || !st->counters || !st->stats) {
+            free_bufs(st->pixel_bufs);
+            st->pixels = 0;
+            return S2_ERR_OOM;
+        }
+        cudaMemsetAsync(st->total, 0, sizeof(float4) * pixels, ctx->stream);
+        st->pixels = pixels; st->width = width; st->height = height;
+        st->accumulated_spp = 0;
+    }
+    if (st->capacity < capacity) {
+        free_bufs(st->bufs);
+        st->capacity = 0;
+        for (int k = 0; k < 2; ++k) {
+            st->q[k].s0 = alloc<float4>(ctx, st->bufs, capacity);
+            st->q[k].s1 = alloc<float4>(ctx, st->bufs, capacity);
+            st->q[k].s2 = alloc<float4>(ctx, st->bufs, capacity);
+            st->q[k].s3 = alloc<uint4>(ctx, st->bufs, capacity);
+        }
+        st->hits = alloc<float4>(ctx, st->bufs, capacity);
+        st->sh_o = alloc<float4>(ctx, st->bufs, capacity);
+        st->sh_d = alloc<float4>(ctx, st->bufs, capacity);
+        st->sh_c = alloc<float4>(ctx, st->bufs, capacity);
+        st->accum = alloc<float4>(ctx, st->bufs, capacity);
+        for (auto& b : st->bufs) if (!b.ptr) return S2_ERR_OOM;
+        if (st->bufs.size() != 13) { free_bufs(st->bufs); return S2_ERR_OOM; }
+        cudaMemsetAsync(st->accum, 0, sizeof(float4) * capacity, ctx->stream);
+        st->capacity = capacity;
+    }
+    return S2_OK;
+}
+
+template <bool L, bool R>
+void launch_shade(const PTParams& P, uint32_t parity, int blocks, cudaStream_t s) {
+    k_shade<L, R><<<blocks, 128, 0, s>>>(P, parity);
+}
+
+}  // namespace
 }  // namespace s2
+
+using namespace s2;
 
 extern "C" void s2_default_render_params(S2RenderParams* p) {
     if (!p) return;
-    *p = S2RenderParams{};
+    std::memset(p, 0, sizeof(*p));
     p->min_path_length = 0;
-    p->max_path_length = 5;
+    p->max_path_length = 5;         // mMaxDepth (TestRenderer.cpp:38)
     p->exposure = 0.f;
     p->spp = 1;
-    p->environment_sample_probability = 0.9f;
-    p->restir_candidates = 32;
-    p->restir_max_m = 3.f;
+    p->environment_sample_probability = 0.9f;  // TestRenderer.cpp:41
+    p->restir_candidates = 32;      // TestRenderer.cpp:42
+    p->restir_max_m = 3.f;          // TestRenderer.cpp:43
+    p->restir_spatial_radius = 30.f;
 }
 
-extern "C" int s2_render(S2Context* ctx, const S2View*, const S2RenderParams*, const S2Aovs*, int, S2RenderStats*) {
-    return s2::set_error(ctx, S2_ERR_UNSUPPORTED, "render not built yet");
+extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParams* prm, const S2Aovs* out, int out_on_host,
+                         S2RenderStats* stats_out) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!view || !prm) return set_error(ctx, S2_ERR_INVALID, "view and params are required");
+    if (!ctx->has_bvh) return set_error(ctx, S2_ERR_NO_SCENE, "s2_render before s2_scene_upload + s2_build_bvh");
+    const int W = view->image_max[0] - view->image_min[0], H = view->image_max[1] - view->image_min[1];
+    if (W <= 0 || H <= 0 || (int64_t)W * H > (1ll << 28)) return set_error(ctx, S2_ERR_INVALID, "invalid view extent");
+    if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
+    if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
+    if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
+        return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
+    cudaSetDevice(ctx->device);
+    const uint32_t pixels = (uint32_t)W * (uint32_t)H;
+    uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 22);
+    uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, target / pixels));
+    const uint32_t capacity = slots * pixels;
+    int rc = ensure_state(ctx, (uint32_t)W, (uint32_t)H, capacity);
+    if (rc != S2_OK) return rc;
+    RenderState* st = ctx->render;
+    cudaStream_t s = ctx->stream;
+
+    PTParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.scene = ctx->scene;
+    P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
+    std::memcpy(P.proj, view->projection, sizeof(P.proj));
+    P.imin[0] = view->image_min[0]; P.imin[1] = view->image_min[1];
+    P.imax[0] = view->image_max[0]; P.imax[1] = view->image_max[1];
+    std::memcpy(P.cam, view->camera_to_world, sizeof(P.cam));
+    std::memcpy(P.prev_inv, view->prev_world_to_camera, sizeof(P.prev_inv));
+    P.width = (uint32_t)W; P.height = (uint32_t)H; P.pixels = pixels;
+    P.min_len = prm->min_path_length;
+    P.max_len = prm->max_path_length;
+    P.flags = prm->flags;
+    P.frame_seed = prm->frame_seed;
+    P.restir_m = prm->restir_candidates ? prm->restir_candidates : 32;
+    P.exposure = prm->exposure;
+    P.q[0] = st->q[0]; P.q[1] = st->q[1];
+    P.hits = st->hits; P.sh_o = st->sh_o; P.sh_d = st->sh_d; P.sh_c = st->sh_c;
+    P.accum = st->accum;
+    P.counters = st->counters;
+    P.stats = st->stats;
+    P.status = ctx->status_dev;
+    const bool host = out_on_host != 0;
+    auto pick = [&](void* user, void* internal) -> void* { return !out ? nullptr : (user ? (host ? internal : user) : nullptr); };
+    P.aov_albedo = (float4*)pick(out ? out->albedo : nullptr, st->aov_albedo);
+    P.aov_vis = (uint2*)pick(out ? out->visibility : nullptr, st->aov_vis);
+    P.aov_depth = (float4*)pick(out ? out->depth : nullptr, st->aov_depth);
+    P.aov_prev_uv = (float2*)pick(out ? out->prev_uv : nullptr, st->aov_prev_uv);
+    P.aov_ids = (uint2*)pick(out ? out->ids32 : nullptr, st->aov_ids);
+
+    if (!(prm->flags & S2_FLAG_ACCUMULATE)) {
+        cudaMemsetAsync(st->total, 0, sizeof(float4) * pixels, s);
+        st->accumulated_spp = 0;
+    }
+    cudaMemsetAsync(st->stats, 0, sizeof(unsigned long long) * S_COUNT, s);
+    cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), s);
+    cudaEventRecord(ctx->ev0, s);
+    const bool lam = (prm->flags & S2_FLAG_LAMBERTIAN) != 0, restir = (prm->flags & S2_FLAG_RESTIR_DI) != 0;
+    for (uint32_t done = 0; done < prm->spp; done += slots) {
+        P.wave_base_sample = done;
+        P.wave_samples = std::min(slots, prm->spp - done);
+        const uint32_t n = P.wave_samples * pixels;
+        k_raygen<<<(n + 255) / 256, 256, 0, s>>>(P);
+        for (uint32_t b = 0; b < prm->max_path_length; ++b) {
+            const uint32_t parity = b & 1u;
+            k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
+            k_extend<<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
+            else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
+            k_occlude<<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+        }
+        k_wave_finish<<<1, 32, 0, s>>>(P);
+        k_reduce<<<(pixels + 255) / 256, 256, 0, s>>>(P, st->total);
+    }
+    st->accumulated_spp += prm->spp;
+    float4* rad = (out && out->radiance) ? (host ? st->out_radiance : (float4*)out->radiance) : st->out_radiance;
+    k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(st->total, pixels, (float)(1.0 / (double)st->accumulated_spp),
+                                                   exp2f(prm->exposure), rad);
+    cudaEventRecord(ctx->ev1, s);
+    rc = check_cuda(ctx, cudaGetLastError(), "render kernel launch");
+    if (rc != S2_OK) return rc;
+    if (host && out) {
+        if (out->radiance) cudaMemcpyAsync(out->radiance, st->out_radiance, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
+        if (out->albedo) cudaMemcpyAsync(out->albedo, st->aov_albedo, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
+        if (out->visibility) cudaMemcpyAsync(out->visibility, st->aov_vis, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, s);
+        if (out->depth) cudaMemcpyAsync(out->depth, st->aov_depth, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
+        if (out->prev_uv) cudaMemcpyAsync(out->prev_uv, st->aov_prev_uv, sizeof(float2) * pixels, cudaMemcpyDeviceToHost, s);
+        if (out->ids32) cudaMemcpyAsync(out->ids32, st->aov_ids, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, s);
+    }
+    if (stats_out || host) {
+        unsigned long long sv[S_COUNT] = {0, 0, 0, 0};
+        int status = 0;
+        cudaMemcpyAsync(sv, st->stats, sizeof(sv), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&status, ctx->status_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+        rc = check_cuda(ctx, cudaStreamSynchronize(s), "render");
+        if (rc != S2_OK) return rc;
+        if (status) return set_error(ctx, S2_ERR_DEVICE, "traversal stack overflow during render");
+        if (stats_out) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            stats_out->extension_rays = sv[S_EXT];
+            stats_out->shadow_rays = sv[S_SHADOW];
+            stats_out->paths = (uint64_t)pixels * prm->spp;
+            stats_out->nan_count = sv[S_NAN];
+            stats_out->gpu_ms = ms;
+        }
+    }
+    return S2_OK;
 }

@@ -1,0 +1,251 @@
+// Shade kernel of the wavefront path tracer: the body of ProcessInteraction
+// (src/Shaders/kernels/testrenderer.slang:816-935) with TraceRay's miss handling (:1026-1058),
+// AddEmission (:788-808), ConnectToLight (:751-779; ReSTIR variant :665-683, :730-747) and
+// StoreAuxillaryData (:195-218), plus the minPathLength gate of vcm.slang:922,960,977.
+#pragma once
+#include "s2_wavefront.cuh"
+
+namespace s2 {
+
+// Appends `want` lanes of the warp to a queue: one atomic per warp.  All 32 lanes must call.
+S2D uint32_t warp_append(uint32_t* counter, bool want) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (mask) {
+        const uint32_t leader = __ffs(mask) - 1;
+        if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+S2D void add_accum(float4* accum, uint32_t slot, float3 v) {
+    float4 a = accum[slot];
+    a.x += v.x; a.y += v.y; a.z += v.z;
+    accum[slot] = a;
+}
+
+struct ShadowOut { float3 o, d, c; float tmax; bool valid; };
+
+// One NEE connection: plain light sample, or RIS over restir_m candidates.
+template <bool LAMBERT, bool RESTIR>
+S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, float3 in, float3 thr, Rng& rng, uint32_t len,
+                               bool sn) {
+    ShadowOut so;
+    so.valid = false;
+    const DevScene& s = P.scene;
+    const float cp = (P.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
+    float3 dir, contrib;
+    float dist, w;
+    if (RESTIR) {
+        float best_t = 0.f, best_wtoa = 0.f, best_mis = 0.f, best_dist = 0.f, wsum = 0.f;
+        float3 best_c = f3(0.f), best_d = f3(0.f);
+        for (uint32_t i = 0; i < P.restir_m; ++i) {
+            const float4 x = rng.next_float();
+            const Illum r = sample_illum(s, x, sd.pos, sn);
+            float target = 0.f, wtoa = 0.f, misw = 0.f;
+            float3 c = f3(0.f);
+            if (luminance(r.radiance) > 0.f && r.pdf > 0.f) {
+                const float3 out = sd.to_local(r.dir);
+                float3 f; float fwd, rev;
+                bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
+                f = f * sd.snc(in, out);
+                fwd *= cp;
+                c = f * r.radiance;
+                wtoa = r.finite ? r.cos_light / pow2(r.dist) : 1.f;
+                const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
+                misw = mis_w(r.pdf, fwd / AtoW);
+                target = luminance(c) * wtoa;
+            }
+            if (target <= 0.f) continue;
+            const float risw = target / r.pdf;
+            wsum += risw;
+            const float4 u = rng.next_float();
+            if (u.x <= risw / wsum) {
+                best_t = target; best_wtoa = wtoa; best_mis = misw; best_c = c; best_d = r.dir; best_dist = r.dist;
+            }
+        }
+        if (!(best_t > 0.f)) return so;
+        float iw = wsum / ((float)P.restir_m * best_t);
+        if (!(iw > 0.f)) return so;
+        iw *= best_wtoa;
+        contrib = thr * best_c * iw;
+        w = best_mis;
+        dir = best_d;
+        dist = best_dist;
+    } else {
+        const float4 x = rng.next_float();
+        const Illum r = sample_illum(s, x, sd.pos, sn);
+        if (all_nonpos(r.radiance) || r.pdf <= 0.f) return so;
+        const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
+        const float dpw = r.pdf * AtoW;
+        const float3 out = sd.to_local(r.dir);
+        float3 f; float fwd, rev;
+        bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
+        f = f * sd.snc(in, out);
+        fwd *= cp;
+        contrib = thr * r.radiance * f / dpw;
+        w = mis_w(r.pdf, fwd / AtoW);
+        dir = r.dir;
+        dist = r.dist;
+    }
+    if (!(w > 0.f) || all_nonpos(contrib)) return so;
+    if (len + 1 < P.min_len) return so;
+    so.o = ray_offset(sd.pos, sd.gn, dir);
+    so.d = dir;
+    so.tmax = adjust_distance(dist);
+    so.c = f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
+    so.valid = true;
+    return so;
+}
+
+template <bool LAMBERT, bool RESTIR>
+__global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
+    const uint32_t count = P.counters[parity];
+    const PathQueue qi = P.q[parity];
+    const PathQueue qo = P.q[1 - parity];
+    const DevScene& s = P.scene;
+    const bool nee = !(P.flags & S2F_NO_NEE);
+    const bool sn = !(P.flags & S2F_NO_SN);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounded = (count + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += stride) {
+        bool alive = false, shadow = false;
+        float4 n0, n1, n2;
+        uint4 n3;
+        ShadowOut so;
+        so.valid = false;
+        uint32_t slot = 0;
+        if (i < count) {
+            const float4 a = qi.s0[i], b = qi.s1[i], c = qi.s2[i];
+            const uint4 rs = qi.s3[i];
+            const float4 h = P.hits[i];
+            float3 org = f3(a.x, a.y, a.z);
+            float dir_pdf = a.w;
+            const float3 dir = f3(b.x, b.y, b.z);
+            float3 thr = f3(b.w, c.x, c.y);
+            slot = __float_as_uint(c.z);
+            const uint32_t meta = __float_as_uint(c.w);
+            const uint32_t len = (meta & 0xffu) + 1u;  // TraceRay: mPathLength++
+            const bool aov = (meta & 0x100u) && len == 1;
+            Rng rng;
+            rng.px = rs.x; rng.py = rs.y; rng.seed = rs.z; rng.ctr = rs.w; rng.pcg32 = (P.flags & S2F_PCG32) != 0;
+            const uint32_t tri = __float_as_uint(h.y);
+            const uint32_t pix = slot % P.pixels;
+            if (tri == 0xffffffffu) {
+                // ---- miss: environment emission (TraceRay, testrenderer.slang:1036-1054)
+                if (aov) {
+                    if (P.aov_albedo) P.aov_albedo[pix] = make_float4(1.f, 1.f, 1.f, 1.f);
+                    if (P.aov_vis) P.aov_vis[pix] = make_uint2(0xffffffffu, pack_normal(dir));
+                    if (P.aov_depth) P.aov_depth[pix] = make_float4(S2_INF, S2_INF, 1.f, 1.f);
+                    if (P.aov_prev_uv) {
+                        const uint32_t px = pix % P.width, py = pix / P.width;
+                        P.aov_prev_uv[pix] = make_float2(((float)px + 0.5f) / (float)(P.imax[0] - P.imin[0]),
+                                                         ((float)py + 0.5f) / (float)(P.imax[1] - P.imin[1]));
+                    }
+                    if (P.aov_ids) P.aov_ids[pix] = make_uint2(0xffffffffu, 0xffffffffu);
+                }
+                float env_pdf;
+                const float3 e = thr * eval_env(s, dir, env_pdf);
+                if (any_pos(e) && len >= P.min_len) {
+                    float w = 1.f;
+                    if (len > 1 && nee && dir_pdf > 0.f) {
+                        const float lp = (P.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;
+                        w = mis_w(dir_pdf, lp);
+                    }
+                    if (w > 0.f) add_accum(P.accum, slot, e * w);
+                }
+            } else {
+                const float4 tr0 = s.tris[3 * (size_t)tri], tr1 = s.tris[3 * (size_t)tri + 1];
+                const uint32_t inst = __float_as_uint(tr0.w), prim = __float_as_uint(tr1.w);
+                const SD sd = make_shading(s, inst, prim, h.z, h.w, sn);
+                const float isect_dist = half_round(h.x);
+                const float isect_pdfa = half_round(light_pdfa(s, inst, sd.area));
+                const Mat m = load_material(s, sd.mat, sd.uv);
+                const float3 in = sd.to_local(-dir);
+                const float cos_in = fabsf(in.z);
+                if (aov) {
+                    // StoreAuxillaryData (testrenderer.slang:195-218)
+                    const float3 bc = m.base();
+                    if (P.aov_albedo) P.aov_albedo[pix] = make_float4(bc.x, bc.y, bc.z, 1.f);
+                    if (P.aov_vis) P.aov_vis[pix] = make_uint2((inst & 0xffffu) | (prim << 16), sd.ns);
+                    if (P.aov_ids) P.aov_ids[pix] = make_uint2(inst, prim);
+                    const float3 pw = xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos);
+                    const float* pv = P.prev_inv;
+                    const float3 pc = f3(pv[0] * pw.x + pv[1] * pw.y + pv[2] * pw.z + pv[3],
+                                         pv[4] * pw.x + pv[5] * pw.y + pv[6] * pw.z + pv[7],
+                                         pv[8] * pw.x + pv[9] * pw.y + pv[10] * pw.z + pv[11]);
+                    const uint32_t px = pix % P.width, py = pix / P.width;
+                    const float W = (float)(P.imax[0] - P.imin[0]), H = (float)(P.imax[1] - P.imin[1]);
+                    float ppx = (float)px + 0.5f, ppy = (float)py + 0.5f;
+                    const float nr = P.proj[4];
+                    if ((pc.z > 0.f) == (nr > 0.f) && pc.z != 0.f) {
+                        // ViewData::toRaster (compat/scene.h:158-165), perspective projectPoint
+                        const float x4 = pc.x * P.proj[0] + pc.z * P.proj[2], y4 = pc.y * P.proj[1] + pc.z * P.proj[3];
+                        const float z4 = fabsf(nr), w4 = pc.z * (nr > 0.f ? 1.f : -1.f);
+                        if (!(fabsf(x4) >= fabsf(w4) || fabsf(y4) >= fabsf(w4) || fabsf(z4) >= fabsf(w4))) {
+                            ppx = P.imin[0] + W * (x4 / w4 * 0.5f + 0.5f);
+                            ppy = P.imin[1] + H * (-y4 / w4 * 0.5f + 0.5f);
+                        }
+                    }
+                    if (P.aov_prev_uv) P.aov_prev_uv[pix] = make_float2(ppx / W, ppy / H);
+                    if (P.aov_depth) P.aov_depth[pix] = make_float4(isect_dist, length(pc), 1.f, 1.f);
+                }
+                // ---- emission (surface lights are one-sided)
+                if (in.z > 0.f) {
+                    const float3 e = thr * m.emission();
+                    if (any_pos(e) && len >= P.min_len) {
+                        float w = 1.f;
+                        if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
+                        if (w > 0.f) add_accum(P.accum, slot, e * w);
+                    }
+                }
+                if (len < P.max_len && any_pos(m.base())) {
+                    const bool sing = mat_singular<LAMBERT>(m);
+                    if (!sing && nee) so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn);
+                    const float cp = fminf(1.f, cont_prob(m));
+                    bool cont = true;
+                    if (!(P.flags & S2F_NO_RR)) {
+                        const float4 u = rng.next_float();
+                        if (u.x > cp) cont = false;
+                    }
+                    if (cont) {
+                        const float4 rnd = rng.next_float();
+                        float3 sdir, refl;
+                        float fwd, rev, rough;
+                        bsdf_sample<LAMBERT>(m, in, rnd, sdir, refl, fwd, rev, rough);
+                        const float cpm = (P.flags & S2F_NO_RR) ? 1.f : cp;
+                        fwd *= cpm;
+                        thr = thr * refl / fwd;
+                        dir_pdf = (rough == 0.f || sing) ? 0.f : half_round(fwd);
+                        thr = thr * sd.snc(in, sdir);
+                        const float3 wd = sd.to_world(sdir);
+                        const float3 nd = unpack_normal(pack_normal(wd));
+                        org = ray_offset(sd.pos, sd.gn, wd);
+                        if (any_nan(thr)) {
+                            atomicAdd(&P.stats[S_NAN], 1ull);
+                        } else if (any_pos(thr)) {
+                            alive = true;
+                            n0 = make_float4(org.x, org.y, org.z, dir_pdf);
+                            n1 = make_float4(nd.x, nd.y, nd.z, thr.x);
+                            n2 = make_float4(thr.y, thr.z, __uint_as_float(slot), __uint_as_float((meta & ~0xffu) | len));
+                            n3 = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+                        }
+                    }
+                }
+            }
+            shadow = so.valid;
+        }
+        const uint32_t qi_out = warp_append(&P.counters[1 - parity], alive);
+        if (alive) { qo.s0[qi_out] = n0; qo.s1[qi_out] = n1; qo.s2[qi_out] = n2; qo.s3[qi_out] = n3; }
+        const uint32_t si = warp_append(&P.counters[C_SHADOW], shadow);
+        if (shadow) {
+            P.sh_o[si] = make_float4(so.o.x, so.o.y, so.o.z, so.tmax);
+            P.sh_d[si] = make_float4(so.d.x, so.d.y, so.d.z, __uint_as_float(slot));
+            P.sh_c[si] = make_float4(so.c.x, so.c.y, so.c.z, 0.f);
+        }
+    }
+}
+
+}  // namespace s2

@@ -1,0 +1,215 @@
+// Wavefront path tracer kernels.
+//
+// The reference runs one thread per pixel with a 64-byte PathState reloaded each bounce
+// (Render / RenderIteration, src/Shaders/kernels/testrenderer.slang:1087-1144) and appends
+// deferred shadow rays for one ProcessShadowRays pass (:296-323, :1147-1166).  Here every bounce
+// is three kernels over compacted structure-of-arrays queues:
+//   extend  -- closest-hit BVH8 traversal of the live path queue (persistent, warp work fetch)
+//   shade   -- hit reconstruction, emission + MIS, NEE light sample, Russian roulette and BSDF
+//              sampling; survivors are appended to the next queue and shadow rays to the shadow
+//              queue with warp-aggregated atomics
+//   occlude -- first-hit traversal of the shadow queue, adding unoccluded contributions
+// A wave holds `pixels x slots` camera paths; path p owns accumulator slot p, so every
+// accumulator element has exactly one writer per kernel and needs no atomics: the summation
+// order is fixed and results are deterministic.
+#pragma once
+#include "s2_lights.cuh"
+#include "s2_traverse.cuh"
+
+namespace s2 {
+
+enum Counter : uint32_t {
+    C_QUEUE0 = 0,   // live paths in queue 0 / 1 (by bounce parity)
+    C_QUEUE1 = 1,
+    C_SHADOW = 2,   // shadow rays appended this bounce
+    C_WORK_EXT = 3, // warp work counters for the persistent traversal kernels
+    C_WORK_OCC = 4,
+    C_COUNT = 8
+};
+enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_COUNT = 4 };
+
+struct PathQueue { float4* s0; float4* s1; float4* s2; uint4* s3; };
+
+struct PTParams {
+    DevScene scene;
+    // view (ViewData + camera transform)
+    float proj[8];
+    int imin[2], imax[2];
+    float cam[12];
+    float prev_inv[12];
+    uint32_t width, height, pixels;
+    // render parameters
+    uint32_t min_len, max_len, flags, frame_seed, restir_m;
+    float exposure;
+    // wave
+    uint32_t wave_base_sample, wave_samples;
+    // buffers
+    PathQueue q[2];
+    float4* hits;
+    float4 *sh_o, *sh_d, *sh_c;
+    float4* accum;
+    uint32_t* counters;
+    unsigned long long* stats;
+    int* status;
+    // AOVs (device, may be null)
+    float4* aov_albedo;
+    uint2* aov_vis;
+    float4* aov_depth;
+    float2* aov_prev_uv;
+    uint2* aov_ids;
+};
+
+#define S2F_JITTER (1u << 0)
+#define S2F_LAMBERT (1u << 1)
+#define S2F_PCG32 (1u << 2)
+#define S2F_NO_NEE (1u << 3)
+#define S2F_RESTIR (1u << 4)
+#define S2F_REF_ENV_MIS (1u << 5)
+#define S2F_NO_RR (1u << 6)
+#define S2F_NO_SN (1u << 8)
+
+constexpr int kTravBlock = 128;
+
+// ---------------------------------------------------------------- camera rays
+// InitializeCameraPath (testrenderer.slang:938-957): ViewData::toWorld (compat/scene.h:152-157)
+// through ProjectionData::backProject (compat/transform.h:159-170); the direction is stored
+// octahedral-packed as the reference's PathState.mRayDirection is.
+__global__ void k_raygen(PTParams P) {
+    const uint32_t n = P.pixels * P.wave_samples;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        P.counters[C_QUEUE0] = n;
+        P.counters[C_QUEUE1] = 0;
+        P.counters[C_SHADOW] = 0;
+        P.counters[C_WORK_EXT] = 0;
+        P.counters[C_WORK_OCC] = 0;
+    }
+    if (i >= n) return;
+    const uint32_t k = i / P.pixels, pix = i - k * P.pixels;
+    const uint32_t px = pix % P.width, py = pix / P.width;
+    const uint32_t sample = P.wave_base_sample + k;
+    Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
+    float ox = 0.5f, oy = 0.5f;
+    if (P.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
+    const float W = (float)(P.imax[0] - P.imin[0]), H = (float)(P.imax[1] - P.imin[1]);
+    const float uvx = ((float)px + ox - P.imin[0]) / W, uvy = ((float)py + oy - P.imin[1]) / H;
+    const float cx = 2.f * uvx - 1.f, cy = -(2.f * uvy - 1.f);
+    const float sx = P.proj[0], sy = P.proj[1], offx = P.proj[2], offy = P.proj[3], nr = P.proj[4];
+    float3 ld;
+    if (P.proj[7] < 0.f) ld = f3((cx - offx) / sx, (cy - offy) / sy, nr);
+    else {
+        const float sg = nr > 0.f ? 1.f : (nr < 0.f ? -1.f : 0.f);
+        ld = f3(nr * (cx * sg - offx) / sx, nr * (cy * sg - offy) / sy, nr);
+    }
+    ld = normalize(ld);
+    const float* c = P.cam;
+    const float3 wd = normalize(f3(c[0] * ld.x + c[1] * ld.y + c[2] * ld.z, c[4] * ld.x + c[5] * ld.y + c[6] * ld.z,
+                                   c[8] * ld.x + c[9] * ld.y + c[10] * ld.z));
+    const float3 d = unpack_normal(pack_normal(wd));
+    const uint32_t meta = (sample == 0 ? 0x100u : 0u);  // path length 0; bit 8: write AOVs
+    const PathQueue& q = P.q[0];
+    q.s0[i] = make_float4(c[3], c[7], c[11], 0.f);
+    q.s1[i] = make_float4(d.x, d.y, d.z, 1.f);
+    q.s2[i] = make_float4(1.f, 1.f, __uint_as_float(i), __uint_as_float(meta));
+    q.s3[i] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+}
+
+// ---------------------------------------------------------------- per-bounce bookkeeping
+__global__ void k_bounce_setup(PTParams P, uint32_t parity, int first) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!first) P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    P.stats[S_EXT] += P.counters[parity];
+    P.counters[1 - parity] = 0;
+    P.counters[C_SHADOW] = 0;
+    P.counters[C_WORK_EXT] = 0;
+    P.counters[C_WORK_OCC] = 0;
+}
+__global__ void k_wave_finish(PTParams P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    P.counters[C_SHADOW] = 0;
+}
+
+// ---------------------------------------------------------------- extend: closest hit
+// Persistent kernel: each warp takes 32 rays at a time from a global work counter (dynamic load
+// balancing of incoherent traversal).  Hit record: {t, triangle record index, b1, b2}.
+__global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t parity) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    const uint32_t count = P.counters[parity];
+    const PathQueue q = P.q[parity];
+    const uint32_t lane = threadIdx.x & 31u;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&P.counters[C_WORK_EXT], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane;
+        if (i < count) {
+            const float4 a = q.s0[i], b = q.s1[i];
+            const TravRay r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
+            TravHit h;
+            TravCounters c;
+            if (!traverse<false, false>(r, S2_INF, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
+                atomicOr(P.status, 1);
+            P.hits[i] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- occlude: first hit
+// ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
+// ray belongs to one accumulator slot and adds its contribution when unoccluded.
+__global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    const uint32_t count = P.counters[C_SHADOW];
+    const uint32_t lane = threadIdx.x & 31u;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&P.counters[C_WORK_OCC], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane;
+        if (i < count) {
+            const float4 o = P.sh_o[i], d = P.sh_d[i];
+            const TravRay r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
+            TravHit h;
+            TravCounters c;
+            if (!traverse<true, false>(r, o.w, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
+                atomicOr(P.status, 1);
+            if (h.tri == 0xffffffffu) {
+                const float4 cc = P.sh_c[i];
+                const uint32_t slot = __float_as_uint(d.w);
+                float4 acc = P.accum[slot];
+                acc.x += cc.x; acc.y += cc.y; acc.z += cc.z;
+                P.accum[slot] = acc;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- accumulation
+// Sum the wave's per-sample slots into the per-pixel total in a fixed order and clear them.
+__global__ void k_reduce(PTParams P, float4* __restrict__ total) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.pixels) return;
+    float4 t = total[p];
+    for (uint32_t k = 0; k < P.wave_samples; ++k) {
+        const size_t idx = (size_t)k * P.pixels + p;
+        const float4 a = P.accum[idx];
+        t.x += a.x; t.y += a.y; t.z += a.z;
+        P.accum[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    total[p] = t;
+}
+
+// Mean over samples times 2^exposure (tonemap.slang:154), alpha 1.
+__global__ void k_resolve(const float4* __restrict__ total, uint32_t pixels, float inv_spp, float exposure_scale,
+                          float4* __restrict__ out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    const float4 t = total[p];
+    const float s = inv_spp * exposure_scale;
+    out[p] = make_float4(t.x * s, t.y * s, t.z * s, 1.f);
+}
+
+}  // namespace s2

@@ -1,0 +1,66 @@
+"""Generates the FP64 oracle reference images used by the GPU convergence tests.
+
+    python tests/golden/make_golden.py
+
+Each fixture is an .npz with the per-pixel mean radiance and the variance of that mean, rendered
+by the FP64 oracle (oracle/oracle.cpp) at high sample counts with frame seeds disjoint from the
+ones the GPU tests use.  Scenes come from stratum2_b200.scenegen with fixed seeds.
+"""
+from __future__ import annotations
+
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+sys.path.insert(0, str(HERE.parent))
+
+from oracle_lib import OracleScene  # noqa: E402
+from stratum2_b200 import _abi  # noqa: E402
+from stratum2_b200.scenegen import box_scene, terrain_scene  # noqa: E402
+
+GOLDEN_SEED = 1_000_000  # frame seeds of the oracle images; GPU tests use seeds < 100000
+
+
+def box_case():
+    wl = box_scene(seed=1, width=64, height=64)
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length = 2, 5
+    p.flags = _abi.FLAG_LAMBERTIAN
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    return wl, p
+
+
+def terrain_case():
+    wl = terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length = 1, 6
+    p.flags = 0
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    return wl, p
+
+
+CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 16384)}
+
+
+def make(name: str, out_dir: Path = HERE):
+    fn, spp = CASES[name]
+    wl, p = fn()
+    p.spp = spp
+    p.frame_seed = GOLDEN_SEED
+    osc = OracleScene(wl.scene, 1)
+    t = time.time()
+    r = osc.render(wl.view, p, wl.width, wl.height, precision=64)
+    np.savez_compressed(out_dir / f"{name}_fp64_{spp}spp.npz", mean=r["mean"].astype(np.float32),
+                        var_of_mean=r["var_of_mean"].astype(np.float32), spp=spp, seed=GOLDEN_SEED)
+    print(name, f"{time.time() - t:.1f}s", float(r["mean"].mean()))
+
+
+if __name__ == "__main__":
+    for n in (sys.argv[1:] or CASES):
+        make(n)

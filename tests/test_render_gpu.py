@@ -1,0 +1,189 @@
+"""Parity of the wavefront path tracer (CUDA) with the FP64 oracle.
+
+Same-seed tests: the GPU and the oracle draw the same random numbers per (pixel, sample) (the
+reference's counter-based pcg4d stream, or PCG32), so the images agree sample by sample up to
+floating-point divergence of individual paths.  The floor of that divergence is set by the
+reference's own path-state packing: ray directions are stored octahedral SNORM16
+(testrenderer.slang:119-122), so a 1e-7 rounding difference flips ~2% of direction components by
+one 3e-5 rad step, which occasionally moves a hit across a small triangle's edge.  The oracle's
+own FP32 build differs from its FP64 build by the same amount (box scene, 16 spp: relMSE 1.6e-5
+with pixel jitter; 3.8e-4 without jitter, where the symmetric box puts diagonal pixels' camera
+rays exactly on its corner seams).  Tolerances: relMSE < 2e-4 (jittered) / 1e-3 (pixel
+centres) and 97% of pixel channels within 1e-3 relative (+1e-4 absolute).
+
+Convergence tests: a high-spp GPU image against a committed FP64 oracle image rendered with
+disjoint seeds (tests/golden/make_golden.py): relMSE <= 1e-3 and a per-pixel z-test of the
+estimator means (|z| < 5 for all but 0.1% of pixel channels).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle_lib import OracleScene
+from stratum2_b200 import _abi
+from stratum2_b200.metrics import relmse, z_scores
+from stratum2_b200.scenegen import box_scene, terrain_scene
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def make_params(spp, min_len, max_len, flags, seed=0, restir_m=32):
+    p = _abi.S2RenderParams()
+    _abi.lib().s2_default_render_params(p)
+    p.spp, p.min_path_length, p.max_path_length, p.flags, p.frame_seed = spp, min_len, max_len, flags, seed
+    p.restir_candidates = restir_m
+    return p
+
+
+def box_wl():
+    return box_scene(seed=1, width=64, height=64)
+
+
+def terrain_wl():
+    return terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+
+
+def assert_same_seed(g, o, tag="", jitter=True):
+    gm = g.radiance[..., :3].astype(np.float64)
+    om = o["mean"]
+    rm = relmse(gm, om)
+    close = np.abs(gm - om) <= 1e-3 * np.abs(om) + 1e-4
+    assert rm < (2e-4 if jitter else 1e-3), f"{tag} relMSE {rm}"
+    assert close.mean() > 0.97, f"{tag} only {close.mean():.4f} of pixel channels agree"
+
+
+@pytest.fixture(scope="module")
+def box(device):
+    wl = box_wl()
+    device.upload_scene(wl.scene)
+    return wl, OracleScene(wl.scene, 1)
+
+
+J = _abi.FLAG_PIXEL_JITTER
+
+
+@pytest.mark.parametrize("min_len,max_len,extra", [(2, 5, 0), (2, 5, J), (0, 3, J), (1, 8, _abi.FLAG_PCG32 | J),
+                                                   (2, 5, _abi.FLAG_NO_NEE | J), (2, 5, _abi.FLAG_NO_RR | J)])
+def test_box_same_seed_matches_fp64_oracle(device, box, min_len, max_len, extra):
+    wl, osc = box
+    device.upload_scene(wl.scene)
+    p = make_params(16, min_len, max_len, _abi.FLAG_LAMBERTIAN | extra, seed=7)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    o = osc.render(wl.view, p, wl.width, wl.height)
+    assert_same_seed(g, o, f"min{min_len} max{max_len} flags{extra}", jitter=bool(extra & J))
+    assert g.stats.extension_rays > 0 and g.stats.nan_count == 0
+
+
+def test_box_aovs_match_oracle(device, box):
+    wl, osc = box
+    device.upload_scene(wl.scene)
+    p = make_params(2, 2, 5, _abi.FLAG_LAMBERTIAN, seed=0)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    o = osc.render(wl.view, p, wl.width, wl.height)
+    ids_same = (g.ids32 == o["ids32"]).all(-1)
+    assert ids_same.mean() > 0.999
+    np.testing.assert_array_equal(g.visibility[..., 0][ids_same], o["visibility"][..., 0][ids_same])
+    np.testing.assert_allclose(g.albedo[ids_same], o["albedo"][ids_same], atol=1e-6)
+    np.testing.assert_allclose(g.depth[..., 0][ids_same], o["depth"][..., 0][ids_same], rtol=1e-3)
+    np.testing.assert_allclose(g.prev_uv[ids_same], o["prev_uv"][ids_same], atol=1e-4)
+    # packed shading normals agree to within one SNORM16 step per component
+    a = g.visibility[..., 1][ids_same].astype(np.int64)
+    b = o["visibility"][..., 1][ids_same].astype(np.int64)
+    dx = np.abs(((a & 0xFFFF) ^ 0x8000) - ((b & 0xFFFF) ^ 0x8000))
+    dy = np.abs(((a >> 16) ^ 0x8000) - ((b >> 16) ^ 0x8000))
+    assert dx.max() <= 1 and dy.max() <= 1
+
+
+def test_exposure_deterministic_and_accumulate(device, box):
+    wl, _ = box
+    device.upload_scene(wl.scene)
+    p = make_params(8, 2, 5, _abi.FLAG_LAMBERTIAN, seed=3)
+    a = device.render(wl.view, wl.width, wl.height, params=p)
+    b = device.render(wl.view, wl.width, wl.height, params=p)
+    np.testing.assert_array_equal(a.radiance, b.radiance)  # deterministic (no atomics on the accumulators)
+    p.exposure = 1.5
+    c = device.render(wl.view, wl.width, wl.height, params=p)
+    np.testing.assert_allclose(c.radiance[..., :3], a.radiance[..., :3] * 2 ** 1.5, rtol=1e-6)
+    # two progressive calls of 8 spp == one call of 16 spp
+    p16 = make_params(16, 2, 5, _abi.FLAG_LAMBERTIAN, seed=3)
+    p16.wave_paths = 8 * wl.width * wl.height
+    full = device.render(wl.view, wl.width, wl.height, params=p16)
+    p8 = make_params(8, 2, 5, _abi.FLAG_LAMBERTIAN, seed=3)
+    device.render(wl.view, wl.width, wl.height, params=p8)
+    p8b = make_params(8, 2, 5, _abi.FLAG_LAMBERTIAN | _abi.FLAG_ACCUMULATE, seed=11)
+    acc = device.render(wl.view, wl.width, wl.height, params=p8b)
+    np.testing.assert_allclose(acc.radiance, full.radiance, rtol=1e-6, atol=1e-7)
+
+
+def test_box_converges_to_fp64_golden(device, box):
+    wl, _ = box
+    device.upload_scene(wl.scene)
+    gold = np.load(GOLDEN / "box_64x64_fp64_16384spp.npz")
+    p = make_params(4096, 2, 5, _abi.FLAG_LAMBERTIAN, seed=0)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    rm = relmse(g.radiance, gold["mean"])
+    assert rm <= 1e-3, rm
+    # GPU estimator variance from a second independent render
+    p2 = make_params(4096, 2, 5, _abi.FLAG_LAMBERTIAN, seed=50_000)
+    g2 = device.render(wl.view, wl.width, wl.height, params=p2)
+    var_g = (g.radiance[..., :3].astype(np.float64) - g2.radiance[..., :3]) ** 2 / 2
+    z = z_scores(g.radiance, gold["mean"], var_g, gold["var_of_mean"])
+    assert np.mean(np.abs(z) > 5) < 1e-3
+
+
+@pytest.fixture(scope="module")
+def terrain(device):
+    wl = terrain_wl()
+    return wl, OracleScene(wl.scene, 1)
+
+
+@pytest.mark.parametrize("extra", [0, _abi.FLAG_REFERENCE_ENV_MIS, _abi.FLAG_SHADING_NORMALS_OFF])
+def test_terrain_disney_env_same_seed(device, terrain, extra):
+    wl, osc = terrain
+    device.upload_scene(wl.scene)
+    p = make_params(16, 1, 6, extra | J, seed=5)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    o = osc.render(wl.view, p, wl.width, wl.height)
+    assert_same_seed(g, o, f"terrain flags{extra}")
+
+
+def test_terrain_converges_to_fp64_golden(device, terrain):
+    wl, _ = terrain
+    device.upload_scene(wl.scene)
+    gold = np.load(GOLDEN / "terrain_64x36_fp64_16384spp.npz")
+    p = make_params(8192, 1, 6, 0, seed=0)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    rm = relmse(g.radiance, gold["mean"])
+    assert rm <= 1e-3, rm
+
+
+@pytest.mark.parametrize("scene_name", ["box", "terrain"])
+def test_restir_di_same_seed_and_unbiased(device, box, terrain, scene_name):
+    wl, osc = box if scene_name == "box" else terrain
+    base = _abi.FLAG_LAMBERTIAN if scene_name == "box" else 0
+    minl, maxl = (2, 5) if scene_name == "box" else (1, 6)
+    device.upload_scene(wl.scene)
+    p = make_params(4, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, seed=9, restir_m=8)
+    g = device.render(wl.view, wl.width, wl.height, params=p)
+    o = osc.render(wl.view, p, wl.width, wl.height)
+    assert_same_seed(g, o, f"restir {scene_name}")
+    # RIS with M candidates converges to the same image as plain NEE
+    pr = make_params(2048, minl, maxl, base | _abi.FLAG_RESTIR_DI, seed=100, restir_m=8)
+    pn = make_params(2048, minl, maxl, base, seed=200)
+    r = device.render(wl.view, wl.width, wl.height, params=pr).radiance
+    n = device.render(wl.view, wl.width, wl.height, params=pn).radiance
+    assert relmse(r, n) < 5e-3
+
+
+def test_invalid_arguments_return_errors(device, box):
+    wl, _ = box
+    device.upload_scene(wl.scene)
+    p = make_params(0, 2, 5, _abi.FLAG_LAMBERTIAN)
+    with pytest.raises(_abi.S2Error) as e:
+        device.render(wl.view, wl.width, wl.height, params=p)
+    assert e.value.code == _abi.S2_ERR_INVALID
+    p = make_params(1, 2, 300, _abi.FLAG_LAMBERTIAN)
+    with pytest.raises(_abi.S2Error):
+        device.render(wl.view, wl.width, wl.height, params=p)

@@ -2,7 +2,9 @@
 
 * FP32 replica: the oracle evaluates the same watertight test in IEEE single precision, so
   t, instance, primitive and barycentrics must be bit-identical.
-* FP64 oracle: t within 1e-5 relative; instance/primitive identical except documented ties
+* FP64 oracle: t within 1e-5 relative (relative to max(t, 0.05): below 0.05 units of these unit-size
+  scenes the float rounding of ray origins and vertices, up to ~2e-7 absolute, dominates); instance/primitive
+  identical except documented ties
   (rays whose closest hits on two different triangles are at equal distance, i.e. rays through
   shared edges/vertices), which must stay below 1e-4 of the rays and be equal-t within 1e-5.
 """
@@ -42,7 +44,7 @@ def test_closest_hit_bit_exact_vs_fp32_oracle(device, scene_case):
     g = device.trace(rays)
     o = osc.trace(rays, precision=32)
     hit = g["instance"] != INV
-    assert hit.mean() > 0.3, "test rays should mostly hit"
+    assert hit.mean() > 0.2, "test rays should often hit"
     np.testing.assert_array_equal(g["instance"], o["instance"])
     np.testing.assert_array_equal(g["primitive"], o["primitive"])
     np.testing.assert_array_equal(g["t"][hit], o["t"][hit].astype(np.float32))
@@ -60,7 +62,7 @@ def test_closest_hit_vs_fp64_oracle(device, scene_case):
     # every mismatch must be a tie (equal distance), and ties are rare
     assert mismatch.mean() < 1e-4, f"{mismatch.sum()} id mismatches of {len(rays)}"
     assert np.all(both[mismatch]), "a ray hit in one implementation and missed in the other"
-    rel = np.abs(g["t"][both].astype(np.float64) - o["t"][both]) / np.maximum(o["t"][both], 1e-6)
+    rel = np.abs(g["t"][both].astype(np.float64) - o["t"][both]) / np.maximum(o["t"][both], 5e-2)
     assert rel.max() < 1e-5, rel.max()
 
 
