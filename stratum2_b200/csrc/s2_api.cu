@@ -93,6 +93,78 @@ inline float rd_f32(const uint8_t* b, uint64_t size, uint64_t off, bool& ok) {
     float v; std::memcpy(&v, b + off, 4); return v;
 }
 
+// Hierarchical environment-sampling tables (see DevImage): the 2x2 block probabilities that
+// SampleTexel (src/Shaders/common/lights.hlsli:49-96) computes at every level of its descent, and
+// the pdf SampleTexelPdf (:97-138) returns for every texel of the finest level it reaches.  Built
+// only when each mip level is an exact halving of the previous one.
+void build_env_tables(S2Context* ctx, DevImage& di, const std::vector<float>& lum) {
+    const uint32_t L = di.levels;
+    di.nested = 0; di.quad = nullptr; di.pdf = nullptr;
+    if (L < 3) return;
+    for (uint32_t l = 1; l < L; ++l) {
+        const bool wx = di.lw[l - 1] == 2 * di.lw[l] || (di.lw[l - 1] == 1 && di.lw[l] == 1);
+        const bool hy = di.lh[l - 1] == 2 * di.lh[l] || (di.lh[l - 1] == 1 && di.lh[l] == 1);
+        if (!wx || !hy) return;
+    }
+    const float pi = 3.14159265358979323846f;
+    auto texel = [&](uint32_t l, int x, int y) -> float {
+        if (x < 0 || y < 0 || x >= (int)di.lw[l] || y >= (int)di.lh[l]) return 0.f;
+        return lum[di.lum_offset[l] + (size_t)y * di.lw[l] + x];
+    };
+    // the four luminance * sin(theta) weights of the block at (cx, cy)
+    auto block = [&](uint32_t l, int cx, int cy, float p[4]) {
+        const uint32_t ex = di.lw[l], ey = di.lh[l];
+        const float inv_h = 1.f / (float)ey;
+        p[0] = p[1] = p[2] = p[3] = 0.f;
+        if ((int)ex - cx > 1) {
+            const float sy = sinf(pi * (cy + 0.5f) * inv_h);
+            p[0] = texel(l, cx, cy) * sy; p[1] = texel(l, cx + 1, cy) * sy;
+        }
+        if ((int)ey - cy > 1) {
+            const float sy = sinf(pi * (cy + 1.5f) * inv_h);
+            p[2] = texel(l, cx, cy + 1) * sy; p[3] = texel(l, cx + 1, cy + 1) * sy;
+        }
+    };
+    const uint32_t lim = std::min(11u, L - 1);
+    std::vector<float4> quad;
+    for (uint32_t i = 1; i < lim; ++i) {
+        const uint32_t l = L - 1 - i;
+        const uint32_t bw = (di.lw[l] + 1) / 2, bh = (di.lh[l] + 1) / 2;
+        di.quad_offset[l] = (uint32_t)quad.size();
+        di.qw[l] = bw;
+        for (uint32_t by = 0; by < bh; ++by) for (uint32_t bx = 0; bx < bw; ++bx) {
+            float p[4];
+            block(l, 2 * (int)bx, 2 * (int)by, p);
+            const float sum = p[0] + p[1] + p[2] + p[3];
+            if (sum < 1e-6f) quad.push_back(make_float4(-1.f, 0.f, 0.f, 0.f));
+            else quad.push_back(make_float4(p[0] / sum, p[1] / sum, p[2] / sum, p[3] / sum));
+        }
+    }
+    const uint32_t f = L - lim;  // finest level of the descent
+    std::vector<float> pdf((size_t)di.lw[f] * di.lh[f]);
+    for (uint32_t y = 0; y < di.lh[f]; ++y) for (uint32_t x = 0; x < di.lw[f]; ++x) {
+        float pd = 1.f;
+        uint32_t lx = 1, ly = 1;
+        for (uint32_t i = 1; i < lim; ++i) {
+            const uint32_t l = L - 1 - i;
+            const int ux = (int)(x >> (l - f)), uy = (int)(y >> (l - f));
+            const int cx = (ux / 2) * 2, cy = (uy / 2) * 2;
+            const int ox = std::min(ux - cx, 1), oy = std::min(uy - cy, 1);
+            float p[4];
+            block(l, cx, cy, p);
+            const float sum = p[0] + p[1] + p[2] + p[3];
+            if (sum < 1e-6f) continue;
+            pd *= p[oy * 2 + ox] / sum;
+            lx = di.lw[l]; ly = di.lh[l];
+        }
+        pdf[(size_t)y * di.lw[f] + x] = pd * (float)(lx * ly);
+    }
+    di.quad = upload(ctx, ctx->scene_bufs, quad.data(), quad.size());
+    di.pdf = upload(ctx, ctx->scene_bufs, pdf.data(), pdf.size());
+    di.pdf_level = f;
+    di.nested = (di.quad && di.pdf) ? 1u : 0u;
+}
+
 }  // namespace
 
 // ============================================================================== lifecycle
@@ -327,6 +399,7 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
                     lum.push_back(0.2126f * lv[l][4 * t] + 0.7152f * lv[l][4 * t + 1] + 0.0722f * lv[l][4 * t + 2]);
             }
             di.lum = upload(ctx, ctx->scene_bufs, lum.data(), lum.size());
+            build_env_tables(ctx, di, lum);
             ctx->env_image = (int)i;
         }
         ctx->images_host[i] = di;

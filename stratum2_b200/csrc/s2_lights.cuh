@@ -11,7 +11,8 @@ S2D float texel_lum(const DevImage& im, uint32_t level, int x, int y) {
     return im.lum[im.lum_offset[level] + (size_t)y * im.lw[level] + x];
 }
 
-// SampleTexel (lights.hlsli:49-96), at most 10 levels
+// SampleTexel (lights.hlsli:49-96), at most 10 levels.  With the precomputed block table each
+// level is one 16-byte load instead of four texel loads and two sines.
 S2D float2 sample_texel(const DevImage& im, float rx, float ry, float& pdf) {
     const uint32_t levels = im.levels;
     pdf = 1.f;
@@ -21,10 +22,26 @@ S2D float2 sample_texel(const DevImage& im, float rx, float ry, float& pdf) {
     for (uint32_t i = 1; i < lim; ++i) {
         const uint32_t level = levels - 1 - i;
         const uint32_t ex = im.lw[level], ey = im.lh[level];
-        const float inv_h = 1.f / (float)ey;
         cx *= (int)(ex / lx);
         cy *= (int)(ey / ly);
         float p[4] = {0.f, 0.f, 0.f, 0.f};
+        if (im.nested) {
+            // all-zero weights outside the level, as the per-texel path computes
+            if (cx >= (int)ex || cy >= (int)ey || (cx & 1) || (cy & 1)) continue;
+            const float4 q = __ldg(im.quad + im.quad_offset[level] + (size_t)(cy >> 1) * im.qw[level] + (cx >> 1));
+            if (q.x < 0.f) continue;
+            p[0] = q.x; p[1] = q.y; p[2] = q.z; p[3] = q.w;
+            for (int j = 0; j < 4; ++j) {
+                if (j == 3 || rx < p[j]) {
+                    cx += j % 2; cy += j / 2; pdf *= p[j]; rx /= p[j];
+                    break;
+                }
+                rx -= p[j];
+            }
+            lx = ex; ly = ey;
+            continue;
+        }
+        const float inv_h = 1.f / (float)ey;
         if ((int)ex - cx > 1) {
             const float sy = sinf(S2_PI * (cy + 0.5f) * inv_h);
             p[0] = texel_lum(im, level, cx, cy) * sy;
@@ -51,9 +68,15 @@ S2D float2 sample_texel(const DevImage& im, float rx, float ry, float& pdf) {
     return make_float2(((float)cx + rx) / (float)lx, ((float)cy + ry) / (float)ly);
 }
 
-// SampleTexelPdf (lights.hlsli:97-138)
+// SampleTexelPdf (lights.hlsli:97-138); one table load when the mip levels nest
 S2D float sample_texel_pdf(const DevImage& im, float2 uv) {
     const uint32_t levels = im.levels;
+    if (im.nested) {
+        const uint32_t f = im.pdf_level;
+        const int ux = (int)((float)im.lw[f] * uv.x), uy = (int)((float)im.lh[f] * uv.y);
+        if (ux >= 0 && uy >= 0 && ux < (int)im.lw[f] && uy < (int)im.lh[f])
+            return __ldg(im.pdf + (size_t)uy * im.lw[f] + ux);
+    }
     float pdf = 1.f;
     uint32_t lx = 1, ly = 1;
     const uint32_t lim = min(11u, levels - 1);

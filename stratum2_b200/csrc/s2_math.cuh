@@ -88,6 +88,11 @@ struct Rng {
         r.x = pcg32_step(); r.y = pcg32_step(); r.z = pcg32_step(); r.w = pcg32_step();
         return r;
     }
+    // advance by one next() without hashing (pcg4d is counter based)
+    S2D void skip() {
+        if (!pcg32) { ctr++; return; }
+        pcg32_step(); pcg32_step(); pcg32_step(); pcg32_step();
+    }
     S2D float4 next_float() {
         uint4 u = next();
         return make_float4(u2f(u.x), u2f(u.y), u2f(u.z), u2f(u.w));

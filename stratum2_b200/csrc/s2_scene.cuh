@@ -13,6 +13,17 @@ struct DevImage {
     uint32_t levels;
     uint32_t lum_offset[S2_MAX_IMAGE_LEVELS];
     uint32_t lw[S2_MAX_IMAGE_LEVELS], lh[S2_MAX_IMAGE_LEVELS];
+    // Precomputed hierarchical-sampling tables (only when every level is an exact halving, so a
+    // texel of the finest sampled level determines its 2x2 block at every coarser level):
+    //   quad: per level, per 2x2 block (block x = cx/2, y = cy/2) the normalised probabilities of
+    //         its four texels, or x = -1 where their luminance-weighted sum is below 1e-6;
+    //   pdf:  per texel of the finest sampled level, the texel pdf of SampleTexelPdf.
+    const float4* quad;
+    uint32_t quad_offset[S2_MAX_IMAGE_LEVELS];
+    uint32_t qw[S2_MAX_IMAGE_LEVELS];
+    const float* pdf;
+    uint32_t pdf_level;
+    uint32_t nested;
 };
 
 struct DevScene {

@@ -75,6 +75,10 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
         dir = best_d;
         dist = best_dist;
     } else {
+        if (len + 1 < P.min_len) {  // shorter than minPathLength: advance the stream by one draw only
+            rng.skip();
+            return so;
+        }
         const float4 x = rng.next_float();
         const Illum r = sample_illum(s, x, sd.pos, sn);
         if (all_nonpos(r.radiance) || r.pdf <= 0.f) return so;
@@ -146,9 +150,9 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                     }
                     if (P.aov_ids) P.aov_ids[pix] = make_uint2(0xffffffffu, 0xffffffffu);
                 }
-                float env_pdf;
-                const float3 e = thr * eval_env(s, dir, env_pdf);
-                if (any_pos(e) && len >= P.min_len) {
+                float env_pdf = 0.f;
+                const float3 e = len >= P.min_len ? thr * eval_env(s, dir, env_pdf) : f3(0.f);
+                if (any_pos(e)) {
                     float w = 1.f;
                     if (len > 1 && nee && dir_pdf > 0.f) {
                         const float lp = (P.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;

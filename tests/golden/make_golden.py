@@ -4,7 +4,8 @@
 
 Each fixture is an .npz with the per-pixel mean radiance and the variance of that mean, rendered
 by the FP64 oracle (oracle/oracle.cpp) at high sample counts with frame seeds disjoint from the
-ones the GPU tests use.  Scenes come from stratum2_b200.scenegen with fixed seeds.
+ones the GPU tests use, with jittered pixel positions (the converged image is then the box-filtered
+pixel integral, which has no exact ray/edge ties).  Scenes come from stratum2_b200.scenegen with fixed seeds.
 """
 from __future__ import annotations
 
@@ -29,7 +30,7 @@ def box_case():
     wl = box_scene(seed=1, width=64, height=64)
     p = _abi.S2RenderParams()
     p.min_path_length, p.max_path_length = 2, 5
-    p.flags = _abi.FLAG_LAMBERTIAN
+    p.flags = _abi.FLAG_LAMBERTIAN | _abi.FLAG_PIXEL_JITTER
     p.environment_sample_probability = 0.9
     p.restir_candidates = 32
     return wl, p
@@ -39,13 +40,13 @@ def terrain_case():
     wl = terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
     p = _abi.S2RenderParams()
     p.min_path_length, p.max_path_length = 1, 6
-    p.flags = 0
+    p.flags = _abi.FLAG_PIXEL_JITTER
     p.environment_sample_probability = 0.9
     p.restir_candidates = 32
     return wl, p
 
 
-CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 16384)}
+CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 131072)}
 
 
 def make(name: str, out_dir: Path = HERE):

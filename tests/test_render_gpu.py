@@ -5,15 +5,20 @@ reference's counter-based pcg4d stream, or PCG32), so the images agree sample by
 floating-point divergence of individual paths.  The floor of that divergence is set by the
 reference's own path-state packing: ray directions are stored octahedral SNORM16
 (testrenderer.slang:119-122), so a 1e-7 rounding difference flips ~2% of direction components by
-one 3e-5 rad step, which occasionally moves a hit across a small triangle's edge.  The oracle's
-own FP32 build differs from its FP64 build by the same amount (box scene, 16 spp: relMSE 1.6e-5
-with pixel jitter; 3.8e-4 without jitter, where the symmetric box puts diagonal pixels' camera
-rays exactly on its corner seams).  Tolerances: relMSE < 2e-4 (jittered) / 1e-3 (pixel
-centres) and 97% of pixel channels within 1e-3 relative (+1e-4 absolute).
+one 3e-5 rad step, which occasionally moves a hit across a small triangle's edge; and at pixel
+centres the symmetric box puts diagonal pixels' camera rays exactly on its corner seams, where
+float and double tie-break differently.  The oracle's own FP32 build differs from its FP64 build
+by the same amount.  The criterion is therefore normalised by the estimator noise: with
+z = (gpu - oracle) / (oracle standard error), mean(z^2) is 0 for identical samples and ~2 for
+independent ones; it must stay below 0.05 (pixel jitter) / 0.2 (pixel centres), and 97% of pixel
+channels must agree within 1e-3 relative (+1e-4 absolute).
 
-Convergence tests: a high-spp GPU image against a committed FP64 oracle image rendered with
-disjoint seeds (tests/golden/make_golden.py): relMSE <= 1e-3 and a per-pixel z-test of the
-estimator means (|z| < 5 for all but 0.1% of pixel channels).
+Convergence tests: the mean of 16 independent GPU batches against a committed FP64 oracle image
+rendered with disjoint seeds (tests/golden/make_golden.py).  Per pixel channel
+z = (gpu - oracle) / sqrt(var_gpu + var_oracle) with var_gpu from the 16 batches (t, 15 dof):
+|z| > 5 for at most 0.1% of channels, |mean z| < 0.1 (no global bias), and relMSE below 1e-3
+(box) or twice the noise floor the two estimators' variances predict (terrain: its 5e3 sun seen
+through glossy spheres gives a relative per-sample variance of ~24).
 """
 from pathlib import Path
 
@@ -22,7 +27,7 @@ import pytest
 
 from oracle_lib import OracleScene
 from stratum2_b200 import _abi
-from stratum2_b200.metrics import relmse, z_scores
+from stratum2_b200.metrics import relmse
 from stratum2_b200.scenegen import box_scene, terrain_scene
 
 pytestmark = pytest.mark.gpu
@@ -48,10 +53,31 @@ def terrain_wl():
 def assert_same_seed(g, o, tag="", jitter=True):
     gm = g.radiance[..., :3].astype(np.float64)
     om = o["mean"]
-    rm = relmse(gm, om)
+    se2 = o["var_of_mean"]
+    live = se2 > 0
+    z2 = np.where(live, (gm - om) ** 2 / np.where(live, se2, 1), 0.0)
     close = np.abs(gm - om) <= 1e-3 * np.abs(om) + 1e-4
-    assert rm < (2e-4 if jitter else 1e-3), f"{tag} relMSE {rm}"
+    assert z2.mean() < (0.05 if jitter else 0.2), f"{tag} mean z^2 {z2.mean()}"
     assert close.mean() > 0.97, f"{tag} only {close.mean():.4f} of pixel channels agree"
+
+
+def batches(device, wl, p, n, spp, seed0):
+    """Mean and variance of the mean over n independent GPU renders of `spp` samples."""
+    imgs = []
+    for b in range(n):
+        p.spp, p.frame_seed = spp, seed0 + b * spp
+        imgs.append(device.render(wl.view, wl.width, wl.height, params=p).radiance[..., :3].astype(np.float64))
+    imgs = np.stack(imgs)
+    return imgs.mean(0), imgs.var(0, ddof=1) / n
+
+
+def assert_converged(mean_a, var_a, mean_b, var_b, relmse_max, tag=""):
+    z = (mean_a - mean_b) / np.sqrt(np.maximum(var_a + var_b, 1e-30))
+    frac = np.mean(np.abs(z) > 5)
+    assert frac <= 1e-3, f"{tag}: {frac:.4%} of pixel channels with |z| > 5"
+    assert abs(z.mean()) < 0.1, f"{tag}: mean z {z.mean():.3f} (bias)"
+    rm = relmse(mean_a, mean_b)
+    assert rm <= relmse_max, f"{tag}: relMSE {rm} > {relmse_max}"
 
 
 @pytest.fixture(scope="module")
@@ -121,16 +147,9 @@ def test_box_converges_to_fp64_golden(device, box):
     wl, _ = box
     device.upload_scene(wl.scene)
     gold = np.load(GOLDEN / "box_64x64_fp64_16384spp.npz")
-    p = make_params(4096, 2, 5, _abi.FLAG_LAMBERTIAN, seed=0)
-    g = device.render(wl.view, wl.width, wl.height, params=p)
-    rm = relmse(g.radiance, gold["mean"])
-    assert rm <= 1e-3, rm
-    # GPU estimator variance from a second independent render
-    p2 = make_params(4096, 2, 5, _abi.FLAG_LAMBERTIAN, seed=50_000)
-    g2 = device.render(wl.view, wl.width, wl.height, params=p2)
-    var_g = (g.radiance[..., :3].astype(np.float64) - g2.radiance[..., :3]) ** 2 / 2
-    z = z_scores(g.radiance, gold["mean"], var_g, gold["var_of_mean"])
-    assert np.mean(np.abs(z) > 5) < 1e-3
+    p = make_params(1, 2, 5, _abi.FLAG_LAMBERTIAN | J)
+    m, v = batches(device, wl, p, 16, 256, seed0=0)  # 4096 spp in total
+    assert_converged(m, v, gold["mean"], gold["var_of_mean"], 1e-3, "box 4096 spp")
 
 
 @pytest.fixture(scope="module")
@@ -152,11 +171,11 @@ def test_terrain_disney_env_same_seed(device, terrain, extra):
 def test_terrain_converges_to_fp64_golden(device, terrain):
     wl, _ = terrain
     device.upload_scene(wl.scene)
-    gold = np.load(GOLDEN / "terrain_64x36_fp64_16384spp.npz")
-    p = make_params(8192, 1, 6, 0, seed=0)
-    g = device.render(wl.view, wl.width, wl.height, params=p)
-    rm = relmse(g.radiance, gold["mean"])
-    assert rm <= 1e-3, rm
+    gold = np.load(GOLDEN / "terrain_64x36_fp64_131072spp.npz")
+    p = make_params(1, 1, 6, J)
+    m, v = batches(device, wl, p, 16, 4096, seed0=0)  # 65536 spp in total
+    floor = np.mean((v + gold["var_of_mean"]) / (gold["mean"] ** 2 + 1e-2))
+    assert_converged(m, v, gold["mean"], gold["var_of_mean"], max(1e-3, 2 * floor), "terrain 65536 spp")
 
 
 @pytest.mark.parametrize("scene_name", ["box", "terrain"])
@@ -170,11 +189,10 @@ def test_restir_di_same_seed_and_unbiased(device, box, terrain, scene_name):
     o = osc.render(wl.view, p, wl.width, wl.height)
     assert_same_seed(g, o, f"restir {scene_name}")
     # RIS with M candidates converges to the same image as plain NEE
-    pr = make_params(2048, minl, maxl, base | _abi.FLAG_RESTIR_DI, seed=100, restir_m=8)
-    pn = make_params(2048, minl, maxl, base, seed=200)
-    r = device.render(wl.view, wl.width, wl.height, params=pr).radiance
-    n = device.render(wl.view, wl.width, wl.height, params=pn).radiance
-    assert relmse(r, n) < 5e-3
+    mr, vr = batches(device, wl, make_params(1, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, restir_m=8), 16, 512, 100)
+    mn, vn = batches(device, wl, make_params(1, minl, maxl, base | J), 16, 512, 20000)
+    floor = np.mean((vr + vn) / (mn ** 2 + 1e-2))
+    assert_converged(mr, vr, mn, vn, 3 * floor, f"restir vs nee {scene_name}")
 
 
 def test_invalid_arguments_return_errors(device, box):
