@@ -1,0 +1,324 @@
+"""Benchmark of the plain wavefront path tracer on the terrain workload.
+
+Workload (one step): heightfield terrain on a 1024x1024 grid (2,093,058 triangles, 6 octaves of
+seeded value noise, amplitude 0.2) plus 64 instanced level-5 icospheres (20,480 triangles each)
+under seeded transforms, GLTF metallic-roughness materials, a 512x256 procedural HDR sky with a 5e3
+sun lobe over 0.5 degrees; 1920x1080 pixels, 64 samples per pixel, path length 3..12 with Russian
+roulette.  The BVH and triangles (~200 MB) exceed the 126 MB L2, so no flush is needed between
+steps.
+
+Metric: Mrays/s = (extension + shadow rays traced) / GPU time, summed over all ranks.
+Multi-GPU (torchrun): every rank renders the same view with its own frame seeds (weak scaling),
+and the per-rank images are summed into rank 0 with one NCCL reduce per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SPP = 64
+MIN_LEN, MAX_LEN = 3, 12
+WORKLOAD = ("terrain 1024^2 grid (2.09M tris) + 64 icospheres (1.31M tris), GLTF MR materials, 512x256 HDR sky "
+            "with 5e3 sun; 1920x1080, 64 spp, path length 3..12, Russian roulette")
+NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES = 80, 48, 32, 16
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def extend_traffic_per_ray() -> float | None:
+    """DRAM bytes per extension ray of k_extend from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "k_extend_terrain.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+-]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        if not sm:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if "Active" in r[5 + k]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "samples": len(sm), "reasons": reasons}
+
+
+def cpu_oracle(wl):
+    """FP32 build of the oracle (the CPU restatement of the same path), used as the CPU baseline."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import OracleScene  # noqa: E402 (checker code: CPU baseline leg only)
+    return OracleScene(wl.scene, 2)
+
+
+def cpu_stride(osc, wl, p, seconds: float, threads: int) -> int:
+    """Pixel stride whose render takes about `seconds` on the host cores."""
+    probe = 24
+    t0 = time.perf_counter()
+    osc.render(wl.view, p, wl.width, wl.height, precision=32, stride=probe, threads=threads)
+    dt = time.perf_counter() - t0
+    per_px = dt / (len(range(0, wl.height, probe)) * len(range(0, wl.width, probe)))
+    return max(2, int(np.sqrt(wl.width * wl.height * per_px / max(seconds, 0.5))))
+
+
+def cpu_sample(osc, wl, p, stride: int, threads: int) -> dict:
+    """Times the oracle's FP32 build on every `stride`-th pixel of the workload."""
+    t0 = time.perf_counter()
+    r = osc.render(wl.view, p, wl.width, wl.height, precision=32, stride=stride, threads=threads)
+    dt = time.perf_counter() - t0
+    rays = r["extension_rays"] + r["shadow_rays"]
+    npx = len(range(0, wl.height, stride)) * len(range(0, wl.width, stride))
+    return {"rays": rays, "seconds": dt, "mrays_per_s": rays / dt / 1e6, "pixels": npx, "stride": stride}
+
+
+def params(dev, spp: int, seed: int, flags: int = 0):
+    p = dev.default_params() if dev is not None else None
+    if p is None:
+        from stratum2_b200 import _abi
+        p = _abi.S2RenderParams()
+        _abi.lib().s2_default_render_params(p)
+    p.spp, p.frame_seed, p.min_path_length, p.max_path_length, p.flags = spp, seed, MIN_LEN, MAX_LEN, flags
+    return p
+
+
+def run_reference(args, rank: int, world: int):
+    """Reference arm: the CPU restatement of the path on the host cores (the reference's own
+    Vulkan/Slang implementation cannot be built or run here)."""
+    if rank != 0:
+        return
+    from stratum2_b200 import _abi
+    from stratum2_b200.scenegen import terrain_scene
+    wl = terrain_scene()
+    p = _abi.S2RenderParams()
+    _abi.lib().s2_default_render_params(p)
+    p.spp, p.min_path_length, p.max_path_length = SPP, MIN_LEN, MAX_LEN
+    threads = os.cpu_count() or 1
+    osc = cpu_oracle(wl)
+    stride = cpu_stride(osc, wl, p, 5.0, threads)
+    total_rays = 0.0
+    total_s = 0.0
+    for step in range(args.warmup + args.steps):
+        p.frame_seed = 1000 * step
+        r = cpu_sample(osc, wl, p, stride, threads)
+        if step >= args.warmup:
+            total_rays += r["rays"]
+            total_s += r["seconds"]
+    v = total_rays / total_s / 1e6
+    line = {"metric": "Mrays/s", "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "min_path_length": MIN_LEN,
+                                                     "max_path_length": MAX_LEN, "spp": SPP},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": f"pixel subset (stride {r['stride']}, {r['pixels']} pixels) x {SPP} spp per step"},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+
+    from stratum2_b200 import Device, _abi
+    from stratum2_b200.scenegen import terrain_scene
+
+    torch.cuda.set_device(local_rank)
+    dev = Device(local_rank)
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    wl = terrain_scene()
+    dev.upload_scene(wl.scene)
+    W, H = wl.width, wl.height
+    rad = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+
+    def seed(step: int) -> int:
+        return (step * world + rank) * SPP  # disjoint frame seeds per rank and step
+
+    # fetch counts for the algorithmic-byte model (untimed run, same seeds as timed step 0)
+    cnt = dev.render_device(wl.view, params(dev, SPP, seed(0), _abi.FLAG_COUNT_FETCHES), aovs)
+    for w in range(args.warmup):
+        dev.render_device(wl.view, params(dev, SPP, seed(w + 1000)), aovs)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    e0.record(stream)
+    for step in range(args.steps):
+        stats.append(dev.render_device(wl.view, params(dev, SPP, seed(step), _abi.FLAG_PROFILE_KERNELS), aovs))
+        if world > 1:
+            dist.reduce(rad, dst=0)  # combine the ranks' sample partitions of the frame
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    rays = float(sum(s.extension_rays + s.shadow_rays for s in stats))
+    paths = float(sum(s.paths for s in stats))
+    t = torch.tensor([ms, rays, paths], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tmax = t[:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t[1:].clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms, rays, paths = float(tmax[0]), float(tsum[0]), float(tsum[1])
+    value = rays / ms / 1e3
+
+    # end to end through the public API with host buffers (view/params in, all AOVs out)
+    dev.set_stream(None)
+    for w in range(1):
+        dev.render(wl.view, W, H, params=params(dev, SPP, seed(w + 2000)))
+    t0 = time.perf_counter()
+    e2e_rays = 0
+    for step in range(args.steps):
+        r = dev.render(wl.view, W, H, params=params(dev, SPP, seed(step + 3000)))
+        e2e_rays += r.stats.extension_rays + r.stats.shadow_rays
+    e2e_s = time.perf_counter() - t0
+    e2e = torch.tensor([e2e_s, float(e2e_rays)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        es = e2e[:1].clone(); dist.all_reduce(es, op=dist.ReduceOp.MAX)
+        er = e2e[1:].clone(); dist.all_reduce(er, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_rays = float(es[0]), float(er[0])
+    if rank != 0:
+        return
+
+    # roofline of the dominant kernel
+    ext_ms = sum(s.extend_ms for s in stats); sh_ms = sum(s.shade_ms for s in stats); oc_ms = sum(s.occlude_ms for s in stats)
+    ext_launches = sum(s.extend_launches for s in stats)
+    ext_rays = sum(s.extension_rays for s in stats)
+    bytes_per_ray = (RAY_BYTES + HIT_BYTES + NODE_BYTES * cnt.extend_node_fetches / max(cnt.extension_rays, 1)
+                     + TRI_BYTES * cnt.extend_tri_fetches / max(cnt.extension_rays, 1))
+    rays_per_launch = ext_rays / max(ext_launches, 1)
+    avg_launch_s = ext_ms / 1e3 / max(ext_launches, 1)
+    achieved = bytes_per_ray * rays_per_launch / avg_launch_s / 1e9
+    pk = peaks()
+    tpr = extend_traffic_per_ray()
+    dominant = max([("k_extend", ext_ms), ("k_shade", sh_ms), ("k_occlude", oc_ms)], key=lambda x: x[1])[0]
+    roof = {"kernel": "k_extend", "dominant_kernel": dominant, "bound": "hbm", "achieved": achieved,
+            "peak": pk["hbm_gbs"], "peak_source": pk["source"] + " copy bandwidth", "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"],
+            "traffic": (tpr * rays_per_launch) if tpr is not None else None,
+            "algorithmic_bytes_per_launch": bytes_per_ray * rays_per_launch,
+            "bytes_per_ray": bytes_per_ray,
+            "node_fetches_per_ray": cnt.extend_node_fetches / max(cnt.extension_rays, 1),
+            "tri_fetches_per_ray": cnt.extend_tri_fetches / max(cnt.extension_rays, 1),
+            "avg_launch_ms": avg_launch_s * 1e3}
+    line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, no datasets)",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "min_path_length": MIN_LEN,
+                       "max_path_length": MAX_LEN, "triangles": int(dev.bvh_stats.triangle_count),
+                       "bvh8_nodes": int(dev.bvh_stats.node_count), "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"{world} rank(s), disjoint sample seeds"},
+            "mpaths_per_s": paths / ms / 1e3,
+            "kernel_ms_per_step": {"k_extend": ext_ms / args.steps, "k_shade": sh_ms / args.steps,
+                                   "k_occlude": oc_ms / args.steps},
+            "gpu_launches": int(sum(s.kernel_launches for s in stats)),
+            "roofline": roof,
+            "e2e": {"value": e2e_rays / e2e_s / 1e6, "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(C_sizeof_view_params()),
+                    "d2h_bytes_per_step": int(W * H * (16 + 16 + 8 + 16 + 8 + 8))},
+            "clocks": ck}
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        osc = cpu_oracle(wl)
+        pc = params(None, SPP, 0)
+        c = cpu_sample(osc, wl, pc, cpu_stride(osc, wl, pc, args.cpu_seconds, threads), threads)
+        line["cpu_baseline"] = {"value": c["mrays_per_s"], "unit": "Mrays/s", "cores": threads, "kind": "port",
+                                "sample": f"FP32 oracle, every {c['stride']}th pixel ({c['pixels']} pixels) x {SPP} spp, "
+                                          f"{c['seconds']:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+def C_sizeof_view_params() -> int:
+    import ctypes
+    from stratum2_b200 import _abi
+    return ctypes.sizeof(_abi.S2View) + ctypes.sizeof(_abi.S2RenderParams)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -155,6 +155,8 @@ typedef struct S2View {
 #define S2_FLAG_NO_RR               (1u << 6)  /* disable Russian roulette */
 #define S2_FLAG_ACCUMULATE          (1u << 7)  /* add into the previous accumulation (progressive) */
 #define S2_FLAG_SHADING_NORMALS_OFF (1u << 8)  /* ignore vertex normals (gShadingNormals false) */
+#define S2_FLAG_PROFILE_KERNELS     (1u << 9)  /* time extend/shade/occlude launches with CUDA events */
+#define S2_FLAG_COUNT_FETCHES       (1u << 10) /* count BVH node and triangle fetches (slower) */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */
@@ -192,6 +194,12 @@ typedef struct S2RenderStats {
     uint64_t paths;            /* camera paths (pixels x spp) */
     uint64_t nan_count;        /* paths dropped for NaN/Inf throughput */
     double gpu_ms;             /* device time of the call (CUDA events) */
+    uint64_t kernel_launches;  /* kernels launched by the call */
+    /* S2_FLAG_PROFILE_KERNELS: summed device time per kernel kind */
+    double extend_ms, shade_ms, occlude_ms;
+    uint32_t extend_launches, shade_launches, occlude_launches, reserved;
+    /* S2_FLAG_COUNT_FETCHES: BVH node / triangle fetches of extension and shadow rays */
+    uint64_t extend_node_fetches, extend_tri_fetches, shadow_node_fetches, shadow_tri_fetches;
 } S2RenderStats;
 
 /* ---- lifecycle --------------------------------------------------------------------------- */

@@ -34,6 +34,8 @@ FLAG_REFERENCE_ENV_MIS = 1 << 5
 FLAG_NO_RR = 1 << 6
 FLAG_ACCUMULATE = 1 << 7
 FLAG_SHADING_NORMALS_OFF = 1 << 8
+FLAG_PROFILE_KERNELS = 1 << 9
+FLAG_COUNT_FETCHES = 1 << 10
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -116,7 +118,11 @@ class S2Aovs(C.Structure):
 
 class S2RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
-                ("nan_count", C.c_uint64), ("gpu_ms", C.c_double)]
+                ("nan_count", C.c_uint64), ("gpu_ms", C.c_double), ("kernel_launches", C.c_uint64),
+                ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("occlude_ms", C.c_double),
+                ("extend_launches", C.c_uint32), ("shade_launches", C.c_uint32), ("occlude_launches", C.c_uint32),
+                ("reserved", C.c_uint32), ("extend_node_fetches", C.c_uint64), ("extend_tri_fetches", C.c_uint64),
+                ("shadow_node_fetches", C.c_uint64), ("shadow_tri_fetches", C.c_uint64)]
 
 
 assert C.sizeof(S2Ray) == 32 and C.sizeof(S2Hit) == 20

@@ -30,10 +30,12 @@ struct RenderState {
     unsigned long long* stats = nullptr;
     uint64_t accumulated_spp = 0;
     int ext_blocks = 0, occ_blocks = 0, shade_blocks = 0;
+    std::vector<cudaEvent_t> events;  // reusable start/stop pairs for S2_FLAG_PROFILE_KERNELS
 };
 
 void destroy_render_state(S2Context* ctx) {
     if (!ctx->render) return;
+    for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -55,9 +57,9 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
         cudaDeviceProp prop;
         cudaGetDeviceProperties(&prop, ctx->device);
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, kTravBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend<false>, kTravBlock, 0);
         st->ext_blocks = std::max(1, b) * prop.multiProcessorCount;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_occlude, kTravBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_occlude<false>, kTravBlock, 0);
         st->occ_blocks = std::max(1, b) * prop.multiProcessorCount;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, false>, 128, 0);
         st->shade_blocks = std::max(1, b) * prop.multiProcessorCount;
@@ -188,6 +190,18 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), s);
     cudaEventRecord(ctx->ev0, s);
     const bool lam = (prm->flags & S2_FLAG_LAMBERTIAN) != 0, restir = (prm->flags & S2_FLAG_RESTIR_DI) != 0;
+    const bool count = (prm->flags & S2_FLAG_COUNT_FETCHES) != 0, prof = (prm->flags & S2_FLAG_PROFILE_KERNELS) != 0;
+    uint64_t launches = 0;
+    // profiling: an event pair around every extend / shade / occlude launch (kind 0 / 1 / 2)
+    std::vector<int> prof_kind;
+    auto ev_begin = [&](int kind) {
+        if (!prof) return;
+        const size_t k = 2 * prof_kind.size();
+        while (st->events.size() < k + 2) { cudaEvent_t e; cudaEventCreate(&e); st->events.push_back(e); }
+        cudaEventRecord(st->events[k], s);
+        prof_kind.push_back(kind);
+    };
+    auto ev_end = [&]() { if (prof) cudaEventRecord(st->events[2 * prof_kind.size() - 1], s); };
     for (uint32_t done = 0; done < prm->spp; done += slots) {
         P.wave_base_sample = done;
         P.wave_samples = std::min(slots, prm->spp - done);
@@ -196,14 +210,25 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         for (uint32_t b = 0; b < prm->max_path_length; ++b) {
             const uint32_t parity = b & 1u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
-            k_extend<<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            ev_begin(0);
+            if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            ev_end();
+            ev_begin(1);
             if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
             else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
-            k_occlude<<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            ev_end();
+            ev_begin(2);
+            if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            ev_end();
+            launches += 4;
         }
         k_wave_finish<<<1, 32, 0, s>>>(P);
         k_reduce<<<(pixels + 255) / 256, 256, 0, s>>>(P, st->total);
+        launches += 3;
     }
+    launches += 1;  // resolve
     st->accumulated_spp += prm->spp;
     float4* rad = (out && out->radiance) ? (host ? st->out_radiance : (float4*)out->radiance) : st->out_radiance;
     k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(st->total, pixels, (float)(1.0 / (double)st->accumulated_spp),
@@ -220,7 +245,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         if (out->ids32) cudaMemcpyAsync(out->ids32, st->aov_ids, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, s);
     }
     if (stats_out || host) {
-        unsigned long long sv[S_COUNT] = {0, 0, 0, 0};
+        unsigned long long sv[S_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
         int status = 0;
         cudaMemcpyAsync(sv, st->stats, sizeof(sv), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&status, ctx->status_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -235,6 +260,21 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             stats_out->paths = (uint64_t)pixels * prm->spp;
             stats_out->nan_count = sv[S_NAN];
             stats_out->gpu_ms = ms;
+            stats_out->kernel_launches = launches;
+            stats_out->extend_node_fetches = sv[S_EXT_NODES];
+            stats_out->extend_tri_fetches = sv[S_EXT_TRIS];
+            stats_out->shadow_node_fetches = sv[S_SH_NODES];
+            stats_out->shadow_tri_fetches = sv[S_SH_TRIS];
+            double kms[3] = {0, 0, 0};
+            uint32_t kn[3] = {0, 0, 0};
+            for (size_t k = 0; k < prof_kind.size(); ++k) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, st->events[2 * k], st->events[2 * k + 1]);
+                kms[prof_kind[k]] += t;
+                kn[prof_kind[k]]++;
+            }
+            stats_out->extend_ms = kms[0]; stats_out->shade_ms = kms[1]; stats_out->occlude_ms = kms[2];
+            stats_out->extend_launches = kn[0]; stats_out->shade_launches = kn[1]; stats_out->occlude_launches = kn[2];
         }
     }
     return S2_OK;

@@ -26,7 +26,7 @@ enum Counter : uint32_t {
     C_WORK_OCC = 4,
     C_COUNT = 8
 };
-enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_COUNT = 4 };
+enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_EXT_NODES = 3, S_EXT_TRIS = 4, S_SH_NODES = 5, S_SH_TRIS = 6, S_COUNT = 8 };
 
 struct PathQueue { float4* s0; float4* s1; float4* s2; uint4* s3; };
 
@@ -133,11 +133,20 @@ __global__ void k_wave_finish(PTParams P) {
 // ---------------------------------------------------------------- extend: closest hit
 // Persistent kernel: each warp takes 32 rays at a time from a global work counter (dynamic load
 // balancing of incoherent traversal).  Hit record: {t, triangle record index, b1, b2}.
+// Warp-sum of the fetch counters, one 64-bit atomic per warp (counting runs only).
+S2D void add_fetches(unsigned long long* stats, uint32_t node_stat, const TravCounters& c) {
+    uint32_t n = c.nodes, t = c.tris;
+    for (int o = 16; o > 0; o >>= 1) { n += __shfl_xor_sync(0xffffffffu, n, o); t += __shfl_xor_sync(0xffffffffu, t, o); }
+    if ((threadIdx.x & 31u) == 0) { atomicAdd(&stats[node_stat], (unsigned long long)n); atomicAdd(&stats[node_stat + 1], (unsigned long long)t); }
+}
+
+template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t parity) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     const uint32_t count = P.counters[parity];
     const PathQueue q = P.q[parity];
     const uint32_t lane = threadIdx.x & 31u;
+    TravCounters c{0, 0};
     while (true) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&P.counters[C_WORK_EXT], 32u);
@@ -148,21 +157,23 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t pari
             const float4 a = q.s0[i], b = q.s1[i];
             const TravRay r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
             TravHit h;
-            TravCounters c;
-            if (!traverse<false, false>(r, S2_INF, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
+            if (!traverse<false, COUNT>(r, S2_INF, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
                 atomicOr(P.status, 1);
             P.hits[i] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
         }
     }
+    if (COUNT) add_fetches(P.stats, S_EXT_NODES, c);
 }
 
 // ---------------------------------------------------------------- occlude: first hit
 // ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
 // ray belongs to one accumulator slot and adds its contribution when unoccluded.
+template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     const uint32_t count = P.counters[C_SHADOW];
     const uint32_t lane = threadIdx.x & 31u;
+    TravCounters c{0, 0};
     while (true) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&P.counters[C_WORK_OCC], 32u);
@@ -173,8 +184,7 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
             const float4 o = P.sh_o[i], d = P.sh_d[i];
             const TravRay r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
             TravHit h;
-            TravCounters c;
-            if (!traverse<true, false>(r, o.w, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
+            if (!traverse<true, COUNT>(r, o.w, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
                 atomicOr(P.status, 1);
             if (h.tri == 0xffffffffu) {
                 const float4 cc = P.sh_c[i];
@@ -185,6 +195,7 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
             }
         }
     }
+    if (COUNT) add_fetches(P.stats, S_SH_NODES, c);
 }
 
 // ---------------------------------------------------------------- accumulation

@@ -151,7 +151,8 @@ def sky_image(width: int = 512, height: int = 256, sun_dir=(0.3, 0.8, 0.2), sun_
 
 
 def terrain_scene(seed: int = 2, grid: int = 1024, spheres: int = 64, sphere_level: int = 5, width: int = 1920,
-                  height: int = 1080, spp: int = 64, tiles: int = 16, area_lights: int = 0) -> Workload:
+                  height: int = 1080, spp: int = 64, tiles: int = 16, area_lights: int = 0,
+                  sun_radiance: float = 5e3, sun_cone_degrees: float = 0.5) -> Workload:
     rng = np.random.default_rng(seed)
     s = Scene()
     hgt = value_noise(rng, grid)
@@ -190,7 +191,7 @@ def terrain_scene(seed: int = 2, grid: int = 1024, spheres: int = 64, sphere_lev
         p, i = quad(c + (-h, 0, -h), c + (h, 0, -h), c + (h, 0, h), c + (-h, 0, h))
         lm = s.add_material(Material(base_color=(0, 0, 0), emission=tuple(rng.uniform(5, 20, 3))))
         s.add_instance(s.add_mesh(p, i), lm)
-    s.set_environment((1.0, 1.0, 1.0), s.add_image(sky_image()))
+    s.set_environment((1.0, 1.0, 1.0), s.add_image(sky_image(sun_radiance=sun_radiance, sun_cone_degrees=sun_cone_degrees)))
     pos = (0.0, 0.9, 1.9)
     view = make_view(pos, width, height, 45.0, look_at_rotation(pos, (0.0, 0.0, 0.0)))
     return Workload(s, view, width, height, spp, 3, 12, False, f"terrain{grid}_{width}x{height}")

@@ -37,7 +37,8 @@ def box_case():
 
 
 def terrain_case():
-    wl = terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+    wl = terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2,
+                         sun_radiance=50.0, sun_cone_degrees=5.0)
     p = _abi.S2RenderParams()
     p.min_path_length, p.max_path_length = 1, 6
     p.flags = _abi.FLAG_PIXEL_JITTER

@@ -17,8 +17,10 @@ Convergence tests: the mean of 16 independent GPU batches against a committed FP
 rendered with disjoint seeds (tests/golden/make_golden.py).  Per pixel channel
 z = (gpu - oracle) / sqrt(var_gpu + var_oracle) with var_gpu from the 16 batches (t, 15 dof):
 |z| > 5 for at most 0.1% of channels, |mean z| < 0.1 (no global bias), and relMSE below 1e-3
-(box) or twice the noise floor the two estimators' variances predict (terrain: its 5e3 sun seen
-through glossy spheres gives a relative per-sample variance of ~24).
+(box) or twice the noise floor the two estimators' variances predict (terrain: sun and glossy spheres
+give a high relative per-sample variance).  The parity terrain uses a sun of radiance 50 over a
+5 degree cone: the benchmark's 5e3 sun over 0.5 degrees makes per-pixel estimates heavy-tailed
+(rare sun reflections), which no z-test at these sample counts can judge.
 """
 from pathlib import Path
 
@@ -47,16 +49,16 @@ def box_wl():
 
 
 def terrain_wl():
-    return terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+    return terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2,
+                         sun_radiance=50.0, sun_cone_degrees=5.0)
 
 
 def assert_same_seed(g, o, tag="", jitter=True):
     gm = g.radiance[..., :3].astype(np.float64)
     om = o["mean"]
-    se2 = o["var_of_mean"]
-    live = se2 > 0
-    z2 = np.where(live, (gm - om) ** 2 / np.where(live, se2, 1), 0.0)
-    close = np.abs(gm - om) <= 1e-3 * np.abs(om) + 1e-4
+    tol = 1e-3 * np.abs(om) + 1e-4
+    z2 = (gm - om) ** 2 / (o["var_of_mean"] + tol ** 2)  # noise, floored at the agreement tolerance
+    close = np.abs(gm - om) <= tol
     assert z2.mean() < (0.05 if jitter else 0.2), f"{tag} mean z^2 {z2.mean()}"
     assert close.mean() > 0.97, f"{tag} only {close.mean():.4f} of pixel channels agree"
 
@@ -184,7 +186,7 @@ def test_restir_di_same_seed_and_unbiased(device, box, terrain, scene_name):
     base = _abi.FLAG_LAMBERTIAN if scene_name == "box" else 0
     minl, maxl = (2, 5) if scene_name == "box" else (1, 6)
     device.upload_scene(wl.scene)
-    p = make_params(4, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, seed=9, restir_m=8)
+    p = make_params(16, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, seed=9, restir_m=8)
     g = device.render(wl.view, wl.width, wl.height, params=p)
     o = osc.render(wl.view, p, wl.width, wl.height)
     assert_same_seed(g, o, f"restir {scene_name}")
