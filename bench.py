@@ -88,7 +88,7 @@ class ClockSampler:
         if not sm:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if "Active" in r[5 + k]})
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "samples": len(sm), "reasons": reasons}
 
 
@@ -180,8 +180,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     rad = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
     aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
 
+    from stratum2_b200.multi import combine_images, frame_seed, job_time_and_totals
+
     def seed(step: int) -> int:
-        return (step * world + rank) * SPP  # disjoint frame seeds per rank and step
+        return frame_seed(step, rank, world, SPP)  # disjoint frame seeds per rank and step
 
     # fetch counts for the algorithmic-byte model (untimed run, same seeds as timed step 0)
     cnt = dev.render_device(wl.view, params(dev, SPP, seed(0), _abi.FLAG_COUNT_FETCHES), aovs)
@@ -198,8 +200,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e0.record(stream)
     for step in range(args.steps):
         stats.append(dev.render_device(wl.view, params(dev, SPP, seed(step), _abi.FLAG_PROFILE_KERNELS), aovs))
-        if world > 1:
-            dist.reduce(rad, dst=0)  # combine the ranks' sample partitions of the frame
+        combine_images(rad, world, dist)  # sum the ranks' sample partitions of the frame into rank 0
     e1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -208,13 +209,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ms = e0.elapsed_time(e1)
     rays = float(sum(s.extension_rays + s.shadow_rays for s in stats))
     paths = float(sum(s.paths for s in stats))
-    t = torch.tensor([ms, rays, paths], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tmax = t[:1].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t[1:].clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        ms, rays, paths = float(tmax[0]), float(tsum[0]), float(tsum[1])
+    ms, (rays, paths) = job_time_and_totals(ms, [rays, paths], world, dist, device="cuda")
     value = rays / ms / 1e3
 
     # end to end through the public API with host buffers (view/params in, all AOVs out)
@@ -227,11 +222,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         r = dev.render(wl.view, W, H, params=params(dev, SPP, seed(step + 3000)))
         e2e_rays += r.stats.extension_rays + r.stats.shadow_rays
     e2e_s = time.perf_counter() - t0
-    e2e = torch.tensor([e2e_s, float(e2e_rays)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        es = e2e[:1].clone(); dist.all_reduce(es, op=dist.ReduceOp.MAX)
-        er = e2e[1:].clone(); dist.all_reduce(er, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_rays = float(es[0]), float(er[0])
+    e2e_s, (e2e_rays,) = job_time_and_totals(e2e_s, [float(e2e_rays)], world, dist, device="cuda")
     if rank != 0:
         return
 
@@ -297,7 +288,19 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",
+                    help="render one frame of the workload with SPP samples and exit (profiling)")
     args = ap.parse_args()
+    if args.single_frame:
+        from stratum2_b200 import Device
+        from stratum2_b200.scenegen import terrain_scene
+        dev = Device(0)
+        wl = terrain_scene()
+        dev.upload_scene(wl.scene)
+        r = dev.render(wl.view, wl.width, wl.height, params=params(dev, args.single_frame, 0))
+        print(json.dumps({"gpu_ms": r.stats.gpu_ms, "extension_rays": r.stats.extension_rays,
+                          "shadow_rays": r.stats.shadow_rays}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

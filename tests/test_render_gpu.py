@@ -1,17 +1,16 @@
 """Parity of the wavefront path tracer (CUDA) with the FP64 oracle.
 
 Same-seed tests: the GPU and the oracle draw the same random numbers per (pixel, sample) (the
-reference's counter-based pcg4d stream, or PCG32), so the images agree sample by sample up to
+reference's counter-based pcg4d stream, or PCG32), so they trace the same paths up to
 floating-point divergence of individual paths.  The floor of that divergence is set by the
 reference's own path-state packing: ray directions are stored octahedral SNORM16
 (testrenderer.slang:119-122), so a 1e-7 rounding difference flips ~2% of direction components by
 one 3e-5 rad step, which occasionally moves a hit across a small triangle's edge; and at pixel
 centres the symmetric box puts diagonal pixels' camera rays exactly on its corner seams, where
-float and double tie-break differently.  The oracle's own FP32 build differs from its FP64 build
-by the same amount.  The criterion is therefore normalised by the estimator noise: with
-z = (gpu - oracle) / (oracle standard error), mean(z^2) is 0 for identical samples and ~2 for
-independent ones; it must stay below 0.05 (pixel jitter) / 0.2 (pixel centres), and 97% of pixel
-channels must agree within 1e-3 relative (+1e-4 absolute).
+float and double tie-break differently.  The oracle's own FP32 build diverges from its FP64 build
+at the same rate (~0.06% of samples with pixel jitter, ~0.15% at pixel centres).  The tests render
+one sample per call for 16 seeds on both sides and require that at most 1% of (pixel, sample)
+values differ by more than 1e-3 relative (+1e-4 absolute) in any channel.
 
 Convergence tests: the mean of 16 independent GPU batches against a committed FP64 oracle image
 rendered with disjoint seeds (tests/golden/make_golden.py).  Per pixel channel
@@ -53,14 +52,23 @@ def terrain_wl():
                          sun_radiance=50.0, sun_cone_degrees=5.0)
 
 
-def assert_same_seed(g, o, tag="", jitter=True):
-    gm = g.radiance[..., :3].astype(np.float64)
-    om = o["mean"]
-    tol = 1e-3 * np.abs(om) + 1e-4
-    z2 = (gm - om) ** 2 / (o["var_of_mean"] + tol ** 2)  # noise, floored at the agreement tolerance
-    close = np.abs(gm - om) <= tol
-    assert z2.mean() < (0.05 if jitter else 0.2), f"{tag} mean z^2 {z2.mean()}"
-    assert close.mean() > 0.97, f"{tag} only {close.mean():.4f} of pixel channels agree"
+def per_sample_divergence(device, osc, wl, p, n=16):
+    """Fraction of (pixel, sample) radiance values where GPU and oracle differ by more than
+    1e-3 relative + 1e-4 absolute in any channel, over n single-sample renders."""
+    seed0 = p.frame_seed
+    bad = 0
+    for k in range(n):
+        p.spp, p.frame_seed = 1, seed0 + k
+        g = device.render(wl.view, wl.width, wl.height, params=p).radiance[..., :3].astype(np.float64)
+        o = osc.render(wl.view, p, wl.width, wl.height)["mean"]
+        bad += int((np.abs(g - o) > 1e-3 * np.abs(o) + 1e-4).any(-1).sum())
+    p.frame_seed = seed0
+    return bad / (n * wl.width * wl.height)
+
+
+def assert_same_seed(device, osc, wl, p, tag=""):
+    d = per_sample_divergence(device, osc, wl, p)
+    assert d <= 0.01, f"{tag}: {d:.4%} of samples diverge"
 
 
 def batches(device, wl, p, n, spp, seed0):
@@ -74,7 +82,8 @@ def batches(device, wl, p, n, spp, seed0):
 
 
 def assert_converged(mean_a, var_a, mean_b, var_b, relmse_max, tag=""):
-    z = (mean_a - mean_b) / np.sqrt(np.maximum(var_a + var_b, 1e-30))
+    # variance floored at float resolution (directly visible sky has zero variance in both)
+    z = (mean_a - mean_b) / np.sqrt(var_a + var_b + (1e-5 * np.abs(mean_b) + 1e-9) ** 2)
     frac = np.mean(np.abs(z) > 5)
     assert frac <= 1e-3, f"{tag}: {frac:.4%} of pixel channels with |z| > 5"
     assert abs(z.mean()) < 0.1, f"{tag}: mean z {z.mean():.3f} (bias)"
@@ -97,10 +106,10 @@ J = _abi.FLAG_PIXEL_JITTER
 def test_box_same_seed_matches_fp64_oracle(device, box, min_len, max_len, extra):
     wl, osc = box
     device.upload_scene(wl.scene)
-    p = make_params(16, min_len, max_len, _abi.FLAG_LAMBERTIAN | extra, seed=7)
+    p = make_params(1, min_len, max_len, _abi.FLAG_LAMBERTIAN | extra, seed=7)
+    assert_same_seed(device, osc, wl, p, f"min{min_len} max{max_len} flags{extra}")
+    p.spp = 16
     g = device.render(wl.view, wl.width, wl.height, params=p)
-    o = osc.render(wl.view, p, wl.width, wl.height)
-    assert_same_seed(g, o, f"min{min_len} max{max_len} flags{extra}", jitter=bool(extra & J))
     assert g.stats.extension_rays > 0 and g.stats.nan_count == 0
 
 
@@ -164,10 +173,8 @@ def terrain(device):
 def test_terrain_disney_env_same_seed(device, terrain, extra):
     wl, osc = terrain
     device.upload_scene(wl.scene)
-    p = make_params(16, 1, 6, extra | J, seed=5)
-    g = device.render(wl.view, wl.width, wl.height, params=p)
-    o = osc.render(wl.view, p, wl.width, wl.height)
-    assert_same_seed(g, o, f"terrain flags{extra}")
+    p = make_params(1, 1, 6, extra | J, seed=5)
+    assert_same_seed(device, osc, wl, p, f"terrain flags{extra}")
 
 
 def test_terrain_converges_to_fp64_golden(device, terrain):
@@ -186,10 +193,8 @@ def test_restir_di_same_seed_and_unbiased(device, box, terrain, scene_name):
     base = _abi.FLAG_LAMBERTIAN if scene_name == "box" else 0
     minl, maxl = (2, 5) if scene_name == "box" else (1, 6)
     device.upload_scene(wl.scene)
-    p = make_params(16, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, seed=9, restir_m=8)
-    g = device.render(wl.view, wl.width, wl.height, params=p)
-    o = osc.render(wl.view, p, wl.width, wl.height)
-    assert_same_seed(g, o, f"restir {scene_name}")
+    p = make_params(1, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, seed=9, restir_m=8)
+    assert_same_seed(device, osc, wl, p, f"restir {scene_name}")
     # RIS with M candidates converges to the same image as plain NEE
     mr, vr = batches(device, wl, make_params(1, minl, maxl, base | _abi.FLAG_RESTIR_DI | J, restir_m=8), 16, 512, 100)
     mn, vn = batches(device, wl, make_params(1, minl, maxl, base | J), 16, 512, 20000)
