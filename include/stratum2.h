@@ -234,6 +234,23 @@ int  s2_render(S2Context* ctx, const S2View* view, const S2RenderParams* params,
 /* Defaults as in the reference (TestRenderer.cpp:38-43, VCM.cpp:39-40). */
 void s2_default_render_params(S2RenderParams* p);
 
+/* ---- allocation-free rendering ----------------------------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device memory while they
+ * render (a host application that owns the GPU's memory budget and forbids cudaMalloc/cudaFree,
+ * which also synchronise the device, once its frame loop runs; a plugin limited to the buffers
+ * its host hands it).  Same kernels and results as s2_render, but the path queues, hit records,
+ * shadow rays, accumulators and counters live in one 64 MiB file-scope device array of the
+ * library, held on every GPU that loads it until the process exits, and radiance accumulates in
+ * the caller's output.  Allocates nothing.
+ *   - `out` holds DEVICE pointers; out->radiance is required; other AOVs may be NULL.
+ *   - Views above 322,618 pixels (64 MiB / 208 bytes per path, e.g. 512x512 fits, 1920x1080 does
+ *     not) are rejected with S2_ERR_INVALID.  S2_FLAG_ACCUMULATE and S2_FLAG_PROFILE_KERNELS are
+ *     rejected.
+ *   - The first call on a device looks up the array's address; make it before any stream capture.
+ *   - Calls share the array: calls whose GPU work overlaps race; serialise them. */
+int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams* params,
+                       const S2Aovs* out, S2RenderStats* stats_out);
+
 #ifdef __cplusplus
 }
 #endif
