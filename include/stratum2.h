@@ -171,7 +171,7 @@ typedef struct S2RenderParams {
     uint32_t restir_spatial_count;   /* screen-space spatial neighbours (0 = off) */
     float restir_spatial_radius;     /* pixels */
     uint32_t restir_temporal;        /* 1 = reuse the previous call's reservoirs */
-    uint32_t wave_paths;             /* paths in flight per wave (0 = automatic) */
+    uint32_t wave_paths;             /* paths in flight per wave / queue (0 = 2^25) */
     uint32_t reserved[7];
 } S2RenderParams;
 
@@ -230,6 +230,18 @@ int  s2_trace_counted(S2Context* ctx, const S2Ray* rays, uint32_t count, int any
 /* ---- rendering (replaces TestRenderer::render) ------------------------------------------- */
 int  s2_render(S2Context* ctx, const S2View* view, const S2RenderParams* params,
                const S2Aovs* out, int out_on_host, S2RenderStats* stats_out);
+
+/* Batched rendering: `view_count` views (up to 255, any resolutions) in one call, each with
+ * params->spp samples.  Paths of all views stream through one queue of params->wave_paths
+ * entries (0 = 32M): before every bounce the queue is topped up with new camera paths, so
+ * launches stay full however unevenly paths end (Russian roulette, escapes); each pair of bounces
+ * is a captured CUDA graph replayed until the device reports all paths done.  Radiance
+ * accumulates in 2^-24 fixed point (order-independent integer sums: deterministic).  `outs` has
+ * one S2Aovs per view (host or device pointers per `out_on_host`).  S2_FLAG_ACCUMULATE adds to the
+ * previous call with the same view extents.  Results equal s2_render's per view up to the
+ * fixed-point rounding. */
+int  s2_render_views(S2Context* ctx, const S2View* views, uint32_t view_count, const S2RenderParams* params,
+                     const S2Aovs* outs, int out_on_host, S2RenderStats* stats_out);
 
 /* Defaults as in the reference (TestRenderer.cpp:38-43, VCM.cpp:39-40). */
 void s2_default_render_params(S2RenderParams* p);

@@ -41,7 +41,7 @@ FLAG_COUNT_FETCHES = 1 << 10
 EXPORTED_SYMBOLS = [
     "s2_get_abi_version", "s2_create", "s2_destroy", "s2_last_error", "s2_sync", "s2_set_stream",
     "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
-    "s2_default_render_params", "s2_render_noalloc",
+    "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
 ]
 
 
@@ -153,6 +153,8 @@ def lib() -> C.CDLL:
     L.s2_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_int]
     L.s2_trace_counted.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
     L.s2_render.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), C.c_int, P(S2RenderStats)]
+    L.s2_render_views.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, P(S2RenderParams), C.c_void_p, C.c_int,
+                                  P(S2RenderStats)]
     L.s2_render_noalloc.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), P(S2RenderStats)]
     L.s2_default_render_params.argtypes = [P(S2RenderParams)]
     L.s2_default_render_params.restype = None

@@ -137,6 +137,30 @@ class Device:
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(p), C.byref(aov), 1, C.byref(st)))
         return RenderResult(rad, alb, vis, dep, puv, ids, st)
 
+    def render_views(self, views, params: _abi.S2RenderParams, aovs: bool = True):
+        """Batched render of several views (any resolutions) in one call (s2_render_views).
+        Returns one RenderResult per view (host arrays) and the call's statistics."""
+        n = len(views)
+        arr = (_abi.S2View * n)(*views)
+        outs = (_abi.S2Aovs * n)()
+        results = []
+        for k, v in enumerate(views):
+            w = v.image_max[0] - v.image_min[0]
+            h = v.image_max[1] - v.image_min[1]
+            rad = np.zeros((h, w, 4), np.float32)
+            alb = np.zeros((h, w, 4), np.float32) if aovs else None
+            vis = np.zeros((h, w, 2), np.uint32) if aovs else None
+            dep = np.zeros((h, w, 4), np.float32) if aovs else None
+            puv = np.zeros((h, w, 2), np.float32) if aovs else None
+            ids = np.zeros((h, w, 2), np.uint32) if aovs else None
+            ptr = lambda a: a.ctypes.data if a is not None else None
+            outs[k] = _abi.S2Aovs(ptr(rad), ptr(alb), ptr(vis), ptr(dep), ptr(puv), ptr(ids))
+            results.append((rad, alb, vis, dep, puv, ids))
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_views(self._h, C.cast(arr, C.c_void_p), n, C.byref(params),
+                                              C.cast(outs, C.c_void_p), 1, C.byref(st)))
+        return [RenderResult(*r, st) for r in results], st
+
     def render_device(self, view, params: _abi.S2RenderParams, aovs: _abi.S2Aovs) -> _abi.S2RenderStats:
         st = _abi.S2RenderStats()
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(params), C.byref(aovs), 0, C.byref(st)))

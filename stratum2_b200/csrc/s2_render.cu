@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "s2_context.h"
 #include "s2_shade_kernel.cuh"
@@ -33,7 +34,10 @@ struct RenderState {
     std::vector<cudaEvent_t> events;  // reusable start/stop pairs for S2_FLAG_PROFILE_KERNELS
 };
 
+void destroy_batch_state(S2Context* ctx);
+
 void destroy_render_state(S2Context* ctx) {
+    destroy_batch_state(ctx);
     if (!ctx->render) return;
     for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
     free_bufs(ctx->render->bufs);
@@ -144,7 +148,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     cudaSetDevice(ctx->device);
     const uint32_t pixels = (uint32_t)W * (uint32_t)H;
-    uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 22);
+    uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 25);
     uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, target / pixels));
     const uint32_t capacity = slots * pixels;
     int rc = ensure_state(ctx, (uint32_t)W, (uint32_t)H, capacity);
@@ -276,6 +280,292 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             stats_out->extend_ms = kms[0]; stats_out->shade_ms = kms[1]; stats_out->occlude_ms = kms[2];
             stats_out->extend_launches = kn[0]; stats_out->shade_launches = kn[1]; stats_out->occlude_launches = kn[2];
         }
+    }
+    return S2_OK;
+}
+
+// ============================================================================== batched rendering
+namespace s2 {
+namespace {
+
+struct BatchState {
+    uint32_t capacity = 0;
+    std::vector<DevBuf> qbufs;     // path queues, hits, shadow queue
+    PathQueue q[2]{};
+    float4* hits = nullptr;
+    float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
+    std::vector<DevBuf> pbufs;     // per-pixel accumulators, view table, staging
+    uint64_t pixels = 0;
+    std::vector<uint32_t> layout;  // view extents of the current accumulators
+    unsigned long long* total_fx = nullptr;
+    ViewEntry* views_dev = nullptr;
+    uint32_t views_cap = 0;
+    unsigned long long* stream_state = nullptr;
+    uint32_t* counters = nullptr;
+    unsigned long long* stats = nullptr;
+    unsigned long long* done_host = nullptr;  // pinned
+    float4* stage_rad = nullptr;
+    uint64_t accumulated_spp = 0;
+};
+
+BatchState* g_batch_for(S2Context* ctx);
+
+}  // namespace
+}  // namespace s2
+
+// One BatchState per context, kept beside the wave-mode RenderState.
+namespace s2 {
+namespace {
+struct BatchRegistry {
+    std::vector<std::pair<S2Context*, BatchState*>> items;
+};
+BatchRegistry g_registry;
+std::mutex g_registry_mutex;
+BatchState* g_batch_for(S2Context* ctx) {
+    std::lock_guard<std::mutex> lock(g_registry_mutex);
+    for (auto& it : g_registry.items) if (it.first == ctx) return it.second;
+    BatchState* b = new (std::nothrow) BatchState();
+    if (b) g_registry.items.push_back({ctx, b});
+    return b;
+}
+}  // namespace
+
+void destroy_batch_state(S2Context* ctx) {
+    std::lock_guard<std::mutex> lock(g_registry_mutex);
+    for (size_t i = 0; i < g_registry.items.size(); ++i) {
+        if (g_registry.items[i].first != ctx) continue;
+        BatchState* b = g_registry.items[i].second;
+        free_bufs(b->qbufs);
+        free_bufs(b->pbufs);
+        if (b->done_host) cudaFreeHost(b->done_host);
+        delete b;
+        g_registry.items.erase(g_registry.items.begin() + i);
+        return;
+    }
+}
+}  // namespace s2
+
+extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nviews, const S2RenderParams* prm,
+                               const S2Aovs* outs, int out_on_host, S2RenderStats* stats_out) {
+    using namespace s2;
+    if (!ctx) return S2_ERR_INVALID;
+    if (!views || !prm || nviews == 0) return set_error(ctx, S2_ERR_INVALID, "views, view count and params are required");
+    if (nviews > 255) return set_error(ctx, S2_ERR_INVALID, "at most 255 views per call");
+    if (!ctx->has_bvh) return set_error(ctx, S2_ERR_NO_SCENE, "s2_render_views before s2_scene_upload + s2_build_bvh");
+    if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
+    if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
+    if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
+        return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
+    cudaSetDevice(ctx->device);
+    std::vector<ViewEntry> ve(nviews);
+    std::vector<uint32_t> layout;
+    uint64_t pixels = 0, paths = 0;
+    for (uint32_t v = 0; v < nviews; ++v) {
+        const S2View& V = views[v];
+        const int W = V.image_max[0] - V.image_min[0], H = V.image_max[1] - V.image_min[1];
+        if (W <= 0 || H <= 0 || (int64_t)W * H > (1ll << 28)) return set_error(ctx, S2_ERR_INVALID, "invalid extent of view " + std::to_string(v));
+        ViewEntry& e = ve[v];
+        std::memset(&e, 0, sizeof(e));
+        std::memcpy(e.proj, V.projection, sizeof(e.proj));
+        e.imin[0] = V.image_min[0]; e.imin[1] = V.image_min[1]; e.imax[0] = V.image_max[0]; e.imax[1] = V.image_max[1];
+        std::memcpy(e.cam, V.camera_to_world, sizeof(e.cam));
+        std::memcpy(e.prev_inv, V.prev_world_to_camera, sizeof(e.prev_inv));
+        e.width = (uint32_t)W; e.height = (uint32_t)H; e.pixels = (uint32_t)(W * H);
+        e.pixel_offset = (uint32_t)pixels;
+        e.path_offset = paths;
+        pixels += e.pixels;
+        paths += (uint64_t)e.pixels * prm->spp;
+        layout.push_back((uint32_t)W); layout.push_back((uint32_t)H);
+    }
+    if (pixels > (1ull << 30)) return set_error(ctx, S2_ERR_INVALID, "too many pixels in one call");
+    BatchState* B = g_batch_for(ctx);
+    if (!B) return set_error(ctx, S2_ERR_OOM, "batch state allocation failed");
+    cudaStream_t s = ctx->stream;
+    const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(prm->wave_paths ? prm->wave_paths : (1u << 25), paths));
+    if (B->capacity < capacity) {
+        free_bufs(B->qbufs);
+        B->capacity = 0;
+        for (int k = 0; k < 2; ++k) {
+            B->q[k].s0 = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+            B->q[k].s1 = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+            B->q[k].s2 = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+            B->q[k].s3 = (uint4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+        }
+        B->hits = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+        B->sh_o = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+        B->sh_d = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+        B->sh_c = (float4*)dev_alloc(ctx, B->qbufs, 16ull * capacity);
+        if (B->qbufs.size() != 12) { free_bufs(B->qbufs); return S2_ERR_OOM; }
+        B->capacity = capacity;
+    }
+    const bool relayout = B->layout != layout || B->views_cap < nviews;
+    if (relayout) {
+        free_bufs(B->pbufs);
+        B->total_fx = (unsigned long long*)dev_alloc(ctx, B->pbufs, 32ull * pixels);
+        B->views_dev = (ViewEntry*)dev_alloc(ctx, B->pbufs, sizeof(ViewEntry) * 256);
+        B->stream_state = (unsigned long long*)dev_alloc(ctx, B->pbufs, 64);
+        B->counters = (uint32_t*)dev_alloc(ctx, B->pbufs, sizeof(uint32_t) * C_COUNT);
+        B->stats = (unsigned long long*)dev_alloc(ctx, B->pbufs, sizeof(unsigned long long) * S_COUNT);
+        B->stage_rad = (float4*)dev_alloc(ctx, B->pbufs, 16ull * pixels);
+        if (B->pbufs.size() != 6) { free_bufs(B->pbufs); B->layout.clear(); return S2_ERR_OOM; }
+        if (!B->done_host && cudaMallocHost(&B->done_host, 64) != cudaSuccess) { cudaGetLastError(); return set_error(ctx, S2_ERR_OOM, "pinned allocation failed"); }
+        B->layout = layout;
+        B->views_cap = 256;
+        B->pixels = pixels;
+        B->accumulated_spp = 0;
+        cudaMemsetAsync(B->total_fx, 0, 32ull * pixels, s);
+    }
+    // AOV outputs: device pointers directly, or staged per view for host outputs
+    std::vector<DevBuf> stage;
+    for (uint32_t v = 0; v < nviews; ++v) {
+        if (!outs) break;
+        const S2Aovs& o = outs[v];
+        ViewEntry& e = ve[v];
+        auto pick = [&](void* user, size_t elem) -> void* {
+            if (!user) return nullptr;
+            if (!out_on_host) return user;
+            return dev_alloc(ctx, stage, elem * e.pixels);
+        };
+        e.aov_albedo = (float4*)pick(o.albedo, 16);
+        e.aov_vis = (uint2*)pick(o.visibility, 8);
+        e.aov_depth = (float4*)pick(o.depth, 16);
+        e.aov_prev_uv = (float2*)pick(o.prev_uv, 8);
+        e.aov_ids = (uint2*)pick(o.ids32, 8);
+    }
+    cudaMemcpyAsync(B->views_dev, ve.data(), sizeof(ViewEntry) * nviews, cudaMemcpyHostToDevice, s);
+    if (!(prm->flags & S2_FLAG_ACCUMULATE)) {
+        cudaMemsetAsync(B->total_fx, 0, 32ull * pixels, s);
+        B->accumulated_spp = 0;
+    }
+    cudaMemsetAsync(B->stream_state, 0, 64, s);
+    cudaMemsetAsync(B->counters, 0, sizeof(uint32_t) * C_COUNT, s);
+    cudaMemsetAsync(B->stats, 0, sizeof(unsigned long long) * S_COUNT, s);
+    cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), s);
+
+    PTParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.scene = ctx->scene;
+    P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
+    P.min_len = prm->min_path_length;
+    P.max_len = prm->max_path_length;
+    P.flags = prm->flags;
+    P.frame_seed = prm->frame_seed;
+    P.restir_m = prm->restir_candidates ? prm->restir_candidates : 32;
+    P.exposure = prm->exposure;
+    P.q[0] = B->q[0]; P.q[1] = B->q[1];
+    P.hits = B->hits; P.sh_o = B->sh_o; P.sh_d = B->sh_d; P.sh_c = B->sh_c;
+    P.counters = B->counters;
+    P.stats = B->stats;
+    P.status = ctx->status_dev;
+    P.views = B->views_dev;
+    P.nviews = nviews;
+    P.total_fx = B->total_fx;
+    P.total_paths = paths;
+    P.capacity = capacity;
+    P.stream_state = B->stream_state;
+    P.pixels = 1;  // unused in batched mode
+
+    RenderState* st = ctx->render;
+    if (!st) {
+        int rc = ensure_state(ctx, 1, 1, 1);  // occupancy-derived grid sizes
+        if (rc != S2_OK) return rc;
+        st = ctx->render;
+    }
+    const bool lam = (prm->flags & S2_FLAG_LAMBERTIAN) != 0, restir = (prm->flags & S2_FLAG_RESTIR_DI) != 0;
+    const bool count = (prm->flags & S2_FLAG_COUNT_FETCHES) != 0;
+    // one graph = two iterations (parity 0 and 1) of setup, regeneration, extend, shade, occlude
+    auto iteration = [&](uint32_t parity, int first) {
+        k_stream_setup<<<1, 32, 0, s>>>(P, parity, first);
+        k_regen<<<std::min<uint32_t>((capacity + 255) / 256, 148u * 16u), 256, 0, s>>>(P, parity);
+        if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+        else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+        if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
+        else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
+        if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+        else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+    };
+    cudaEventRecord(ctx->ev0, s);
+    iteration(0, 1);  // first iteration outside the graph (it skips the shadow accounting)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rc = check_cuda(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    if (rc != S2_OK) return rc;
+    iteration(1, 0);
+    iteration(0, 0);
+    rc = check_cuda(ctx, cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
+    if (rc == S2_OK) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
+    if (rc != S2_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+    uint64_t launches = 5;
+    // replay until the device reports every path finished; the check trails one group behind so
+    // the host never waits on the group it just queued
+    const uint64_t lower = (paths + capacity - 1) / capacity;
+    const uint64_t cap_iters = paths * (uint64_t)std::max(1u, prm->max_path_length) / std::max<uint64_t>(1, capacity) + prm->max_path_length + 4;
+    const uint32_t group = 4;  // graph launches (8 iterations) per done check
+    uint64_t iters = 1;
+    cudaEvent_t pending = nullptr;
+    cudaEventCreateWithFlags(&pending, cudaEventDisableTiming);
+    bool done = false, have_pending = false;
+    while (!done && iters < cap_iters + 2) {
+        for (uint32_t g = 0; g < group; ++g) { cudaGraphLaunch(exec, s); iters += 2; launches += 10; }
+        if (have_pending) {
+            cudaEventSynchronize(pending);
+            done = *B->done_host != 0;
+        }
+        if (iters >= lower) {
+            cudaMemcpyAsync(B->done_host, B->stream_state + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+            cudaEventRecord(pending, s);
+            have_pending = true;
+        }
+    }
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(pending);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (!*B->done_host) return set_error(ctx, S2_ERR_DEVICE, "batched render did not finish within its iteration bound");
+    B->accumulated_spp += prm->spp;
+    const float scale = (float)(1.0 / (double)B->accumulated_spp) * exp2f(prm->exposure);
+    for (uint32_t v = 0; v < nviews; ++v) {
+        float4* dst = (outs && outs[v].radiance && !out_on_host) ? (float4*)outs[v].radiance : B->stage_rad + ve[v].pixel_offset;
+        k_resolve_fx<<<(ve[v].pixels + 255) / 256, 256, 0, s>>>(B->total_fx, ve[v].pixel_offset, ve[v].pixels, scale, dst);
+        launches++;
+    }
+    cudaEventRecord(ctx->ev1, s);
+    rc = check_cuda(ctx, cudaGetLastError(), "batched render");
+    if (rc != S2_OK) { free_bufs(stage); return rc; }
+    if (out_on_host && outs) {
+        for (uint32_t v = 0; v < nviews; ++v) {
+            const S2Aovs& o = outs[v];
+            const ViewEntry& e = ve[v];
+            if (o.radiance) cudaMemcpyAsync(o.radiance, B->stage_rad + e.pixel_offset, 16ull * e.pixels, cudaMemcpyDeviceToHost, s);
+            if (o.albedo) cudaMemcpyAsync(o.albedo, e.aov_albedo, 16ull * e.pixels, cudaMemcpyDeviceToHost, s);
+            if (o.visibility) cudaMemcpyAsync(o.visibility, e.aov_vis, 8ull * e.pixels, cudaMemcpyDeviceToHost, s);
+            if (o.depth) cudaMemcpyAsync(o.depth, e.aov_depth, 16ull * e.pixels, cudaMemcpyDeviceToHost, s);
+            if (o.prev_uv) cudaMemcpyAsync(o.prev_uv, e.aov_prev_uv, 8ull * e.pixels, cudaMemcpyDeviceToHost, s);
+            if (o.ids32) cudaMemcpyAsync(o.ids32, e.aov_ids, 8ull * e.pixels, cudaMemcpyDeviceToHost, s);
+        }
+    }
+    unsigned long long sv[S_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int status = 0;
+    cudaMemcpyAsync(sv, B->stats, sizeof(sv), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&status, ctx->status_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "batched render");
+    free_bufs(stage);
+    if (rc != S2_OK) return rc;
+    if (status) return set_error(ctx, S2_ERR_DEVICE, "traversal stack overflow during render");
+    if (stats_out) {
+        std::memset(stats_out, 0, sizeof(*stats_out));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats_out->extension_rays = sv[S_EXT];
+        stats_out->shadow_rays = sv[S_SHADOW];
+        stats_out->paths = paths;
+        stats_out->nan_count = sv[S_NAN];
+        stats_out->gpu_ms = ms;
+        stats_out->kernel_launches = launches;
+        stats_out->extend_node_fetches = sv[S_EXT_NODES];
+        stats_out->extend_tri_fetches = sv[S_EXT_TRIS];
+        stats_out->shadow_node_fetches = sv[S_SH_NODES];
+        stats_out->shadow_tri_fetches = sv[S_SH_TRIS];
     }
     return S2_OK;
 }

@@ -20,10 +20,33 @@ S2D uint32_t warp_append(uint32_t* counter, bool want) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-S2D void add_accum(float4* accum, uint32_t slot, float3 v) {
-    float4 a = accum[slot];
-    a.x += v.x; a.y += v.y; a.z += v.z;
-    accum[slot] = a;
+// The view a path belongs to, for its AOV writes: the single view of a wave render, or its entry
+// in the batched view table (view index in meta bits 16..23; slot = pixel_offset + pixel).
+struct AovTarget {
+    const float* proj;
+    const int* imin;
+    const int* imax;
+    const float* prev_inv;
+    uint32_t width, pixel;
+    float4* albedo;
+    uint2* vis;
+    float4* depth;
+    float2* prev_uv;
+    uint2* ids;
+};
+S2D AovTarget aov_target(const PTParams& P, uint32_t slot, uint32_t meta) {
+    AovTarget t;
+    if (P.views) {
+        const ViewEntry& V = P.views[(meta >> 16) & 0xffu];
+        t.proj = V.proj; t.imin = V.imin; t.imax = V.imax; t.prev_inv = V.prev_inv; t.width = V.width;
+        t.pixel = slot - V.pixel_offset;
+        t.albedo = V.aov_albedo; t.vis = V.aov_vis; t.depth = V.aov_depth; t.prev_uv = V.aov_prev_uv; t.ids = V.aov_ids;
+    } else {
+        t.proj = P.proj; t.imin = P.imin; t.imax = P.imax; t.prev_inv = P.prev_inv; t.width = P.width;
+        t.pixel = slot % P.pixels;
+        t.albedo = P.aov_albedo; t.vis = P.aov_vis; t.depth = P.aov_depth; t.prev_uv = P.aov_prev_uv; t.ids = P.aov_ids;
+    }
+    return t;
 }
 
 struct ShadowOut { float3 o, d, c; float tmax; bool valid; };
@@ -136,19 +159,20 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
             Rng rng;
             rng.px = rs.x; rng.py = rs.y; rng.seed = rs.z; rng.ctr = rs.w; rng.pcg32 = (P.flags & S2F_PCG32) != 0;
             const uint32_t tri = __float_as_uint(h.y);
-            const uint32_t pix = slot % P.pixels;
             if (tri == 0xffffffffu) {
                 // ---- miss: environment emission (TraceRay, testrenderer.slang:1036-1054)
                 if (aov) {
-                    if (P.aov_albedo) P.aov_albedo[pix] = make_float4(1.f, 1.f, 1.f, 1.f);
-                    if (P.aov_vis) P.aov_vis[pix] = make_uint2(0xffffffffu, pack_normal(dir));
-                    if (P.aov_depth) P.aov_depth[pix] = make_float4(S2_INF, S2_INF, 1.f, 1.f);
-                    if (P.aov_prev_uv) {
-                        const uint32_t px = pix % P.width, py = pix / P.width;
-                        P.aov_prev_uv[pix] = make_float2(((float)px + 0.5f) / (float)(P.imax[0] - P.imin[0]),
-                                                         ((float)py + 0.5f) / (float)(P.imax[1] - P.imin[1]));
+                    const AovTarget A = aov_target(P, slot, meta);
+                    const uint32_t pix = A.pixel;
+                    if (A.albedo) A.albedo[pix] = make_float4(1.f, 1.f, 1.f, 1.f);
+                    if (A.vis) A.vis[pix] = make_uint2(0xffffffffu, pack_normal(dir));
+                    if (A.depth) A.depth[pix] = make_float4(S2_INF, S2_INF, 1.f, 1.f);
+                    if (A.prev_uv) {
+                        const uint32_t px = pix % A.width, py = pix / A.width;
+                        A.prev_uv[pix] = make_float2(((float)px + 0.5f) / (float)(A.imax[0] - A.imin[0]),
+                                                     ((float)py + 0.5f) / (float)(A.imax[1] - A.imin[1]));
                     }
-                    if (P.aov_ids) P.aov_ids[pix] = make_uint2(0xffffffffu, 0xffffffffu);
+                    if (A.ids) A.ids[pix] = make_uint2(0xffffffffu, 0xffffffffu);
                 }
                 float env_pdf = 0.f;
                 const float3 e = len >= P.min_len ? thr * eval_env(s, dir, env_pdf) : f3(0.f);
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                         const float lp = (P.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;
                         w = mis_w(dir_pdf, lp);
                     }
-                    if (w > 0.f) add_accum(P.accum, slot, e * w);
+                    if (w > 0.f) add_contrib(P, slot, e * w);
                 }
             } else {
                 const float4 tr0 = s.tris[3 * (size_t)tri], tr1 = s.tris[3 * (size_t)tri + 1];
@@ -171,30 +195,32 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                 const float cos_in = fabsf(in.z);
                 if (aov) {
                     // StoreAuxillaryData (testrenderer.slang:195-218)
+                    const AovTarget A = aov_target(P, slot, meta);
+                    const uint32_t pix = A.pixel;
                     const float3 bc = m.base();
-                    if (P.aov_albedo) P.aov_albedo[pix] = make_float4(bc.x, bc.y, bc.z, 1.f);
-                    if (P.aov_vis) P.aov_vis[pix] = make_uint2((inst & 0xffffu) | (prim << 16), sd.ns);
-                    if (P.aov_ids) P.aov_ids[pix] = make_uint2(inst, prim);
+                    if (A.albedo) A.albedo[pix] = make_float4(bc.x, bc.y, bc.z, 1.f);
+                    if (A.vis) A.vis[pix] = make_uint2((inst & 0xffffu) | (prim << 16), sd.ns);
+                    if (A.ids) A.ids[pix] = make_uint2(inst, prim);
                     const float3 pw = xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos);
-                    const float* pv = P.prev_inv;
+                    const float* pv = A.prev_inv;
                     const float3 pc = f3(pv[0] * pw.x + pv[1] * pw.y + pv[2] * pw.z + pv[3],
                                          pv[4] * pw.x + pv[5] * pw.y + pv[6] * pw.z + pv[7],
                                          pv[8] * pw.x + pv[9] * pw.y + pv[10] * pw.z + pv[11]);
-                    const uint32_t px = pix % P.width, py = pix / P.width;
-                    const float W = (float)(P.imax[0] - P.imin[0]), H = (float)(P.imax[1] - P.imin[1]);
+                    const uint32_t px = pix % A.width, py = pix / A.width;
+                    const float W = (float)(A.imax[0] - A.imin[0]), H = (float)(A.imax[1] - A.imin[1]);
                     float ppx = (float)px + 0.5f, ppy = (float)py + 0.5f;
-                    const float nr = P.proj[4];
+                    const float nr = A.proj[4];
                     if ((pc.z > 0.f) == (nr > 0.f) && pc.z != 0.f) {
                         // ViewData::toRaster (compat/scene.h:158-165), perspective projectPoint
-                        const float x4 = pc.x * P.proj[0] + pc.z * P.proj[2], y4 = pc.y * P.proj[1] + pc.z * P.proj[3];
+                        const float x4 = pc.x * A.proj[0] + pc.z * A.proj[2], y4 = pc.y * A.proj[1] + pc.z * A.proj[3];
                         const float z4 = fabsf(nr), w4 = pc.z * (nr > 0.f ? 1.f : -1.f);
                         if (!(fabsf(x4) >= fabsf(w4) || fabsf(y4) >= fabsf(w4) || fabsf(z4) >= fabsf(w4))) {
-                            ppx = P.imin[0] + W * (x4 / w4 * 0.5f + 0.5f);
-                            ppy = P.imin[1] + H * (-y4 / w4 * 0.5f + 0.5f);
+                            ppx = A.imin[0] + W * (x4 / w4 * 0.5f + 0.5f);
+                            ppy = A.imin[1] + H * (-y4 / w4 * 0.5f + 0.5f);
                         }
                     }
-                    if (P.aov_prev_uv) P.aov_prev_uv[pix] = make_float2(ppx / W, ppy / H);
-                    if (P.aov_depth) P.aov_depth[pix] = make_float4(isect_dist, length(pc), 1.f, 1.f);
+                    if (A.prev_uv) A.prev_uv[pix] = make_float2(ppx / W, ppy / H);
+                    if (A.depth) A.depth[pix] = make_float4(isect_dist, length(pc), 1.f, 1.f);
                 }
                 // ---- emission (surface lights are one-sided)
                 if (in.z > 0.f) {
@@ -202,7 +228,7 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                     if (any_pos(e) && len >= P.min_len) {
                         float w = 1.f;
                         if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
-                        if (w > 0.f) add_accum(P.accum, slot, e * w);
+                        if (w > 0.f) add_contrib(P, slot, e * w);
                     }
                 }
                 if (len < P.max_len && any_pos(m.base())) {

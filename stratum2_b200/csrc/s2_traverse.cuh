@@ -150,74 +150,93 @@ S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint
     }
 }
 
-// Traverse.  ANYHIT: stop at the first accepted triangle.  COUNT: count node and triangle
-// fetches into `ctr`.  Returns false if the stack overflowed (result may then be incomplete).
+// Per-ray traversal state for the step-wise traversal: the current node, the stack pointer and
+// the closest hit so far.  The stack lives in shared memory (first S2_STACK_SMEM entries, strided
+// by `lane_stride`) and in a local-memory continuation `lstack`.
+struct TravState {
+    uint32_t node;
+    int sp;
+    bool ok;    // false if the stack overflowed
+};
+
+S2D void trav_begin(TravState& st, TravHit& hit, float tmax) {
+    st.node = 0; st.sp = 0; st.ok = true;
+    hit.t = tmax; hit.tri = 0xffffffffu; hit.instance = 0xffffffffu; hit.primitive = 0xffffffffu;
+    hit.b1 = hit.b2 = 0.f;
+}
+
+// One traversal step: visit st.node (its 8 child boxes and its leaf triangles), then choose the
+// next node (nearest hit child, else the stack).  Returns true when the traversal is finished.
+template <bool ANYHIT, bool COUNT>
+S2D bool trav_step(const TravRay& r, TravState& st, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
+                   uint2* __restrict__ smem_stack, uint32_t lane_stride, uint2* lstack, TravHit& hit, TravCounters& ctr) {
+    uint32_t child_base, imask, hits, tri_base, trimask;
+    intersect_node(r, nodes4, st.node, hit.t, child_base, imask, hits, tri_base, trimask);
+    if (COUNT) ctr.nodes++;
+    while (trimask) {
+        const uint32_t k = __ffs(trimask) - 1;
+        trimask &= trimask - 1;
+        const uint32_t ti = tri_base + k;
+        const float4 a = __ldg(tris4 + 3 * (size_t)ti + 0);
+        const float4 b = __ldg(tris4 + 3 * (size_t)ti + 1);
+        const float4 c = __ldg(tris4 + 3 * (size_t)ti + 2);
+        if (COUNT) ctr.tris++;
+        float t, b1, b2;
+        if (intersect_triangle(r, ld3(a), ld3(b), ld3(c), hit.t, t, b1, b2)) {
+            const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+            if (ANYHIT) {
+                hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+                return true;
+            }
+            // accepted hits have t <= hit.t; equal distances keep the lowest (instance, primitive)
+            if (t < hit.t || inst < hit.instance || (inst == hit.instance && prim < hit.primitive)) {
+                hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+            }
+        }
+    }
+    if (hits) {
+        const uint32_t b = __ffs(hits) - 1;
+        hits &= hits - 1;
+        const uint32_t s = b ^ r.oct;
+        const uint32_t next = child_base + __popc(imask & ((1u << s) - 1u));
+        if (hits) {
+            const uint2 g = make_uint2(child_base, imask | (hits << 8));
+            if (st.sp < S2_STACK_SMEM) smem_stack[st.sp * lane_stride] = g;
+            else if (st.sp < S2_STACK_DEPTH) lstack[st.sp - S2_STACK_SMEM] = g;
+            else st.ok = false;
+            if (st.sp < S2_STACK_DEPTH) st.sp++;
+        }
+        st.node = next;
+        return false;
+    }
+    if (st.sp == 0) return true;
+    // take the nearest remaining child of the top group; pop the group when it empties
+    uint2 g = (st.sp - 1 < S2_STACK_SMEM) ? smem_stack[(st.sp - 1) * lane_stride] : lstack[st.sp - 1 - S2_STACK_SMEM];
+    uint32_t gh = g.y >> 8;
+    const uint32_t b = __ffs(gh) - 1;
+    gh &= gh - 1;
+    const uint32_t gi = g.y & 0xffu;
+    const uint32_t s = b ^ r.oct;
+    st.node = g.x + __popc(gi & ((1u << s) - 1u));
+    if (gh) {
+        g.y = gi | (gh << 8);
+        if (st.sp - 1 < S2_STACK_SMEM) smem_stack[(st.sp - 1) * lane_stride] = g;
+        else lstack[st.sp - 1 - S2_STACK_SMEM] = g;
+    } else {
+        st.sp--;
+    }
+    return false;
+}
+
+// Whole traversal of one ray.  ANYHIT: stop at the first accepted triangle.  COUNT: count node and
+// triangle fetches into `ctr`.  Returns false if the stack overflowed (result may be incomplete).
 template <bool ANYHIT, bool COUNT>
 S2D bool traverse(const TravRay& r, float tmax, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
                   uint2* __restrict__ smem_stack, uint32_t lane_stride, TravHit& hit, TravCounters& ctr) {
-    hit.t = tmax; hit.tri = 0xffffffffu; hit.instance = 0xffffffffu; hit.primitive = 0xffffffffu;
-    hit.b1 = hit.b2 = 0.f;
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
-    int sp = 0;
-    bool ok = true;
-    uint32_t node = 0;
-    float best_t = tmax;
-    while (true) {
-        uint32_t child_base, imask, hits, tri_base, trimask;
-        intersect_node(r, nodes4, node, best_t, child_base, imask, hits, tri_base, trimask);
-        if (COUNT) ctr.nodes++;
-        while (trimask) {
-            const uint32_t k = __ffs(trimask) - 1;
-            trimask &= trimask - 1;
-            const uint32_t ti = tri_base + k;
-            const float4 a = __ldg(tris4 + 3 * (size_t)ti + 0);
-            const float4 b = __ldg(tris4 + 3 * (size_t)ti + 1);
-            const float4 c = __ldg(tris4 + 3 * (size_t)ti + 2);
-            if (COUNT) ctr.tris++;
-            float t, b1, b2;
-            if (intersect_triangle(r, ld3(a), ld3(b), ld3(c), best_t, t, b1, b2)) {
-                const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-                if (ANYHIT) {
-                    hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
-                    return ok;
-                }
-                if (t < best_t || inst < hit.instance || (inst == hit.instance && prim < hit.primitive)) {
-                    best_t = t;
-                    hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
-                }
-            }
-        }
-        if (hits) {
-            const uint32_t b = __ffs(hits) - 1;
-            hits &= hits - 1;
-            const uint32_t s = b ^ r.oct;
-            const uint32_t next = child_base + __popc(imask & ((1u << s) - 1u));
-            if (hits) {
-                const uint2 g = make_uint2(child_base, imask | (hits << 8));
-                if (sp < S2_STACK_SMEM) smem_stack[sp * lane_stride] = g;
-                else if (sp < S2_STACK_DEPTH) lstack[sp - S2_STACK_SMEM] = g;
-                else ok = false;
-                if (sp < S2_STACK_DEPTH) sp++;
-            }
-            node = next;
-            continue;
-        }
-        if (sp == 0) break;
-        // take the nearest remaining child of the top group; pop the group when it empties
-        uint2 g = (sp - 1 < S2_STACK_SMEM) ? smem_stack[(sp - 1) * lane_stride] : lstack[sp - 1 - S2_STACK_SMEM];
-        uint32_t gh = g.y >> 8;
-        const uint32_t b = __ffs(gh) - 1;
-        gh &= gh - 1;
-        const uint32_t gi = g.y & 0xffu;
-        const uint32_t s = b ^ r.oct;
-        node = g.x + __popc(gi & ((1u << s) - 1u));
-        if (gh) {
-            g.y = gi | (gh << 8);
-            if (sp - 1 < S2_STACK_SMEM) smem_stack[(sp - 1) * lane_stride] = g;
-            else lstack[sp - 1 - S2_STACK_SMEM] = g;
-        } else {
-            sp--;
-        }
+    TravState st;
+    trav_begin(st, hit, tmax);
+    while (!trav_step<ANYHIT, COUNT>(r, st, nodes4, tris4, smem_stack, lane_stride, lstack, hit, ctr)) {
     }
-    return ok;
+    return st.ok;
 }

@@ -30,6 +30,23 @@ enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_EXT_NODES = 3, S_EX
 
 struct PathQueue { float4* s0; float4* s1; float4* s2; uint4* s3; };
 
+// One view of a batched (multi-view) render: ViewData + camera transform, its slice of the path
+// space (path_offset .. path_offset + pixels * spp), its slice of the concatenated per-pixel
+// accumulators (pixel_offset), and its AOV outputs.
+struct ViewEntry {
+    float proj[8];
+    int imin[2], imax[2];
+    float cam[12];
+    float prev_inv[12];
+    uint32_t width, height, pixels, pixel_offset;
+    unsigned long long path_offset;
+    float4* aov_albedo;
+    uint2* aov_vis;
+    float4* aov_depth;
+    float2* aov_prev_uv;
+    uint2* aov_ids;
+};
+
 struct PTParams {
     DevScene scene;
     // view (ViewData + camera transform)
@@ -57,7 +74,34 @@ struct PTParams {
     float4* aov_depth;
     float2* aov_prev_uv;
     uint2* aov_ids;
+    // batched streaming mode (s2_render_views): view table, fixed-point per-pixel accumulators,
+    // path-space size and queue capacity; null / 0 in wave mode
+    const ViewEntry* views;
+    uint32_t nviews;
+    unsigned long long* total_fx;   // 4 x u64 per pixel: r, g, b fixed point (2^-24), unused
+    unsigned long long total_paths;
+    uint32_t capacity;
+    unsigned long long* stream_state; // [0] next path id, [1] regen base, [2] regen count, [3] done
 };
+
+// fixed-point scale of the batched accumulators: integer sums are independent of the order of the
+// (atomic) additions, so batched renders are deterministic
+#define S2_FX_SCALE 16777216.0f
+
+// Adds a contribution to a path's accumulator: an exclusive float slot in wave mode, or an atomic
+// fixed-point add into the pixel's total in batched mode.
+S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
+    if (P.total_fx) {
+        unsigned long long* t = P.total_fx + 4 * (size_t)slot;
+        if (v.x > 0.f) atomicAdd(t + 0, (unsigned long long)__float2ull_rn(v.x * S2_FX_SCALE));
+        if (v.y > 0.f) atomicAdd(t + 1, (unsigned long long)__float2ull_rn(v.y * S2_FX_SCALE));
+        if (v.z > 0.f) atomicAdd(t + 2, (unsigned long long)__float2ull_rn(v.z * S2_FX_SCALE));
+        return;
+    }
+    float4 a = P.accum[slot];
+    a.x += v.x; a.y += v.y; a.z += v.z;
+    P.accum[slot] = a;
+}
 
 #define S2F_JITTER (1u << 0)
 #define S2F_LAMBERT (1u << 1)
@@ -74,6 +118,26 @@ constexpr int kTravBlock = 128;
 // InitializeCameraPath (testrenderer.slang:938-957): ViewData::toWorld (compat/scene.h:152-157)
 // through ProjectionData::backProject (compat/transform.h:159-170); the direction is stored
 // octahedral-packed as the reference's PathState.mRayDirection is.
+// Camera ray through pixel (px, py) (+ offset) of a view: InitializeCameraPath
+// (testrenderer.slang:938-957), ViewData::toWorld / ProjectionData::backProject.
+S2D float3 camera_dir(const float* proj, const int* imin, const int* imax, const float* c, uint32_t px, uint32_t py,
+                      float ox, float oy) {
+    const float W = (float)(imax[0] - imin[0]), H = (float)(imax[1] - imin[1]);
+    const float uvx = ((float)px + ox - imin[0]) / W, uvy = ((float)py + oy - imin[1]) / H;
+    const float cx = 2.f * uvx - 1.f, cy = -(2.f * uvy - 1.f);
+    const float sx = proj[0], sy = proj[1], offx = proj[2], offy = proj[3], nr = proj[4];
+    float3 ld;
+    if (proj[7] < 0.f) ld = f3((cx - offx) / sx, (cy - offy) / sy, nr);
+    else {
+        const float sg = nr > 0.f ? 1.f : (nr < 0.f ? -1.f : 0.f);
+        ld = f3(nr * (cx * sg - offx) / sx, nr * (cy * sg - offy) / sy, nr);
+    }
+    ld = normalize(ld);
+    const float3 wd = normalize(f3(c[0] * ld.x + c[1] * ld.y + c[2] * ld.z, c[4] * ld.x + c[5] * ld.y + c[6] * ld.z,
+                                   c[8] * ld.x + c[9] * ld.y + c[10] * ld.z));
+    return unpack_normal(pack_normal(wd));
+}
+
 __global__ void k_raygen(PTParams P) {
     const uint32_t n = P.pixels * P.wave_samples;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -130,9 +194,77 @@ __global__ void k_wave_finish(PTParams P) {
     P.counters[C_SHADOW] = 0;
 }
 
-// ---------------------------------------------------------------- extend: closest hit
-// Persistent kernel: each warp takes 32 rays at a time from a global work counter (dynamic load
-// balancing of incoherent traversal).  Hit record: {t, triangle record index, b1, b2}.
+// ---------------------------------------------------------------- batched streaming mode
+// Path regeneration: before every bounce the queue is topped up to capacity with new camera paths
+// (taken in path-id order across all views), so every launch works on a full queue however
+// unevenly Russian roulette and escapes shorten the paths.
+__global__ void k_stream_setup(PTParams P, uint32_t parity, int first) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long* ss = P.stream_state;
+    if (!first) P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    const uint32_t live = P.counters[parity];
+    const unsigned long long left = P.total_paths - ss[0];
+    const uint32_t fill = (uint32_t)min((unsigned long long)(P.capacity - live), left);
+    ss[1] = ss[0];
+    ss[2] = fill;
+    ss[0] += fill;
+    ss[3] = (live + fill == 0) ? 1ull : 0ull;
+    P.counters[parity] = live + fill;
+    P.stats[S_EXT] += live + fill;
+    P.counters[1 - parity] = 0;
+    P.counters[C_SHADOW] = 0;
+    P.counters[C_WORK_EXT] = 0;
+    P.counters[C_WORK_OCC] = 0;
+}
+
+// New camera paths for path ids [base, base + fill), appended after the live paths.
+S2D void regen_one(const PTParams& P, uint32_t parity, uint32_t fill, uint32_t i) {
+    const unsigned long long id = P.stream_state[1] + i;
+    uint32_t v = 0;
+    while (v + 1 < P.nviews && P.views[v + 1].path_offset <= id) ++v;
+    const ViewEntry& V = P.views[v];
+    const unsigned long long local = id - V.path_offset;
+    const uint32_t sample = (uint32_t)(local / V.pixels), pix = (uint32_t)(local - (unsigned long long)sample * V.pixels);
+    const uint32_t px = pix % V.width, py = pix / V.width;
+    Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
+    float ox = 0.5f, oy = 0.5f;
+    if (P.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
+    const float3 d = camera_dir(V.proj, V.imin, V.imax, V.cam, px, py, ox, oy);
+    // meta: path length 0, bit 8 = write AOVs, bits 16..23 = view
+    const uint32_t meta = (sample == 0 ? 0x100u : 0u) | (v << 16);
+    const uint32_t q = P.counters[parity] - fill + i;
+    const PathQueue& Q = P.q[parity];
+    Q.s0[q] = make_float4(V.cam[3], V.cam[7], V.cam[11], 0.f);
+    Q.s1[q] = make_float4(d.x, d.y, d.z, 1.f);
+    Q.s2[q] = make_float4(1.f, 1.f, __uint_as_float(V.pixel_offset + pix), __uint_as_float(meta));
+    Q.s3[q] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+}
+
+__global__ void k_regen(PTParams P, uint32_t parity) {
+    const uint32_t fill = (uint32_t)P.stream_state[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < fill; i += gridDim.x * blockDim.x)
+        regen_one(P, parity, fill, i);
+}
+
+// Fixed-point totals -> mean radiance * 2^exposure for one view.
+__global__ void k_resolve_fx(const unsigned long long* __restrict__ total_fx, uint32_t pixel_offset, uint32_t pixels,
+                             float scale, float4* __restrict__ out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    const unsigned long long* t = total_fx + 4 * (size_t)(pixel_offset + p);
+    const float s = scale / S2_FX_SCALE;
+    out[p] = make_float4((float)((double)t[0] * s), (float)((double)t[1] * s), (float)((double)t[2] * s), 1.f);
+}
+
+// ---------------------------------------------------------------- extend / occlude
+// Persistent traversal with lane refill: every lane owns one ray at a time and advances it one
+// node per loop iteration; when at least kRefillMin lanes of a warp have finished their rays (or
+// all have), the warp fetches that many new rays from the global work counter with one atomic.
+// Lanes therefore stay busy while long rays finish, instead of the whole warp waiting for its
+// slowest ray (dynamic ray fetch in the manner of Aila and Laine, HPG 2009).
+constexpr uint32_t kRefillMin = 8;
+constexpr uint32_t kNoRay = 0xffffffffu;
+
 // Warp-sum of the fetch counters, one 64-bit atomic per warp (counting runs only).
 S2D void add_fetches(unsigned long long* stats, uint32_t node_stat, const TravCounters& c) {
     uint32_t n = c.nodes, t = c.tris;
@@ -140,58 +272,89 @@ S2D void add_fetches(unsigned long long* stats, uint32_t node_stat, const TravCo
     if ((threadIdx.x & 31u) == 0) { atomicAdd(&stats[node_stat], (unsigned long long)n); atomicAdd(&stats[node_stat + 1], (unsigned long long)t); }
 }
 
+// Gives idle lanes new work items [0, count) from `work`; returns the lane's item or kNoRay.
+S2D uint32_t refill(uint32_t* work, uint32_t count, uint32_t item, bool& exhausted) {
+    const bool need = item == kNoRay && !exhausted;
+    const uint32_t needm = __ballot_sync(0xffffffffu, need);
+    const uint32_t activem = __ballot_sync(0xffffffffu, item != kNoRay);
+    if (needm && (__popc(needm) >= kRefillMin || activem == 0)) {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t leader = __ffs(needm) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(needm));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (need) {
+            const uint32_t idx = base + __popc(needm & ((1u << lane) - 1u));
+            if (idx < count) item = idx;
+            else exhausted = true;
+        }
+    }
+    return item;
+}
+
+// Closest hit of the live path queue.  Hit record: {t, triangle record index, b1, b2}.
 template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t parity) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[parity];
     const PathQueue q = P.q[parity];
-    const uint32_t lane = threadIdx.x & 31u;
     TravCounters c{0, 0};
+    TravRay r;
+    TravState st;
+    TravHit h;
+    uint32_t ray = kNoRay;
+    bool exhausted = false;
     while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&P.counters[C_WORK_EXT], 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane;
-        if (i < count) {
-            const float4 a = q.s0[i], b = q.s1[i];
-            const TravRay r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
-            TravHit h;
-            if (!traverse<false, COUNT>(r, S2_INF, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
-                atomicOr(P.status, 1);
-            P.hits[i] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
+        const uint32_t prev = ray;
+        ray = refill(&P.counters[C_WORK_EXT], count, ray, exhausted);
+        if (!__any_sync(0xffffffffu, ray != kNoRay)) break;
+        if (ray != kNoRay && prev == kNoRay) {
+            const float4 a = q.s0[ray], b = q.s1[ray];
+            r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
+            trav_begin(st, h, S2_INF);
+        }
+        if (ray != kNoRay) {
+            if (trav_step<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c)) {
+                if (!st.ok) atomicOr(P.status, 1);
+                P.hits[ray] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
+                ray = kNoRay;
+            }
         }
     }
     if (COUNT) add_fetches(P.stats, S_EXT_NODES, c);
 }
 
-// ---------------------------------------------------------------- occlude: first hit
 // ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
 // ray belongs to one accumulator slot and adds its contribution when unoccluded.
 template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[C_SHADOW];
-    const uint32_t lane = threadIdx.x & 31u;
     TravCounters c{0, 0};
+    TravRay r;
+    TravState st;
+    TravHit h;
+    uint32_t ray = kNoRay;
+    bool exhausted = false;
     while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&P.counters[C_WORK_OCC], 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane;
-        if (i < count) {
-            const float4 o = P.sh_o[i], d = P.sh_d[i];
-            const TravRay r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
-            TravHit h;
-            if (!traverse<true, COUNT>(r, o.w, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, h, c))
-                atomicOr(P.status, 1);
-            if (h.tri == 0xffffffffu) {
-                const float4 cc = P.sh_c[i];
-                const uint32_t slot = __float_as_uint(d.w);
-                float4 acc = P.accum[slot];
-                acc.x += cc.x; acc.y += cc.y; acc.z += cc.z;
-                P.accum[slot] = acc;
+        const uint32_t prev = ray;
+        ray = refill(&P.counters[C_WORK_OCC], count, ray, exhausted);
+        if (!__any_sync(0xffffffffu, ray != kNoRay)) break;
+        if (ray != kNoRay && prev == kNoRay) {
+            const float4 o = P.sh_o[ray], d = P.sh_d[ray];
+            r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
+            trav_begin(st, h, o.w);
+        }
+        if (ray != kNoRay) {
+            if (trav_step<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c)) {
+                if (!st.ok) atomicOr(P.status, 1);
+                if (h.tri == 0xffffffffu) {
+                    const float4 cc = P.sh_c[ray];
+                    add_contrib(P, __float_as_uint(P.sh_d[ray].w), f3(cc.x, cc.y, cc.z));
+                }
+                ray = kNoRay;
             }
         }
     }
