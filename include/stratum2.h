@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define S2_ABI_VERSION 1
+#define S2_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------------------------ */
 #define S2_OK               0
@@ -157,6 +157,11 @@ typedef struct S2View {
 #define S2_FLAG_SHADING_NORMALS_OFF (1u << 8)  /* ignore vertex normals (gShadingNormals false) */
 #define S2_FLAG_PROFILE_KERNELS     (1u << 9)  /* time extend/shade/occlude launches with CUDA events */
 #define S2_FLAG_COUNT_FETCHES       (1u << 10) /* count BVH node and triangle fetches (slower) */
+#define S2_FLAG_RESTIR_REUSE        (1u << 11) /* gReSTIR_DI_Reuse: with S2_FLAG_RESTIR_DI, reuse one
+                                                  reservoir per vertex from the previous s2_render
+                                                  call's world-space hash grid and store this call's
+                                                  reservoirs for the next call (testrenderer.slang:
+                                                  608-726).  Results depend on atomic append order. */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */
@@ -168,10 +173,10 @@ typedef struct S2RenderParams {
     float environment_sample_probability; /* default 0.9 (TestRenderer.cpp:41) */
     uint32_t restir_candidates;      /* mCandidateSamples (default 32) */
     float restir_max_m;              /* mMaxM (default 3) */
-    uint32_t restir_spatial_count;   /* screen-space spatial neighbours (0 = off) */
-    float restir_spatial_radius;     /* pixels */
-    uint32_t restir_temporal;        /* 1 = reuse the previous call's reservoirs */
     uint32_t wave_paths;             /* paths in flight per wave / queue (0 = 2^25) */
+    uint32_t restir_grid_cells;      /* hash-grid cell count (0 = 100000, TestRenderer.cpp:52) */
+    float restir_grid_cell_size;     /* minimum cell size (0 = 0.5, TestRenderer.cpp:52) */
+    float restir_grid_pixel_radius;  /* mCellPixelRadius: 0 = constant cell size */
     uint32_t reserved[7];
 } S2RenderParams;
 

@@ -16,7 +16,8 @@
 namespace orc {
 
 constexpr uint32_t FLAG_PIXEL_JITTER = 1u << 0, FLAG_LAMBERTIAN = 1u << 1, FLAG_PCG32 = 1u << 2, FLAG_NO_NEE = 1u << 3,
-                   FLAG_RESTIR = 1u << 4, FLAG_REF_ENV_MIS = 1u << 5, FLAG_NO_RR = 1u << 6, FLAG_NO_SHADING_NORMALS = 1u << 8;
+                   FLAG_RESTIR = 1u << 4, FLAG_REF_ENV_MIS = 1u << 5, FLAG_NO_RR = 1u << 6, FLAG_NO_SHADING_NORMALS = 1u << 8,
+                   FLAG_RESTIR_REUSE = 1u << 11;
 
 template <class R> R un8(uint32_t w, int shift) { return R((w >> shift) & 0xffu) / R(255); }
 inline uint32_t pk8(double v) { v = std::min(std::max(v, 0.0), 1.0); return (uint32_t)std::floor((float)v * 255.f + 0.5f); }
@@ -74,12 +75,93 @@ template <class R> struct SD {
 struct Params {
     uint32_t min_len, max_len, spp, seed, flags, restir_m;
     float exposure, env_prob;
+    float max_m = 3.f;
+};
+
+// pcg / xxhash32 (rng.hlsli:5-22): the hash-grid keys
+inline uint32_t pcg_hash(uint32_t v) {
+    const uint32_t state = v * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+inline uint32_t xxhash32(uint32_t p) {
+    uint32_t h = p + 374761393u;
+    h = 668265263u * ((h << 17) | (h >> 15));
+    h = 2246822519u * (h ^ (h >> 15));
+    h = 3266489917u * (h ^ (h >> 13));
+    return h ^ (h >> 16);
+}
+
+// HashGridData of the ReSTIR DI reuse (testrenderer.slang:152-168)
+template <class R> struct GridRecord {
+    V3<R> local_pos;
+    uint32_t inst = 0, prim = 0;
+    float rnd[4] = {0, 0, 0, 0};
+    R target = 0, W = 0, M = 0;
+    V3<R> dir_in;
+};
+
+// HashGrid<T> (hashgrid.hlsli:14-119) and GpuHashGrid::clear/build (GpuHashGrid.cpp:71-111),
+// sequential: appends are serialised by a mutex and the per-cell offsets are a prefix sum in
+// cell order (the GPU assigns them in atomic order; only the order inside a cell differs).
+template <class R> struct CpuGrid {
+    uint32_t cells = 0, max_size = 0;
+    float min_cell = 0.5f, pixel_radius = 0.f, dscale = 0.f;
+    V3<R> cam;
+    std::vector<uint32_t> checksum, counter, offset, data_index;
+    std::vector<GridRecord<R>> data;
+    std::vector<std::pair<uint32_t, uint32_t>> app;
+    std::mutex mu;
+
+    void clear(uint32_t c, uint32_t size) {
+        cells = c; max_size = size;
+        checksum.assign(c, 0u); counter.assign(c, 0u); offset.assign(c, 0u);
+        data.clear(); app.clear(); data_index.clear();
+    }
+    // GetCellSize (hashgrid.hlsli:43-49)
+    float cell_size(const V3<R>& pos) const {
+        if (pixel_radius <= 0.f) return min_cell;
+        const float step = (float)length(cam - pos) * dscale;
+        const float l = std::log2(step / min_cell);
+        const uint32_t e = l > 0.f ? std::min<uint32_t>((uint32_t)l, 31u) : 0u;
+        return min_cell * (float)(1u << e);
+    }
+    // FindCellIndex (hashgrid.hlsli:51-75)
+    uint32_t find(const V3<R>& pos, float cs, bool insert) {
+        const int x = (int)std::floor((float)pos.x / cs), y = (int)std::floor((float)pos.y / cs), z = (int)std::floor((float)pos.z / cs);
+        uint32_t cb; std::memcpy(&cb, &cs, 4);
+        const uint32_t sum = std::max(1u, xxhash32(xxhash32(cb) + xxhash32((uint32_t)z + xxhash32((uint32_t)y + xxhash32((uint32_t)x)))));
+        const uint32_t base = pcg_hash(pcg_hash(cb) + pcg_hash((uint32_t)z + pcg_hash((uint32_t)y + pcg_hash((uint32_t)x)))) % cells;
+        for (uint32_t i = 0; i < 32; ++i) {
+            const uint32_t c = (base + i) % cells;
+            if (insert && checksum[c] == 0u) { checksum[c] = sum; return c; }
+            if (checksum[c] == sum) return c;
+        }
+        return 0xffffffffu;
+    }
+    // Append (hashgrid.hlsli:77-97)
+    void append(const V3<R>& pos, const GridRecord<R>& rec) {
+        std::lock_guard<std::mutex> lk(mu);
+        const uint32_t c = find(pos, cell_size(pos), true);
+        if (c == 0xffffffffu || data.size() >= max_size) return;
+        app.emplace_back(c, counter[c]++);
+        data.push_back(rec);
+    }
+    // ComputeIndices + Swizzle (hashgrid.hlsli:101-119)
+    void build() {
+        uint32_t acc = 0;
+        for (uint32_t c = 0; c < cells; ++c) { offset[c] = acc; acc += counter[c]; }
+        data_index.assign(data.size(), 0u);
+        for (uint32_t i = 0; i < (uint32_t)data.size(); ++i) data_index[offset[app[i].first] + app[i].second] = i;
+    }
 };
 
 template <class R> struct Tracer {
     const Scene<R>& s;
     Params p;
     uint64_t ext_rays = 0, shadow_rays = 0;
+    CpuGrid<R>* grid_cur = nullptr;    // ReSTIR DI reuse: grid appended to by this call
+    CpuGrid<R>* grid_prev = nullptr;   // the previous call's grid (null: none)
     Tracer(const Scene<R>& sc, const Params& pp) : s(sc), p(pp) {}
 
     bool has_env() const { return s.env_addr != S2_NO_ENVIRONMENT; }
@@ -138,6 +220,18 @@ template <class R> struct Tracer {
     V3<R> sample_image(uint32_t img, R u, R v) const { return s.images[img].sample(u, v); }
 
     // LoadMaterial (material.hlsli:15-46)
+    // makeTriangleShadingData from an object-space position (shading_data.hlsli:153-173)
+    SD<R> shading_local(uint32_t inst, uint32_t prim, const V3<R>& lp) const {
+        uint32_t idx[3]; s.tri_indices(inst, prim, idx);
+        const V3<R> v0 = s.position(inst, idx[0]), v1 = s.position(inst, idx[1]), v2 = s.position(inst, idx[2]);
+        const V3<R> e1 = v1 - v0, e2 = v2 - v0, pv = lp - v0;
+        const R d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(pv, e1), d21 = dot(pv, e2);
+        const R den = d00 * d11 - d01 * d01;
+        SD<R> r = shading(inst, prim, (d11 * d20 - d01 * d21) / den, (d00 * d21 - d01 * d20) / den);
+        r.pos = s.xpoint(&s.xf[12 * (size_t)inst], lp);
+        return r;
+    }
+
     Mat<R> material(uint32_t addr, R u, R v) const {
         Mat<R> m;
         for (int k = 0; k < 4; ++k) m.w[k] = s.u32(s.mat, addr + 4 * k);
@@ -640,7 +734,7 @@ template <class R> struct Tracer {
             if (len >= p.max_len) break;
             if (!can_eval(m)) break;
             const bool sing = singular(m);
-            if (!sing && nee) connect_to_light(m, sd, in, thr, rng, len, add);
+            if (!sing && nee) connect_to_light(m, sd, in, thr, rng, len, add, inst, prim);
             const R cp = std::min(R(1), cont_prob(m));
             if (!(p.flags & FLAG_NO_RR)) {
                 float f[4]; rng.next_float(f);
@@ -663,37 +757,98 @@ template <class R> struct Tracer {
         }
     }
 
+    // ReservoirSampleDataDI (testrenderer.slang:568-606): a light sample evaluated at one vertex
+    struct DI {
+        float x[4] = {0, 0, 0, 0};
+        R src_pdf = 0, wtoa = 0, misw = 0, dist = 0;
+        V3<R> contrib = V3<R>(0), dir = V3<R>(0);
+        R target() const { return luminance(contrib) * wtoa; }
+    };
+    DI eval_di(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, const float x[4], R cp) const {
+        DI c;
+        for (int k = 0; k < 4; ++k) c.x[k] = x[k];
+        const Illum r = sample_illum(x, sd.pos);
+        c.src_pdf = r.pdf;
+        if (luminance(r.radiance) > 0 && r.pdf > 0) {
+            const V3<R> out = sd.to_local(r.dir);
+            V3<R> f; R fwd, rev; eval(m, in, out, f, fwd, rev);
+            f = f * sd.snc(in, out);
+            fwd *= cp;
+            c.contrib = f * r.radiance;
+            c.wtoa = r.finite ? r.cos_light / pow2(r.dist) : R(1);
+            const R AtoW = r.finite ? pow2(r.dist) / r.cos_light : R(1);
+            c.misw = mis(r.pdf, fwd / AtoW);
+            c.dir = r.dir; c.dist = r.dist;
+        }
+        return c;
+    }
+
+    // ReservoirReuse (testrenderer.slang:608-663): pairwise MIS between the current reservoir
+    // and the stored one
+    void reservoir_reuse(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, R cp, const GridRecord<R>& q, DI& cur,
+                         R& iw, R& M, Rng& rng) const {
+        const DI nw = eval_di(m, sd, in, q.rnd, cp);
+        R phat_q = 0;
+        {
+            const SD<R> sdq = shading_local(q.inst, q.prim, q.local_pos);
+            const Mat<R> mq = material(sdq.mat, sdq.u, sdq.v);
+            const R cpq = (p.flags & FLAG_NO_RR) ? R(1) : cont_prob(mq);
+            const DI cq = eval_di(mq, sdq, q.dir_in, cur.x, cpq);
+            if (cq.target() > 0) phat_q = cq.target();
+        }
+        const R m0 = mis(M * cur.target(), q.M * phat_q);
+        const R m1 = mis(q.M * q.target, M * nw.target());
+        const R w0 = m0 * cur.target() * iw, w1 = m1 * nw.target() * q.W;
+        M += q.M;
+        const R total = w0 + w1;
+        float u[4]; rng.next_float(u);
+        if ((R)u[0] * total <= w1) cur = nw;
+        iw = cur.target() > 0 ? total / cur.target() : R(0);
+    }
+
     template <class Add>
-    void connect_to_light(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, const V3<R>& thr, Rng& rng, uint32_t len, Add& add) {
+    void connect_to_light(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, const V3<R>& thr, Rng& rng, uint32_t len,
+                          Add& add, uint32_t inst, uint32_t prim) {
         const R cp = (p.flags & FLAG_NO_RR) ? R(1) : cont_prob(m);
         if (p.flags & FLAG_RESTIR) {
-            // SampleIlluminationReSTIR initial RIS (testrenderer.slang:665-683) + ConnectToLight (:730-747)
-            struct Cand { R target = 0, wtoa = 0, misw = 0; V3<R> contrib; V3<R> dir; R dist = 0; bool finite = true; };
-            Cand best; R wsum = 0;
+            // SampleIlluminationReSTIR (testrenderer.slang:665-726) + ConnectToLight (:730-747)
+            DI best; R wsum = 0;
             for (uint32_t i = 0; i < p.restir_m; ++i) {
                 float x[4]; rng.next_float(x);
-                const Illum r = sample_illum(x, sd.pos);
-                Cand c; c.contrib = V3<R>(0);
-                if (luminance(r.radiance) > 0 && r.pdf > 0) {
-                    const V3<R> out = sd.to_local(r.dir);
-                    V3<R> f; R fwd, rev; eval(m, in, out, f, fwd, rev);
-                    f = f * sd.snc(in, out);
-                    fwd *= cp;
-                    c.contrib = f * r.radiance;
-                    c.wtoa = r.finite ? r.cos_light / pow2(r.dist) : R(1);
-                    const R AtoW = r.finite ? pow2(r.dist) / r.cos_light : R(1);
-                    c.misw = mis(r.pdf, fwd / AtoW);
-                    c.dir = r.dir; c.dist = r.dist; c.finite = r.finite;
-                    c.target = luminance(c.contrib) * c.wtoa;
-                }
-                if (c.target <= 0) continue;
-                const R risw = c.target / r.pdf;
+                const DI c = eval_di(m, sd, in, x, cp);
+                if (c.target() <= 0) continue;
+                const R risw = c.target() / c.src_pdf;
                 wsum += risw;
                 float u[4]; rng.next_float(u);
                 if ((R)u[0] <= risw / wsum) best = c;
             }
-            if (!(best.target > 0)) return;
-            R iw = wsum / ((R)p.restir_m * best.target);
+            R iw = best.target() > 0 ? wsum / ((R)p.restir_m * best.target()) : R(0);
+            if (grid_cur) {
+                R M = (R)p.restir_m;
+                if (grid_prev) {
+                    float dr[4]; rng.next_float(dr);
+                    R dx, dy; sample_concentric_disc<R>((R)dr[0], (R)dr[1], dx, dy);
+                    const R csz = (R)grid_prev->cell_size(sd.pos);
+                    const V3<R> qp = sd.pos + sd.to_world(V3<R>(dx * csz, dy * csz, 0));
+                    const uint32_t cell = grid_prev->find(qp, grid_prev->cell_size(qp), false);
+                    if (cell != 0xffffffffu && grid_prev->counter[cell] > 0) {
+                        const uint32_t k = rng.next().x % grid_prev->counter[cell];
+                        const GridRecord<R>& q = grid_prev->data[grid_prev->data_index[grid_prev->offset[cell] + k]];
+                        reservoir_reuse(m, sd, in, cp, q, best, iw, M, rng);
+                    }
+                }
+                if (iw > 0) {
+                    GridRecord<R> rec;
+                    rec.local_pos = s.xpoint(&s.inv[12 * (size_t)inst], sd.pos);
+                    rec.inst = inst; rec.prim = prim;
+                    for (int k = 0; k < 4; ++k) rec.rnd[k] = best.x[k];
+                    rec.target = best.target();
+                    rec.W = iw;
+                    rec.M = std::min(M, (R)p.max_m * (R)p.restir_m);
+                    rec.dir_in = in;
+                    grid_cur->append(sd.pos, rec);
+                }
+            }
             if (!(iw > 0)) return;
             iw *= best.wtoa;
             const V3<R> contrib = thr * best.contrib * iw;
@@ -726,10 +881,21 @@ template <class R> struct Tracer {
 }  // namespace orc
 
 // ============================================================================== C entry points
+// The two ReSTIR reuse grids of one precision: the one the next call appends to and the previous.
+template <class R> struct GridPair {
+    std::unique_ptr<orc::CpuGrid<R>> g[2];
+    int cur = 0;
+    bool valid = false;
+};
+
 struct OracleScene {
     orc::Scene<double> d;
     orc::Scene<float> f;
     bool has_d = false, has_f = false;
+    GridPair<double> grid_d;
+    GridPair<float> grid_f;
+    GridPair<double>& grids(orc::Scene<double>&) { return grid_d; }
+    GridPair<float>& grids(orc::Scene<float>&) { return grid_f; }
 };
 
 extern "C" {
@@ -783,12 +949,34 @@ int oracle_render(void* sp, const S2View* view, const S2RenderParams* rp, int pr
     std::vector<std::pair<int, int>> px;
     for (int y = y0; y < y1; y += stride) for (int x = x0; x < x1; x += stride) px.emplace_back(x, y);
     std::atomic<uint64_t> ext{0}, shd{0};
+    const bool reuse = (rp->flags & orc::FLAG_RESTIR) && (rp->flags & orc::FLAG_RESTIR_REUSE);
+    p.max_m = rp->restir_max_m > 0 ? rp->restir_max_m : 3.f;
     auto run = [&](auto& scene) {
-        using Rt = typename std::remove_reference<decltype(scene)>::type;
-        (void)sizeof(Rt);
+        using R = std::remove_const_t<std::remove_reference_t<decltype(scene.tv[0])>>;
+        auto& gp = s->grids(scene);
+        orc::CpuGrid<R>* gcur = nullptr;
+        orc::CpuGrid<R>* gprev = nullptr;
+        if (reuse) {
+            // TestRenderer.cpp:472-493: append to one grid, read the previous call's
+            for (auto& g : gp.g) if (!g) g.reset(new orc::CpuGrid<R>());
+            gcur = gp.g[gp.cur].get();
+            gprev = gp.valid ? gp.g[gp.cur ^ 1].get() : nullptr;
+            const uint64_t per = (uint64_t)px.size() * std::max(1u, std::min(2u, p.max_len ? p.max_len - 1 : 1u));
+            gcur->clear(rp->restir_grid_cells ? rp->restir_grid_cells : 100000u,
+                        (uint32_t)std::min<uint64_t>(per * p.spp, 1u << 24));
+            gcur->min_cell = rp->restir_grid_cell_size > 0 ? rp->restir_grid_cell_size : 0.5f;
+            gcur->pixel_radius = rp->restir_grid_pixel_radius;
+            gcur->cam = orc::V3<R>(view->camera_to_world[3], view->camera_to_world[7], view->camera_to_world[11]);
+            const int H = view->image_max[1] - view->image_min[1];
+            gcur->dscale = std::tan(gcur->pixel_radius * view->projection[7] * std::max(1.f / (float)H, (float)H / ((float)W * (float)W)));
+        } else {
+            gp.valid = false;
+        }
 #pragma omp parallel num_threads(threads > 0 ? threads : omp_get_max_threads())
         {
-            auto tr = orc::Tracer<std::remove_reference_t<decltype(scene.tv[0])>>(scene, p);
+            auto tr = orc::Tracer<R>(scene, p);
+            tr.grid_cur = gcur;
+            tr.grid_prev = gprev;
 #pragma omp for schedule(dynamic, 16)
             for (int64_t k = 0; k < (int64_t)px.size(); ++k) {
                 const int x = px[k].first, y = px[k].second;
@@ -810,6 +998,11 @@ int oracle_render(void* sp, const S2View* view, const S2RenderParams* rp, int pr
                 if (sumsq) for (int c = 0; c < 3; ++c) sumsq[3 * pi + c] = acc2[c];
             }
             ext += tr.ext_rays; shd += tr.shadow_rays;
+        }
+        if (reuse) {
+            gcur->build();
+            gp.cur ^= 1;
+            gp.valid = true;
         }
     };
     if (precision == 64) { if (!s->has_d) return -1; run(s->d); }
@@ -851,3 +1044,8 @@ void oracle_bsdf_sample(const uint32_t* mat_words, int lambertian, const double*
 }
 
 }  // extern "C"
+
+extern "C" {
+uint32_t oracle_pcg_hash(uint32_t v) { return orc::pcg_hash(v); }
+uint32_t oracle_xxhash32(uint32_t v) { return orc::xxhash32(v); }
+}

@@ -10,6 +10,8 @@ from pathlib import Path
 
 _LIB_PATH = Path(__file__).resolve().parent / "libstratum2_b200.so"
 
+ABI_VERSION = 2  # S2_ABI_VERSION
+
 S2_OK = 0
 S2_ERR_INVALID = -1
 S2_ERR_CUDA = -2
@@ -36,6 +38,7 @@ FLAG_ACCUMULATE = 1 << 7
 FLAG_SHADING_NORMALS_OFF = 1 << 8
 FLAG_PROFILE_KERNELS = 1 << 9
 FLAG_COUNT_FETCHES = 1 << 10
+FLAG_RESTIR_REUSE = 1 << 11
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -105,9 +108,9 @@ class S2RenderParams(C.Structure):
         ("min_path_length", C.c_uint32), ("max_path_length", C.c_uint32), ("exposure", C.c_float),
         ("spp", C.c_uint32), ("frame_seed", C.c_uint32), ("flags", C.c_uint32),
         ("environment_sample_probability", C.c_float), ("restir_candidates", C.c_uint32),
-        ("restir_max_m", C.c_float), ("restir_spatial_count", C.c_uint32),
-        ("restir_spatial_radius", C.c_float), ("restir_temporal", C.c_uint32),
-        ("wave_paths", C.c_uint32), ("reserved", C.c_uint32 * 7),
+        ("restir_max_m", C.c_float), ("wave_paths", C.c_uint32), ("restir_grid_cells", C.c_uint32),
+        ("restir_grid_cell_size", C.c_float), ("restir_grid_pixel_radius", C.c_float),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 
@@ -160,6 +163,8 @@ def lib() -> C.CDLL:
     L.s2_default_render_params.restype = None
     for name in EXPORTED_SYMBOLS:
         getattr(L, name)
+    if L.s2_get_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{_LIB_PATH} has ABI {L.s2_get_abi_version()}, expected {ABI_VERSION}: rebuild it")
     _lib = L
     return L
 

@@ -32,6 +32,13 @@ struct RenderState {
     uint64_t accumulated_spp = 0;
     int ext_blocks = 0, occ_blocks = 0, shade_blocks = 0;
     std::vector<cudaEvent_t> events;  // reusable start/stop pairs for S2_FLAG_PROFILE_KERNELS
+    // ReSTIR DI reuse: the grid appended to by this call and the previous call's grid
+    struct Grid {
+        std::vector<DevBuf> bufs;
+        HashGridDev g{};
+    } grid[2];
+    uint32_t grid_cur = 0;
+    bool grid_prev_valid = false;
 };
 
 void destroy_batch_state(S2Context* ctx);
@@ -40,6 +47,7 @@ void destroy_render_state(S2Context* ctx) {
     destroy_batch_state(ctx);
     if (!ctx->render) return;
     for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
+    for (auto& g : ctx->render->grid) free_bufs(g.bufs);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -112,6 +120,28 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
     return S2_OK;
 }
 
+// (Re)allocates one hash grid for `cells` cells and `size` records (GpuHashGrid::init,
+// src/App/GpuHashGrid.cpp:17-69).
+int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t size) {
+    if (G.g.checksums && G.g.cell_count == cells && G.g.max_size >= size) return S2_OK;
+    free_bufs(G.bufs);
+    G.g = HashGridDev{};
+    HashGridDev g{};
+    g.checksums = alloc<uint32_t>(ctx, G.bufs, cells);
+    g.cell_counters = alloc<uint32_t>(ctx, G.bufs, cells);
+    g.other = alloc<uint32_t>(ctx, G.bufs, 4);
+    g.append_indices = alloc<uint2>(ctx, G.bufs, size);
+    g.data = alloc<ReservoirRecord>(ctx, G.bufs, size);
+    g.indices = alloc<uint32_t>(ctx, G.bufs, cells);
+    g.data_indices = alloc<uint32_t>(ctx, G.bufs, size);
+    for (auto& b : G.bufs) if (!b.ptr) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    if (G.bufs.size() != 7) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    g.cell_count = cells;
+    g.max_size = size;
+    G.g = g;
+    return S2_OK;
+}
+
 template <bool L, bool R>
 void launch_shade(const PTParams& P, uint32_t parity, int blocks, cudaStream_t s) {
     k_shade<L, R><<<blocks, 128, 0, s>>>(P, parity);
@@ -132,7 +162,8 @@ extern "C" void s2_default_render_params(S2RenderParams* p) {
     p->environment_sample_probability = 0.9f;  // TestRenderer.cpp:41
     p->restir_candidates = 32;      // TestRenderer.cpp:42
     p->restir_max_m = 3.f;          // TestRenderer.cpp:43
-    p->restir_spatial_radius = 30.f;
+    p->restir_grid_cells = 100000;  // TestRenderer.cpp:52
+    p->restir_grid_cell_size = 0.5f;
 }
 
 extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParams* prm, const S2Aovs* out, int out_on_host,
@@ -146,6 +177,11 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
+    const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
+    if (reuse && (prm->restir_grid_cells > (1u << 26) || prm->restir_grid_cell_size < 0.f ||
+                  !std::isfinite(prm->restir_grid_cell_size) || !(prm->restir_grid_pixel_radius >= 0.f) ||
+                  !std::isfinite(prm->restir_grid_pixel_radius) || !(prm->restir_max_m > 0.f)))
+        return set_error(ctx, S2_ERR_INVALID, "invalid ReSTIR hash-grid parameters");
     cudaSetDevice(ctx->device);
     const uint32_t pixels = (uint32_t)W * (uint32_t)H;
     uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 25);
@@ -186,6 +222,35 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     P.aov_prev_uv = (float2*)pick(out ? out->prev_uv : nullptr, st->aov_prev_uv);
     P.aov_ids = (uint2*)pick(out ? out->ids32 : nullptr, st->aov_ids);
 
+    if (reuse) {
+        // TestRenderer.cpp:472-493 and :595-628: this call appends to one grid while reading the
+        // previous call's; the grid holds pixels x min(2, maxDepth-1) records per sample pass
+        // (appends beyond that are dropped, as in HashGrid::Append).
+        const uint32_t cells = prm->restir_grid_cells ? prm->restir_grid_cells : 100000u;
+        const uint64_t per_pass = (uint64_t)pixels * std::max(1u, std::min(2u, prm->max_path_length ? prm->max_path_length - 1 : 1u));
+        const uint32_t size = (uint32_t)std::min<uint64_t>(per_pass * prm->spp, 1u << 24);
+        RenderState::Grid& cur = st->grid[st->grid_cur];
+        RenderState::Grid& prev = st->grid[st->grid_cur ^ 1];
+        rc = ensure_grid(ctx, cur, cells, size);
+        if (rc != S2_OK) return set_error(ctx, rc, "hash grid allocation failed");
+        HashGridDev& g = cur.g;
+        g.min_cell_size = prm->restir_grid_cell_size > 0.f ? prm->restir_grid_cell_size : 0.5f;
+        g.cell_pixel_radius = prm->restir_grid_pixel_radius;
+        g.camera_position = make_float3(view->camera_to_world[3], view->camera_to_world[7], view->camera_to_world[11]);
+        // GpuHashGrid.cpp:34: tan(radius * vfov * max(1/h, h/w^2))
+        g.distance_scale = tanf(g.cell_pixel_radius * view->projection[7] *
+                                std::max(1.f / (float)H, (float)H / ((float)W * (float)W)));
+        cudaMemsetAsync(g.checksums, 0, sizeof(uint32_t) * cells, s);       // GpuHashGrid::clear
+        cudaMemsetAsync(g.cell_counters, 0, sizeof(uint32_t) * cells, s);
+        cudaMemsetAsync(g.other, 0, sizeof(uint32_t) * 4, s);
+        P.grid_cur = g;
+        P.grid_prev = prev.g;
+        P.prev_valid = st->grid_prev_valid && prev.g.checksums ? 1u : 0u;
+        P.reuse = 1;
+        P.max_m = prm->restir_max_m;
+    } else {
+        st->grid_prev_valid = false;  // TestRenderer.cpp:495-498 drops the grids when reuse is off
+    }
     if (!(prm->flags & S2_FLAG_ACCUMULATE)) {
         cudaMemsetAsync(st->total, 0, sizeof(float4) * pixels, s);
         st->accumulated_spp = 0;
@@ -231,6 +296,15 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         k_wave_finish<<<1, 32, 0, s>>>(P);
         k_reduce<<<(pixels + 255) / 256, 256, 0, s>>>(P, st->total);
         launches += 3;
+    }
+    if (reuse) {
+        // GpuHashGrid::build (GpuHashGrid.cpp:84-111), then this grid becomes the previous one
+        const HashGridDev& g = st->grid[st->grid_cur].g;
+        k_hg_compute_indices<<<(g.cell_count + 255) / 256, 256, 0, s>>>(g);
+        k_hg_swizzle<<<(g.max_size + 255) / 256, 256, 0, s>>>(g);
+        launches += 2;
+        st->grid_cur ^= 1u;
+        st->grid_prev_valid = true;
     }
     launches += 1;  // resolve
     st->accumulated_spp += prm->spp;
@@ -356,6 +430,8 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
+    if (prm->flags & S2_FLAG_RESTIR_REUSE)
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE is supported by s2_render only");
     cudaSetDevice(ctx->device);
     std::vector<ViewEntry> ve(nviews);
     std::vector<uint32_t> layout;

@@ -151,3 +151,21 @@ S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, f
     r.gn = unpack_normal(r.ng);
     return r;
 }
+
+// makeTriangleShadingData from an object-space position (shading_data.hlsli:153-173): the
+// barycentrics are recovered from the position (used for vertices stored in the hash grid).
+S2D SD make_shading_local(const DevScene& s, uint32_t inst, uint32_t prim, float3 lp, bool shading_normals) {
+    const uint2 id = s.instances[inst];
+    const VInfo vi = load_vinfo(s, id.y & 0xffffu);
+    const uint3 tri = load_triangle_indices(s.vbufs[vi_index_buffer(vi)], vi_index_offset(vi), vi_index_stride(vi), prim);
+    const uint8_t* pb = s.vbufs[vi_position_buffer(vi)];
+    const uint32_t po = vi_position_offset(vi), ps = vi_position_stride(vi);
+    const float3 v0 = load_f3(pb, po, ps, tri.x), v1 = load_f3(pb, po, ps, tri.y), v2 = load_f3(pb, po, ps, tri.z);
+    const float3 e1 = v1 - v0, e2 = v2 - v0, pv = lp - v0;
+    const float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(pv, e1), d21 = dot(pv, e2);
+    const float den = d00 * d11 - d01 * d01;
+    const float b1 = (d11 * d20 - d01 * d21) / den, b2 = (d00 * d21 - d01 * d20) / den;
+    SD r = make_shading(s, inst, prim, b1, b2, shading_normals);
+    r.pos = xform_point(s.transforms + 3 * (size_t)inst, lp);
+    return r;
+}

@@ -51,10 +51,69 @@ S2D AovTarget aov_target(const PTParams& P, uint32_t slot, uint32_t meta) {
 
 struct ShadowOut { float3 o, d, c; float tmax; bool valid; };
 
-// One NEE connection: plain light sample, or RIS over restir_m candidates.
+// A light sample evaluated at one vertex: ReservoirSampleDataDI (testrenderer.slang:568-606).
+struct DISample {
+    float4 rnd;        // the sample (its four random numbers)
+    float src_pdf;     // light-sampling pdf (area measure, or solid angle for the environment)
+    float wtoa;        // cos_light / d^2 (1 for the environment)
+    float mis;         // MIS weight against BSDF sampling
+    float dist;
+    float3 contrib;    // f * Le (shading-normal corrected)
+    float3 dir;
+    S2D float target() const { return luminance(contrib) * wtoa; }
+};
+
+template <bool LAMBERT>
+S2D DISample eval_di(const DevScene& s, const Mat& m, const SD& sd, float3 in, float4 x, bool sn, float cp) {
+    DISample c;
+    c.rnd = x; c.contrib = f3(0.f); c.wtoa = 0.f; c.mis = 0.f; c.dist = 0.f; c.dir = f3(0.f);
+    const Illum r = sample_illum(s, x, sd.pos, sn);
+    c.src_pdf = r.pdf;
+    if (luminance(r.radiance) > 0.f && r.pdf > 0.f) {
+        const float3 out = sd.to_local(r.dir);
+        float3 f; float fwd, rev;
+        bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
+        f = f * sd.snc(in, out);
+        fwd *= cp;
+        c.contrib = f * r.radiance;
+        c.wtoa = r.finite ? r.cos_light / pow2(r.dist) : 1.f;
+        const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
+        c.mis = mis_w(r.pdf, fwd / AtoW);
+        c.dist = r.dist;
+        c.dir = r.dir;
+    }
+    return c;
+}
+
+// ReservoirReuse (testrenderer.slang:608-663): combines the current reservoir with a stored one
+// (q) with pairwise power-heuristic MIS over the two domains' target pdfs.
+template <bool LAMBERT>
+S2D void reservoir_reuse(const PTParams& P, const Mat& m, const SD& sd, float3 in, float cp, const ReservoirRecord& q,
+                         DISample& cur, float& iw, float& M, Rng& rng, bool sn) {
+    const DevScene& s = P.scene;
+    const DISample nw = eval_di<LAMBERT>(s, m, sd, in, q.rnd, sn, cp);  // q's sample in the current domain
+    float phat_q = 0.f;                                                 // current sample in q's domain
+    {
+        const SD sdq = make_shading_local(s, q.instance, q.primitive, q.local_pos, sn);
+        const Mat mq = load_material(s, sdq.mat, sdq.uv);
+        const float cpq = (P.flags & S2F_NO_RR) ? 1.f : cont_prob(mq);
+        const DISample cq = eval_di<LAMBERT>(s, mq, sdq, q.local_dir_in, cur.rnd, sn, cpq);
+        if (cq.target() > 0.f) phat_q = cq.target();
+    }
+    const float m0 = mis_w(M * cur.target(), q.M * phat_q);
+    const float m1 = mis_w(q.M * q.target_pdf, M * nw.target());
+    const float w0 = m0 * cur.target() * iw;
+    const float w1 = m1 * nw.target() * q.W;
+    M += q.M;
+    const float total = w0 + w1;
+    if (rng.next_float().x * total <= w1) cur = nw;
+    iw = cur.target() > 0.f ? total / cur.target() : 0.f;
+}
+
+// One NEE connection: plain light sample, or RIS over restir_m candidates (+ hash-grid reuse).
 template <bool LAMBERT, bool RESTIR>
 S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, float3 in, float3 thr, Rng& rng, uint32_t len,
-                               bool sn) {
+                               bool sn, uint32_t inst, uint32_t prim) {
     ShadowOut so;
     so.valid = false;
     const DevScene& s = P.scene;
@@ -62,41 +121,58 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
     float3 dir, contrib;
     float dist, w;
     if (RESTIR) {
-        float best_t = 0.f, best_wtoa = 0.f, best_mis = 0.f, best_dist = 0.f, wsum = 0.f;
-        float3 best_c = f3(0.f), best_d = f3(0.f);
+        // SampleIlluminationReSTIR (testrenderer.slang:665-726)
+        DISample best;
+        best.rnd = make_float4(0.f, 0.f, 0.f, 0.f); best.contrib = f3(0.f); best.wtoa = 0.f; best.mis = 0.f;
+        best.dist = 0.f; best.dir = f3(0.f); best.src_pdf = 0.f;
+        float wsum = 0.f;
         for (uint32_t i = 0; i < P.restir_m; ++i) {
-            const float4 x = rng.next_float();
-            const Illum r = sample_illum(s, x, sd.pos, sn);
-            float target = 0.f, wtoa = 0.f, misw = 0.f;
-            float3 c = f3(0.f);
-            if (luminance(r.radiance) > 0.f && r.pdf > 0.f) {
-                const float3 out = sd.to_local(r.dir);
-                float3 f; float fwd, rev;
-                bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
-                f = f * sd.snc(in, out);
-                fwd *= cp;
-                c = f * r.radiance;
-                wtoa = r.finite ? r.cos_light / pow2(r.dist) : 1.f;
-                const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
-                misw = mis_w(r.pdf, fwd / AtoW);
-                target = luminance(c) * wtoa;
-            }
+            const DISample c = eval_di<LAMBERT>(s, m, sd, in, rng.next_float(), sn, cp);
+            const float target = c.target();
             if (target <= 0.f) continue;
-            const float risw = target / r.pdf;
+            const float risw = target / c.src_pdf;
             wsum += risw;
-            const float4 u = rng.next_float();
-            if (u.x <= risw / wsum) {
-                best_t = target; best_wtoa = wtoa; best_mis = misw; best_c = c; best_d = r.dir; best_dist = r.dist;
+            if (rng.next_float().x <= risw / wsum) best = c;
+        }
+        float iw = best.target() > 0.f ? wsum / ((float)P.restir_m * best.target()) : 0.f;
+        if (P.reuse) {
+            float M = (float)P.restir_m;
+            if (P.prev_valid) {
+                const float4 dr = rng.next_float();
+                const float2 disc = sample_concentric_disc(dr.x, dr.y);
+                const float csz = hg_cell_size(P.grid_prev, sd.pos);
+                const float3 qp = sd.pos + sd.to_world(f3(disc.x * csz, disc.y * csz, 0.f));
+                const uint32_t cell = hg_find_cell<false>(P.grid_prev, qp, hg_cell_size(P.grid_prev, qp));
+                if (cell != 0xffffffffu) {
+                    const uint32_t count = P.grid_prev.cell_counters[cell];
+                    if (count > 0) {
+                        const uint32_t off = P.grid_prev.indices[cell];
+                        const uint32_t k = rng.next().x % count;
+                        const ReservoirRecord q = P.grid_prev.data[P.grid_prev.data_indices[off + k]];
+                        reservoir_reuse<LAMBERT>(P, m, sd, in, cp, q, best, iw, M, rng, sn);
+                    }
+                }
+            }
+            if (iw > 0.f) {
+                ReservoirRecord rec;
+                rec.local_pos = xform_point(s.inv_transforms + 3 * (size_t)inst, sd.pos);
+                rec.instance = inst;
+                rec.primitive = prim;
+                rec.rnd = best.rnd;
+                rec.target_pdf = best.target();
+                rec.W = iw;
+                rec.M = fminf(M, P.max_m * (float)P.restir_m);
+                rec.local_dir_in = in;
+                rec.pad = 0.f;
+                hg_append(P.grid_cur, sd.pos, rec);
             }
         }
-        if (!(best_t > 0.f)) return so;
-        float iw = wsum / ((float)P.restir_m * best_t);
         if (!(iw > 0.f)) return so;
-        iw *= best_wtoa;
-        contrib = thr * best_c * iw;
-        w = best_mis;
-        dir = best_d;
-        dist = best_dist;
+        iw *= best.wtoa;  // 1/pdfA -> 1/pdfW
+        contrib = thr * best.contrib * iw;
+        w = best.mis;
+        dir = best.dir;
+        dist = best.dist;
     } else {
         if (len + 1 < P.min_len) {  // shorter than minPathLength: advance the stream by one draw only
             rng.skip();
@@ -233,7 +309,7 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                 }
                 if (len < P.max_len && any_pos(m.base())) {
                     const bool sing = mat_singular<LAMBERT>(m);
-                    if (!sing && nee) so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn);
+                    if (!sing && nee) so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim);
                     const float cp = fminf(1.f, cont_prob(m));
                     bool cont = true;
                     if (!(P.flags & S2F_NO_RR)) {

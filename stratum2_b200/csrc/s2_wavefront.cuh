@@ -13,6 +13,7 @@
 // accumulator element has exactly one writer per kernel and needs no atomics: the summation
 // order is fixed and results are deterministic.
 #pragma once
+#include "s2_hashgrid.cuh"
 #include "s2_lights.cuh"
 #include "s2_traverse.cuh"
 
@@ -82,6 +83,10 @@ struct PTParams {
     unsigned long long total_paths;
     uint32_t capacity;
     unsigned long long* stream_state; // [0] next path id, [1] regen base, [2] regen count, [3] done
+    // ReSTIR DI reuse through the world-space hash grids (S2_FLAG_RESTIR_REUSE)
+    HashGridDev grid_cur, grid_prev;
+    uint32_t reuse, prev_valid;
+    float max_m;
 };
 
 // fixed-point scale of the batched accumulators: integer sums are independent of the order of the
@@ -111,6 +116,7 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_REF_ENV_MIS (1u << 5)
 #define S2F_NO_RR (1u << 6)
 #define S2F_NO_SN (1u << 8)
+#define S2F_REUSE (1u << 11)
 
 constexpr int kTravBlock = 128;
 

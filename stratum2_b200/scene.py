@@ -128,6 +128,7 @@ class Scene:
         self.material_data = bytearray()
         self.materials: list[Material] = []
         self.material_addresses: list[int] = []
+        self._material_at: dict[int, Material] = {}
         self.instances: list[tuple[int, int]] = []
         self.primitive_counts: list[int] = []
         self.transforms: list[np.ndarray] = []
@@ -166,6 +167,7 @@ class Scene:
         self.material_data += m.pack()
         self.materials.append(m)
         self.material_addresses.append(addr)
+        self._material_at[addr] = m
         return addr
 
     def add_instance(self, mesh: Mesh, material_address: int, transform=None) -> int:
@@ -178,7 +180,7 @@ class Scene:
         self.primitive_counts.append(mesh.primitive_count)
         self.transforms.append(transform)
         self.instance_material.append(material_address)
-        m = self.materials[self.material_addresses.index(material_address)]
+        m = self._material_at[material_address]
         if m.has_emission():
             self.instance_light_map.append(len(self.light_instance_map))
             self.light_instance_map.append(idx)

@@ -8,6 +8,8 @@ All scenes are generated from fixed seeds with numpy; nothing is read from disk.
       level-5 icospheres (20,480 triangles each) under seeded transforms; GLTF metallic-roughness
       materials; 512x256 procedural HDR sky with a 5e3 sun lobe over a 0.5 degree cone;
       1920x1080, 64 spp, path length 3..12 with Russian roulette)
+  terrain_scene(..., emissive_triangles=100_000) (the many-lights form: small one-sided emissive
+      triangles hovering over the terrain, one instance each, power lognormal(0, 2))
 """
 from __future__ import annotations
 
@@ -150,9 +152,48 @@ def sky_image(width: int = 512, height: int = 256, sun_dir=(0.3, 0.8, 0.2), sun_
     return img.astype(np.float32)
 
 
+def add_emissive_triangles(s: Scene, rng: np.random.Generator, hgt: np.ndarray, n: int, sigma: float, power: float,
+                           height=(0.02, 0.08), edge_range=(0.01, 0.03)):
+    """`n` small emissive triangles (edge in `edge_range`) hovering `height` above the heightfield
+    `hgt` (spanning [-1,1] in x and z), each its own instance and material, emitting downwards
+    (front face tilted up to 60 degrees from -y).  Emitted power (radiance x area x pi) is
+    `power` x lognormal(0, sigma) with a random tint."""
+    grid = hgt.shape[0]
+    # canonical triangle in the xz plane; its front face (cross(v0 - v2, v1 - v2)) points to -y
+    tri = np.array([[0.0, 0.0, 0.577], [0.5, 0.0, -0.289], [-0.5, 0.0, -0.289]], np.float32)
+    nrm = np.cross(tri[0] - tri[2], tri[1] - tri[2])
+    if nrm[1] > 0:
+        tri = tri[[0, 2, 1]]
+    mesh = s.add_mesh(tri, np.array([[0, 1, 2]], np.uint32))
+    area1 = 0.5 * np.linalg.norm(np.cross(tri[0] - tri[2], tri[1] - tri[2]))
+    xz = rng.uniform(-0.95, 0.95, size=(n, 2))
+    gi = np.clip(np.round((xz + 1) / 2 * (grid - 1)).astype(int), 0, grid - 1)
+    y = hgt[gi[:, 1], gi[:, 0]] + rng.uniform(height[0], height[1], n)
+    edge = rng.uniform(edge_range[0], edge_range[1], n)
+    tilt = np.arccos(rng.uniform(0.5, 1.0, n))
+    azim = rng.uniform(0, 2 * np.pi, n)
+    spin = rng.uniform(0, 2 * np.pi, n)
+    pw = power * rng.lognormal(0.0, sigma, n)
+    tint = rng.uniform(0.5, 1.0, size=(n, 3))
+    for k in range(n):
+        cs, sn = math.cos(spin[k]), math.sin(spin[k])
+        r_spin = np.array([[cs, 0, sn], [0, 1, 0], [-sn, 0, cs]])
+        ax = np.array([math.cos(azim[k]), 0.0, math.sin(azim[k])])   # tilt about a horizontal axis
+        ct, st = math.cos(tilt[k]), math.sin(tilt[k])
+        K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+        r_tilt = np.eye(3) + st * K + (1 - ct) * (K @ K)
+        rot = r_tilt @ r_spin
+        area = area1 * edge[k] ** 2
+        radiance = pw[k] / (area * math.pi) * tint[k] / tint[k].max()
+        m = s.add_material(Material(base_color=(0, 0, 0), emission=tuple(radiance)))
+        s.add_instance(mesh, m, transform_trs((xz[k, 0], y[k], xz[k, 1]), rot, (edge[k],) * 3))
+
+
 def terrain_scene(seed: int = 2, grid: int = 1024, spheres: int = 64, sphere_level: int = 5, width: int = 1920,
                   height: int = 1080, spp: int = 64, tiles: int = 16, area_lights: int = 0,
-                  sun_radiance: float = 5e3, sun_cone_degrees: float = 0.5) -> Workload:
+                  sun_radiance: float = 5e3, sun_cone_degrees: float = 0.5, emissive_triangles: int = 0,
+                  emissive_sigma: float = 2.0, emissive_power: float = 2e-3, sky_scale: float = 1.0,
+                  emissive_height=(0.02, 0.08), emissive_edge=(0.01, 0.03)) -> Workload:
     rng = np.random.default_rng(seed)
     s = Scene()
     hgt = value_noise(rng, grid)
@@ -191,7 +232,10 @@ def terrain_scene(seed: int = 2, grid: int = 1024, spheres: int = 64, sphere_lev
         p, i = quad(c + (-h, 0, -h), c + (h, 0, -h), c + (h, 0, h), c + (-h, 0, h))
         lm = s.add_material(Material(base_color=(0, 0, 0), emission=tuple(rng.uniform(5, 20, 3))))
         s.add_instance(s.add_mesh(p, i), lm)
-    s.set_environment((1.0, 1.0, 1.0), s.add_image(sky_image(sun_radiance=sun_radiance, sun_cone_degrees=sun_cone_degrees)))
+    if emissive_triangles:
+        add_emissive_triangles(s, rng, hgt, emissive_triangles, emissive_sigma, emissive_power, emissive_height,
+                               emissive_edge)
+    s.set_environment((sky_scale,) * 3, s.add_image(sky_image(sun_radiance=sun_radiance, sun_cone_degrees=sun_cone_degrees)))
     pos = (0.0, 0.9, 1.9)
     view = make_view(pos, width, height, 45.0, look_at_rotation(pos, (0.0, 0.0, 0.0)))
     return Workload(s, view, width, height, spp, 3, 12, False, f"terrain{grid}_{width}x{height}")

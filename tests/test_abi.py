@@ -40,7 +40,7 @@ def test_struct_sizes_match_header():
 
 def test_calls_that_need_no_gpu():
     lib = _abi.lib()
-    assert lib.s2_get_abi_version() == 1
+    assert lib.s2_get_abi_version() == _abi.ABI_VERSION == 2
     assert lib.s2_last_error(None) == b"null context"
     p = _abi.S2RenderParams()
     lib.s2_default_render_params(p)
