@@ -35,6 +35,8 @@ MIN_LEN, MAX_LEN = 3, 12
 WORKLOAD = ("terrain 1024^2 grid (2.09M tris) + 64 icospheres (1.31M tris), GLTF MR materials, 512x256 HDR sky "
             "with 5e3 sun; 1920x1080, 64 spp, path length 3..12, Russian roulette")
 NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES = 80, 48, 32, 16
+GOLDEN_CFG2 = ROOT / "tests" / "golden" / "cfg2_1920x1080_subset30_fp64_262144spp.npz"
+RELMSE_TARGET = 0.01
 
 
 def peaks() -> dict:
@@ -263,6 +265,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                     "h2d_bytes_per_step": int(C_sizeof_view_params()),
                     "d2h_bytes_per_step": int(W * H * (16 + 16 + 8 + 16 + 8 + 8))},
             "clocks": ck}
+    if world == 1 and not args.no_quality:
+        line["batched_16_views"] = batched_line(dev, args.steps)
+        if GOLDEN_CFG2.exists():
+            line["time_to_relmse_0.01"] = {
+                "plain": time_to_quality(dev, wl, False, 50000, max_spp=args.quality_spp),
+                "batched": time_to_quality(dev, wl, True, 50000, max_spp=args.quality_spp),
+                "reference_image": f"FP64 oracle, {int(np.load(GOLDEN_CFG2)['spp'])} spp, 64x36 pixel subset (stride 30)",
+                "note": "GPU time of progressive 128-spp calls; radiance cache not built yet"}
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         osc = cpu_oracle(wl)
@@ -272,6 +282,87 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                 "sample": f"FP32 oracle, every {c['stride']}th pixel ({c['pixels']} pixels) x {SPP} spp, "
                                           f"{c['seconds']:.1f} s"}
     print(json.dumps(line), flush=True)
+
+
+def batched_views(seed: int = 7, n: int = 16):
+    """16 camera views of the terrain with resolutions log-uniform between 256x256 and 1920x1080."""
+    from stratum2_b200.scene import look_at_rotation, make_view
+    rng = np.random.default_rng(seed)
+    views = []
+    for _ in range(n):
+        w = int(round(np.exp(rng.uniform(np.log(256), np.log(1920)))))
+        h = int(round(np.exp(rng.uniform(np.log(256), np.log(1080)))))
+        pos = (rng.uniform(-0.9, 0.9), rng.uniform(0.5, 1.2), rng.uniform(1.2, 2.0))
+        views.append(make_view(pos, w, h, 45.0, look_at_rotation(pos, (0.0, 0.0, 0.0))))
+    return views
+
+
+def time_to_quality(dev, wl, batched: bool, seed0: int, chunk: int = 128, max_spp: int = 2048) -> dict:
+    """GPU milliseconds of progressive rendering (`chunk` spp per call, S2_FLAG_ACCUMULATE) until the
+    relMSE (eps 1e-2) of the 64x36 pixel subset (x = 15 + 30 i, y = 15 + 30 j) against the FP64
+    oracle image reaches 0.01, or until `max_spp`.  The oracle image's own noise (its variance of
+    the mean, relMSE ~1e-3 at 262144 spp) is subtracted.  When the budget ends first, the time is
+    extrapolated with relMSE proportional to 1/spp (an unbiased estimator's variance), and marked so.
+    `batched` uses the streaming entry point s2_render_views."""
+    import torch
+
+    from stratum2_b200 import _abi
+    from stratum2_b200.metrics import relmse
+    g = np.load(GOLDEN_CFG2)
+    ref = g["mean"].astype(np.float64)
+    noise = float(np.mean(g["var_of_mean"].astype(np.float64) / (ref ** 2 + 1e-2)))
+    x0, y0, st = int(g["rect"][0]), int(g["rect"][1]), int(g["stride"])
+    W, H = wl.width, wl.height
+    rad = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+    total_ms, spp, rm, curve = 0.0, 0, float("inf"), []
+    while spp < max_spp:
+        p = params(dev, chunk, seed0 + spp, _abi.FLAG_ACCUMULATE if spp else 0)
+        s = dev.render_views_device([wl.view], p, [aovs]) if batched else dev.render_device(wl.view, p, aovs)
+        total_ms += s.gpu_ms
+        spp += chunk
+        sub = rad[y0::st, x0::st, :3].double().cpu().numpy()[:ref.shape[0], :ref.shape[1]]
+        rm = relmse(sub, ref) - noise
+        if spp in (256, 1024, 4096) or rm <= RELMSE_TARGET:
+            curve.append([spp, round(total_ms, 1), round(rm, 5)])
+        if rm <= RELMSE_TARGET:
+            break
+    reached = rm <= RELMSE_TARGET
+    return {"ms": total_ms if reached else total_ms * rm / RELMSE_TARGET, "measured_to_target": reached,
+            "spp": spp, "gpu_ms_run": total_ms, "relmse": rm, "curve_spp_ms_relmse": curve}
+
+
+def batched_line(dev, steps: int, spp: int = 8) -> dict:
+    """The 16-view batched form in one s2_render_views call per step (device AOV buffers)."""
+    import torch
+
+    from stratum2_b200 import _abi
+    views = batched_views()
+    bufs, outs = [], []
+    for v in views:
+        w, h = v.image_max[0] - v.image_min[0], v.image_max[1] - v.image_min[1]
+        t = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+        bufs.append(t)
+        outs.append(_abi.S2Aovs(t.data_ptr(), None, None, None, None, None))
+    dev.render_views_device(views, params(dev, spp, 77), outs)  # warm-up (builds the graphs)
+    ms, rays, paths, launches = 0.0, 0, 0, 0
+    for k in range(steps):
+        s = dev.render_views_device(views, params(dev, spp, 100 + k * spp), outs)
+        ms += s.gpu_ms
+        rays += s.extension_rays + s.shadow_rays
+        paths += s.paths
+        launches += s.kernel_launches
+    # the same views one s2_render call each, for comparison
+    ms_seq, rays_seq = 0.0, 0
+    for k in range(steps):
+        for v, o in zip(views, outs):
+            s = dev.render_device(v, params(dev, spp, 100 + k * spp), o)
+            ms_seq += s.gpu_ms
+            rays_seq += s.extension_rays + s.shadow_rays
+    pixels = sum((v.image_max[0] - v.image_min[0]) * (v.image_max[1] - v.image_min[1]) for v in views)
+    return {"views": len(views), "pixels": int(pixels), "spp": spp, "steps": steps,
+            "mrays_per_s": rays / ms / 1e3, "mpaths_per_s": paths / ms / 1e3, "ms_per_step": ms / steps,
+            "gpu_launches": int(launches), "per_view_calls_mrays_per_s": rays_seq / ms_seq / 1e3}
 
 
 def C_sizeof_view_params() -> int:
@@ -288,6 +379,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-quality", action="store_true", help="skip the batched and time-to-relMSE measurements")
+    ap.add_argument("--quality-spp", type=int, default=2048,
+                    help="sample budget of the time-to-relMSE runs (extrapolated beyond it)")
     ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",
                     help="render one frame of the workload with SPP samples and exit (profiling)")
     args = ap.parse_args()

@@ -162,6 +162,8 @@ typedef struct S2View {
                                                   call's world-space hash grid and store this call's
                                                   reservoirs for the next call (testrenderer.slang:
                                                   608-726).  Results depend on atomic append order. */
+#define S2_FLAG_ALPHA_TEST_OFF      (1u << 12) /* disable gAlphaTest (on in the reference) */
+#define S2_FLAG_NORMAL_MAPS_OFF     (1u << 13) /* disable gNormalMaps (on in the reference) */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */

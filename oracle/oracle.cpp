@@ -513,7 +513,24 @@ template <class R> bool isect_tri(const WRay<R>& r, const R* v, R tmax, R& t_out
 
 template <class R> struct Hit { R t; uint32_t tri; R b1, b2; bool hit; };
 
-template <class R> Hit<R> trace(const Scene<R>& s, const V3<R>& o, const V3<R>& d, R tmin, R tmax, bool anyhit) {
+// Candidate test of a non-opaque triangle (intersection.hlsli:125-146): the alpha-mask image of
+// the instance's material (index and cutoff at bytes 48/52, material.hlsli:72-76) at the hit's
+// texture coordinate, level 0, red channel, >= cutoff.  Materials without a mask always pass.
+template <class R> bool alpha_pass(const Scene<R>& s, uint32_t inst, uint32_t prim, R b1, R b2) {
+    const uint32_t mat = s.inst_word0[inst] >> 4;
+    const uint32_t mask = s.u32(s.mat, mat + 48);
+    if (mask >= s.images.size()) return true;
+    const float cutoff = s.f32(s.mat, mat + 52);
+    uint32_t idx[3]; s.tri_indices(inst, prim, idx);
+    R t0[2] = {0, 0}, t1[2] = {0, 0}, t2[2] = {0, 0};
+    if (s.attr2(inst, idx[0], t0)) { s.attr2(inst, idx[1], t1); s.attr2(inst, idx[2], t2); }
+    const R u = t0[0] + (t1[0] - t0[0]) * b1 + (t2[0] - t0[0]) * b2;
+    const R v = t0[1] + (t1[1] - t0[1]) * b1 + (t2[1] - t0[1]) * b2;
+    return s.images[mask].sample(u, v).x >= (R)cutoff;
+}
+
+template <class R> Hit<R> trace(const Scene<R>& s, const V3<R>& o, const V3<R>& d, R tmin, R tmax, bool anyhit,
+                                bool alpha_test = true) {
     Hit<R> h{tmax, 0xffffffffu, 0, 0, false};
     if (s.nodes.empty() || s.tid.empty()) return h;
     const WRay<R> r = make_wray(o, d, tmin);
@@ -539,6 +556,7 @@ template <class R> Hit<R> trace(const Scene<R>& s, const V3<R>& o, const V3<R>& 
                 R t, b1, b2;
                 if (isect_tri(r, &s.tv[9 * (size_t)ti], h.t, t, b1, b2)) {
                     const uint32_t inst = s.tid[ti].inst, prim = s.tid[ti].prim;
+                    if (alpha_test && !alpha_pass(s, inst, prim, b1, b2)) continue;
                     if (anyhit) { h.t = t; h.tri = ti; h.b1 = b1; h.b2 = b2; h.hit = true; return h; }
                     if (t < h.t || inst < best_inst || (inst == best_inst && prim < best_prim)) {
                         h.t = t; h.tri = ti; h.b1 = b1; h.b2 = b2; h.hit = true; best_inst = inst; best_prim = prim;

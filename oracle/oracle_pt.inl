@@ -17,7 +17,8 @@ namespace orc {
 
 constexpr uint32_t FLAG_PIXEL_JITTER = 1u << 0, FLAG_LAMBERTIAN = 1u << 1, FLAG_PCG32 = 1u << 2, FLAG_NO_NEE = 1u << 3,
                    FLAG_RESTIR = 1u << 4, FLAG_REF_ENV_MIS = 1u << 5, FLAG_NO_RR = 1u << 6, FLAG_NO_SHADING_NORMALS = 1u << 8,
-                   FLAG_RESTIR_REUSE = 1u << 11;
+                   FLAG_RESTIR_REUSE = 1u << 11, FLAG_NO_ALPHA = 1u << 12,
+                   FLAG_NO_NORMAL_MAPS = 1u << 13;
 
 template <class R> R un8(uint32_t w, int shift) { return R((w >> shift) & 0xffu) / R(255); }
 inline uint32_t pk8(double v) { v = std::min(std::max(v, 0.0), 1.0); return (uint32_t)std::floor((float)v * 255.f + 0.5f); }
@@ -219,7 +220,24 @@ template <class R> struct Tracer {
 
     V3<R> sample_image(uint32_t img, R u, R v) const { return s.images[img].sample(u, v); }
 
-    // LoadMaterial (material.hlsli:15-46)
+    // ApplyNormalMap (material.hlsli:78-105): bump image index, strength and channel count at
+    // bytes 36..47 of the material record; bitangent sign +1
+    void normal_map(SD<R>& sd) const {
+        const uint32_t img = s.u32(s.mat, sd.mat + 36), channels = s.u32(s.mat, sd.mat + 44);
+        const R scale = (R)s.f32(s.mat, sd.mat + 40);
+        if (img >= s.images.size() || !(scale > 0)) return;
+        R a;
+        const V3<R> t = s.images[img].sample(sd.u, sd.v, &a);
+        V3<R> bump = channels == 2 ? V3<R>(t.x, t.y, 1) : t;
+        bump.x = (bump.x * 2 - 1) * scale;
+        bump.y = -(bump.y * 2 - 1) * scale;
+        const V3<R> n = normalize(sd.t * bump.x + cross(sd.n, sd.t) * bump.y + sd.n * bump.z);
+        const V3<R> tg = normalize(sd.t - n * dot(n, sd.t));
+        sd.ns = pack_normal(n);
+        sd.tg = pack_normal(tg);
+        sd.unpack();
+    }
+
     // makeTriangleShadingData from an object-space position (shading_data.hlsli:153-173)
     SD<R> shading_local(uint32_t inst, uint32_t prim, const V3<R>& lp) const {
         uint32_t idx[3]; s.tri_indices(inst, prim, idx);
@@ -232,6 +250,7 @@ template <class R> struct Tracer {
         return r;
     }
 
+    // LoadMaterial (material.hlsli:15-46)
     Mat<R> material(uint32_t addr, R u, R v) const {
         Mat<R> m;
         for (int k = 0; k < 4; ++k) m.w[k] = s.u32(s.mat, addr + 4 * k);
@@ -622,7 +641,7 @@ template <class R> struct Tracer {
 
     bool occluded(const V3<R>& o, const V3<R>& d, R tmax) {
         shadow_rays++;
-        return trace(s, o, d, R(0), tmax, true).hit;
+        return trace(s, o, d, R(0), tmax, true, !(p.flags & FLAG_NO_ALPHA)).hit;
     }
 
     // ---------------------------------------------------------------- camera path
@@ -669,7 +688,7 @@ template <class R> struct Tracer {
         while (len + 1 <= p.max_len) {
             // TraceRay (testrenderer.slang:1026-1058)
             ext_rays++;
-            const Hit<R> h = trace(s, org, dir, R(0), std::numeric_limits<R>::infinity(), false);
+            const Hit<R> h = trace(s, org, dir, R(0), std::numeric_limits<R>::infinity(), false, !(p.flags & FLAG_NO_ALPHA));
             len++;
             const uint32_t inst = h.hit ? s.tid[h.tri].inst : 0xffffffffu;
             const uint32_t prim = h.hit ? s.tid[h.tri].prim : 0xffffffffu;
@@ -695,6 +714,7 @@ template <class R> struct Tracer {
                 break;
             }
             SD<R> sd = shading(inst, prim, h.b1, h.b2);
+            if (!(p.flags & FLAG_NO_NORMAL_MAPS)) normal_map(sd);
             isect_dist = (R)half_round((float)h.t);
             isect_pdfa = (R)half_round((float)light_pdfa(inst, sd.area));
             const Mat<R> m = material(sd.mat, sd.u, sd.v);
@@ -790,7 +810,8 @@ template <class R> struct Tracer {
         const DI nw = eval_di(m, sd, in, q.rnd, cp);
         R phat_q = 0;
         {
-            const SD<R> sdq = shading_local(q.inst, q.prim, q.local_pos);
+            SD<R> sdq = shading_local(q.inst, q.prim, q.local_pos);
+            if (!(p.flags & FLAG_NO_NORMAL_MAPS)) normal_map(sdq);
             const Mat<R> mq = material(sdq.mat, sdq.u, sdq.v);
             const R cpq = (p.flags & FLAG_NO_RR) ? R(1) : cont_prob(mq);
             const DI cq = eval_di(mq, sdq, q.dir_in, cur.x, cpq);

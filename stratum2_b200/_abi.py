@@ -39,6 +39,8 @@ FLAG_SHADING_NORMALS_OFF = 1 << 8
 FLAG_PROFILE_KERNELS = 1 << 9
 FLAG_COUNT_FETCHES = 1 << 10
 FLAG_RESTIR_REUSE = 1 << 11
+FLAG_ALPHA_TEST_OFF = 1 << 12
+FLAG_NORMAL_MAPS_OFF = 1 << 13
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [

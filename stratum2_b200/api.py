@@ -161,6 +161,16 @@ class Device:
                                               C.cast(outs, C.c_void_p), 1, C.byref(st)))
         return [RenderResult(*r, st) for r in results], st
 
+    def render_views_device(self, views, params: _abi.S2RenderParams, outs) -> _abi.S2RenderStats:
+        """s2_render_views with caller-owned device AOV buffers (one S2Aovs per view)."""
+        n = len(views)
+        arr = (_abi.S2View * n)(*views)
+        oarr = (_abi.S2Aovs * n)(*outs)
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_views(self._h, C.cast(arr, C.c_void_p), n, C.byref(params),
+                                              C.cast(oarr, C.c_void_p), 0, C.byref(st)))
+        return st
+
     def render_device(self, view, params: _abi.S2RenderParams, aovs: _abi.S2Aovs) -> _abi.S2RenderStats:
         st = _abi.S2RenderStats()
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(params), C.byref(aovs), 0, C.byref(st)))

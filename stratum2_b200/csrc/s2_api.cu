@@ -249,7 +249,19 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     // ---- flatten mesh instances to world-space triangles (host copy for the BVH build)
     ctx->tri_v0.clear(); ctx->tri_v1.clear(); ctx->tri_v2.clear(); ctx->tri_inst.clear(); ctx->tri_prim.clear();
     ctx->inst_tri_offset.assign(ni, 0);
+    ctx->inst_alpha.assign(ni, 0);
     std::vector<uint32_t> prim_counts(ni, 0);
+    std::vector<float> image_min_red(d->image_count, NAN);  // computed on first use
+    auto min_red = [&](uint32_t k) {
+        if (std::isnan(image_min_red[k])) {
+            const S2Image& im = d->images[k];
+            float mn = INFINITY;
+            if (im.texels && im.channels >= 1)
+                for (size_t t = 0; t < (size_t)im.width * im.height; ++t) mn = std::min(mn, im.texels[t * im.channels]);
+            image_min_red[k] = mn;
+        }
+        return image_min_red[k];
+    };
     for (uint32_t i = 0; i < ni; ++i) {
         const uint32_t type = d->instances[2 * i] & 0xfu;
         const uint32_t data = d->instances[2 * i + 1];
@@ -272,6 +284,14 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
         const uint32_t mat_addr = d->instances[2 * i] >> 4;
         if ((uint64_t)mat_addr + S2_MATERIAL_RECORD_BYTES > d->material_bytes)
             return set_error(ctx, S2_ERR_INVALID, "instance " + std::to_string(i) + ": material address out of range");
+        {
+            // non-opaque when the alpha mask has texels below the cutoff (Material::alphaTest,
+            // Material.hpp:20, and the BLAS geometry flag, Scene.cpp:575)
+            uint32_t mask; float cutoff;
+            std::memcpy(&mask, (const uint8_t*)d->material_data + mat_addr + 48, 4);
+            std::memcpy(&cutoff, (const uint8_t*)d->material_data + mat_addr + 52, 4);
+            if (mask < d->image_count && !(min_red(mask) >= cutoff)) ctx->inst_alpha[i] = 1;
+        }
         uint32_t max_index = 0;
         for (uint32_t p = 0; p < prim_counts[i]; ++p) {
             bool ok = true;
@@ -430,6 +450,8 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
     BuildOutput out;
     std::string err;
     if (build_bvh8(in, bp, out, err) != 0) return set_error(ctx, S2_ERR_INVALID, "BVH build failed: " + err);
+    for (S2TriRecord& r : out.tris)
+        if (ctx->inst_alpha[r.instance]) r.flat_id |= S2_TRI_ALPHA_TESTED;
     cudaStreamSynchronize(ctx->stream);
     free_bufs(ctx->bvh_bufs);
     ctx->scene.nodes = (const uint4*)upload(ctx, ctx->bvh_bufs, out.nodes.data(), out.nodes.size());
@@ -455,7 +477,7 @@ namespace {
 constexpr int kTraceBlock = 128;
 
 template <bool ANYHIT, bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock) trace_kernel(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
+__global__ void __launch_bounds__(kTraceBlock) trace_kernel(const __grid_constant__ DevScene scene,
                                                            const S2Ray* __restrict__ rays, uint32_t n, S2Hit* __restrict__ hits,
                                                            uint2* __restrict__ counts, int* __restrict__ status) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTraceBlock];
@@ -466,7 +488,8 @@ __global__ void __launch_bounds__(kTraceBlock) trace_kernel(const uint4* __restr
     const TravRay r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w);
     TravHit h;
     TravCounters c{0, 0};
-    const bool ok = traverse<ANYHIT, COUNT>(r, b.w, nodes, tris, stack + threadIdx.x, kTraceBlock, h, c);
+    const bool ok = traverse<ANYHIT, COUNT>(r, b.w, scene.nodes, scene.tris, stack + threadIdx.x, kTraceBlock, h, c,
+                                            SceneAlphaTest{&scene, true});
     if (!ok) atomicOr(status, 1);
     S2Hit out;
     out.t = h.t;
@@ -499,11 +522,11 @@ int trace_impl(S2Context* ctx, const S2Ray* rays, uint32_t count, int anyhit, S2
     const dim3 grid((count + kTraceBlock - 1) / kTraceBlock);
     const bool counted = fetch_counts != nullptr;
     if (anyhit) {
-        if (counted) trace_kernel<true, true><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene.nodes, ctx->scene.tris, drays, count, dhits, dcounts, ctx->status_dev);
-        else trace_kernel<true, false><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene.nodes, ctx->scene.tris, drays, count, dhits, dcounts, ctx->status_dev);
+        if (counted) trace_kernel<true, true><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene, drays, count, dhits, dcounts, ctx->status_dev);
+        else trace_kernel<true, false><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene, drays, count, dhits, dcounts, ctx->status_dev);
     } else {
-        if (counted) trace_kernel<false, true><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene.nodes, ctx->scene.tris, drays, count, dhits, dcounts, ctx->status_dev);
-        else trace_kernel<false, false><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene.nodes, ctx->scene.tris, drays, count, dhits, dcounts, ctx->status_dev);
+        if (counted) trace_kernel<false, true><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene, drays, count, dhits, dcounts, ctx->status_dev);
+        else trace_kernel<false, false><<<grid, kTraceBlock, 0, ctx->stream>>>(ctx->scene, drays, count, dhits, dcounts, ctx->status_dev);
     }
     int rc = check_cuda(ctx, cudaGetLastError(), "trace kernel launch");
     int status = 0;

@@ -45,10 +45,14 @@ struct alignas(128) S2BvhNode {
 static_assert(sizeof(S2BvhNode) == 128, "node must fill one 128-byte line");
 
 // One triangle record = 48 bytes: world-space vertices, with the instance and primitive index
-// in the w components: {v0, instance}, {v1, primitive}, {v2, flattened triangle id}.
+// in the w components: {v0, instance}, {v1, primitive}, {v2, flattened triangle id}.  Bit 31 of
+// the flattened id marks triangles whose material has an alpha mask with texels below its cutoff
+// (the reference builds those as non-opaque geometry, Scene.cpp:575, and tests them in the ray
+// query, intersection.hlsli:125-146).
 struct alignas(16) S2TriRecord {
     float v0[3]; uint32_t instance;
     float v1[3]; uint32_t primitive;
     float v2[3]; uint32_t flat_id;
 };
 static_assert(sizeof(S2TriRecord) == 48, "triangle record is 48 bytes");
+#define S2_TRI_ALPHA_TESTED 0x80000000u

@@ -40,6 +40,7 @@ struct S2Context {
     std::vector<float> tri_v0, tri_v1, tri_v2;
     std::vector<uint32_t> tri_inst, tri_prim;
     std::vector<uint32_t> inst_tri_offset;  // flattened triangle base per instance
+    std::vector<uint8_t> inst_alpha;        // 1: the instance's triangles need the alpha test
 
     // device scene description (pointers into scene_bufs / bvh_bufs)
     DevScene scene{};

@@ -135,3 +135,30 @@ S2D float4 sample_image(const DevImage& im, float2 uv) {
                        a.z * w00 + b.z * w10 + c.z * w01 + d.z * w11,
                        a.w * w00 + b.w * w10 + c.w * w01 + d.w * w11);
 }
+
+// The candidate test of a non-opaque triangle (intersection.hlsli:125-146, gAlphaTest): the
+// material's alpha-mask image (getMaterialAlphaMask, material.hlsli:72-76: index and cutoff at
+// bytes 48 and 52 of the record) sampled at the hit's texture coordinate, level 0, red channel,
+// accepted when >= cutoff.  `on` false (S2_FLAG_ALPHA_TEST_OFF) accepts every triangle.
+struct SceneAlphaTest {
+    const DevScene* s;
+    bool on;
+    S2D bool operator()(uint32_t inst, uint32_t prim, float b1, float b2) const {
+        if (!on) return true;
+        const DevScene& sc = *s;
+        const uint32_t mat = sc.instances[inst].x >> 4;
+        const uint2 am = *(const uint2*)(sc.material_data + mat + 48);
+        if (am.x >= sc.image_count) return true;
+        const VInfo vi = load_vinfo(sc, sc.instances[inst].y & 0xffffu);
+        float2 uv = make_float2(0.f, 0.f);
+        const uint32_t tb = vi_texcoord_buffer(vi);
+        if (tb < sc.vbuf_count) {
+            const uint3 tri = load_triangle_indices(sc.vbufs[vi_index_buffer(vi)], vi_index_offset(vi), vi_index_stride(vi), prim);
+            const uint8_t* tbuf = sc.vbufs[tb];
+            const uint32_t to = vi_texcoord_offset(vi), ts = vi_texcoord_stride(vi);
+            const float2 t0 = load_f2(tbuf, to, ts, tri.x), t1 = load_f2(tbuf, to, ts, tri.y), t2 = load_f2(tbuf, to, ts, tri.z);
+            uv = make_float2(t0.x + (t1.x - t0.x) * b1 + (t2.x - t0.x) * b2, t0.y + (t1.y - t0.y) * b1 + (t2.y - t0.y) * b2);
+        }
+        return sample_image(sc.images[am.x], uv).x >= __uint_as_float(am.y);
+    }
+};

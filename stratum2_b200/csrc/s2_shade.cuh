@@ -152,6 +152,28 @@ S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, f
     return r;
 }
 
+// ApplyNormalMap (material.hlsli:78-105, gNormalMaps): the bump image (index, strength and
+// channel count at bytes 36..47 of the material record) perturbs the shading normal in the
+// tangent frame; normal and tangent are re-packed octahedrally as the reference stores them.
+// The bitangent sign is +1: the reference never sets SHADING_FLAG_FLIP_BITANGENT.
+S2D void apply_normal_map(const DevScene& s, SD& sd) {
+    const uint8_t* rec = s.material_data + sd.mat + 36;
+    const uint32_t img = ld_u32(rec, 0), channels = ld_u32(rec, 8);
+    const float scale = ld_f32(rec, 4);
+    if (img >= s.image_count || !(scale > 0.f)) return;
+    const float4 t = sample_image(s.images[img], sd.uv);
+    float3 bump = channels == 2 ? f3(t.x, t.y, 1.f) : f3(t.x, t.y, t.z);
+    bump.x = (bump.x * 2.f - 1.f) * scale;
+    bump.y = -(bump.y * 2.f - 1.f) * scale;
+    const float3 n = normalize(sd.t * bump.x + cross(sd.n, sd.t) * bump.y + sd.n * bump.z);
+    const float3 tg = normalize(sd.t - n * dot(n, sd.t));
+    sd.ns = pack_normal(n);
+    sd.tg = pack_normal(tg);
+    sd.n = unpack_normal(sd.ns);
+    sd.t = unpack_normal(sd.tg);
+    sd.b = cross(sd.n, sd.t);
+}
+
 // makeTriangleShadingData from an object-space position (shading_data.hlsli:153-173): the
 // barycentrics are recovered from the position (used for vertices stored in the hash grid).
 S2D SD make_shading_local(const DevScene& s, uint32_t inst, uint32_t prim, float3 lp, bool shading_normals) {

@@ -94,7 +94,8 @@ S2D void reservoir_reuse(const PTParams& P, const Mat& m, const SD& sd, float3 i
     const DISample nw = eval_di<LAMBERT>(s, m, sd, in, q.rnd, sn, cp);  // q's sample in the current domain
     float phat_q = 0.f;                                                 // current sample in q's domain
     {
-        const SD sdq = make_shading_local(s, q.instance, q.primitive, q.local_pos, sn);
+        SD sdq = make_shading_local(s, q.instance, q.primitive, q.local_pos, sn);
+        if (!(P.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sdq);
         const Mat mq = load_material(s, sdq.mat, sdq.uv);
         const float cpq = (P.flags & S2F_NO_RR) ? 1.f : cont_prob(mq);
         const DISample cq = eval_di<LAMBERT>(s, mq, sdq, q.local_dir_in, cur.rnd, sn, cpq);
@@ -263,7 +264,8 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
             } else {
                 const float4 tr0 = s.tris[3 * (size_t)tri], tr1 = s.tris[3 * (size_t)tri + 1];
                 const uint32_t inst = __float_as_uint(tr0.w), prim = __float_as_uint(tr1.w);
-                const SD sd = make_shading(s, inst, prim, h.z, h.w, sn);
+                SD sd = make_shading(s, inst, prim, h.z, h.w, sn);
+                if (!(P.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
                 const float isect_dist = half_round(h.x);
                 const float isect_pdfa = half_round(light_pdfa(s, inst, sd.area));
                 const Mat m = load_material(s, sd.mat, sd.uv);

@@ -153,6 +153,11 @@ S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint
 // Per-ray traversal state for the step-wise traversal: the current node, the stack pointer and
 // the closest hit so far.  The stack lives in shared memory (first S2_STACK_SMEM entries, strided
 // by `lane_stride`) and in a local-memory continuation `lstack`.
+// Alpha test of a candidate hit (closest or any hit); NoAlphaTest accepts every triangle.
+struct NoAlphaTest {
+    S2D bool operator()(uint32_t, uint32_t, float, float) const { return true; }
+};
+
 struct TravState {
     uint32_t node;
     int sp;
@@ -167,9 +172,11 @@ S2D void trav_begin(TravState& st, TravHit& hit, float tmax) {
 
 // One traversal step: visit st.node (its 8 child boxes and its leaf triangles), then choose the
 // next node (nearest hit child, else the stack).  Returns true when the traversal is finished.
-template <bool ANYHIT, bool COUNT>
+// Triangles flagged S2_TRI_ALPHA_TESTED are accepted only when `alpha(instance, primitive, b1, b2)`.
+template <bool ANYHIT, bool COUNT, class Alpha = NoAlphaTest>
 S2D bool trav_step(const TravRay& r, TravState& st, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
-                   uint2* __restrict__ smem_stack, uint32_t lane_stride, uint2* lstack, TravHit& hit, TravCounters& ctr) {
+                   uint2* __restrict__ smem_stack, uint32_t lane_stride, uint2* lstack, TravHit& hit, TravCounters& ctr,
+                   const Alpha& alpha = Alpha()) {
     uint32_t child_base, imask, hits, tri_base, trimask;
     intersect_node(r, nodes4, st.node, hit.t, child_base, imask, hits, tri_base, trimask);
     if (COUNT) ctr.nodes++;
@@ -184,6 +191,7 @@ S2D bool trav_step(const TravRay& r, TravState& st, const uint4* __restrict__ no
         float t, b1, b2;
         if (intersect_triangle(r, ld3(a), ld3(b), ld3(c), hit.t, t, b1, b2)) {
             const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+            if ((__float_as_uint(c.w) & S2_TRI_ALPHA_TESTED) && !alpha(inst, prim, b1, b2)) continue;
             if (ANYHIT) {
                 hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
                 return true;
@@ -230,13 +238,14 @@ S2D bool trav_step(const TravRay& r, TravState& st, const uint4* __restrict__ no
 
 // Whole traversal of one ray.  ANYHIT: stop at the first accepted triangle.  COUNT: count node and
 // triangle fetches into `ctr`.  Returns false if the stack overflowed (result may be incomplete).
-template <bool ANYHIT, bool COUNT>
+template <bool ANYHIT, bool COUNT, class Alpha = NoAlphaTest>
 S2D bool traverse(const TravRay& r, float tmax, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
-                  uint2* __restrict__ smem_stack, uint32_t lane_stride, TravHit& hit, TravCounters& ctr) {
+                  uint2* __restrict__ smem_stack, uint32_t lane_stride, TravHit& hit, TravCounters& ctr,
+                  const Alpha& alpha = Alpha()) {
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     TravState st;
     trav_begin(st, hit, tmax);
-    while (!trav_step<ANYHIT, COUNT>(r, st, nodes4, tris4, smem_stack, lane_stride, lstack, hit, ctr)) {
+    while (!trav_step<ANYHIT, COUNT, Alpha>(r, st, nodes4, tris4, smem_stack, lane_stride, lstack, hit, ctr, alpha)) {
     }
     return st.ok;
 }

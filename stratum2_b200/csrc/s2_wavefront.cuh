@@ -117,6 +117,8 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_NO_RR (1u << 6)
 #define S2F_NO_SN (1u << 8)
 #define S2F_REUSE (1u << 11)
+#define S2F_NO_ALPHA (1u << 12)
+#define S2F_NO_NORMAL_MAPS (1u << 13)
 
 constexpr int kTravBlock = 128;
 
@@ -300,7 +302,7 @@ S2D uint32_t refill(uint32_t* work, uint32_t count, uint32_t item, bool& exhaust
 
 // Closest hit of the live path queue.  Hit record: {t, triangle record index, b1, b2}.
 template <bool COUNT>
-__global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t parity) {
+__global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ PTParams P, uint32_t parity) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[parity];
@@ -321,7 +323,8 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t pari
             trav_begin(st, h, S2_INF);
         }
         if (ray != kNoRay) {
-            if (trav_step<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c)) {
+            if (trav_step<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                        SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
                 if (!st.ok) atomicOr(P.status, 1);
                 P.hits[ray] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
                 ray = kNoRay;
@@ -334,7 +337,7 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(PTParams P, uint32_t pari
 // ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
 // ray belongs to one accumulator slot and adds its contribution when unoccluded.
 template <bool COUNT>
-__global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
+__global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ PTParams P) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[C_SHADOW];
@@ -354,7 +357,8 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(PTParams P) {
             trav_begin(st, h, o.w);
         }
         if (ray != kNoRay) {
-            if (trav_step<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c)) {
+            if (trav_step<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                       SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
                 if (!st.ok) atomicOr(P.status, 1);
                 if (h.tri == 0xffffffffu) {
                     const float4 cc = P.sh_c[ray];

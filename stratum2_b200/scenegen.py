@@ -8,6 +8,7 @@ All scenes are generated from fixed seeds with numpy; nothing is read from disk.
       level-5 icospheres (20,480 triangles each) under seeded transforms; GLTF metallic-roughness
       materials; 512x256 procedural HDR sky with a 5e3 sun lobe over a 0.5 degree cone;
       1920x1080, 64 spp, path length 3..12 with Russian roulette)
+  cutout_scene (the box with normal-mapped, textured walls and an alpha-masked quad)
   terrain_scene(..., emissive_triangles=100_000) (the many-lights form: small one-sided emissive
       triangles hovering over the terrain, one instance each, power lognormal(0, 2))
 """
@@ -18,6 +19,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import _abi
 from .scene import Material, Scene, look_at_rotation, make_view, rotation_from_quaternion, transform_trs
 
 
@@ -73,6 +75,57 @@ def box_scene(seed: int = 1, n_random: int = 1000, width: int = 256, height: int
         s.add_instance(s.add_mesh(verts, tri_idx), m)
     view = make_view((0.0, 0.0, 3.0), width, height, 40.0)
     return Workload(s, view, width, height, spp, 2, 5, True, f"box{n_random}_{width}x{height}")
+
+
+def cutout_scene(seed: int = 3, n_random: int = 200, width: int = 64, height: int = 64, spp: int = 16) -> Workload:
+    """The box with textured walls: floor and back wall carry a tangent-space normal map (3
+    channels, strength 1) and an albedo texture; a 1.4 x 1.4 quad at z = 0.2 facing the camera has
+    an alpha mask (R32F, 0 inside 12 random discs, 1 elsewhere, cutoff 0.5) so the random
+    triangles behind it show through the holes."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    uv4 = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    # normal map from value-noise heights (RGB = 0.5 + 0.5 * (nx, -ny, nz): the reference flips y)
+    hgt = value_noise(rng, 128, octaves=4, amplitude=1.0)
+    gy, gx = np.gradient(hgt.astype(np.float64))
+    n = np.stack([-gx * 8, -gy * 8, np.ones_like(gx)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    nmap = s.add_image(np.stack([0.5 + 0.5 * n[..., 0], 0.5 - 0.5 * n[..., 1], 0.5 + 0.5 * n[..., 2]], -1).astype(np.float32))
+    tex = s.add_image(rng.uniform(0.3, 1.0, size=(32, 32, 3)).astype(np.float32))
+    yy, xx = np.mgrid[0:64, 0:64] / 64.0
+    mask = np.ones((64, 64), np.float32)
+    for _ in range(12):
+        cx, cy, r = rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.05, 0.15)
+        mask[(xx - cx) ** 2 + (yy - cy) ** 2 < r * r] = 0.0
+    amask = s.add_image(mask)
+    walls = [
+        ((-1, -1, -1), (-1, -1, 1), (1, -1, 1), (1, -1, -1)),
+        ((-1, 1, -1), (1, 1, -1), (1, 1, 1), (-1, 1, 1)),
+        ((-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1)),
+        ((-1, -1, -1), (-1, 1, -1), (-1, 1, 1), (-1, -1, 1)),
+        ((1, -1, -1), (1, -1, 1), (1, 1, 1), (1, 1, -1)),
+    ]
+    bumpy = s.add_material(Material(base_color=(0.8, 0.8, 0.8), roughness=0.4, images=(tex, _abi.NO_IMAGE, _abi.NO_IMAGE, _abi.NO_IMAGE),
+                                    bump_image=nmap, bump_strength=1.0, bump_channels=3))
+    plain = s.add_material(Material(base_color=(0.7, 0.7, 0.7)))
+    for k, w in enumerate(walls):
+        p, i = quad(*w)
+        s.add_instance(s.add_mesh(p, i, uvs=uv4 * 3.0), bumpy if k in (0, 2) else plain)
+    h, y = 0.25, 1.0 - 1e-3
+    p, i = quad((-h, y, -h), (h, y, -h), (h, y, h), (-h, y, h))
+    s.add_instance(s.add_mesh(p, i), s.add_material(Material(base_color=(0, 0, 0), emission=(10.0,) * 3)))
+    p, i = quad((-0.7, -0.7, 0.2), (0.7, -0.7, 0.2), (0.7, 0.7, 0.2), (-0.7, 0.7, 0.2))
+    cut = s.add_material(Material(base_color=(0.9, 0.5, 0.2), roughness=0.3, alpha_mask=amask, alpha_cutoff=0.5))
+    s.add_instance(s.add_mesh(p, i, uvs=uv4), cut)
+    cent = rng.uniform(-0.8, 0.8, size=(n_random, 3))
+    cent[:, 2] = rng.uniform(-0.9, 0.1, n_random)
+    offs = rng.uniform(-0.08, 0.08, size=(n_random, 3, 3))
+    alb = rng.uniform(0.2, 0.8, size=(n_random, 3))
+    for k in range(n_random):
+        m = s.add_material(Material(base_color=tuple(alb[k])))
+        s.add_instance(s.add_mesh((cent[k][None, :] + offs[k]).astype(np.float32), np.array([[0, 1, 2]], np.uint32)), m)
+    view = make_view((0.0, 0.0, 3.0), width, height, 40.0)
+    return Workload(s, view, width, height, spp, 2, 5, False, f"cutout_{width}x{height}")
 
 
 # ------------------------------------------------------------------------------ terrain

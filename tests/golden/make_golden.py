@@ -21,7 +21,7 @@ sys.path.insert(0, str(HERE.parent))
 
 from oracle_lib import OracleScene  # noqa: E402
 from stratum2_b200 import _abi  # noqa: E402
-from stratum2_b200.scenegen import box_scene, terrain_scene  # noqa: E402
+from stratum2_b200.scenegen import box_scene, cutout_scene, terrain_scene  # noqa: E402
 
 GOLDEN_SEED = 1_000_000  # frame seeds of the oracle images; GPU tests use seeds < 100000
 
@@ -47,7 +47,31 @@ def terrain_case():
     return wl, p
 
 
-CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 131072)}
+def cutout_case():
+    wl = cutout_scene(seed=3, width=64, height=64)
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length = 0, 5
+    p.flags = _abi.FLAG_PIXEL_JITTER
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    return wl, p
+
+
+def cfg2_case():
+    """The benchmark workload (1920x1080 terrain, 5e3 sun, path length 3..12, pixel centres) on
+    the pixel subset x = 15 + 30 i, y = 15 + 30 j (64 x 36 pixels)."""
+    wl = terrain_scene(seed=2)
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length = 3, 12
+    p.flags = 0
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    return wl, p
+
+
+SUBSET = {"cfg2_1920x1080_subset30": ((15, 15, 1920, 1080), 30)}
+CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 131072), "cutout_64x64": (cutout_case, 16384),
+         "cfg2_1920x1080_subset30": (cfg2_case, 262144)}
 
 
 def make(name: str, out_dir: Path = HERE):
@@ -57,9 +81,17 @@ def make(name: str, out_dir: Path = HERE):
     p.frame_seed = GOLDEN_SEED
     osc = OracleScene(wl.scene, 1)
     t = time.time()
-    r = osc.render(wl.view, p, wl.width, wl.height, precision=64)
-    np.savez_compressed(out_dir / f"{name}_fp64_{spp}spp.npz", mean=r["mean"].astype(np.float32),
-                        var_of_mean=r["var_of_mean"].astype(np.float32), spp=spp, seed=GOLDEN_SEED)
+    if name in SUBSET:
+        rect, stride = SUBSET[name]
+        r = osc.render(wl.view, p, wl.width, wl.height, precision=64, rect=rect, stride=stride)
+        sel = (slice(rect[1], rect[3], stride), slice(rect[0], rect[2], stride))
+        np.savez_compressed(out_dir / f"{name}_fp64_{spp}spp.npz", mean=r["mean"][sel].astype(np.float32),
+                            var_of_mean=r["var_of_mean"][sel].astype(np.float32), spp=spp, seed=GOLDEN_SEED,
+                            rect=np.array(rect), stride=stride)
+    else:
+        r = osc.render(wl.view, p, wl.width, wl.height, precision=64)
+        np.savez_compressed(out_dir / f"{name}_fp64_{spp}spp.npz", mean=r["mean"].astype(np.float32),
+                            var_of_mean=r["var_of_mean"].astype(np.float32), spp=spp, seed=GOLDEN_SEED)
     print(name, f"{time.time() - t:.1f}s", float(r["mean"].mean()))
 
 
