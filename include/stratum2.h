@@ -270,6 +270,38 @@ void s2_default_render_params(S2RenderParams* p);
 int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams* params,
                        const S2Aovs* out, S2RenderStats* stats_out);
 
+/* ---------------------------------------------------------------- learned radiance cache
+ * No counterpart in the reference.  A multiresolution hash-grid encoding of world-space position
+ * (16 levels x 2 features, 2^log2_table entries per level, resolutions geometric from
+ * base_resolution to max_resolution over the cache box) feeding a 32 -> 64 -> 64 -> 3 ReLU MLP
+ * without biases (6,336 weights).  f16 parameters on the device with f32 master copies; inference
+ * and training run on the tensor cores (f16 operands, f32 accumulation).  Parameter order of the
+ * weights: W1 (64 x 32, row = output), W2 (64 x 64), W3 (3 x 64); the table: [level][entry][2]. */
+#define S2_CACHE_WEIGHTS 6336
+#define S2_CACHE_LEVELS  16
+
+typedef struct S2CacheParams {
+    float box_min[3], box_max[3];   /* encoding domain; box_min >= box_max: the scene bounding sphere's box */
+    uint32_t log2_table;            /* default 19 */
+    uint32_t base_resolution;       /* default 16 */
+    uint32_t max_resolution;        /* default 2048 */
+    float learning_rate;            /* Adam, default 1e-2 */
+    float beta1, beta2, epsilon;    /* default 0.9, 0.99, 1e-15 */
+    uint32_t seed;                  /* parameter initialisation */
+    uint32_t reserved[6];
+} S2CacheParams;                    /* 80 B */
+
+void s2_cache_default_params(S2CacheParams* p);
+/* (Re)creates the cache with freshly initialised parameters (table U(-1e-4, 1e-4), weights
+ * U(+-sqrt(6 / (fan_in + fan_out))) from `seed`). */
+int  s2_cache_init(S2Context* ctx, const S2CacheParams* params);
+/* Copies the f32 parameters out / in (weights: S2_CACHE_WEIGHTS floats; table: 16 * 2^log2_table
+ * * 2 floats; either pointer may be NULL).  Setting resets the optimiser state. */
+int  s2_cache_get_params(S2Context* ctx, float* weights, float* table);
+int  s2_cache_set_params(S2Context* ctx, const float* weights, const float* table);
+/* Evaluates the cache at n positions: positions and radiance are float4 per entry (xyz used). */
+int  s2_cache_query(S2Context* ctx, const float* positions, uint32_t n, float* radiance, int on_device);
+
 #ifdef __cplusplus
 }
 #endif

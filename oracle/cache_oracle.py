@@ -1,0 +1,78 @@
+"""ORACLE -- test infrastructure only.  numpy FP64 restatement of the learned radiance cache
+(stratum2_b200/csrc/s2_cache.cuh): the multiresolution hash-grid encoding (Instant-NGP, Mueller et
+al. 2022) and the 32 -> 64 -> 64 -> 3 ReLU MLP without biases, with the device's f16 roundings of
+parameters, encoded features and hidden activations, and the relative L2 loss with its gradients.
+The radiance cache has no counterpart in the reference."""
+from __future__ import annotations
+
+import numpy as np
+
+LEVELS, FEATURES, IN, HIDDEN, OUT = 16, 2, 32, 64, 3
+W1, W2, W3 = HIDDEN * IN, HIDDEN * HIDDEN, OUT * HIDDEN
+
+
+def f16(x):
+    return np.asarray(x, np.float64).astype(np.float16).astype(np.float64)
+
+
+def resolutions(base=16, top=2048, log2_table=19):
+    b = np.exp((np.log(top) - np.log(base)) / (LEVELS - 1))
+    res = np.floor(base * b ** np.arange(LEVELS) + 1e-9)
+    dense = (res + 1) ** 3 <= 2 ** log2_table
+    return res, dense
+
+
+def corner_index(level, x, y, z, res, dense, log2_table):
+    mask = (1 << log2_table) - 1
+    x, y, z = (np.asarray(v, np.uint64) for v in (x, y, z))
+    if dense[level]:
+        n = np.uint64(int(res[level]) + 1)
+        return ((x + n * (y + n * z)) & np.uint64(mask)).astype(np.int64)
+    h = (x ^ ((y * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)) ^ ((z * np.uint64(805459861)) & np.uint64(0xFFFFFFFF)))
+    return (h & np.uint64(mask)).astype(np.int64)
+
+
+def unit(pos, box_min, box_max):
+    u = (np.asarray(pos, np.float64) - np.asarray(box_min, np.float64)) / (np.asarray(box_max, np.float64) - box_min)
+    return np.clip(u, 0.0, 0.99999994)
+
+
+def encode(pos, table, box_min, box_max, base=16, top=2048, with_corners=False):
+    """Features (n, 32) in f64 before the f16 rounding; table (levels, T, 2) f64 (already f16-valued).
+    with_corners also returns, per level, the corner indices (n, 8) and weights (n, 8)."""
+    log2_table = int(np.log2(table.shape[1]))
+    res, dense = resolutions(base, top, log2_table)
+    u = unit(pos, box_min, box_max)
+    n = u.shape[0]
+    feats = np.zeros((n, IN))
+    corners = []
+    for l in range(LEVELS):
+        f = u * res[l]
+        i0 = np.floor(f)
+        w = f - i0
+        i0 = i0.astype(np.int64)
+        idx = np.zeros((n, 8), np.int64)
+        wt = np.zeros((n, 8))
+        for k in range(8):
+            d = np.array([k & 1, (k >> 1) & 1, k >> 2])
+            wk = np.prod(np.where(d == 1, w, 1 - w), axis=1)
+            ik = corner_index(l, i0[:, 0] + d[0], i0[:, 1] + d[1], i0[:, 2] + d[2], res, dense, log2_table)
+            idx[:, k] = ik
+            wt[:, k] = wk
+            feats[:, 2 * l:2 * l + 2] += wk[:, None] * table[l, ik]
+        corners.append((idx, wt))
+    return (feats, corners) if with_corners else feats
+
+
+def split(weights):
+    w = np.asarray(weights, np.float64)
+    return w[:W1].reshape(HIDDEN, IN), w[W1:W1 + W2].reshape(HIDDEN, HIDDEN), w[W1 + W2:].reshape(OUT, HIDDEN)
+
+
+def forward(pos, weights, table, box_min, box_max, base=16, top=2048):
+    """Cache output (n, 3) with the device's f16 roundings (f64 accumulation)."""
+    a, b, c = (f16(m) for m in split(weights))
+    x = f16(encode(pos, f16(table), box_min, box_max, base, top))
+    h1 = f16(np.maximum(x @ a.T, 0))
+    h2 = f16(np.maximum(h1 @ b.T, 0))
+    return h2 @ c.T

@@ -47,7 +47,11 @@ EXPORTED_SYMBOLS = [
     "s2_get_abi_version", "s2_create", "s2_destroy", "s2_last_error", "s2_sync", "s2_set_stream",
     "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
     "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
+    "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
 ]
+
+CACHE_WEIGHTS = 6336
+CACHE_LEVELS = 16
 
 
 class S2Image(C.Structure):
@@ -121,6 +125,13 @@ class S2Aovs(C.Structure):
                 ("depth", C.c_void_p), ("prev_uv", C.c_void_p), ("ids32", C.c_void_p)]
 
 
+class S2CacheParams(C.Structure):
+    _fields_ = [("box_min", C.c_float * 3), ("box_max", C.c_float * 3), ("log2_table", C.c_uint32),
+                ("base_resolution", C.c_uint32), ("max_resolution", C.c_uint32), ("learning_rate", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float), ("seed", C.c_uint32),
+                ("reserved", C.c_uint32 * 6)]
+
+
 class S2RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
                 ("nan_count", C.c_uint64), ("gpu_ms", C.c_double), ("kernel_launches", C.c_uint64),
@@ -132,6 +143,7 @@ class S2RenderStats(C.Structure):
 
 assert C.sizeof(S2Ray) == 32 and C.sizeof(S2Hit) == 20
 assert C.sizeof(S2RenderParams) == 80
+assert C.sizeof(S2CacheParams) == 80
 
 _lib = None
 
@@ -163,6 +175,12 @@ def lib() -> C.CDLL:
     L.s2_render_noalloc.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), P(S2RenderStats)]
     L.s2_default_render_params.argtypes = [P(S2RenderParams)]
     L.s2_default_render_params.restype = None
+    L.s2_cache_default_params.argtypes = [P(S2CacheParams)]
+    L.s2_cache_default_params.restype = None
+    L.s2_cache_init.argtypes = [C.c_void_p, P(S2CacheParams)]
+    L.s2_cache_get_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.s2_cache_set_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.s2_cache_query.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
     for name in EXPORTED_SYMBOLS:
         getattr(L, name)
     if L.s2_get_abi_version() != ABI_VERSION:

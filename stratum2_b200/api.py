@@ -175,3 +175,34 @@ class Device:
         st = _abi.S2RenderStats()
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(params), C.byref(aovs), 0, C.byref(st)))
         return st
+
+    # ---- learned radiance cache
+    @staticmethod
+    def cache_default_params() -> _abi.S2CacheParams:
+        p = _abi.S2CacheParams()
+        _abi.lib().s2_cache_default_params(C.byref(p))
+        return p
+
+    def cache_init(self, params: _abi.S2CacheParams | None = None):
+        self._check(self._lib.s2_cache_init(self._h, C.byref(params) if params is not None else None))
+        self._cache_log2 = (params.log2_table if params is not None else self.cache_default_params().log2_table)
+
+    def cache_get_params(self) -> tuple[np.ndarray, np.ndarray]:
+        w = np.zeros(_abi.CACHE_WEIGHTS, np.float32)
+        t = np.zeros((_abi.CACHE_LEVELS, 1 << self._cache_log2, 2), np.float32)
+        self._check(self._lib.s2_cache_get_params(self._h, w.ctypes.data, t.ctypes.data))
+        return w, t
+
+    def cache_set_params(self, weights=None, table=None):
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        t = None if table is None else np.ascontiguousarray(table, np.float32)
+        self._check(self._lib.s2_cache_set_params(self._h, None if w is None else w.ctypes.data,
+                                                  None if t is None else t.ctypes.data))
+
+    def cache_query(self, positions) -> np.ndarray:
+        """Cache radiance at world-space positions (n x 3) -> (n x 3) float32."""
+        p = np.zeros((len(positions), 4), np.float32)
+        p[:, :3] = positions
+        out = np.zeros((len(positions), 4), np.float32)
+        self._check(self._lib.s2_cache_query(self._h, p.ctypes.data, len(p), out.ctypes.data, 0))
+        return out[:, :3]

@@ -18,6 +18,7 @@ struct DevBuf {
 };
 
 struct RenderState;  // wavefront queues and accumulators (s2_render.cu)
+struct CacheState;   // learned radiance cache parameters and optimiser state (s2_cache.cu)
 
 struct HostImage {
     uint32_t w = 0, h = 0;
@@ -50,6 +51,7 @@ struct S2Context {
     int env_image = -1;
 
     s2::RenderState* render = nullptr;
+    s2::CacheState* cache = nullptr;
     int* status_dev = nullptr;              // device status word (stack/queue overflow, timeouts)
 };
 
@@ -59,4 +61,5 @@ int check_cuda(S2Context* ctx, cudaError_t e, const char* what);
 void* dev_alloc(S2Context* ctx, std::vector<DevBuf>& owner, size_t bytes);
 void free_bufs(std::vector<DevBuf>& bufs);
 void destroy_render_state(S2Context* ctx);
+void destroy_cache_state(S2Context* ctx);
 }  // namespace s2
