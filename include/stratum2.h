@@ -301,6 +301,15 @@ int  s2_cache_get_params(S2Context* ctx, float* weights, float* table);
 int  s2_cache_set_params(S2Context* ctx, const float* weights, const float* table);
 /* Evaluates the cache at n positions: positions and radiance are float4 per entry (xyz used). */
 int  s2_cache_query(S2Context* ctx, const float* positions, uint32_t n, float* radiance, int on_device);
+/* One optimiser step (Adam on the f32 masters, then refreshed f16 copies) on n records: float4
+ * positions and float4 target radiances.  Loss per record: sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / 3
+ * with the denominator held constant; `loss` (may be NULL) receives its mean over the records. */
+int  s2_cache_train(S2Context* ctx, const float* positions, const float* targets, uint32_t n, float* loss,
+                    int on_device);
+/* The gradients of the mean loss over n records without an optimiser step (host outputs: weights
+ * S2_CACHE_WEIGHTS floats, table 16 * 2^log2_table * 2 floats; either may be NULL). */
+int  s2_cache_gradients(S2Context* ctx, const float* positions, const float* targets, uint32_t n,
+                        float* grad_weights, float* grad_table, float* loss, int on_device);
 
 #ifdef __cplusplus
 }

@@ -76,3 +76,54 @@ def forward(pos, weights, table, box_min, box_max, base=16, top=2048):
     h1 = f16(np.maximum(x @ a.T, 0))
     h2 = f16(np.maximum(h1 @ b.T, 0))
     return h2 @ c.T
+
+
+def _r(x, exact):
+    return np.asarray(x, np.float64) if exact else f16(x)
+
+
+def loss_and_grads(pos, targets, weights, table, box_min, box_max, base=16, top=2048, exact=False,
+                   grad_scale=1.0 / 64.0):
+    """Mean relative L2 loss over the records (sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / 3 per record,
+    denominator held constant) and its gradients with respect to the weights (6336) and the table
+    (levels, T, 2).  exact=False applies the device's f16 roundings (parameters, features, hidden
+    activations and the backward activations scaled by grad_scale); exact=True is plain f64 math."""
+    n = len(pos)
+    a, b, c = (_r(m, exact) for m in split(weights))
+    tab = _r(table, exact)
+    feats, corners = encode(pos, tab, box_min, box_max, base, top, with_corners=True)
+    x = _r(feats, exact)
+    h1 = _r(np.maximum(x @ a.T, 0), exact)
+    h2 = _r(np.maximum(h1 @ b.T, 0), exact)
+    y = h2 @ c.T
+    t = np.asarray(targets, np.float64)[:, :3]
+    d = y - t
+    den = y * y + 0.01
+    loss = float(np.mean(np.sum(d * d / den, 1) / 3))
+    dy = 2 * d / den / 3
+    if not exact:
+        dy = np.clip(dy, -1e4, 1e4)
+    s = 1.0 if exact else grad_scale
+    dw3 = dy.T @ h2
+    dh2 = _r((dy @ c) * (h2 > 0) * s, exact)
+    dw2 = dh2.T @ h1 / s
+    dh1 = _r((dh2 @ b) * (h1 > 0), exact)
+    dw1 = dh1.T @ x / s
+    dx = dh1 @ a / s
+    gt = np.zeros_like(np.asarray(table, np.float64))
+    for l, (idx, wt) in enumerate(corners):
+        for k in range(8):
+            np.add.at(gt[l, :, 0], idx[:, k], wt[:, k] * dx[:, 2 * l])
+            np.add.at(gt[l, :, 1], idx[:, k], wt[:, k] * dx[:, 2 * l + 1])
+    gw = np.concatenate([dw1.ravel(), dw2.ravel(), dw3.ravel()])
+    return loss, gw / n, gt / n
+
+
+def loss_only(pos, targets, weights, table, box_min, box_max, base=16, top=2048):
+    """f64 loss with the denominator evaluated at the given parameters (for finite differences of
+    loss_and_grads(exact=True), hold `den` by passing the same parameters)."""
+    a, b, c = split(weights)
+    x = encode(pos, np.asarray(table, np.float64), box_min, box_max, base, top)
+    y = np.maximum(np.maximum(x @ a.T, 0) @ b.T, 0) @ c.T
+    t = np.asarray(targets, np.float64)[:, :3]
+    return y, t

@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = [
     "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
     "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
+    "s2_cache_train", "s2_cache_gradients",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -181,6 +182,9 @@ def lib() -> C.CDLL:
     L.s2_cache_get_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_cache_set_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_cache_query.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+    L.s2_cache_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, P(C.c_float), C.c_int]
+    L.s2_cache_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     P(C.c_float), C.c_int]
     for name in EXPORTED_SYMBOLS:
         getattr(L, name)
     if L.s2_get_abi_version() != ABI_VERSION:

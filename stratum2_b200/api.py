@@ -206,3 +206,28 @@ class Device:
         out = np.zeros((len(positions), 4), np.float32)
         self._check(self._lib.s2_cache_query(self._h, p.ctypes.data, len(p), out.ctypes.data, 0))
         return out[:, :3]
+
+    @staticmethod
+    def _records(positions, targets):
+        p = np.zeros((len(positions), 4), np.float32)
+        p[:, :3] = positions
+        t = np.zeros((len(targets), 4), np.float32)
+        t[:, :3] = np.asarray(targets)[:, :3]
+        return p, t
+
+    def cache_train(self, positions, targets) -> float:
+        """One Adam step on the records; returns the mean loss before the step."""
+        p, t = self._records(positions, targets)
+        loss = C.c_float(0)
+        self._check(self._lib.s2_cache_train(self._h, p.ctypes.data, t.ctypes.data, len(p), C.byref(loss), 0))
+        return loss.value
+
+    def cache_gradients(self, positions, targets):
+        """(mean loss, d loss / d weights, d loss / d table) without an optimiser step."""
+        p, t = self._records(positions, targets)
+        gw = np.zeros(_abi.CACHE_WEIGHTS, np.float32)
+        gt = np.zeros((_abi.CACHE_LEVELS, 1 << self._cache_log2, 2), np.float32)
+        loss = C.c_float(0)
+        self._check(self._lib.s2_cache_gradients(self._h, p.ctypes.data, t.ctypes.data, len(p), gw.ctypes.data,
+                                                 gt.ctypes.data, C.byref(loss), 0))
+        return loss.value, gw, gt

@@ -22,6 +22,7 @@ struct CacheState {
     float* adam_t = nullptr;         // m, v for the table (2 * entries * 2)
     float* grad_w = nullptr;         // weight gradient accumulator
     float* grad_t = nullptr;         // table gradient accumulator
+    float* loss = nullptr;           // summed per-record loss of the last pass
     uint64_t step = 0;
     CacheDev dev{};
     int sms = 148;
@@ -54,6 +55,15 @@ __global__ void k_cache_pack(const float* __restrict__ w32, const float* __restr
         const uint32_t o = i / kCacheHidden, k = i % kCacheHidden;
         const float v = o < kCacheOut ? w32[kCacheW1 + kCacheW2 + i] : 0.f;
         *(__half*)(wimage + kW1Bytes + kW2Bytes + kmaj_offset(o, k, kCacheHidden)) = __float2half_rn(v);
+    }
+    // transposed copies: W2T (i, o) = W2[o][i], W1T (i, o) = W1[o][i]
+    if (i < kCacheW2) {
+        const uint32_t o = i / kCacheHidden, k = i % kCacheHidden;
+        *(__half*)(wimage + kWImageBytes + kmaj_offset(k, o, kCacheHidden)) = __float2half_rn(w32[kCacheW1 + i]);
+    }
+    if (i < kCacheW1) {
+        const uint32_t o = i / kCacheIn, k = i % kCacheIn;
+        *(__half*)(wimage + kWImageBytes + kW2TBytes + kmaj_offset(k, o, kCacheHidden)) = __float2half_rn(w32[i]);
     }
 }
 
@@ -119,13 +129,14 @@ extern "C" int s2_cache_init(S2Context* ctx, const S2CacheParams* params) {
     c->w32 = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * kCacheWeights);
     c->t32 = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * 2 * ne);
     c->t16 = (__half2*)dev_alloc(ctx, c->bufs, sizeof(__half2) * ne);
-    c->wimage = (uint4*)dev_alloc(ctx, c->bufs, kWImageBytes);
+    c->wimage = (uint4*)dev_alloc(ctx, c->bufs, kWImageTrainBytes);
+    c->loss = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * 4);
     c->adam_w = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * 2 * kCacheWeights);
     c->adam_t = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * 4 * ne);
     c->grad_w = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * kCacheWeights);
     c->grad_t = (float*)dev_alloc(ctx, c->bufs, sizeof(float) * 2 * ne);
     for (auto& b : c->bufs) if (!b.ptr) { destroy_cache_state(ctx); return set_error(ctx, S2_ERR_OOM, "cache allocation failed"); }
-    if (c->bufs.size() != 8) { destroy_cache_state(ctx); return set_error(ctx, S2_ERR_OOM, "cache allocation failed"); }
+    if (c->bufs.size() != 9) { destroy_cache_state(ctx); return set_error(ctx, S2_ERR_OOM, "cache allocation failed"); }
     // initial parameters
     uint64_t rs = 0x5eedull ^ ((uint64_t)p.seed << 17);
     std::vector<float> w(kCacheWeights), t(2 * ne);
@@ -171,6 +182,9 @@ extern "C" int s2_cache_set_params(S2Context* ctx, const float* weights, const f
                                    1.f / (c->prm.box_max[2] - c->prm.box_min[2]));
     d.wimage = c->wimage;
     d.status = ctx->status_dev;
+    d.grad_w = c->grad_w;
+    d.grad_t = c->grad_t;
+    d.loss_sum = c->loss;
     return check_cuda(ctx, cudaStreamSynchronize(s), "cache parameter upload");
 }
 
@@ -228,4 +242,126 @@ extern "C" int s2_cache_query(S2Context* ctx, const float* positions, uint32_t n
     free_bufs(tmp);
     if (rc == S2_OK && (status & 4)) rc = set_error(ctx, S2_ERR_TIMEOUT, "tensor-core wait timed out in cache inference");
     return rc;
+}
+
+namespace s2 {
+// One forward/backward pass over n device records; gradients are summed into grad_w / grad_t.
+int cache_backward_device(S2Context* ctx, const float4* pos, const float4* target, uint32_t n) {
+    CacheState* c = ctx->cache;
+    if (n == 0) return S2_OK;
+    static bool attr_set[64] = {};
+    if (ctx->device < 64 && !attr_set[ctx->device]) {
+        const cudaError_t e = cudaFuncSetAttribute(k_cache_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmemBytes);
+        if (e != cudaSuccess) return check_cuda(ctx, e, "cache training kernel attributes");
+        attr_set[ctx->device] = true;
+    }
+    const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
+    k_cache_train<<<grid, 128, kTrSmemBytes, ctx->stream>>>(c->dev, pos, target, n);
+    return check_cuda(ctx, cudaGetLastError(), "cache training launch");
+}
+
+// Adam step with the summed gradients of `n` records, then the f16 copies are refreshed.
+int cache_adam_device(S2Context* ctx, uint32_t n) {
+    CacheState* c = ctx->cache;
+    c->step++;
+    const S2CacheParams& p = c->prm;
+    const float c1 = 1.f - std::pow(p.beta1, (float)c->step), c2 = 1.f - std::pow(p.beta2, (float)c->step);
+    const float inv_n = 1.f / (float)std::max<uint32_t>(n, 1);
+    k_cache_adam<<<(kCacheWeights + 255) / 256, 256, 0, ctx->stream>>>(c->w32, c->grad_w, c->adam_w, c->adam_w + kCacheWeights,
+                                                                       kCacheWeights, inv_n, p.learning_rate, p.beta1, p.beta2,
+                                                                       p.epsilon, c1, c2);
+    const size_t nt = 2 * (size_t)c->table_entries;
+    k_cache_adam<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(c->t32, c->grad_t, c->adam_t, c->adam_t + nt, nt, inv_n,
+                                                                        p.learning_rate, p.beta1, p.beta2, p.epsilon, c1, c2);
+    int rc = check_cuda(ctx, cudaGetLastError(), "cache Adam launch");
+    if (rc != S2_OK) return rc;
+    return repack(ctx);
+}
+}  // namespace s2
+
+namespace {
+// host/device staging shared by s2_cache_train and s2_cache_gradients
+int stage_records(S2Context* ctx, std::vector<DevBuf>& tmp, const float* positions, const float* targets, uint32_t n,
+                  int on_device, const float4*& dpos, const float4*& dtgt) {
+    dpos = (const float4*)positions;
+    dtgt = (const float4*)targets;
+    if (on_device) return S2_OK;
+    dpos = (const float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)n);
+    dtgt = (const float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)n);
+    if (!dpos || !dtgt) return S2_ERR_OOM;
+    cudaMemcpyAsync((void*)dpos, positions, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync((void*)dtgt, targets, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream);
+    return S2_OK;
+}
+
+int finish(S2Context* ctx, std::vector<DevBuf>& tmp, int rc, float* loss_out, uint32_t n) {
+    CacheState* c = ctx->cache;
+    int status = 0;
+    float loss = 0.f;
+    if (rc == S2_OK) {
+        cudaMemcpyAsync(&status, ctx->status_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(&loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cache training");
+    }
+    cudaStreamSynchronize(ctx->stream);
+    free_bufs(tmp);
+    if (rc == S2_OK && (status & 4)) rc = set_error(ctx, S2_ERR_TIMEOUT, "tensor-core wait timed out in cache training");
+    if (rc == S2_OK && loss_out) *loss_out = loss / (float)std::max<uint32_t>(n, 1);
+    return rc;
+}
+}  // namespace
+
+extern "C" int s2_cache_train(S2Context* ctx, const float* positions, const float* targets, uint32_t n, float* loss,
+                              int on_device) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!ctx->cache) return set_error(ctx, S2_ERR_NO_SCENE, "s2_cache_train before s2_cache_init");
+    if (n == 0) { if (loss) *loss = 0.f; return S2_OK; }
+    if (!positions || !targets) return set_error(ctx, S2_ERR_INVALID, "positions/targets is null");
+    cudaSetDevice(ctx->device);
+    std::vector<DevBuf> tmp;
+    const float4 *dpos, *dtgt;
+    int rc = stage_records(ctx, tmp, positions, targets, n, on_device, dpos, dtgt);
+    if (rc != S2_OK) { free_bufs(tmp); return rc; }
+    cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(ctx->cache->loss, 0, sizeof(float), ctx->stream);
+    rc = cache_backward_device(ctx, dpos, dtgt, n);
+    if (rc == S2_OK) rc = cache_adam_device(ctx, n);
+    return finish(ctx, tmp, rc, loss, n);
+}
+
+extern "C" int s2_cache_gradients(S2Context* ctx, const float* positions, const float* targets, uint32_t n,
+                                  float* grad_weights, float* grad_table, float* loss, int on_device) {
+    if (!ctx) return S2_ERR_INVALID;
+    CacheState* c = ctx->cache;
+    if (!c) return set_error(ctx, S2_ERR_NO_SCENE, "s2_cache_gradients before s2_cache_init");
+    if (n == 0) return set_error(ctx, S2_ERR_INVALID, "s2_cache_gradients needs at least one record");
+    if (!positions || !targets) return set_error(ctx, S2_ERR_INVALID, "positions/targets is null");
+    cudaSetDevice(ctx->device);
+    std::vector<DevBuf> tmp;
+    const float4 *dpos, *dtgt;
+    int rc = stage_records(ctx, tmp, positions, targets, n, on_device, dpos, dtgt);
+    if (rc != S2_OK) { free_bufs(tmp); return rc; }
+    const size_t nt = 2 * (size_t)c->table_entries;
+    cudaMemsetAsync(c->grad_w, 0, sizeof(float) * kCacheWeights, ctx->stream);
+    cudaMemsetAsync(c->grad_t, 0, sizeof(float) * nt, ctx->stream);
+    cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(c->loss, 0, sizeof(float), ctx->stream);
+    rc = cache_backward_device(ctx, dpos, dtgt, n);
+    std::vector<float> gw(kCacheWeights), gt;
+    if (rc == S2_OK) {
+        cudaMemcpyAsync(gw.data(), c->grad_w, sizeof(float) * kCacheWeights, cudaMemcpyDeviceToHost, ctx->stream);
+        if (grad_table) {
+            gt.resize(nt);
+            cudaMemcpyAsync(gt.data(), c->grad_t, sizeof(float) * nt, cudaMemcpyDeviceToHost, ctx->stream);
+        }
+        cudaMemsetAsync(c->grad_w, 0, sizeof(float) * kCacheWeights, ctx->stream);
+        cudaMemsetAsync(c->grad_t, 0, sizeof(float) * nt, ctx->stream);
+    }
+    rc = finish(ctx, tmp, rc, loss, n);
+    if (rc != S2_OK) return rc;
+    const float inv_n = 1.f / (float)n;
+    if (grad_weights) for (uint32_t i = 0; i < kCacheWeights; ++i) grad_weights[i] = gw[i] * inv_n;
+    if (grad_table) for (size_t i = 0; i < nt; ++i) grad_table[i] = gt[i] * inv_n;
+    return S2_OK;
 }

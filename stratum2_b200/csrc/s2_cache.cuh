@@ -33,6 +33,14 @@ constexpr uint32_t kW1Bytes = kCacheHidden * kCacheIn * 2;      // 4096
 constexpr uint32_t kW2Bytes = kCacheHidden * kCacheHidden * 2;  // 8192
 constexpr uint32_t kW3Bytes = kCacheOutPad * kCacheHidden * 2;  // 2048
 constexpr uint32_t kWImageBytes = kW1Bytes + kW2Bytes + kW3Bytes;
+// Transposed copies for the backward pass (B operands of dH1 = dH2 W2 and dX = dH1 W1):
+// W2T 64 x 64 with element (i, o) = W2[o][i], W1T 32 x 64 with element (i, o) = W1[o][i].
+constexpr uint32_t kW2TBytes = kCacheHidden * kCacheHidden * 2;  // 8192
+constexpr uint32_t kW1TBytes = kCacheIn * kCacheHidden * 2;      // 4096
+constexpr uint32_t kWImageTrainBytes = kWImageBytes + kW2TBytes + kW1TBytes;
+// Backward activations are scaled by this power of two before their f16 rounding (keeps them in
+// range), and unscaled in f32 when gradients leave the tensor cores.
+constexpr float kCacheGradScale = 1.f / 64.f;
 
 struct CacheDev {
     const __half2* table;        // [levels][2^log2_table] feature pairs
@@ -40,8 +48,12 @@ struct CacheDev {
     float res[kCacheLevels];     // grid resolution per level
     uint32_t dense[kCacheLevels];// 1: level indexed densely ((res+1)^3 <= table size)
     float3 box_min, box_inv_extent;
-    const uint4* wimage;         // kWImageBytes, the three weight tiles in operand layout
+    const uint4* wimage;         // kWImageTrainBytes: W1, W2, W3 (padded), W2T, W1T in operand layout
     int* status;                 // bit 2: a tensor-core wait timed out
+    // training
+    float* grad_w;               // summed per-record gradients of the weights
+    float* grad_t;               // summed per-record gradients of the table, [levels][entries][2]
+    float* loss_sum;             // summed per-record losses
 };
 
 // Normalised position in [0, 1) of the cache box.
@@ -169,8 +181,11 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
             umma_gemm(tmem, s_x, s_w1, kCacheIn, kCacheHidden, false);
             umma_commit(&bar);
         }
-        ok = mbar_wait(&bar, phase);
-        if (ok) phase ^= 1u;
+        {
+            const bool w = mbar_wait(&bar, phase);
+            if (w) phase ^= 1u;
+            ok = __all_sync(0xffffffffu, w);
+        }
         tc_fence_after_sync();
         if (ok) tmem_relu_to_tile(tlane, 0, smem + kInfSmemH, t);
         // layer 2: D[64:128) = H1 W2^T
@@ -182,8 +197,11 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
             umma_gemm(tmem + 64u, s_h, s_w2, kCacheHidden, kCacheHidden, false);
             umma_commit(&bar);
         }
-        ok = ok && mbar_wait(&bar, phase);
-        if (ok) phase ^= 1u;
+        {
+            const bool w = ok && mbar_wait(&bar, phase);
+            if (w) phase ^= 1u;
+            ok = __all_sync(0xffffffffu, w);
+        }
         tc_fence_after_sync();
         if (ok) tmem_relu_to_tile(tlane, 64u, smem + kInfSmemH, t);
         // layer 3: D[0:16) = H2 W3^T
@@ -195,8 +213,11 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
             umma_gemm(tmem, s_h, s_w3, kCacheHidden, kCacheOutPad, false);
             umma_commit(&bar);
         }
-        ok = ok && mbar_wait(&bar, phase);
-        if (ok) phase ^= 1u;
+        {
+            const bool w = ok && mbar_wait(&bar, phase);
+            if (w) phase ^= 1u;
+            ok = __all_sync(0xffffffffu, w);
+        }
         tc_fence_after_sync();
         if (ok) {
             float v[16];
@@ -217,6 +238,315 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
     tc_fence_before_sync();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// ---------------------------------------------------------------- training
+// Shared-memory plan of the training kernel (bytes).  The dW GEMMs use M = 128 with the 64 real
+// rows of dH2T / dH1T first; rows 64..127 of those A operands read the next 16 KB of the plan (dH1T
+// and H2), so the unused accumulator rows hold garbage and every descriptor stays inside the plan.
+constexpr uint32_t kTrW = 0;
+constexpr uint32_t kTrX = kTrW + kWImageTrainBytes;   // 128 x 32, K-major
+constexpr uint32_t kTrXT = kTrX + 8192;              // 32 x 128 (x transposed), B of dW1
+constexpr uint32_t kTrH1 = kTrXT + 8192;             // 128 x 64
+constexpr uint32_t kTrH1T = kTrH1 + 16384;           // 64 x 128, B of dW2
+constexpr uint32_t kTrDH2 = kTrH1T + 16384;          // 128 x 64, A of dH1
+constexpr uint32_t kTrDH1 = kTrDH2 + 16384;          // 128 x 64, A of dX
+constexpr uint32_t kTrDH2T = kTrDH1 + 16384;         // 64 x 128, A of dW2
+constexpr uint32_t kTrDH1T = kTrDH2T + 16384;        // 64 x 128, A of dW1
+constexpr uint32_t kTrH2 = kTrDH1T + 16384;          // 128 x 64
+constexpr uint32_t kTrDY = kTrH2 + 16384;            // 128 x 3 f32
+constexpr uint32_t kTrW3F = kTrDY + 128 * 3 * 4;     // 3 x 64 f32 (f16-rounded W3)
+constexpr uint32_t kTrSmemBytes = kTrW3F + 3 * 64 * 4;
+// TMEM columns of the training kernel
+constexpr uint32_t kTcD1 = 0, kTcD2 = 64, kTcD3 = 128, kTcDH1 = 192, kTcDX = 256, kTcDW2 = 320, kTcDW1 = 384;
+constexpr uint32_t kTrTmemCols = 512;
+
+S2D void st_half(uint8_t* base, uint32_t off, float v) { *(__half*)(base + off) = __float2half_rn(v); }
+S2D float ld_half(const uint8_t* base, uint32_t off) { return __half2float(*(const __half*)(base + off)); }
+
+// Bounded wait + state bookkeeping shared by the training steps.
+struct TcSync {
+    uint64_t* bar;
+    uint32_t phase;
+    bool ok;
+    // wait for the committed MMAs; `ok` is made warp-uniform so the collective tcgen05.ld calls
+    // that it guards are executed by whole warps
+    S2D void mma_done() {
+        const bool w = ok && mbar_wait(bar, phase);
+        if (w) phase ^= 1u;
+        ok = __all_sync(0xffffffffu, w);
+        tc_fence_after_sync();
+    }
+};
+
+S2D void block_sync_tc() {
+    fence_smem_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+}
+
+// One pass over n training records (position, target radiance): forward, relative L2 loss
+// sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / 3 per record (denominator not differentiated), backward
+// through the MLP on the tensor cores, and the summed per-record gradients of the weights
+// (grad_w) and of the table entries (grad_t, scattered with atomics).  128 threads,
+// kTrSmemBytes dynamic shared memory, 512 TMEM columns (one CTA per SM).
+__global__ void __launch_bounds__(128, 1) k_cache_train(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
+                                                        const float4* __restrict__ target, uint32_t n) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ float loss_part[4];
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+    for (uint32_t i = t; i < kWImageTrainBytes / 16; i += 128) ((uint4*)(smem + kTrW))[i] = c.wimage[i];
+    if (warp == 0) {
+        tmem_alloc(&tmem_base, kTrTmemCols);
+        tmem_relinquish();
+    }
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    block_sync_tc();
+    float* dy_s = (float*)(smem + kTrDY);
+    float* w3f = (float*)(smem + kTrW3F);
+    for (uint32_t e = t; e < kCacheW3; e += 128) {
+        const uint32_t ch = e / kCacheHidden, i = e % kCacheHidden;
+        w3f[e] = ld_half(smem, kTrW + kW1Bytes + kW2Bytes + kmaj_offset(ch, i, kCacheHidden));
+    }
+    const uint32_t tmem = tmem_base;
+    const uint32_t tlane = tmem + ((32u * (warp & 3u)) << 16);
+    const uint32_t s0 = smem_addr(smem);
+    const uint32_t s_w1 = s0 + kTrW, s_w2 = s_w1 + kW1Bytes, s_w3 = s_w2 + kW2Bytes, s_w2t = s_w3 + kW3Bytes,
+                   s_w1t = s_w2t + kW2TBytes;
+    TcSync sy{&bar, 0u, true};
+    float acc3[2] = {0.f, 0.f};  // dW3 entries t and t + 128 (CUDA cores)
+    float loss = 0.f;
+    bool first = true;
+    const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
+    for (uint32_t tile = blockIdx.x; tile < tiles && sy.ok; tile += gridDim.x) {
+        const uint32_t q = tile * kCacheTile + t;
+        const bool valid = q < n;
+        float3 p = f3(0.f), tg = f3(0.f);
+        if (valid) {
+            const float4 a = pos[q], b = target[q];
+            p = f3(a.x, a.y, a.z);
+            tg = f3(b.x, b.y, b.z);
+        }
+        // ---- forward
+        __half2 f[kCacheLevels];
+        if (valid) cache_encode(c, p, f);
+        else
+#pragma unroll
+            for (uint32_t l = 0; l < kCacheLevels; ++l) f[l] = __floats2half2_rn(0.f, 0.f);
+#pragma unroll
+        for (uint32_t ch = 0; ch < 4; ++ch) store_chunk(smem + kTrX, t, ch, kCacheIn, f + 4 * ch);
+#pragma unroll
+        for (uint32_t l = 0; l < kCacheLevels; ++l) {
+            *(__half*)(smem + kTrXT + kmaj_offset(2 * l, t, 128)) = __low2half(f[l]);
+            *(__half*)(smem + kTrXT + kmaj_offset(2 * l + 1, t, 128)) = __high2half(f[l]);
+        }
+        block_sync_tc();
+        if (t == 0) {
+            umma_gemm(tmem + kTcD1, s0 + kTrX, s_w1, kCacheIn, kCacheHidden, false);
+            umma_commit(&bar);
+        }
+        sy.mma_done();
+        if (sy.ok) {
+#pragma unroll
+            for (uint32_t g = 0; g < 4; ++g) {
+                float v[16];
+                tmem_ld16(tlane + kTcD1 + 16u * g, v);
+                __half2 h[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) h[i] = __floats2half2_rn(fmaxf(v[2 * i], 0.f), fmaxf(v[2 * i + 1], 0.f));
+                store_chunk(smem + kTrH1, t, 2 * g, kCacheHidden, h);
+                store_chunk(smem + kTrH1, t, 2 * g + 1, kCacheHidden, h + 4);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    *(__half*)(smem + kTrH1T + kmaj_offset(16 * g + 2 * i, t, 128)) = __low2half(h[i]);
+                    *(__half*)(smem + kTrH1T + kmaj_offset(16 * g + 2 * i + 1, t, 128)) = __high2half(h[i]);
+                }
+            }
+        }
+        block_sync_tc();
+        if (t == 0 && sy.ok) {
+            umma_gemm(tmem + kTcD2, s0 + kTrH1, s_w2, kCacheHidden, kCacheHidden, false);
+            umma_commit(&bar);
+        }
+        sy.mma_done();
+        if (sy.ok) tmem_relu_to_tile(tlane, kTcD2, smem + kTrH2, t);
+        block_sync_tc();
+        if (t == 0 && sy.ok) {
+            umma_gemm(tmem + kTcD3, s0 + kTrH2, s_w3, kCacheHidden, kCacheOutPad, false);
+            umma_commit(&bar);
+        }
+        sy.mma_done();
+        // ---- loss and output gradient; dH2 = (dY W3) masked by h2 > 0
+        float dy[3] = {0.f, 0.f, 0.f};
+        if (sy.ok) {
+            float v[16];
+            tmem_ld16(tlane + kTcD3, v);
+            if (valid) {
+                const float yt[3] = {tg.x, tg.y, tg.z};
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    const float d = v[ch] - yt[ch], den = v[ch] * v[ch] + 0.01f;
+                    loss += d * d / den / 3.f;
+                    dy[ch] = fminf(fmaxf(2.f * d / den / 3.f, -1e4f), 1e4f);
+                }
+            }
+        }
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) dy_s[3 * t + ch] = dy[ch];
+#pragma unroll
+        for (uint32_t g = 0; g < 8; ++g) {
+            const uint4 hv = *(const uint4*)(smem + kTrH2 + kmaj_offset(t, 8 * g, kCacheHidden));
+            const __half* hh = (const __half*)&hv;
+            __half2 o[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float r2[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t i = 8 * g + 2 * j + u;
+                    const float s = dy[0] * w3f[i] + dy[1] * w3f[64 + i] + dy[2] * w3f[128 + i];
+                    r2[u] = __half2float(hh[2 * j + u]) > 0.f ? s * kCacheGradScale : 0.f;
+                }
+                o[j] = __floats2half2_rn(r2[0], r2[1]);
+                *(__half*)(smem + kTrDH2T + kmaj_offset(8 * g + 2 * j, t, 128)) = __low2half(o[j]);
+                *(__half*)(smem + kTrDH2T + kmaj_offset(8 * g + 2 * j + 1, t, 128)) = __high2half(o[j]);
+            }
+            store_chunk(smem + kTrDH2, t, g, kCacheHidden, o);
+        }
+        block_sync_tc();
+        // dW3 on the CUDA cores: entry e = (channel e / 64, input e % 64), summed over the tile
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t e = t + 128u * k;
+            if (e < kCacheW3) {
+                const uint32_t ch = e / kCacheHidden, i = e % kCacheHidden;
+                float a = 0.f;
+                for (uint32_t b = 0; b < kCacheTile; ++b) a += dy_s[3 * b + ch] * ld_half(smem + kTrH2, kmaj_offset(b, i, kCacheHidden));
+                acc3[k] += a;
+            }
+        }
+        if (t == 0 && sy.ok) {
+            umma_gemm(tmem + kTcDH1, s0 + kTrDH2, s_w2t, kCacheHidden, kCacheHidden, false);
+            umma_gemm(tmem + kTcDW2, s0 + kTrDH2T, s0 + kTrH1T, kCacheTile, kCacheHidden, !first);
+            umma_commit(&bar);
+        }
+        sy.mma_done();
+        // dH1 = (dH2 W2) masked by h1 > 0
+        if (sy.ok) {
+#pragma unroll
+            for (uint32_t g = 0; g < 4; ++g) {
+                float v[16];
+                tmem_ld16(tlane + kTcDH1 + 16u * g, v);
+                const uint4 m0 = *(const uint4*)(smem + kTrH1 + kmaj_offset(t, 16 * g, kCacheHidden));
+                const uint4 m1 = *(const uint4*)(smem + kTrH1 + kmaj_offset(t, 16 * g + 8, kCacheHidden));
+                const __half* h0 = (const __half*)&m0;
+                const __half* h1 = (const __half*)&m1;
+                __half2 o[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float a = __half2float((2 * i < 8) ? h0[2 * i] : h1[2 * i - 8]) > 0.f ? v[2 * i] : 0.f;
+                    const float b = __half2float((2 * i + 1 < 8) ? h0[2 * i + 1] : h1[2 * i + 1 - 8]) > 0.f ? v[2 * i + 1] : 0.f;
+                    o[i] = __floats2half2_rn(a, b);
+                    *(__half*)(smem + kTrDH1T + kmaj_offset(16 * g + 2 * i, t, 128)) = __low2half(o[i]);
+                    *(__half*)(smem + kTrDH1T + kmaj_offset(16 * g + 2 * i + 1, t, 128)) = __high2half(o[i]);
+                }
+                store_chunk(smem + kTrDH1, t, 2 * g, kCacheHidden, o);
+                store_chunk(smem + kTrDH1, t, 2 * g + 1, kCacheHidden, o + 4);
+            }
+        }
+        block_sync_tc();
+        if (t == 0 && sy.ok) {
+            umma_gemm(tmem + kTcDX, s0 + kTrDH1, s_w1t, kCacheHidden, kCacheIn, false);
+            umma_gemm(tmem + kTcDW1, s0 + kTrDH1T, s0 + kTrXT, kCacheTile, kCacheIn, !first);
+            umma_commit(&bar);
+        }
+        sy.mma_done();
+        // dX -> table gradients (same corners and weights as the encoding)
+        float dx[32];
+        if (sy.ok) {
+            tmem_ld16(tlane + kTcDX, dx);
+            tmem_ld16(tlane + kTcDX + 16u, dx + 16);
+        }
+        if (sy.ok && valid) {
+            const float3 u = cache_unit(c, p);
+            for (uint32_t l = 0; l < kCacheLevels; ++l) {
+                const float r = c.res[l];
+                const float fx = u.x * r, fy = u.y * r, fz = u.z * r;
+                const float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
+                const float wx = fx - ix, wy = fy - iy, wz = fz - iz;
+                const uint32_t x0 = (uint32_t)ix, y0 = (uint32_t)iy, z0 = (uint32_t)iz;
+                const float g0 = dx[2 * l] / kCacheGradScale, g1 = dx[2 * l + 1] / kCacheGradScale;
+                float* gt = c.grad_t + ((size_t)l << c.log2_table) * 2;
+                for (uint32_t k = 0; k < 8; ++k) {
+                    const uint32_t ddx = k & 1u, ddy = (k >> 1) & 1u, ddz = k >> 2;
+                    const float w = (ddx ? wx : 1.f - wx) * (ddy ? wy : 1.f - wy) * (ddz ? wz : 1.f - wz);
+                    const uint32_t idx = cache_index(c, l, x0 + ddx, y0 + ddy, z0 + ddz);
+                    atomicAdd(gt + 2 * idx, w * g0);
+                    atomicAdd(gt + 2 * idx + 1, w * g1);
+                }
+            }
+        }
+        first = false;
+        tc_fence_before_sync();
+        __syncthreads();
+        tc_fence_after_sync();
+        sy.ok = __syncthreads_and(sy.ok);
+    }
+    // ---- weight gradients leave TMEM (rows 0..63 = output features live in warps 0 and 1)
+    if (sy.ok && !first && warp < 2) {
+        for (uint32_t g = 0; g < 4; ++g) {
+            float v[16];
+            tmem_ld16(tlane + kTcDW2 + 16u * g, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) atomicAdd(c.grad_w + kCacheW1 + t * kCacheHidden + 16 * g + i, v[i] / kCacheGradScale);
+        }
+        for (uint32_t g = 0; g < 2; ++g) {
+            float v[16];
+            tmem_ld16(tlane + kTcDW1 + 16u * g, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) atomicAdd(c.grad_w + t * kCacheIn + 16 * g + i, v[i] / kCacheGradScale);
+        }
+    }
+    if (sy.ok && !first) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t e = t + 128u * k;
+            if (e < kCacheW3) atomicAdd(c.grad_w + kCacheW1 + kCacheW2 + e, acc3[k]);
+        }
+    }
+    // loss: warp sums, then one atomic per CTA
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0) loss_part[warp] = loss;
+    __syncthreads();
+    if (t == 0) atomicAdd(c.loss_sum, loss_part[0] + loss_part[1] + loss_part[2] + loss_part[3]);
+    if (!sy.ok) {
+        if (t == 0) atomicOr(c.status, 4);
+        mbar_wait(&bar, sy.phase);
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kTrTmemCols);
+}
+
+// Adam on the f32 master parameters with the summed gradients scaled by 1/n; clears the gradients.
+__global__ void k_cache_adam(float* __restrict__ param, float* __restrict__ grad, float* __restrict__ m,
+                             float* __restrict__ v, size_t count, float inv_n, float lr, float b1, float b2, float eps,
+                             float c1, float c2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float g = grad[i] * inv_n;
+    grad[i] = 0.f;
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    param[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
 }  // namespace s2

@@ -63,3 +63,43 @@ def test_cache_params_round_trip_and_init(device):
     device.cache_init(cache_params(19))
     g = device.cache_query(np.zeros((3, 3)))
     assert np.isfinite(g).all()
+
+
+@pytest.mark.parametrize("n", [128, 1000, 4099])
+def test_cache_gradients_match_oracle(device, n):
+    log2 = 12
+    device.cache_init(cache_params(log2))
+    rng = np.random.default_rng(10 + n)
+    w, t = random_params(rng, log2)
+    t *= 0.3
+    device.cache_set_params(w, t)
+    pos = rng.uniform(BOX_MIN, BOX_MAX, (n, 3))
+    tgt = rng.uniform(0, 2, (n, 3))
+    loss, gw, gt = device.cache_gradients(pos, tgt)
+    oloss, ow, ot = co.loss_and_grads(pos, tgt, w, t, BOX_MIN, BOX_MAX)
+    assert abs(loss - oloss) <= 1e-3 * abs(oloss) + 1e-6, (loss, oloss)
+    for name, g, o in (("W1", gw[:co.W1], ow[:co.W1]), ("W2", gw[co.W1:co.W1 + co.W2], ow[co.W1:co.W1 + co.W2]),
+                       ("W3", gw[co.W1 + co.W2:], ow[co.W1 + co.W2:]), ("table", gt.ravel(), ot.ravel())):
+        rel = np.linalg.norm(g - o) / (np.linalg.norm(o) + 1e-12)
+        assert rel < 2e-2, f"{name}: relative gradient error {rel:.4f}"
+
+
+def test_cache_training_fits_a_smooth_field(device):
+    """Online training on a smooth radiance field: the loss falls and held-out predictions follow it."""
+    device.cache_init(cache_params(16))
+    rng = np.random.default_rng(5)
+
+    def field(p):
+        return np.stack([1 + 0.5 * np.sin(3 * p[:, 0]), 1 + 0.5 * np.cos(2 * p[:, 1] + p[:, 2]),
+                         0.5 + 0.25 * np.sin(p[:, 0] * p[:, 2] * 4)], 1)
+
+    losses = []
+    for step in range(300):
+        pos = rng.uniform(BOX_MIN, BOX_MAX, (1 << 14, 3))
+        losses.append(device.cache_train(pos, field(pos)))
+    test = rng.uniform(BOX_MIN, BOX_MAX, (4096, 3))
+    pred = device.cache_query(test)
+    ref = field(test)
+    rel = np.mean((pred - ref) ** 2 / (ref ** 2 + 1e-2))
+    assert np.mean(losses[-10:]) < 0.05 * np.mean(losses[:3]), (losses[:3], losses[-10:])
+    assert rel < 5e-3, rel
