@@ -164,6 +164,12 @@ typedef struct S2View {
                                                   608-726).  Results depend on atomic append order. */
 #define S2_FLAG_ALPHA_TEST_OFF      (1u << 12) /* disable gAlphaTest (on in the reference) */
 #define S2_FLAG_NORMAL_MAPS_OFF     (1u << 13) /* disable gNormalMaps (on in the reference) */
+#define S2_FLAG_RADIANCE_CACHE      (1u << 14) /* learned radiance cache (no counterpart in the
+                                                  reference; needs s2_cache_init): paths end at
+                                                  vertex cache_bounces + 1 with the cache's
+                                                  scattered radiance there, and one path in
+                                                  (paths / cache_train_paths) runs to its end and
+                                                  trains the cache after each wave (s2_render only) */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */
@@ -179,7 +185,9 @@ typedef struct S2RenderParams {
     uint32_t restir_grid_cells;      /* hash-grid cell count (0 = 100000, TestRenderer.cpp:52) */
     float restir_grid_cell_size;     /* minimum cell size (0 = 0.5, TestRenderer.cpp:52) */
     float restir_grid_pixel_radius;  /* mCellPixelRadius: 0 = constant cell size */
-    uint32_t reserved[7];
+    uint32_t cache_bounces;          /* S2_FLAG_RADIANCE_CACHE: bounces before the cache (0 = 2) */
+    uint32_t cache_train_paths;      /* training paths per wave (0 = 65536) */
+    uint32_t reserved[5];
 } S2RenderParams;
 
 /* Output AOVs (caller-allocated, device or host pointers per s2_render's `out_on_host`).

@@ -41,6 +41,7 @@ FLAG_COUNT_FETCHES = 1 << 10
 FLAG_RESTIR_REUSE = 1 << 11
 FLAG_ALPHA_TEST_OFF = 1 << 12
 FLAG_NORMAL_MAPS_OFF = 1 << 13
+FLAG_RADIANCE_CACHE = 1 << 14
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -117,7 +118,7 @@ class S2RenderParams(C.Structure):
         ("environment_sample_probability", C.c_float), ("restir_candidates", C.c_uint32),
         ("restir_max_m", C.c_float), ("wave_paths", C.c_uint32), ("restir_grid_cells", C.c_uint32),
         ("restir_grid_cell_size", C.c_float), ("restir_grid_pixel_radius", C.c_float),
-        ("reserved", C.c_uint32 * 7),
+        ("cache_bounces", C.c_uint32), ("cache_train_paths", C.c_uint32), ("reserved", C.c_uint32 * 5),
     ]
 
 

@@ -199,6 +199,17 @@ extern "C" int s2_cache_get_params(S2Context* ctx, float* weights, float* table)
 }
 
 namespace s2 {
+// Path-tracer terminal vertices: accum[slot] += tput * cache(pos) for up to `cap` queries, the
+// count read from n_dev.
+int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
+                       float4* accum) {
+    CacheState* c = ctx->cache;
+    const uint32_t tiles = (cap + kCacheTile - 1) / kCacheTile;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
+    k_cache_infer<<<grid, 128, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum);
+    return check_cuda(ctx, cudaGetLastError(), "cache apply launch");
+}
+
 // Launches the inference kernel for n float4 positions already on the device.
 int cache_infer_device(S2Context* ctx, const float4* pos, uint32_t n, float4* out) {
     CacheState* c = ctx->cache;
@@ -210,7 +221,7 @@ int cache_infer_device(S2Context* ctx, const float4* pos, uint32_t n, float4* ou
     }
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
-    k_cache_infer<<<grid, 128, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, out);
+    k_cache_infer<<<grid, 128, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr);
     return check_cuda(ctx, cudaGetLastError(), "cache inference launch");
 }
 }  // namespace s2
@@ -245,8 +256,9 @@ extern "C" int s2_cache_query(S2Context* ctx, const float* positions, uint32_t n
 }
 
 namespace s2 {
-// One forward/backward pass over n device records; gradients are summed into grad_w / grad_t.
-int cache_backward_device(S2Context* ctx, const float4* pos, const float4* target, uint32_t n) {
+// One forward/backward pass over n device records (n_dev: optional device count capping n);
+// gradients are summed into grad_w / grad_t.
+int cache_backward_device(S2Context* ctx, const float4* pos, const float4* target, uint32_t n, const uint32_t* n_dev) {
     CacheState* c = ctx->cache;
     if (n == 0) return S2_OK;
     static bool attr_set[64] = {};
@@ -257,23 +269,25 @@ int cache_backward_device(S2Context* ctx, const float4* pos, const float4* targe
     }
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
-    k_cache_train<<<grid, 128, kTrSmemBytes, ctx->stream>>>(c->dev, pos, target, n);
+    k_cache_train<<<grid, 128, kTrSmemBytes, ctx->stream>>>(c->dev, pos, target, n, n_dev);
     return check_cuda(ctx, cudaGetLastError(), "cache training launch");
 }
 
-// Adam step with the summed gradients of `n` records, then the f16 copies are refreshed.
-int cache_adam_device(S2Context* ctx, uint32_t n) {
+// Adam step with the summed gradients of `n` records (or of *n_dev, capped at n), then the f16
+// copies are refreshed.
+int cache_adam_device(S2Context* ctx, uint32_t n, const uint32_t* n_dev) {
     CacheState* c = ctx->cache;
     c->step++;
     const S2CacheParams& p = c->prm;
     const float c1 = 1.f - std::pow(p.beta1, (float)c->step), c2 = 1.f - std::pow(p.beta2, (float)c->step);
     const float inv_n = 1.f / (float)std::max<uint32_t>(n, 1);
     k_cache_adam<<<(kCacheWeights + 255) / 256, 256, 0, ctx->stream>>>(c->w32, c->grad_w, c->adam_w, c->adam_w + kCacheWeights,
-                                                                       kCacheWeights, inv_n, p.learning_rate, p.beta1, p.beta2,
-                                                                       p.epsilon, c1, c2);
+                                                                       kCacheWeights, inv_n, n_dev, n, p.learning_rate, p.beta1,
+                                                                       p.beta2, p.epsilon, c1, c2);
     const size_t nt = 2 * (size_t)c->table_entries;
     k_cache_adam<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(c->t32, c->grad_t, c->adam_t, c->adam_t + nt, nt, inv_n,
-                                                                        p.learning_rate, p.beta1, p.beta2, p.epsilon, c1, c2);
+                                                                        n_dev, n, p.learning_rate, p.beta1, p.beta2, p.epsilon,
+                                                                        c1, c2);
     int rc = check_cuda(ctx, cudaGetLastError(), "cache Adam launch");
     if (rc != S2_OK) return rc;
     return repack(ctx);
@@ -325,8 +339,8 @@ extern "C" int s2_cache_train(S2Context* ctx, const float* positions, const floa
     if (rc != S2_OK) { free_bufs(tmp); return rc; }
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaMemsetAsync(ctx->cache->loss, 0, sizeof(float), ctx->stream);
-    rc = cache_backward_device(ctx, dpos, dtgt, n);
-    if (rc == S2_OK) rc = cache_adam_device(ctx, n);
+    rc = cache_backward_device(ctx, dpos, dtgt, n, nullptr);
+    if (rc == S2_OK) rc = cache_adam_device(ctx, n, nullptr);
     return finish(ctx, tmp, rc, loss, n);
 }
 
@@ -347,7 +361,7 @@ extern "C" int s2_cache_gradients(S2Context* ctx, const float* positions, const 
     cudaMemsetAsync(c->grad_t, 0, sizeof(float) * nt, ctx->stream);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaMemsetAsync(c->loss, 0, sizeof(float), ctx->stream);
-    rc = cache_backward_device(ctx, dpos, dtgt, n);
+    rc = cache_backward_device(ctx, dpos, dtgt, n, nullptr);
     std::vector<float> gw(kCacheWeights), gt;
     if (rc == S2_OK) {
         cudaMemcpyAsync(gw.data(), c->grad_w, sizeof(float) * kCacheWeights, cudaMemcpyDeviceToHost, ctx->stream);

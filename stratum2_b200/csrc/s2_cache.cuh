@@ -131,10 +131,15 @@ S2D void tmem_relu_to_tile(uint32_t tlane, uint32_t col, uint8_t* dst, uint32_t 
     }
 }
 
-// Radiance cache inference: out[i] = MLP(encode(pos[i])), raw (unclamped) outputs.
+// Radiance cache inference: out[i] = MLP(encode(pos[i])), raw (unclamped) outputs.  With `tput`
+// (the path tracer's terminal vertices) the result is instead added to the path's accumulator:
+// accum[slot] += tput[i] * max(y, 0), slot in pos[i].w.  n_dev (optional) caps n with a device count.
 // Persistent: grid-stride over tiles of 128 queries; 128 threads; kInfSmemBytes dynamic smem.
 __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
-                                                        uint32_t n, float4* __restrict__ out) {
+                                                        uint32_t n, const uint32_t* __restrict__ n_dev,
+                                                        float4* __restrict__ out, const float4* __restrict__ tput,
+                                                        float4* __restrict__ accum) {
+    if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_base;
@@ -222,7 +227,20 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
         if (ok) {
             float v[16];
             tmem_ld16(tlane, v);
-            if (q < n) out[q] = make_float4(v[0], v[1], v[2], 0.f);
+            if (q < n) {
+                if (tput) {
+                    const float4 tp = tput[q];
+                    const uint32_t slot = __float_as_uint(pos[q].w);
+                    const float r = fmaxf(v[0], 0.f) * tp.x, g = fmaxf(v[1], 0.f) * tp.y, b = fmaxf(v[2], 0.f) * tp.z;
+                    if (isfinite(r) && isfinite(g) && isfinite(b)) {
+                        float4 a = accum[slot];
+                        a.x += r; a.y += g; a.z += b;
+                        accum[slot] = a;
+                    }
+                } else {
+                    out[q] = make_float4(v[0], v[1], v[2], 0.f);
+                }
+            }
         }
         tc_fence_before_sync();
         __syncthreads();
@@ -292,7 +310,9 @@ S2D void block_sync_tc() {
 // (grad_w) and of the table entries (grad_t, scattered with atomics).  128 threads,
 // kTrSmemBytes dynamic shared memory, 512 TMEM columns (one CTA per SM).
 __global__ void __launch_bounds__(128, 1) k_cache_train(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
-                                                        const float4* __restrict__ target, uint32_t n) {
+                                                        const float4* __restrict__ target, uint32_t n,
+                                                        const uint32_t* __restrict__ n_dev) {
+    if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_base;
@@ -535,11 +555,13 @@ __global__ void __launch_bounds__(128, 1) k_cache_train(const __grid_constant__ 
 }
 
 // Adam on the f32 master parameters with the summed gradients scaled by 1/n; clears the gradients.
+// n_dev (optional): the record count is read on the device (capped at n_cap) instead of inv_n.
 __global__ void k_cache_adam(float* __restrict__ param, float* __restrict__ grad, float* __restrict__ m,
-                             float* __restrict__ v, size_t count, float inv_n, float lr, float b1, float b2, float eps,
-                             float c1, float c2) {
+                             float* __restrict__ v, size_t count, float inv_n, const uint32_t* __restrict__ n_dev,
+                             uint32_t n_cap, float lr, float b1, float b2, float eps, float c1, float c2) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
+    if (n_dev) inv_n = 1.f / (float)max(1u, min(*n_dev, n_cap));
     const float g = grad[i] * inv_n;
     grad[i] = 0.f;
     const float mi = b1 * m[i] + (1.f - b1) * g;

@@ -39,6 +39,10 @@ struct RenderState {
     } grid[2];
     uint32_t grid_cur = 0;
     bool grid_prev_valid = false;
+    // radiance cache queues: terminal-vertex queries and training vertices
+    std::vector<DevBuf> cache_bufs;
+    float4 *cq_pos = nullptr, *cq_thr = nullptr, *tr_pos = nullptr, *tr_thr = nullptr, *tr_rad = nullptr;
+    uint32_t cq_cap = 0, tr_cap = 0;
 };
 
 void destroy_batch_state(S2Context* ctx);
@@ -48,6 +52,7 @@ void destroy_render_state(S2Context* ctx) {
     if (!ctx->render) return;
     for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
     for (auto& g : ctx->render->grid) free_bufs(g.bufs);
+    free_bufs(ctx->render->cache_bufs);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -120,6 +125,24 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
     return S2_OK;
 }
 
+// Radiance-cache queues: `cq` terminal-vertex queries and `tr` training vertices.
+int ensure_cache_queues(S2Context* ctx, RenderState* st, uint32_t cq, uint32_t tr) {
+    if (st->cq_cap >= cq && st->tr_cap >= tr) return S2_OK;
+    free_bufs(st->cache_bufs);
+    st->cq_cap = st->tr_cap = 0;
+    cq = std::max(cq, st->cq_cap);
+    st->cq_pos = alloc<float4>(ctx, st->cache_bufs, cq);
+    st->cq_thr = alloc<float4>(ctx, st->cache_bufs, cq);
+    st->tr_pos = alloc<float4>(ctx, st->cache_bufs, tr);
+    st->tr_thr = alloc<float4>(ctx, st->cache_bufs, tr);
+    st->tr_rad = alloc<float4>(ctx, st->cache_bufs, tr);
+    for (auto& b : st->cache_bufs) if (!b.ptr) { free_bufs(st->cache_bufs); return S2_ERR_OOM; }
+    if (st->cache_bufs.size() != 5) { free_bufs(st->cache_bufs); return S2_ERR_OOM; }
+    st->cq_cap = cq;
+    st->tr_cap = tr;
+    return S2_OK;
+}
+
 // (Re)allocates one hash grid for `cells` cells and `size` records (GpuHashGrid::init,
 // src/App/GpuHashGrid.cpp:17-69).
 int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t size) {
@@ -144,7 +167,8 @@ int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t s
 
 template <bool L, bool R>
 void launch_shade(const PTParams& P, uint32_t parity, int blocks, cudaStream_t s) {
-    k_shade<L, R><<<blocks, 128, 0, s>>>(P, parity);
+    if (P.cache_on) k_shade<L, R, true><<<blocks, 128, 0, s>>>(P, parity);
+    else k_shade<L, R><<<blocks, 128, 0, s>>>(P, parity);
 }
 
 }  // namespace
@@ -178,6 +202,8 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
+    const bool cache = (prm->flags & S2_FLAG_RADIANCE_CACHE) != 0;
+    if (cache && !ctx->cache) return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RADIANCE_CACHE needs s2_cache_init");
     if (reuse && (prm->restir_grid_cells > (1u << 26) || prm->restir_grid_cell_size < 0.f ||
                   !std::isfinite(prm->restir_grid_cell_size) || !(prm->restir_grid_pixel_radius >= 0.f) ||
                   !std::isfinite(prm->restir_grid_pixel_radius) || !(prm->restir_max_m > 0.f)))
@@ -251,6 +277,17 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     } else {
         st->grid_prev_valid = false;  // TestRenderer.cpp:495-498 drops the grids when reuse is off
     }
+    const uint32_t cache_len = (prm->cache_bounces ? prm->cache_bounces : 2u) + 1u;
+    const uint32_t train_paths = prm->cache_train_paths ? prm->cache_train_paths : 65536u;
+    if (cache) {
+        const uint64_t tr_cap64 = std::min<uint64_t>((uint64_t)train_paths * std::max(1u, prm->max_path_length), 1u << 26);
+        rc = ensure_cache_queues(ctx, st, capacity, (uint32_t)tr_cap64);
+        if (rc != S2_OK) return set_error(ctx, rc, "radiance cache queue allocation failed");
+        P.cache_on = 1;
+        P.cache_len = cache_len;
+        P.cq_pos = st->cq_pos; P.cq_thr = st->cq_thr; P.cq_cap = st->cq_cap;
+        P.tr_pos = st->tr_pos; P.tr_thr = st->tr_thr; P.tr_rad = st->tr_rad; P.tr_cap = st->tr_cap;
+    }
     if (!(prm->flags & S2_FLAG_ACCUMULATE)) {
         cudaMemsetAsync(st->total, 0, sizeof(float4) * pixels, s);
         st->accumulated_spp = 0;
@@ -275,6 +312,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         P.wave_base_sample = done;
         P.wave_samples = std::min(slots, prm->spp - done);
         const uint32_t n = P.wave_samples * pixels;
+        if (cache) P.train_mod = std::max(1u, n / train_paths);
         k_raygen<<<(n + 255) / 256, 256, 0, s>>>(P);
         for (uint32_t b = 0; b < prm->max_path_length; ++b) {
             const uint32_t parity = b & 1u;
@@ -287,11 +325,24 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
             else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
             ev_end();
+            if (cache && b + 1 == cache_len) {
+                rc = cache_apply_device(ctx, st->cq_pos, st->cq_thr, st->cq_cap, st->counters + C_CACHEQ, st->accum);
+                if (rc != S2_OK) return rc;
+                launches += 1;
+            }
             ev_begin(2);
             if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
             else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
             ev_end();
             launches += 4;
+        }
+        if (cache) {
+            // training: per-vertex targets from the finished training paths, one optimiser step
+            k_cache_targets<<<std::max(1, st->shade_blocks / 2), 256, 0, s>>>(P);
+            rc = cache_backward_device(ctx, st->tr_pos, st->tr_rad, st->tr_cap, st->counters + C_TRAIN);
+            if (rc == S2_OK) rc = cache_adam_device(ctx, st->tr_cap, st->counters + C_TRAIN);
+            if (rc != S2_OK) return rc;
+            launches += 5;
         }
         k_wave_finish<<<1, 32, 0, s>>>(P);
         k_reduce<<<(pixels + 255) / 256, 256, 0, s>>>(P, st->total);
@@ -329,6 +380,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         cudaMemcpyAsync(&status, ctx->status_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
         rc = check_cuda(ctx, cudaStreamSynchronize(s), "render");
         if (rc != S2_OK) return rc;
+        if (status & 4) return set_error(ctx, S2_ERR_TIMEOUT, "tensor-core wait timed out in the radiance cache");
         if (status) return set_error(ctx, S2_ERR_DEVICE, "traversal stack overflow during render");
         if (stats_out) {
             float ms = 0.f;
@@ -430,8 +482,8 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
-    if (prm->flags & S2_FLAG_RESTIR_REUSE)
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE is supported by s2_render only");
+    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RADIANCE_CACHE))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RADIANCE_CACHE are supported by s2_render only");
     cudaSetDevice(ctx->device);
     std::vector<ViewEntry> ve(nviews);
     std::vector<uint32_t> layout;

@@ -204,7 +204,7 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
     return so;
 }
 
-template <bool LAMBERT, bool RESTIR>
+template <bool LAMBERT, bool RESTIR, bool CACHE = false>
 __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
     const uint32_t count = P.counters[parity];
     const PathQueue qi = P.q[parity];
@@ -215,9 +215,10 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t rounded = (count + 31u) & ~31u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += stride) {
-        bool alive = false, shadow = false;
+        bool alive = false, shadow = false, cq = false, tr = false;
         float4 n0, n1, n2;
         uint4 n3;
+        float4 c_pos, c_thr, c_rad;
         ShadowOut so;
         so.valid = false;
         uint32_t slot = 0;
@@ -309,7 +310,26 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
                         if (w > 0.f) add_contrib(P, slot, e * w);
                     }
                 }
-                if (len < P.max_len && any_pos(m.base())) {
+                // ---- learned radiance cache: the terminal vertex of a non-training path takes its
+                // scattered radiance from the cache; training paths record their vertices
+                bool cached = false;
+                if (CACHE && P.cache_on) {
+                    const float4 pw = make_float4(sd.pos.x, sd.pos.y, sd.pos.z, __uint_as_float(slot));
+                    if (!(meta & 0x200u)) {
+                        if (len == P.cache_len) {
+                            cached = true;
+                            cq = any_pos(m.base());
+                            c_pos = pw;
+                            c_thr = make_float4(thr.x, thr.y, thr.z, 0.f);
+                        }
+                    } else if (len + 1 >= P.min_len && len < P.max_len) {
+                        tr = true;
+                        c_pos = pw;
+                        c_thr = make_float4(thr.x, thr.y, thr.z, 0.f);
+                        c_rad = P.accum[slot];
+                    }
+                }
+                if (!cached && len < P.max_len && any_pos(m.base())) {
                     const bool sing = mat_singular<LAMBERT>(m);
                     if (!sing && nee) so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim);
                     const float cp = fminf(1.f, cont_prob(m));
@@ -352,6 +372,12 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
             P.sh_o[si] = make_float4(so.o.x, so.o.y, so.o.z, so.tmax);
             P.sh_d[si] = make_float4(so.d.x, so.d.y, so.d.z, __uint_as_float(slot));
             P.sh_c[si] = make_float4(so.c.x, so.c.y, so.c.z, 0.f);
+        }
+        if (CACHE && P.cache_on) {
+            const uint32_t ci = warp_append(&P.counters[C_CACHEQ], cq);
+            if (cq && ci < P.cq_cap) { P.cq_pos[ci] = c_pos; P.cq_thr[ci] = c_thr; }
+            const uint32_t ti = warp_append(&P.counters[C_TRAIN], tr);
+            if (tr && ti < P.tr_cap) { P.tr_pos[ti] = c_pos; P.tr_thr[ti] = c_thr; P.tr_rad[ti] = c_rad; }
         }
     }
 }

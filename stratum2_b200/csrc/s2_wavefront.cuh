@@ -25,6 +25,8 @@ enum Counter : uint32_t {
     C_SHADOW = 2,   // shadow rays appended this bounce
     C_WORK_EXT = 3, // warp work counters for the persistent traversal kernels
     C_WORK_OCC = 4,
+    C_CACHEQ = 5,   // radiance-cache queries appended this bounce
+    C_TRAIN = 6,    // radiance-cache training vertices appended this wave
     C_COUNT = 8
 };
 enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_EXT_NODES = 3, S_EXT_TRIS = 4, S_SH_NODES = 5, S_SH_TRIS = 6, S_COUNT = 8 };
@@ -87,6 +89,14 @@ struct PTParams {
     HashGridDev grid_cur, grid_prev;
     uint32_t reuse, prev_valid;
     float max_m;
+    // learned radiance cache (S2_FLAG_RADIANCE_CACHE): non-training paths end at vertex cache_len
+    // with a query {position, slot} + throughput; training paths (meta bit 9, one in train_mod)
+    // record every vertex {position, slot}, throughput, accumulated radiance
+    uint32_t cache_on, cache_len, train_mod;
+    float4 *cq_pos, *cq_thr;
+    uint32_t cq_cap;
+    float4 *tr_pos, *tr_thr, *tr_rad;
+    uint32_t tr_cap;
 };
 
 // fixed-point scale of the batched accumulators: integer sums are independent of the order of the
@@ -119,6 +129,7 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_REUSE (1u << 11)
 #define S2F_NO_ALPHA (1u << 12)
 #define S2F_NO_NORMAL_MAPS (1u << 13)
+#define S2F_CACHE (1u << 14)
 
 constexpr int kTravBlock = 128;
 
@@ -155,6 +166,8 @@ __global__ void k_raygen(PTParams P) {
         P.counters[C_SHADOW] = 0;
         P.counters[C_WORK_EXT] = 0;
         P.counters[C_WORK_OCC] = 0;
+        P.counters[C_CACHEQ] = 0;
+        P.counters[C_TRAIN] = 0;
     }
     if (i >= n) return;
     const uint32_t k = i / P.pixels, pix = i - k * P.pixels;
@@ -178,7 +191,8 @@ __global__ void k_raygen(PTParams P) {
     const float3 wd = normalize(f3(c[0] * ld.x + c[1] * ld.y + c[2] * ld.z, c[4] * ld.x + c[5] * ld.y + c[6] * ld.z,
                                    c[8] * ld.x + c[9] * ld.y + c[10] * ld.z));
     const float3 d = unpack_normal(pack_normal(wd));
-    const uint32_t meta = (sample == 0 ? 0x100u : 0u);  // path length 0; bit 8: write AOVs
+    uint32_t meta = (sample == 0 ? 0x100u : 0u);  // path length 0; bit 8: write AOVs
+    if (P.cache_on && pcg_hash(i ^ pcg_hash(P.frame_seed + sample)) % P.train_mod == 0u) meta |= 0x200u;  // training path
     const PathQueue& q = P.q[0];
     q.s0[i] = make_float4(c[3], c[7], c[11], 0.f);
     q.s1[i] = make_float4(d.x, d.y, d.z, 1.f);
@@ -195,6 +209,7 @@ __global__ void k_bounce_setup(PTParams P, uint32_t parity, int first) {
     P.counters[C_SHADOW] = 0;
     P.counters[C_WORK_EXT] = 0;
     P.counters[C_WORK_OCC] = 0;
+    P.counters[C_CACHEQ] = 0;
 }
 __global__ void k_wave_finish(PTParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -396,4 +411,20 @@ __global__ void k_resolve(const float4* __restrict__ total, uint32_t pixels, flo
     out[p] = make_float4(t.x * s, t.y * s, t.z * s, 1.f);
 }
 
+}  // namespace s2
+
+namespace s2 {
+// Radiance-cache training targets: the radiance a training path gathered after each recorded vertex
+// (its final accumulator minus the value when the vertex was reached), per unit throughput.
+__global__ void k_cache_targets(PTParams P) {
+    const uint32_t n = min(P.counters[C_TRAIN], P.tr_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = __float_as_uint(P.tr_pos[i].w);
+        const float4 fin = P.accum[slot], r0 = P.tr_rad[i], t = P.tr_thr[i];
+        const float tx = t.x > 1e-8f ? (fin.x - r0.x) / t.x : 0.f;
+        const float ty = t.y > 1e-8f ? (fin.y - r0.y) / t.y : 0.f;
+        const float tz = t.z > 1e-8f ? (fin.z - r0.z) / t.z : 0.f;
+        P.tr_rad[i] = make_float4(fmaxf(tx, 0.f), fmaxf(ty, 0.f), fmaxf(tz, 0.f), 0.f);
+    }
+}
 }  // namespace s2

@@ -1,0 +1,68 @@
+"""The radiance cache inside the path tracer (S2_FLAG_RADIANCE_CACHE): with the cache beyond the
+maximum path length the render is the plain render (training paths are plain paths and training
+does not touch the image; the shade kernel's cache instantiation may round a few contributions
+differently, so the comparison allows 1e-5 relative); with paths ending in the cache, the
+progressive image after online training stays close to the FP64 golden image while its per-frame
+noise is lower than the plain path tracer's."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from stratum2_b200 import _abi
+from stratum2_b200.metrics import relmse
+from test_render_gpu import make_params, terrain_wl
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+J = _abi.FLAG_PIXEL_JITTER
+CACHE = _abi.FLAG_RADIANCE_CACHE
+
+
+@pytest.fixture(scope="module")
+def terrain(device):
+    wl = terrain_wl()
+    device.upload_scene(wl.scene)
+    device.cache_init()
+    return wl
+
+
+def test_cache_beyond_max_length_is_the_plain_render(device, terrain):
+    wl = terrain
+    device.upload_scene(wl.scene)
+    device.cache_init()
+    p = make_params(4, 1, 6, J, seed=21)
+    plain = device.render(wl.view, wl.width, wl.height, params=p)
+    p.flags |= CACHE
+    p.cache_bounces = 10
+    p.cache_train_paths = 512
+    cached = device.render(wl.view, wl.width, wl.height, params=p)
+    np.testing.assert_allclose(cached.radiance, plain.radiance, rtol=1e-5, atol=1e-7)
+    w_after, _ = device.cache_get_params()
+    device.cache_init()
+    w0, _ = device.cache_get_params()
+    assert not np.array_equal(w_after, w0)  # the render trained the cache
+
+
+def test_cached_render_close_to_golden_with_less_noise(device, terrain):
+    wl = terrain
+    device.upload_scene(wl.scene)
+    device.cache_init()
+    gold = np.load(GOLDEN / "terrain_64x36_fp64_131072spp.npz")
+    ref = gold["mean"].astype(np.float64)
+    p = make_params(1, 1, 6, J | CACHE)
+    p.cache_train_paths = 1024
+    frames = []
+    for f in range(1024):
+        p.frame_seed = 7000 + f
+        frames.append(device.render(wl.view, wl.width, wl.height, params=p).radiance[..., :3].astype(np.float64))
+    frames = np.stack(frames)
+    late = frames[512:]
+    plain = np.stack([device.render(wl.view, wl.width, wl.height, params=make_params(1, 1, 6, J, seed=90000 + f))
+                      .radiance[..., :3].astype(np.float64) for f in range(512)])
+    err_cache = relmse(late.mean(0), ref)
+    var_cache = np.mean(late.var(0) / (ref ** 2 + 1e-2))
+    var_plain = np.mean(plain.var(0) / (ref ** 2 + 1e-2))
+    print("cache relMSE", err_cache, "per-frame relvar cache", var_cache, "plain", var_plain)
+    assert err_cache < 0.02, err_cache
+    assert var_cache < var_plain, (var_cache, var_plain)
