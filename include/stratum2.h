@@ -278,6 +278,29 @@ void s2_default_render_params(S2RenderParams* p);
 int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams* params,
                        const S2Aovs* out, S2RenderStats* stats_out);
 
+/* Replaces the texels of uploaded image `index` (same width, height and channel count as at
+ * s2_scene_upload; host or device pointer).  An environment image gets its sampling tables rebuilt.
+ * The alpha-test flags baked into the BVH at s2_build_bvh are not recomputed. */
+int  s2_update_image(S2Context* ctx, uint32_t index, const float* texels, int on_device);
+
+/* ---------------------------------------------------------------- differentiable rendering
+ * No counterpart in the reference.  The same path tracer as s2_render (NEE + MIS, Russian
+ * roulette, path-length gates, the same random numbers per pixel and sample) with textured material
+ * parameters kept in f32 instead of being re-quantised to 8 bits, so the image is differentiable in
+ * the texels.  Not supported: ReSTIR, the radiance cache, accumulation, profiling flags, AOVs. */
+/* radiance: float4 per pixel (mean * 2^exposure, w = 1), host (out_on_host) or device. */
+int  s2_render_diff(S2Context* ctx, const S2View* view, const S2RenderParams* params, float* radiance,
+                    int out_on_host, S2RenderStats* stats_out);
+/* Adjoint path replay: d_images[k] (float4 per texel of image k, or NULL to skip) receives the
+ * gradient of sum(d_radiance * radiance) with respect to image k's texels, where radiance is the
+ * s2_render_diff image for the same view and params.  Every path is replayed twice from its seed:
+ * once for its radiance, once to push the adjoint through its vertices.  Sampling pdfs, MIS weights
+ * and Russian roulette are held constant.  Gradients reach base-colour textures (rgb), packed[2]
+ * textures (roughness channel, y) and the environment image (rgb).  on_host applies to d_radiance
+ * and d_images alike. */
+int  s2_render_adjoint(S2Context* ctx, const S2View* view, const S2RenderParams* params, const float* d_radiance,
+                       int on_host, float* const* d_images, S2RenderStats* stats_out);
+
 /* ---------------------------------------------------------------- learned radiance cache
  * No counterpart in the reference.  A multiresolution hash-grid encoding of world-space position
  * (16 levels x 2 features, 2^log2_table entries per level, resolutions geometric from

@@ -18,27 +18,34 @@ namespace orc {
 constexpr uint32_t FLAG_PIXEL_JITTER = 1u << 0, FLAG_LAMBERTIAN = 1u << 1, FLAG_PCG32 = 1u << 2, FLAG_NO_NEE = 1u << 3,
                    FLAG_RESTIR = 1u << 4, FLAG_REF_ENV_MIS = 1u << 5, FLAG_NO_RR = 1u << 6, FLAG_NO_SHADING_NORMALS = 1u << 8,
                    FLAG_RESTIR_REUSE = 1u << 11, FLAG_NO_ALPHA = 1u << 12,
-                   FLAG_NO_NORMAL_MAPS = 1u << 13;
+                   FLAG_NO_NORMAL_MAPS = 1u << 13,
+                   FLAG_F32_MATERIALS = 1u << 30;  // oracle only: the materials of s2_render_diff
 
 template <class R> R un8(uint32_t w, int shift) { return R((w >> shift) & 0xffu) / R(255); }
 inline uint32_t pk8(double v) { v = std::min(std::max(v, 0.0), 1.0); return (uint32_t)std::floor((float)v * 255.f + 0.5f); }
 
 // PackedMaterialData (compat/material_data.h:12-73)
+// With `f32` set (the differentiable renderer's materials) the getters return the unquantised
+// parameters in `f` instead: base rgb, emission rgb, then specular .. eta as in the packed order.
 template <class R> struct Mat {
     uint32_t w[4];
     R escale;
-    V3<R> base() const { return V3<R>(un8<R>(w[0], 0), un8<R>(w[0], 8), un8<R>(w[0], 16)); }
-    V3<R> emission() const { return V3<R>(un8<R>(w[1], 0), un8<R>(w[1], 8), un8<R>(w[1], 16)) * escale; }
-    R specular() const { return un8<R>(w[0], 24); }
-    R sheen() const { return un8<R>(w[1], 24); }
-    R metallic() const { return un8<R>(w[2], 0); }
-    R roughness() const { return un8<R>(w[2], 8); }
-    R anisotropic() const { return un8<R>(w[2], 16); }
-    R subsurface() const { return un8<R>(w[2], 24); }
-    R clearcoat() const { return un8<R>(w[3], 0); }
-    R clearcoat_gloss() const { return un8<R>(w[3], 8); }
-    R transmission() const { return un8<R>(w[3], 16); }
-    R eta1() const { return un8<R>(w[3], 24) + 1; }
+    bool f32 = false;
+    R f[16];
+    V3<R> base() const { return f32 ? V3<R>(f[0], f[1], f[2]) : V3<R>(un8<R>(w[0], 0), un8<R>(w[0], 8), un8<R>(w[0], 16)); }
+    V3<R> emission() const {
+        return f32 ? V3<R>(f[3], f[4], f[5]) : V3<R>(un8<R>(w[1], 0), un8<R>(w[1], 8), un8<R>(w[1], 16)) * escale;
+    }
+    R specular() const { return f32 ? f[6] : un8<R>(w[0], 24); }
+    R sheen() const { return f32 ? f[7] : un8<R>(w[1], 24); }
+    R metallic() const { return f32 ? f[8] : un8<R>(w[2], 0); }
+    R roughness() const { return f32 ? f[9] : un8<R>(w[2], 8); }
+    R anisotropic() const { return f32 ? f[10] : un8<R>(w[2], 16); }
+    R subsurface() const { return f32 ? f[11] : un8<R>(w[2], 24); }
+    R clearcoat() const { return f32 ? f[12] : un8<R>(w[3], 0); }
+    R clearcoat_gloss() const { return f32 ? f[13] : un8<R>(w[3], 8); }
+    R transmission() const { return f32 ? f[14] : un8<R>(w[3], 16); }
+    R eta1() const { return (f32 ? f[15] : un8<R>(w[3], 24)) + 1; }
     void set_base(const V3<R>& c) {
         w[0] = (w[0] & 0xff000000u) | pk8(c.x) | pk8(c.y) << 8 | pk8(c.z) << 16;
     }
@@ -163,6 +170,10 @@ template <class R> struct Tracer {
     uint64_t ext_rays = 0, shadow_rays = 0;
     CpuGrid<R>* grid_cur = nullptr;    // ReSTIR DI reuse: grid appended to by this call
     CpuGrid<R>* grid_prev = nullptr;   // the previous call's grid (null: none)
+    // Detached sampling (test infrastructure for the adjoint renderer): materials for sampling
+    // decisions, pdfs, MIS and Russian roulette come from this scene (same geometry, other images),
+    // BSDF values and emission from `s`; null: both from `s`.
+    const Scene<R>* samp = nullptr;
     Tracer(const Scene<R>& sc, const Params& pp) : s(sc), p(pp) {}
 
     bool has_env() const { return s.env_addr != S2_NO_ENVIRONMENT; }
@@ -251,22 +262,43 @@ template <class R> struct Tracer {
     }
 
     // LoadMaterial (material.hlsli:15-46)
-    Mat<R> material(uint32_t addr, R u, R v) const {
+    Mat<R> material(uint32_t addr, R u, R v, const Scene<R>* sc = nullptr) const {
+        const Scene<R>& S = sc ? *sc : s;
         Mat<R> m;
-        for (int k = 0; k < 4; ++k) m.w[k] = s.u32(s.mat, addr + 4 * k);
+        for (int k = 0; k < 4; ++k) m.w[k] = S.u32(S.mat, addr + 4 * k);
         uint32_t img[4];
-        for (int k = 0; k < 4; ++k) img[k] = s.u32(s.mat, addr + 16 + 4 * k);
-        m.escale = (R)s.f32(s.mat, addr + 32);
-        const uint32_t nimg = (uint32_t)s.images.size();
-        if (img[0] < nimg) m.set_base(m.base() * sample_image(img[0], u, v));
-        if (img[1] < nimg) m.set_emission(m.emission() * sample_image(img[1], u, v));
+        for (int k = 0; k < 4; ++k) img[k] = S.u32(S.mat, addr + 16 + 4 * k);
+        m.escale = (R)S.f32(S.mat, addr + 32);
+        const uint32_t nimg = (uint32_t)S.images.size();
+        if (p.flags & FLAG_F32_MATERIALS) {
+            // the differentiable renderer's materials: texture modulation in floating point
+            const V3<R> b = m.base(), e = m.emission();
+            const R q[16] = {b.x, b.y, b.z, e.x, e.y, e.z, m.specular(), m.sheen(), m.metallic(), m.roughness(),
+                             m.anisotropic(), m.subsurface(), m.clearcoat(), m.clearcoat_gloss(), m.transmission(),
+                             un8<R>(m.w[3], 24)};
+            for (int k = 0; k < 16; ++k) m.f[k] = q[k];
+            m.f32 = true;
+            if (img[0] < nimg) { const V3<R> t = S.images[img[0]].sample(u, v); m.f[0] *= t.x; m.f[1] *= t.y; m.f[2] *= t.z; }
+            if (img[1] < nimg) { const V3<R> t = S.images[img[1]].sample(u, v); m.f[3] *= t.x; m.f[4] *= t.y; m.f[5] *= t.z; }
+            if (img[2] < nimg) {
+                R a; const V3<R> t = S.images[img[2]].sample(u, v, &a);
+                m.f[8] *= t.x; m.f[9] = 1 - (1 - m.f[9]) * (1 - t.y); m.f[10] *= t.z; m.f[11] *= a;
+            }
+            if (img[3] < nimg) {
+                R a; const V3<R> t = S.images[img[3]].sample(u, v, &a);
+                m.f[12] *= t.x; m.f[13] *= t.y; m.f[14] *= t.z; m.f[15] *= a;
+            }
+            return m;
+        }
+        if (img[0] < nimg) m.set_base(m.base() * S.images[img[0]].sample(u, v));
+        if (img[1] < nimg) m.set_emission(m.emission() * S.images[img[1]].sample(u, v));
         if (img[2] < nimg) {
-            R a; const V3<R> vi = s.images[img[2]].sample(u, v, &a);
+            R a; const V3<R> vi = S.images[img[2]].sample(u, v, &a);
             R x = un8<R>(m.w[2], 0) * vi.x, y = 1 - (1 - un8<R>(m.w[2], 8)) * (1 - vi.y), z = un8<R>(m.w[2], 16) * vi.z, ww = un8<R>(m.w[2], 24) * a;
             m.w[2] = pk8(x) | pk8(y) << 8 | pk8(z) << 16 | pk8(ww) << 24;
         }
         if (img[3] < nimg) {
-            R a; const V3<R> vi = s.images[img[3]].sample(u, v, &a);
+            R a; const V3<R> vi = S.images[img[3]].sample(u, v, &a);
             m.w[3] = pk8(un8<R>(m.w[3], 0) * vi.x) | pk8(un8<R>(m.w[3], 8) * vi.y) << 8 | pk8(un8<R>(m.w[3], 16) * vi.z) << 16 | pk8(un8<R>(m.w[3], 24) * a) << 24;
         }
         return m;
@@ -752,10 +784,11 @@ template <class R> struct Tracer {
                 }
             }
             if (len >= p.max_len) break;
-            if (!can_eval(m)) break;
-            const bool sing = singular(m);
-            if (!sing && nee) connect_to_light(m, sd, in, thr, rng, len, add, inst, prim);
-            const R cp = std::min(R(1), cont_prob(m));
+            const Mat<R> ms = samp ? material(sd.mat, sd.u, sd.v, samp) : m;
+            if (!can_eval(ms)) break;
+            const bool sing = singular(ms);
+            if (!sing && nee) connect_to_light(m, sd, in, thr, rng, len, add, inst, prim, samp ? &ms : nullptr);
+            const R cp = std::min(R(1), cont_prob(ms));
             if (!(p.flags & FLAG_NO_RR)) {
                 float f[4]; rng.next_float(f);
                 if ((R)f[0] > cp) break;
@@ -763,7 +796,8 @@ template <class R> struct Tracer {
             float f[4]; rng.next_float(f);
             const R rnd3[3] = {f[0], f[1], f[2]};
             V3<R> sdir, refl; R fwd, rev, rough;
-            sample_dir(m, in, rnd3, sdir, refl, fwd, rev, rough);
+            sample_dir(ms, in, rnd3, sdir, refl, fwd, rev, rough);
+            if (samp) { V3<R> fe; R a, b; eval(m, in, sdir, fe, a, b); refl = fe; }
             const R cpm = (p.flags & FLAG_NO_RR) ? R(1) : cp;
             fwd *= cpm; rev *= cpm;
             thr = thr * refl / fwd;
@@ -829,8 +863,8 @@ template <class R> struct Tracer {
 
     template <class Add>
     void connect_to_light(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, const V3<R>& thr, Rng& rng, uint32_t len,
-                          Add& add, uint32_t inst, uint32_t prim) {
-        const R cp = (p.flags & FLAG_NO_RR) ? R(1) : cont_prob(m);
+                          Add& add, uint32_t inst, uint32_t prim, const Mat<R>* msamp = nullptr) {
+        const R cp = (p.flags & FLAG_NO_RR) ? R(1) : cont_prob(msamp ? *msamp : m);
         if (p.flags & FLAG_RESTIR) {
             // SampleIlluminationReSTIR (testrenderer.slang:665-726) + ConnectToLight (:730-747)
             DI best; R wsum = 0;
@@ -887,6 +921,7 @@ template <class R> struct Tracer {
         const R dpw = r.pdf * AtoW;
         const V3<R> out = sd.to_local(r.dir);
         V3<R> f; R fwd, rev; eval(m, in, out, f, fwd, rev);
+        if (msamp) { V3<R> fs; eval(*msamp, in, out, fs, fwd, rev); }
         f = f * sd.snc(in, out);
         fwd *= cp;
         const V3<R> contrib = thr * r.radiance * f / dpw;
@@ -915,6 +950,9 @@ struct OracleScene {
     bool has_d = false, has_f = false;
     GridPair<double> grid_d;
     GridPair<float> grid_f;
+    OracleScene* sampling = nullptr;  // detached-sampling scene (see Tracer::samp)
+    const orc::Scene<double>* pick(const orc::Scene<double>&) const { return sampling ? &sampling->d : nullptr; }
+    const orc::Scene<float>* pick(const orc::Scene<float>&) const { return sampling ? &sampling->f : nullptr; }
     GridPair<double>& grids(orc::Scene<double>&) { return grid_d; }
     GridPair<float>& grids(orc::Scene<float>&) { return grid_f; }
 };
@@ -996,6 +1034,7 @@ int oracle_render(void* sp, const S2View* view, const S2RenderParams* rp, int pr
 #pragma omp parallel num_threads(threads > 0 ? threads : omp_get_max_threads())
         {
             auto tr = orc::Tracer<R>(scene, p);
+            tr.samp = s->pick(scene);
             tr.grid_cur = gcur;
             tr.grid_prev = gprev;
 #pragma omp for schedule(dynamic, 16)
@@ -1069,4 +1108,10 @@ void oracle_bsdf_sample(const uint32_t* mat_words, int lambertian, const double*
 extern "C" {
 uint32_t oracle_pcg_hash(uint32_t v) { return orc::pcg_hash(v); }
 uint32_t oracle_xxhash32(uint32_t v) { return orc::xxhash32(v); }
+}
+
+extern "C" {
+// Detached sampling for the adjoint checks: renders of `sp` take sampling decisions from `samp`
+// (a scene with the same geometry and other images); NULL restores the normal mode.
+void oracle_scene_set_sampling(void* sp, void* samp) { ((OracleScene*)sp)->sampling = (OracleScene*)samp; }
 }

@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = [
     "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
     "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
-    "s2_cache_train", "s2_cache_gradients",
+    "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -177,6 +177,10 @@ def lib() -> C.CDLL:
     L.s2_render_noalloc.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), P(S2RenderStats)]
     L.s2_default_render_params.argtypes = [P(S2RenderParams)]
     L.s2_default_render_params.restype = None
+    L.s2_update_image.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+    L.s2_render_diff.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, P(S2RenderStats)]
+    L.s2_render_adjoint.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, C.c_void_p,
+                                    P(S2RenderStats)]
     L.s2_cache_default_params.argtypes = [P(S2CacheParams)]
     L.s2_cache_default_params.restype = None
     L.s2_cache_init.argtypes = [C.c_void_p, P(S2CacheParams)]

@@ -231,3 +231,46 @@ class Device:
         self._check(self._lib.s2_cache_gradients(self._h, p.ctypes.data, t.ctypes.data, len(p), gw.ctypes.data,
                                                  gt.ctypes.data, C.byref(loss), 0))
         return loss.value, gw, gt
+
+    # ---- textures and differentiable rendering
+    def update_image(self, index: int, texels):
+        """Replaces image `index`'s texels (numpy array on the host, or a torch CUDA tensor)."""
+        if hasattr(texels, "data_ptr") and getattr(texels, "is_cuda", False):
+            t = texels.contiguous()
+            self._check(self._lib.s2_update_image(self._h, index, C.c_void_p(t.data_ptr()), 1))
+            return
+        a = np.ascontiguousarray(texels, np.float32)
+        self._check(self._lib.s2_update_image(self._h, index, a.ctypes.data, 0))
+
+    def render_diff(self, view, width: int, height: int, params: _abi.S2RenderParams):
+        """Image of the differentiable renderer (f32 materials): (H, W, 4) float32 and statistics."""
+        out = np.zeros((height, width, 4), np.float32)
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_diff(self._h, C.byref(view), C.byref(params), out.ctypes.data, 1, C.byref(st)))
+        return out, st
+
+    def render_diff_device(self, view, params: _abi.S2RenderParams, out_ptr: int) -> _abi.S2RenderStats:
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_diff(self._h, C.byref(view), C.byref(params), C.c_void_p(out_ptr), 0, C.byref(st)))
+        return st
+
+    def render_adjoint(self, view, params: _abi.S2RenderParams, d_image: np.ndarray, images=None):
+        """Texel gradients of sum(d_image * render_diff(...)) for the images in `images` (default all):
+        {index: (h, w, 4) float32}."""
+        d = np.ascontiguousarray(d_image, np.float32)
+        n = len(self.scene.images)
+        images = range(n) if images is None else images
+        outs = {k: np.zeros(self.scene.images[k].shape[:2] + (4,), np.float32) for k in images}
+        ptrs = (C.c_void_p * max(n, 1))(*[outs[k].ctypes.data if k in outs else None for k in range(n)])
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_adjoint(self._h, C.byref(view), C.byref(params), d.ctypes.data, 1,
+                                                C.cast(ptrs, C.c_void_p), C.byref(st)))
+        return outs
+
+    def render_adjoint_device(self, view, params: _abi.S2RenderParams, d_ptr: int, grad_ptrs) -> _abi.S2RenderStats:
+        """Device variant: grad_ptrs is one device pointer (or None) per scene image."""
+        ptrs = (C.c_void_p * max(len(grad_ptrs), 1))(*grad_ptrs)
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_adjoint(self._h, C.byref(view), C.byref(params), C.c_void_p(d_ptr), 0,
+                                                C.cast(ptrs, C.c_void_p), C.byref(st)))
+        return st

@@ -97,7 +97,19 @@ inline float rd_f32(const uint8_t* b, uint64_t size, uint64_t off, bool& ok) {
 // SampleTexel (src/Shaders/common/lights.hlsli:49-96) computes at every level of its descent, and
 // the pdf SampleTexelPdf (:97-138) returns for every texel of the finest level it reaches.  Built
 // only when each mip level is an exact halving of the previous one.
-void build_env_tables(S2Context* ctx, DevImage& di, const std::vector<float>& lum) {
+// Uploads `count` elements into a new scene buffer, or, for an update of an existing image (same
+// dimensions, so the same sizes), over the old contents at `into`.
+template <typename T>
+T* put(S2Context* ctx, const T* host, size_t count, const T* into) {
+    if (!into) return upload(ctx, ctx->scene_bufs, host, count);
+    if (count && cudaMemcpyAsync((void*)into, host, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+        set_error(ctx, S2_ERR_CUDA, "cudaMemcpyAsync H2D failed");
+        return nullptr;
+    }
+    return (T*)into;
+}
+
+void build_env_tables(S2Context* ctx, DevImage& di, const std::vector<float>& lum, const DevImage* old) {
     const uint32_t L = di.levels;
     di.nested = 0; di.quad = nullptr; di.pdf = nullptr;
     if (L < 3) return;
@@ -159,10 +171,55 @@ void build_env_tables(S2Context* ctx, DevImage& di, const std::vector<float>& lu
         }
         pdf[(size_t)y * di.lw[f] + x] = pd * (float)(lx * ly);
     }
-    di.quad = upload(ctx, ctx->scene_bufs, quad.data(), quad.size());
-    di.pdf = upload(ctx, ctx->scene_bufs, pdf.data(), pdf.size());
+    di.quad = put(ctx, quad.data(), quad.size(), old ? old->quad : nullptr);
+    di.pdf = put(ctx, pdf.data(), pdf.size(), old ? old->pdf : nullptr);
     di.pdf_level = f;
     di.nested = (di.quad && di.pdf) ? 1u : 0u;
+}
+
+// Device copy of one image (float RGBA texels); an environment image also gets its luminance mip
+// pyramid and sampling tables.  `old`: the same image's current descriptor, overwritten in place.
+int build_image(S2Context* ctx, uint32_t i, const S2Image& im, bool env, const DevImage* old, DevImage& di) {
+    if (!im.texels || im.width == 0 || im.height == 0 || im.channels < 1 || im.channels > 4)
+        return set_error(ctx, S2_ERR_INVALID, "image " + std::to_string(i) + " is malformed");
+    const size_t n = (size_t)im.width * im.height;
+    std::vector<float> rgba(4 * n);
+    for (size_t t = 0; t < n; ++t) {
+        for (uint32_t c = 0; c < 4; ++c) rgba[4 * t + c] = c < im.channels ? im.texels[im.channels * t + c] : (c == 3 ? 1.f : 0.f);
+    }
+    di = DevImage{};
+    di.width = im.width; di.height = im.height;
+    di.texels = put(ctx, (const float4*)rgba.data(), n, old ? old->texels : nullptr);
+    if (env) {
+        // mip chain by 2x2 averaging, then luminance per texel
+        std::vector<std::vector<float>> lv;
+        std::vector<uint32_t> lw, lh;
+        lv.push_back(rgba); lw.push_back(im.width); lh.push_back(im.height);
+        while ((lw.back() > 1 || lh.back() > 1) && lv.size() < S2_MAX_IMAGE_LEVELS) {
+            const uint32_t pw = lw.back(), ph = lh.back();
+            const uint32_t w2 = std::max(1u, pw / 2), h2 = std::max(1u, ph / 2);
+            std::vector<float> nxt(4 * (size_t)w2 * h2);
+            const std::vector<float>& prev = lv.back();
+            for (uint32_t y = 0; y < h2; ++y) for (uint32_t x = 0; x < w2; ++x) for (int c = 0; c < 4; ++c) {
+                const uint32_t x0 = std::min(2 * x, pw - 1), x1 = std::min(2 * x + 1, pw - 1);
+                const uint32_t y0 = std::min(2 * y, ph - 1), y1 = std::min(2 * y + 1, ph - 1);
+                nxt[4 * ((size_t)y * w2 + x) + c] = 0.25f * (prev[4 * ((size_t)y0 * pw + x0) + c] + prev[4 * ((size_t)y0 * pw + x1) + c] +
+                                                             prev[4 * ((size_t)y1 * pw + x0) + c] + prev[4 * ((size_t)y1 * pw + x1) + c]);
+            }
+            lv.push_back(std::move(nxt)); lw.push_back(w2); lh.push_back(h2);
+        }
+        std::vector<float> lum;
+        di.levels = (uint32_t)lv.size();
+        for (uint32_t l = 0; l < di.levels; ++l) {
+            di.lum_offset[l] = (uint32_t)lum.size(); di.lw[l] = lw[l]; di.lh[l] = lh[l];
+            const size_t cnt = (size_t)lw[l] * lh[l];
+            for (size_t t = 0; t < cnt; ++t)
+                lum.push_back(0.2126f * lv[l][4 * t] + 0.7152f * lv[l][4 * t + 1] + 0.0722f * lv[l][4 * t + 2]);
+        }
+        di.lum = put(ctx, lum.data(), lum.size(), old ? old->lum : nullptr);
+        build_env_tables(ctx, di, lum, old);
+    }
+    return S2_OK;
 }
 
 }  // namespace
@@ -381,48 +438,13 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     if (s.env_address != S2_NO_ENVIRONMENT) std::memcpy(&env_img, (const uint8_t*)d->material_data + s.env_address + 12, 4);
     ctx->images_host.assign(d->image_count, DevImage{});
     ctx->env_image = -1;
+    ctx->image_channels.assign(d->image_count, 0);
     for (uint32_t i = 0; i < d->image_count; ++i) {
         const S2Image& im = d->images[i];
-        if (!im.texels || im.width == 0 || im.height == 0 || im.channels < 1 || im.channels > 4)
-            return set_error(ctx, S2_ERR_INVALID, "image " + std::to_string(i) + " is malformed");
-        const size_t n = (size_t)im.width * im.height;
-        std::vector<float> rgba(4 * n);
-        for (size_t t = 0; t < n; ++t) {
-            for (uint32_t c = 0; c < 4; ++c) rgba[4 * t + c] = c < im.channels ? im.texels[im.channels * t + c] : (c == 3 ? 1.f : 0.f);
-        }
         DevImage di{};
-        di.width = im.width; di.height = im.height;
-        di.texels = upload(ctx, ctx->scene_bufs, (const float4*)rgba.data(), n);
-        if (i == env_img) {
-            // mip chain by 2x2 averaging, then luminance per texel
-            std::vector<std::vector<float>> lv;
-            std::vector<uint32_t> lw, lh;
-            lv.push_back(rgba); lw.push_back(im.width); lh.push_back(im.height);
-            while ((lw.back() > 1 || lh.back() > 1) && lv.size() < S2_MAX_IMAGE_LEVELS) {
-                const uint32_t pw = lw.back(), ph = lh.back();
-                const uint32_t w2 = std::max(1u, pw / 2), h2 = std::max(1u, ph / 2);
-                std::vector<float> nxt(4 * (size_t)w2 * h2);
-                const std::vector<float>& prev = lv.back();
-                for (uint32_t y = 0; y < h2; ++y) for (uint32_t x = 0; x < w2; ++x) for (int c = 0; c < 4; ++c) {
-                    const uint32_t x0 = std::min(2 * x, pw - 1), x1 = std::min(2 * x + 1, pw - 1);
-                    const uint32_t y0 = std::min(2 * y, ph - 1), y1 = std::min(2 * y + 1, ph - 1);
-                    nxt[4 * ((size_t)y * w2 + x) + c] = 0.25f * (prev[4 * ((size_t)y0 * pw + x0) + c] + prev[4 * ((size_t)y0 * pw + x1) + c] +
-                                                                 prev[4 * ((size_t)y1 * pw + x0) + c] + prev[4 * ((size_t)y1 * pw + x1) + c]);
-                }
-                lv.push_back(std::move(nxt)); lw.push_back(w2); lh.push_back(h2);
-            }
-            std::vector<float> lum;
-            di.levels = (uint32_t)lv.size();
-            for (uint32_t l = 0; l < di.levels; ++l) {
-                di.lum_offset[l] = (uint32_t)lum.size(); di.lw[l] = lw[l]; di.lh[l] = lh[l];
-                const size_t cnt = (size_t)lw[l] * lh[l];
-                for (size_t t = 0; t < cnt; ++t)
-                    lum.push_back(0.2126f * lv[l][4 * t] + 0.7152f * lv[l][4 * t + 1] + 0.0722f * lv[l][4 * t + 2]);
-            }
-            di.lum = upload(ctx, ctx->scene_bufs, lum.data(), lum.size());
-            build_env_tables(ctx, di, lum);
-            ctx->env_image = (int)i;
-        }
+        S2_TRY(build_image(ctx, i, im, i == env_img, nullptr, di));
+        if (i == env_img) ctx->env_image = (int)i;
+        ctx->image_channels[i] = im.channels;
         ctx->images_host[i] = di;
     }
     ctx->images_dev = upload(ctx, ctx->scene_bufs, ctx->images_host.data(), ctx->images_host.size());
@@ -432,6 +454,31 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     S2_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "scene upload"));
     ctx->has_scene = true;
     return S2_OK;
+}
+
+extern "C" int s2_update_image(S2Context* ctx, uint32_t index, const float* texels, int on_device) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!ctx->has_scene) return set_error(ctx, S2_ERR_NO_SCENE, "s2_update_image before s2_scene_upload");
+    if (index >= ctx->images_host.size()) return set_error(ctx, S2_ERR_INVALID, "image index out of range");
+    if (!texels) return set_error(ctx, S2_ERR_INVALID, "texels is null");
+    cudaSetDevice(ctx->device);
+    const DevImage old = ctx->images_host[index];
+    S2Image im;
+    im.width = old.width; im.height = old.height; im.channels = ctx->image_channels[index];
+    std::vector<float> host;
+    if (on_device) {
+        host.resize((size_t)im.width * im.height * im.channels);
+        cudaMemcpyAsync(host.data(), texels, sizeof(float) * host.size(), cudaMemcpyDeviceToHost, ctx->stream);
+        S2_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "image download"));
+        im.texels = host.data();
+    } else {
+        im.texels = texels;
+    }
+    DevImage di{};
+    S2_TRY(build_image(ctx, index, im, (int)index == ctx->env_image, &old, di));
+    ctx->images_host[index] = di;
+    cudaMemcpyAsync(ctx->images_dev + index, &ctx->images_host[index], sizeof(DevImage), cudaMemcpyHostToDevice, ctx->stream);
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "image update");
 }
 
 extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStats* stats) {

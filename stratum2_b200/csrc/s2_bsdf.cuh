@@ -46,7 +46,8 @@ S2D float3 sample_vndf(float3 in, float ax, float ay, float u1, float u2) {
     return flip ? -out : out;
 }
 
-S2D void disney_alphas(const Mat& m, float& ax, float& ay) {
+template <class M>
+S2D void disney_alphas(const M& m, float& ax, float& ay) {
     const float aspect = sqrtf(1.f - m.anisotropic() * 0.9f);
     const float a = pow2(m.roughness());
     ax = fmaxf(1e-4f, a / aspect);
@@ -54,7 +55,8 @@ S2D void disney_alphas(const Mat& m, float& ax, float& ay) {
 }
 
 // Disney eval<Adjoint=false> (disney.hlsli:9-139): reflectance f*|cos|
-S2D float3 disney_eval(const Mat& m, float3 in, float3 out) {
+template <class M>
+S2D float3 disney_eval(const M& m, float3 in, float3 out) {
     float ax, ay;
     disney_alphas(m, ax, ay);
     const float metallic = m.metallic();
@@ -112,7 +114,8 @@ S2D float3 disney_eval(const Mat& m, float3 in, float3 out) {
 }
 
 // Disney evalPdf (disney.hlsli:141-231)
-S2D float disney_pdf(const Mat& m, float3 in, float3 out) {
+template <class M>
+S2D float disney_pdf(const M& m, float3 in, float3 out) {
     float ax, ay;
     disney_alphas(m, ax, ay);
     const float metallic = m.metallic(), tr = m.transmission();
@@ -148,7 +151,8 @@ S2D float disney_pdf(const Mat& m, float3 in, float3 out) {
 
 // Disney sample (disney.hlsli:233-380).  Returns false on a failed sample (zero direction);
 // rough = 0 marks a singular sample.
-S2D bool disney_sample(const Mat& m, float3 in, float r0, float r1, float r2, float3& dir, float& rough) {
+template <class M>
+S2D bool disney_sample(const M& m, float3 in, float r0, float r1, float r2, float3& dir, float& rough) {
     float ax, ay;
     disney_alphas(m, ax, ay);
     const float ac = (1.f - m.clearcoat_gloss()) * 0.1f + m.clearcoat_gloss() * 0.001f;
@@ -199,8 +203,8 @@ S2D bool disney_sample(const Mat& m, float3 in, float r0, float r1, float r2, fl
 }
 
 // evaluateReflectance: f*|cos|, forward and reverse pdf (lambertian.hlsli:16-27, disney.hlsli:391-403)
-template <bool LAMBERT>
-S2D void bsdf_eval(const Mat& m, float3 in, float3 out, float3& f, float& fwd, float& rev) {
+template <bool LAMBERT, class M>
+S2D void bsdf_eval(const M& m, float3 in, float3 out, float3& f, float& fwd, float& rev) {
     if (LAMBERT) {
         if (in.z * out.z < 0.f) { f = f3(0.f); fwd = rev = 0.f; return; }
         f = m.base() * (fabsf(out.z) / S2_PI);
@@ -214,8 +218,8 @@ S2D void bsdf_eval(const Mat& m, float3 in, float3 out, float3& f, float& fwd, f
 }
 
 // sampleDirection (lambertian.hlsli:29-38, disney.hlsli:415-429)
-template <bool LAMBERT>
-S2D void bsdf_sample(const Mat& m, float3 in, float4 rnd, float3& dir, float3& f, float& fwd, float& rev, float& rough) {
+template <bool LAMBERT, class M>
+S2D void bsdf_sample(const M& m, float3 in, float4 rnd, float3& dir, float3& f, float& fwd, float& rev, float& rough) {
     if (LAMBERT) {
         dir = sample_cos_hemisphere(rnd.x, rnd.y);
         if (in.z < 0.f) dir = -dir;
@@ -229,10 +233,11 @@ S2D void bsdf_sample(const Mat& m, float3 in, float4 rnd, float3& dir, float3& f
     bsdf_eval<false>(m, in, dir, f, fwd, rev);
 }
 
-template <bool LAMBERT>
-S2D bool mat_singular(const Mat& m) {
+template <bool LAMBERT, class M>
+S2D bool mat_singular(const M& m) {
     if (LAMBERT) return false;
     // disney.hlsli:387
     return fmaxf(fmaxf(m.specular(), m.metallic()), m.transmission()) * (1.f - m.roughness()) > 0.75f;
 }
-S2D float cont_prob(const Mat& m) { return saturate(luminance(m.base())); }
+template <class M>
+S2D float cont_prob(const M& m) { return saturate(luminance(m.base())); }

@@ -46,6 +46,7 @@ struct S2Context {
     // device scene description (pointers into scene_bufs / bvh_bufs)
     DevScene scene{};
     std::vector<DevImage> images_host;      // device-side descriptors, host copy
+    std::vector<uint32_t> image_channels;   // channel count of each uploaded image
     DevImage* images_dev = nullptr;
     uint8_t** vbufs_dev = nullptr;
     int env_image = -1;

@@ -1,0 +1,347 @@
+// Differentiable rendering by adjoint path replay (no counterpart in the reference): the same
+// unidirectional path tracer with NEE + MIS as the wavefront renderer (same random-number stream,
+// path-length gates, MIS and Russian roulette), evaluated per path by one thread, with textured
+// material parameters kept in f32 (no 8-bit requantisation, so the image is differentiable in the
+// texels).  The adjoint replays every path from its seed twice (Vicini et al. 2021, path replay
+// backpropagation): the first replay gives the path's radiance L, the second walks the path again
+// and, at every vertex, turns the image adjoint dL/dI into texel gradients:
+//   * NEE at vertex j:        dI += T_j Le w / p * df_j(w_light)   and, for the environment,
+//                             dI += T_j f_j w / p * dLe;
+//   * continuation at j:      dI += (L - L_<=j) / f_j(w_sampled) * df_j(w_sampled)
+//                             (every later contribution carries the factor f_j / p_j);
+//   * environment hits:       dI += T w * dLe.
+// Sampling densities, MIS weights and Russian-roulette probabilities are held constant ("detached"),
+// which keeps each term an unbiased estimate of the derivative of the pixel integral.  BSDF partials
+// are analytic for the Lambertian model and central differences (f32, step 1e-3) for Disney.
+#pragma once
+#include "s2_shade_kernel.cuh"
+
+namespace s2 {
+
+// Material with f32 parameters: the record's 8-bit values modulated by the textures in f32.
+struct MatF {
+    float3 b, e;
+    float spec, shn, metal, rough, aniso, subs, cc, ccg, trans, eta;
+    S2D float3 base() const { return b; }
+    S2D float3 emission() const { return e; }
+    S2D float specular() const { return spec; }
+    S2D float sheen() const { return shn; }
+    S2D float metallic() const { return metal; }
+    S2D float roughness() const { return rough; }
+    S2D float anisotropic() const { return aniso; }
+    S2D float subsurface() const { return subs; }
+    S2D float clearcoat() const { return cc; }
+    S2D float clearcoat_gloss() const { return ccg; }
+    S2D float transmission() const { return trans; }
+    S2D float eta1() const { return eta; }
+};
+
+// The four texels of a bilinear lookup (same footprint and weights as sample_image).
+struct Taps {
+    uint32_t img;       // 0xffffffff: no texture
+    uint32_t idx[4];
+    float w[4];
+};
+
+S2D void bilinear_taps(const DevImage& im, uint32_t img, float2 uv, Taps& t) {
+    const float x = uv.x * im.width - 0.5f, y = uv.y * im.height - 0.5f;
+    const float fx = floorf(x), fy = floorf(y);
+    const float ax = x - fx, ay = y - fy;
+    int x0 = (int)fx, y0 = (int)fy;
+    const int W = (int)im.width, H = (int)im.height;
+    x0 %= W; if (x0 < 0) x0 += W;
+    y0 %= H; if (y0 < 0) y0 += H;
+    const int x1 = (x0 + 1) % W, y1 = (y0 + 1) % H;
+    t.img = img;
+    t.idx[0] = (uint32_t)(y0 * W + x0); t.idx[1] = (uint32_t)(y0 * W + x1);
+    t.idx[2] = (uint32_t)(y1 * W + x0); t.idx[3] = (uint32_t)(y1 * W + x1);
+    t.w[0] = (1 - ax) * (1 - ay); t.w[1] = ax * (1 - ay); t.w[2] = (1 - ax) * ay; t.w[3] = ax * ay;
+}
+
+// LoadMaterial (material.hlsli:15-46) in f32.  tb / tr: the base-colour and packed[2] (metallic,
+// roughness, anisotropic, subsurface) texture taps; base_rec / rough_rec: the record's values.
+S2D MatF load_material_f(const DevScene& s, uint32_t addr, float2 uv, Taps& tb, Taps& tr, float3& base_rec,
+                         float& rough_rec) {
+    const uint4 a = *(const uint4*)(s.material_data + addr);
+    const uint4 img = *(const uint4*)(s.material_data + addr + 16);
+    MatF m;
+    m.b = f3(un8(a.x, 0), un8(a.x, 8), un8(a.x, 16));
+    m.spec = un8(a.x, 24);
+    m.e = f3(un8(a.y, 0), un8(a.y, 8), un8(a.y, 16)) * ld_f32(s.material_data, addr + 32);
+    m.shn = un8(a.y, 24);
+    m.metal = un8(a.z, 0); m.rough = un8(a.z, 8); m.aniso = un8(a.z, 16); m.subs = un8(a.z, 24);
+    m.cc = un8(a.w, 0); m.ccg = un8(a.w, 8); m.trans = un8(a.w, 16);
+    float eta8 = un8(a.w, 24);
+    base_rec = m.b;
+    rough_rec = m.rough;
+    tb.img = tr.img = 0xffffffffu;
+    const uint32_t n = s.image_count;
+    if (img.x < n) {
+        bilinear_taps(s.images[img.x], img.x, uv, tb);
+        const float4 t = sample_image(s.images[img.x], uv);
+        m.b = m.b * f3(t.x, t.y, t.z);
+    }
+    if (img.y < n) {
+        const float4 t = sample_image(s.images[img.y], uv);
+        m.e = m.e * f3(t.x, t.y, t.z);
+    }
+    if (img.z < n) {
+        bilinear_taps(s.images[img.z], img.z, uv, tr);
+        const float4 t = sample_image(s.images[img.z], uv);
+        m.metal *= t.x;
+        m.rough = 1.f - (1.f - m.rough) * (1.f - t.y);  // roughness modulated as smoothness
+        m.aniso *= t.z;
+        m.subs *= t.w;
+    }
+    if (img.w < n) {
+        const float4 t = sample_image(s.images[img.w], uv);
+        m.cc *= t.x; m.ccg *= t.y; m.trans *= t.z; eta8 *= t.w;
+    }
+    m.eta = eta8 + 1.f;
+    return m;
+}
+
+struct DiffArgs {
+    DevScene scene;
+    float proj[8];
+    int imin[2], imax[2];
+    float cam[12];
+    uint32_t width, height, pixels, spp;
+    uint32_t min_len, max_len, flags, frame_seed;
+    float out_scale;                  // 2^exposure / spp
+    float4* image;                    // forward: mean radiance * 2^exposure per pixel
+    const float4* d_image;            // adjoint: dLoss / d image
+    float4* grad;                     // adjoint: texel gradients of every image, concatenated
+    const uint32_t* grad_offset;      // first texel of image k in `grad`
+    unsigned long long* rays;         // [0] extension rays, [1] shadow rays
+    int* status;                      // bit 0: traversal stack overflow
+};
+
+S2D void add_grad(const DiffArgs& A, const Taps& t, float3 g) {
+    if (t.img == 0xffffffffu) return;
+    float4* base = A.grad + A.grad_offset[t.img];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float* p = (float*)(base + t.idx[k]);
+        if (g.x != 0.f) atomicAdd(p + 0, t.w[k] * g.x);
+        if (g.y != 0.f) atomicAdd(p + 1, t.w[k] * g.y);
+        if (g.z != 0.f) atomicAdd(p + 2, t.w[k] * g.z);
+    }
+}
+S2D void add_grad_y(const DiffArgs& A, const Taps& t, float g) {
+    if (t.img == 0xffffffffu || g == 0.f) return;
+    float4* base = A.grad + A.grad_offset[t.img];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) atomicAdd((float*)(base + t.idx[k]) + 1, t.w[k] * g);
+}
+
+// Environment texel gradients for radiance weight `g` (dLoss/dLe per channel) in direction `dir`.
+S2D void env_grad(const DiffArgs& A, float3 dir, float3 g) {
+    const DevScene& s = A.scene;
+    if (!has_env(s)) return;
+    const float4 rec = *(const float4*)(s.material_data + s.env_address);
+    const uint32_t img = __float_as_uint(rec.w);
+    if (img >= s.image_count) return;
+    Taps t;
+    bilinear_taps(s.images[img], img, cartesian_to_spherical_uv(dir), t);
+    add_grad(A, t, f3(rec.x * g.x, rec.y * g.y, rec.z * g.z));
+}
+
+// dLoss / d(base colour) and d(roughness) of the BSDF value at (in, out) weighted per channel by y,
+// pushed to the texels of the vertex's textures.
+template <bool LAMBERT>
+S2D void material_grads(const DiffArgs& A, const MatF& m, float3 in, float3 out, float3 y, const Taps& tb, const Taps& tr,
+                        float3 base_rec, float rough_rec) {
+    if (tb.img != 0xffffffffu) {
+        float3 g;
+        if (LAMBERT) {
+            const float c = (in.z * out.z < 0.f) ? 0.f : fabsf(out.z) / S2_PI;
+            g = y * c;
+        } else {
+            const float h = 1e-3f;
+            float gg[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                MatF mp = m, mm = m;
+                float* bp = &mp.b.x;
+                float* bm = &mm.b.x;
+                bp[j] += h; bm[j] -= h;
+                const float3 fp = disney_eval(mp, in, out), fm = disney_eval(mm, in, out);
+                gg[j] = dot(y, (fp - fm) / (2.f * h));
+            }
+            g = f3(gg[0], gg[1], gg[2]);
+        }
+        add_grad(A, tb, f3(g.x * base_rec.x, g.y * base_rec.y, g.z * base_rec.z));
+    }
+    if (!LAMBERT && tr.img != 0xffffffffu && rough_rec < 1.f) {
+        const float h = 1e-3f;
+        const float lo = fmaxf(m.rough - h, 0.f), hi = fminf(m.rough + h, 1.f);
+        if (hi > lo) {
+            MatF mp = m, mm = m;
+            mp.rough = hi; mm.rough = lo;
+            const float3 df = (disney_eval(mp, in, out) - disney_eval(mm, in, out)) / (hi - lo);
+            add_grad_y(A, tr, dot(y, df) * (1.f - rough_rec));
+        }
+    }
+}
+
+// One path of pixel (px, py), sample `sample`.  adj = false: returns the path's radiance.
+// adj = true: replays the same path and adds the texel gradients for the image adjoint `delta`,
+// with `ltot` the radiance the first replay returned.  Not inlined, so both replays run the same
+// machine code and take the same decisions.
+template <bool LAMBERT>
+__device__ __noinline__ float3 diff_path(const DiffArgs& A, uint32_t px, uint32_t py, uint32_t sample, bool adj, float3 ltot,
+                                         float3 delta, uint2* smem_stack, uint32_t lane_stride, uint32_t& ext_rays,
+                                         uint32_t& shadow_rays, bool& overflow) {
+    const DevScene& s = A.scene;
+    const bool nee = !(A.flags & S2F_NO_NEE), sn = !(A.flags & S2F_NO_SN);
+    const SceneAlphaTest alpha{&s, !(A.flags & S2F_NO_ALPHA)};
+    Rng rng = make_rng(px, py, A.frame_seed + sample, (A.flags & S2F_PCG32) != 0);
+    float ox = 0.5f, oy = 0.5f;
+    if (A.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
+    float3 dir = camera_dir(A.proj, A.imin, A.imax, A.cam, px, py, ox, oy);
+    float3 org = f3(A.cam[3], A.cam[7], A.cam[11]);
+    float3 thr = f3(1.f);
+    float3 L = f3(0.f);
+    float dir_pdf = 0.f;
+    uint32_t len = 0;
+    TravCounters ctr{0, 0};
+    while (true) {
+        TravHit h;
+        ext_rays++;
+        if (!traverse<false, false>(make_trav_ray(org, dir, 0.f), S2_INF, s.nodes, s.tris, smem_stack, lane_stride, h, ctr, alpha))
+            overflow = true;
+        len++;
+        if (h.tri == 0xffffffffu) {
+            // environment (TraceRay, testrenderer.slang:1036-1054)
+            float env_pdf = 0.f;
+            const float3 le = eval_env(s, dir, env_pdf);
+            const float3 e = len >= A.min_len ? thr * le : f3(0.f);
+            if (any_pos(e)) {
+                float w = 1.f;
+                if (len > 1 && nee && dir_pdf > 0.f) {
+                    const float lp = (A.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;
+                    w = mis_w(dir_pdf, lp);
+                }
+                if (w > 0.f) {
+                    L = L + e * w;
+                    if (adj) env_grad(A, dir, delta * thr * w);
+                }
+            }
+            break;
+        }
+        SD sd = make_shading(s, h.instance, h.primitive, h.b1, h.b2, sn);
+        if (!(A.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
+        const float isect_dist = half_round(h.t);
+        const float isect_pdfa = half_round(light_pdfa(s, h.instance, sd.area));
+        Taps tb, tr;
+        float3 base_rec;
+        float rough_rec;
+        const MatF m = load_material_f(s, sd.mat, sd.uv, tb, tr, base_rec, rough_rec);
+        const float3 in = sd.to_local(-dir);
+        const float cos_in = fabsf(in.z);
+        if (in.z > 0.f) {
+            const float3 e = thr * m.emission();
+            if (any_pos(e) && len >= A.min_len) {
+                float w = 1.f;
+                if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
+                if (w > 0.f) L = L + e * w;
+            }
+        }
+        if (!(len < A.max_len && any_pos(m.base()))) break;
+        const bool sing = mat_singular<LAMBERT>(m);
+        const float cp = (A.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
+        // NEE (ConnectToLight, testrenderer.slang:751-779), same stream use as the wavefront shade
+        if (!sing && nee) {
+            if (len + 1 < A.min_len) {
+                rng.skip();
+            } else {
+                const float4 x = rng.next_float();
+                const Illum r = sample_illum(s, x, sd.pos, sn);
+                if (!(all_nonpos(r.radiance) || r.pdf <= 0.f)) {
+                    const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
+                    const float dpw = r.pdf * AtoW;
+                    const float3 out = sd.to_local(r.dir);
+                    float3 f; float fwd, rev;
+                    bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
+                    f = f * sd.snc(in, out);
+                    fwd *= cp;
+                    const float3 contrib = thr * r.radiance * f / dpw;
+                    const float w = mis_w(r.pdf, fwd / AtoW);
+                    if (w > 0.f && !all_nonpos(contrib)) {
+                        TravHit sh;
+                        shadow_rays++;
+                        if (!traverse<true, false>(make_trav_ray(ray_offset(sd.pos, sd.gn, r.dir), r.dir, 0.f),
+                                                   adjust_distance(r.dist), s.nodes, s.tris, smem_stack, lane_stride, sh, ctr, alpha))
+                            overflow = true;
+                        if (sh.tri == 0xffffffffu) {
+                            L = L + f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
+                            if (adj) {
+                                const float k = w / dpw;
+                                material_grads<LAMBERT>(A, m, in, out, delta * thr * r.radiance * k, tb, tr, base_rec, rough_rec);
+                                if (!r.finite) env_grad(A, r.dir, delta * thr * f * k);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (!(A.flags & S2F_NO_RR)) {
+            const float4 u = rng.next_float();
+            if (u.x > fminf(1.f, cp)) break;
+        }
+        const float4 rnd = rng.next_float();
+        float3 sdir, refl;
+        float fwd, rev, rough;
+        bsdf_sample<LAMBERT>(m, in, rnd, sdir, refl, fwd, rev, rough);
+        if (adj) {
+            // every later contribution carries refl / fwd: d/dtheta = (L - L_so_far) * d refl / refl
+            const float3 after = ltot - L;
+            const float3 y = f3(refl.x > 0.f ? delta.x * after.x / refl.x : 0.f, refl.y > 0.f ? delta.y * after.y / refl.y : 0.f,
+                                refl.z > 0.f ? delta.z * after.z / refl.z : 0.f);
+            if (any_pos(f3(fabsf(y.x), fabsf(y.y), fabsf(y.z)))) material_grads<LAMBERT>(A, m, in, sdir, y, tb, tr, base_rec, rough_rec);
+        }
+        const float cpm = (A.flags & S2F_NO_RR) ? 1.f : cp;
+        fwd *= cpm;
+        thr = thr * refl / fwd;
+        dir_pdf = (rough == 0.f || sing) ? 0.f : half_round(fwd);
+        thr = thr * sd.snc(in, sdir);
+        const float3 wd = sd.to_world(sdir);
+        org = ray_offset(sd.pos, sd.gn, wd);
+        dir = unpack_normal(pack_normal(wd));
+        if (any_nan(thr) || !any_pos(thr)) break;
+    }
+    return L;
+}
+
+// Forward (ADJ = false): image[pixel] = mean path radiance * 2^exposure.  Adjoint: texel gradients
+// of sum(d_image * image).  One thread per pixel, looping over its samples (deterministic image).
+template <bool LAMBERT, bool ADJ>
+__global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs A) {
+    __shared__ uint2 stack[S2_STACK_SMEM * 128];
+    const uint32_t pix = blockIdx.x * 128u + threadIdx.x;
+    if (pix >= A.pixels) return;
+    const uint32_t px = pix % A.width, py = pix / A.width;
+    float3 sum = f3(0.f), delta = f3(0.f);
+    if (ADJ) {
+        const float4 d = A.d_image[pix];
+        delta = f3(d.x, d.y, d.z) * A.out_scale;
+    }
+    uint32_t ext = 0, shd = 0;
+    bool overflow = false;
+    for (uint32_t k = 0; k < A.spp; ++k) {
+        const float3 l = diff_path<LAMBERT>(A, px, py, k, false, f3(0.f), f3(0.f), stack + threadIdx.x, 128u, ext, shd, overflow);
+        if (ADJ) {
+            if (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f)
+                diff_path<LAMBERT>(A, px, py, k, true, l, delta, stack + threadIdx.x, 128u, ext, shd, overflow);
+        } else {
+            sum = sum + l;
+        }
+    }
+    if (!ADJ) A.image[pix] = make_float4(sum.x * A.out_scale, sum.y * A.out_scale, sum.z * A.out_scale, 1.f);
+    atomicAdd(A.rays, (unsigned long long)ext);
+    atomicAdd(A.rays + 1, (unsigned long long)shd);
+    if (overflow) atomicOr(A.status, 1);
+}
+
+}  // namespace s2

@@ -128,6 +128,54 @@ def cutout_scene(seed: int = 3, n_random: int = 200, width: int = 64, height: in
     return Workload(s, view, width, height, spp, 2, 5, False, f"cutout_{width}x{height}")
 
 
+def textured_box_scene(seed: int = 4, n_random: int = 100, width: int = 48, height: int = 48, tex_res: int = 32,
+                       env_res=(32, 16), spheres: int = 0, sphere_level: int = 3) -> Workload:
+    """The box (open front) with textured walls for the differentiable renderer: floor, back and left
+    walls take their base colour from an RGB albedo image (image 0) and their roughness from the y
+    channel of a packed[2] image (image 1; material roughness 0 and metallic 0, so roughness =
+    texel); a ceiling quad light; `n_random` small triangles and `spheres` icospheres (level
+    `sphere_level`) inside; a small procedural sky (image 2) seen through the open front."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    albedo = s.add_image(rng.uniform(0.2, 0.9, (tex_res, tex_res, 3)).astype(np.float32))
+    packed = np.ones((tex_res, tex_res, 4), np.float32)
+    packed[..., 1] = rng.uniform(0.2, 0.9, (tex_res, tex_res))
+    rough = s.add_image(packed)
+    uv4 = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    walls = [
+        ((-1, -1, -1), (-1, -1, 1), (1, -1, 1), (1, -1, -1)),
+        ((-1, 1, -1), (1, 1, -1), (1, 1, 1), (-1, 1, 1)),
+        ((-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1)),
+        ((-1, -1, -1), (-1, 1, -1), (-1, 1, 1), (-1, -1, 1)),
+        ((1, -1, -1), (1, -1, 1), (1, 1, 1), (1, 1, -1)),
+    ]
+    tex_mat = s.add_material(Material(base_color=(1, 1, 1), roughness=0.0, metallic=0.0, specular=0.5,
+                                      images=(albedo, _abi.NO_IMAGE, rough, _abi.NO_IMAGE)))
+    plain = s.add_material(Material(base_color=(0.7, 0.7, 0.7), roughness=0.6))
+    for k, w in enumerate(walls):
+        p, i = quad(*w)
+        s.add_instance(s.add_mesh(p, i, uvs=uv4), tex_mat if k in (0, 2, 3) else plain)
+    h, y = 0.25, 1.0 - 1e-3
+    p, i = quad((-h, y, -h), (h, y, -h), (h, y, h), (-h, y, h))
+    s.add_instance(s.add_mesh(p, i), s.add_material(Material(base_color=(0, 0, 0), emission=(10.0,) * 3)))
+    cent = rng.uniform(-0.8, 0.8, size=(n_random, 3))
+    offs = rng.uniform(-0.05, 0.05, size=(n_random, 3, 3))
+    for k in range(n_random):
+        m = s.add_material(Material(base_color=tuple(rng.uniform(0.2, 0.8, 3))))
+        s.add_instance(s.add_mesh((cent[k][None, :] + offs[k]).astype(np.float32), np.array([[0, 1, 2]], np.uint32)), m)
+    if spheres:
+        sv, sf = icosphere(sphere_level)
+        mesh = s.add_mesh(sv, sf)
+        for k in range(spheres):
+            c = rng.uniform(-0.75, 0.75, 3)
+            r = rng.uniform(0.03, 0.12)
+            m = s.add_material(Material(base_color=tuple(rng.uniform(0.2, 0.9, 3)), roughness=float(rng.uniform(0.2, 0.9))))
+            s.add_instance(mesh, m, transform_trs(c, np.eye(3), (r, r, r)))
+    s.set_environment((1.0, 1.0, 1.0), s.add_image(sky_image(env_res[0], env_res[1], sun_radiance=20.0, sun_cone_degrees=10.0)))
+    view = make_view((0.0, 0.0, 3.0), width, height, 40.0)
+    return Workload(s, view, width, height, 16, 0, 4, False, f"textured_box_{width}x{height}")
+
+
 # ------------------------------------------------------------------------------ terrain
 def value_noise(rng: np.random.Generator, n: int, octaves: int = 6, amplitude: float = 0.2) -> np.ndarray:
     """Sum of `octaves` octaves of bilinearly interpolated value noise on an n x n grid,
