@@ -43,8 +43,8 @@ def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d.get("bf16_tflops", 1590.0)), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 def extend_traffic_per_ray() -> float | None:
@@ -277,6 +277,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "note": "GPU time of progressive calls (plain/batched 128 spp per call, extrapolated past the budget "
                         "as relMSE ~ 1/spp; cached: 1 spp frames of the radiance-cache form with online training, "
                         "measured)"}
+    if world == 1 and not args.no_quality:
+        line["radiance_cache_kernels"] = cache_kernel_line(dev, args.steps)
+        line["adjoint"] = adjoint_line(dev)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         osc = cpu_oracle(wl)
@@ -379,6 +382,88 @@ def batched_line(dev, steps: int, spp: int = 8) -> dict:
             "gpu_launches": int(launches), "per_view_calls_mrays_per_s": rays_seq / ms_seq / 1e3}
 
 
+def cache_kernel_line(dev, steps: int) -> dict:
+    """Radiance-cache kernels on their own: inference over 2^21 positions and training steps of
+    2^16 records (forward + backward on the tensor cores, table-gradient scatter, Adam on 16.8M
+    table and 6,336 weight parameters), device buffers, CUDA-event timing on the library's stream."""
+    import torch
+
+    from stratum2_b200 import _abi
+    p = _abi.S2CacheParams()
+    _abi.lib().s2_cache_default_params(p)
+    for k in range(3):
+        p.box_min[k], p.box_max[k] = -1.0, 1.0
+    dev.cache_init(p)
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    nq, nt = 1 << 21, 1 << 16
+    pos = torch.rand((nq, 4), generator=g, device="cuda") * 2 - 1
+    out = torch.empty((nq, 4), device="cuda")
+    tpos = torch.rand((nt, 4), generator=g, device="cuda") * 2 - 1
+    tgt = torch.rand((nt, 4), generator=g, device="cuda")
+    for _ in range(3):
+        dev.cache_query_device(pos.data_ptr(), nq, out.data_ptr())
+        dev.cache_train_device(tpos.data_ptr(), tgt.data_ptr(), nt)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(steps):
+        dev.cache_query_device(pos.data_ptr(), nq, out.data_ptr())
+    e1.record(stream)
+    for _ in range(steps):
+        dev.cache_train_device(tpos.data_ptr(), tgt.data_ptr(), nt)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    dev.set_stream(None)
+    inf_ms, tr_ms = e0.elapsed_time(e1) / steps, e1.elapsed_time(e2) / steps
+    flop_q = 2 * 6336
+    pk = peaks()
+    inf_tflops = flop_q * nq / inf_ms / 1e9
+    return {"inference": {"queries": nq, "ms": inf_ms, "mqueries_per_s": nq / inf_ms / 1e3, "tflops": inf_tflops,
+                          "tensor_frac_of_measured_bf16": inf_tflops / pk["bf16_tflops"],
+                          "table_gather_gbs": 512 * nq / inf_ms / 1e6},
+            "training_step": {"records": nt, "ms": tr_ms, "mrecords_per_s": nt / tr_ms / 1e3,
+                              "note": "forward + backward + table scatter + Adam over all parameters"}}
+
+
+def adjoint_line(dev, steps: int = 2) -> dict:
+    """Differentiable inverse-rendering workload: the box with 200 level-3 icospheres (256k
+    triangles), 1024^2 RGB albedo and 1024^2 roughness textures, a 256x128 environment map; 512x512,
+    64 spp, path length up to 4.  Forward (s2_render_diff) and adjoint (s2_render_adjoint, two
+    replays per path, texel gradients of all three images) timed on the device."""
+    import torch
+
+    from stratum2_b200 import _abi
+    from stratum2_b200.scenegen import textured_box_scene
+    wl = textured_box_scene(n_random=0, width=512, height=512, tex_res=1024, env_res=(256, 128), spheres=200,
+                            sphere_level=3)
+    dev.upload_scene(wl.scene)
+    p = _abi.S2RenderParams()
+    _abi.lib().s2_default_render_params(p)
+    p.spp, p.min_path_length, p.max_path_length, p.flags, p.frame_seed = 64, 0, 4, _abi.FLAG_PIXEL_JITTER, 1
+    img = torch.empty((512, 512, 4), device="cuda")
+    d = torch.rand((512, 512, 4), device="cuda")
+    grads = [torch.zeros(im.shape[:2] + (4,), device="cuda") for im in wl.scene.images]
+    ptrs = [t.data_ptr() for t in grads]
+    dev.render_diff_device(wl.view, p, img.data_ptr())
+    dev.render_adjoint_device(wl.view, p, d.data_ptr(), ptrs)
+    f_ms = b_ms = 0.0
+    rays = 0
+    for k in range(steps):
+        p.frame_seed = 100 + 64 * k
+        s = dev.render_diff_device(wl.view, p, img.data_ptr())
+        f_ms += s.gpu_ms
+        rays += s.extension_rays + s.shadow_rays
+        b_ms += dev.render_adjoint_device(wl.view, p, d.data_ptr(), ptrs).gpu_ms
+    paths = 512 * 512 * 64
+    return {"workload": "box + 200 icospheres (%d triangles), 1024^2 albedo + roughness textures, 256x128 env; "
+                        "512x512, 64 spp, max path length 4" % int(dev.bvh_stats.triangle_count),
+            "forward_ms": f_ms / steps, "forward_mrays_per_s": rays / f_ms / 1e3,
+            "forward_mpaths_per_s": paths / (f_ms / steps) / 1e3, "adjoint_ms": b_ms / steps,
+            "adjoint_mpaths_per_s": paths / (b_ms / steps) / 1e3,
+            "gradient_texels": int(sum(t.shape[0] * t.shape[1] for t in grads))}
+
+
 def C_sizeof_view_params() -> int:
     import ctypes
     from stratum2_b200 import _abi
@@ -398,7 +483,13 @@ def main():
                     help="sample budget of the time-to-relMSE runs (extrapolated beyond it)")
     ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",
                     help="render one frame of the workload with SPP samples and exit (profiling)")
+    ap.add_argument("--cache-kernels", type=int, default=0, metavar="STEPS",
+                    help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
     args = ap.parse_args()
+    if args.cache_kernels:
+        from stratum2_b200 import Device
+        print(json.dumps(cache_kernel_line(Device(0), args.cache_kernels)))
+        return
     if args.single_frame:
         from stratum2_b200 import Device
         from stratum2_b200.scenegen import terrain_scene

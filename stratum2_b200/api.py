@@ -274,3 +274,13 @@ class Device:
         self._check(self._lib.s2_render_adjoint(self._h, C.byref(view), C.byref(params), C.c_void_p(d_ptr), 0,
                                                 C.cast(ptrs, C.c_void_p), C.byref(st)))
         return st
+
+    def cache_query_device(self, pos_ptr: int, n: int, out_ptr: int):
+        """Cache inference on device buffers (float4 positions in, float4 radiance out)."""
+        self._check(self._lib.s2_cache_query(self._h, C.c_void_p(pos_ptr), n, C.c_void_p(out_ptr), 1))
+
+    def cache_train_device(self, pos_ptr: int, target_ptr: int, n: int) -> float:
+        """One optimiser step on device records (float4 positions, float4 targets); mean loss."""
+        loss = C.c_float(0)
+        self._check(self._lib.s2_cache_train(self._h, C.c_void_p(pos_ptr), C.c_void_p(target_ptr), n, C.byref(loss), 1))
+        return loss.value

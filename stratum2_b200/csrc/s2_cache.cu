@@ -199,14 +199,24 @@ extern "C" int s2_cache_get_params(S2Context* ctx, float* weights, float* table)
 }
 
 namespace s2 {
+// The inference kernel's dynamic shared memory exceeds the 48 KB default once per device.
+void set_infer_attributes(S2Context* ctx) {
+    static bool attr_set[64] = {};
+    if (ctx->device < 64 && !attr_set[ctx->device]) {
+        cudaFuncSetAttribute(k_cache_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmemBytes);
+        attr_set[ctx->device] = true;
+    }
+}
+
 // Path-tracer terminal vertices: accum[slot] += tput * cache(pos) for up to `cap` queries, the
 // count read from n_dev.
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
                        float4* accum) {
     CacheState* c = ctx->cache;
+    set_infer_attributes(ctx);
     const uint32_t tiles = (cap + kCacheTile - 1) / kCacheTile;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
-    k_cache_infer<<<grid, 128, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum);
+    const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum);
     return check_cuda(ctx, cudaGetLastError(), "cache apply launch");
 }
 
@@ -214,14 +224,10 @@ int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, ui
 int cache_infer_device(S2Context* ctx, const float4* pos, uint32_t n, float4* out) {
     CacheState* c = ctx->cache;
     if (n == 0) return S2_OK;
-    static bool attr_set[64] = {};
-    if (ctx->device < 64 && !attr_set[ctx->device]) {
-        cudaFuncSetAttribute(k_cache_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmemBytes);
-        attr_set[ctx->device] = true;
-    }
+    set_infer_attributes(ctx);
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->sms);
-    k_cache_infer<<<grid, 128, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr);
+    const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr);
     return check_cuda(ctx, cudaGetLastError(), "cache inference launch");
 }
 }  // namespace s2

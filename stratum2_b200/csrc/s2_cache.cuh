@@ -100,11 +100,47 @@ S2D void cache_encode(const CacheDev& c, float3 p, __half2 out[kCacheLevels]) {
     }
 }
 
+// Levels l0 .. l0+3 of the encoding of one position (see cache_encode).
+S2D void cache_encode4(const CacheDev& c, float3 p, uint32_t l0, __half2 out[4]) {
+    const float3 u = cache_unit(c, p);
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t l = l0 + j;
+        const float r = c.res[l];
+        const float fx = u.x * r, fy = u.y * r, fz = u.z * r;
+        const float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
+        const float wx = fx - ix, wy = fy - iy, wz = fz - iz;
+        const uint32_t x0 = (uint32_t)ix, y0 = (uint32_t)iy, z0 = (uint32_t)iz;
+        const __half2* tab = c.table + ((size_t)l << c.log2_table);
+        float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) {
+            const uint32_t dx = k & 1u, dy = (k >> 1) & 1u, dz = k >> 2;
+            const float w = (dx ? wx : 1.f - wx) * (dy ? wy : 1.f - wy) * (dz ? wz : 1.f - wz);
+            const float2 f = __half22float2(__ldg(tab + cache_index(c, l, x0 + dx, y0 + dy, z0 + dz)));
+            a0 += w * f.x;
+            a1 += w * f.y;
+        }
+        out[j] = __floats2half2_rn(a0, a1);
+    }
+}
+
+S2D void block_sync_tc() {
+    fence_smem_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+}
+
 // Shared-memory plan of the inference kernel (bytes): weights, input tile, hidden tile.
 constexpr uint32_t kInfSmemW = 0;
 constexpr uint32_t kInfSmemX = kWImageBytes;                         // 128 x 32 f16
 constexpr uint32_t kInfSmemH = kInfSmemX + kCacheTile * kCacheIn * 2; // 128 x 64 f16
 constexpr uint32_t kInfSmemBytes = kInfSmemH + kCacheTile * kCacheHidden * 2;
+// Inference CTA: 512 threads; four threads encode one query (four levels = one 16-byte operand
+// chunk each, so four times the table gathers in flight), the first warpgroup runs the MLP.
+constexpr uint32_t kInfThreads = 512;
+constexpr uint32_t kInfCtasPerSm = 1;
 
 // Writes 8 f16 values (one 16-byte chunk) of row r, chunk q of a K-major tile.
 S2D void store_chunk(uint8_t* tile, uint32_t r, uint32_t q, uint32_t K, const __half2 h[4]) {
@@ -135,17 +171,17 @@ S2D void tmem_relu_to_tile(uint32_t tlane, uint32_t col, uint8_t* dst, uint32_t 
 // (the path tracer's terminal vertices) the result is instead added to the path's accumulator:
 // accum[slot] += tput[i] * max(y, 0), slot in pos[i].w.  n_dev (optional) caps n with a device count.
 // Persistent: grid-stride over tiles of 128 queries; 128 threads; kInfSmemBytes dynamic smem.
-__global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
-                                                        uint32_t n, const uint32_t* __restrict__ n_dev,
-                                                        float4* __restrict__ out, const float4* __restrict__ tput,
-                                                        float4* __restrict__ accum) {
+__global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
+                                                                uint32_t n, const uint32_t* __restrict__ n_dev,
+                                                                float4* __restrict__ out, const float4* __restrict__ tput,
+                                                                float4* __restrict__ accum) {
     if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_base;
     const uint32_t t = threadIdx.x, warp = t >> 5;
-    // stage the weight images
-    for (uint32_t i = t; i < kWImageBytes / 16; i += 128) ((uint4*)(smem + kInfSmemW))[i] = c.wimage[i];
+    const bool mlp = warp < 4;  // the warpgroup whose lanes are the tile's rows
+    for (uint32_t i = t; i < kWImageBytes / 16; i += kInfThreads) ((uint4*)(smem + kInfSmemW))[i] = c.wimage[i];
     if (warp == 0) {
         tmem_alloc(&tmem_base, 128);
         tmem_relinquish();
@@ -164,67 +200,56 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
     const uint32_t s_x = smem_addr(smem + kInfSmemX), s_h = smem_addr(smem + kInfSmemH);
     uint32_t phase = 0;
     bool ok = true;
+    // MMA completion for the MLP warps (the others only take part in the block barriers)
+    auto done = [&](bool issued) {
+        if (!mlp) return;
+        const bool w = ok && issued && mbar_wait(&bar, phase);
+        if (w) phase ^= 1u;
+        ok = __all_sync(0xffffffffu, w);
+    };
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const uint32_t q = tile * kCacheTile + t;
-        __half2 f[kCacheLevels];
-        if (q < n) {
-            const float4 p = pos[q];
-            cache_encode(c, f3(p.x, p.y, p.z), f);
-        } else {
+        {
+            // encode: thread t takes query row t / 4, levels 4 * (t % 4) .. +3 (one operand chunk)
+            const uint32_t row = t >> 2, part = t & 3u, q = tile * kCacheTile + row;
+            __half2 f[4];
+            if (q < n) {
+                const float4 p = pos[q];
+                cache_encode4(c, f3(p.x, p.y, p.z), 4u * part, f);
+            } else {
 #pragma unroll
-            for (uint32_t l = 0; l < kCacheLevels; ++l) f[l] = __floats2half2_rn(0.f, 0.f);
+                for (uint32_t j = 0; j < 4; ++j) f[j] = __floats2half2_rn(0.f, 0.f);
+            }
+            store_chunk(smem + kInfSmemX, row, part, kCacheIn, f);
         }
-#pragma unroll
-        for (uint32_t ch = 0; ch < 4; ++ch) store_chunk(smem + kInfSmemX, t, ch, kCacheIn, f + 4 * ch);
+        const uint32_t q = tile * kCacheTile + t;  // MLP row of warps 0..3
         // layer 1: D[0:64) = X W1^T
-        fence_smem_async();
-        tc_fence_before_sync();
-        __syncthreads();
-        tc_fence_after_sync();
-        if (t == 0) {
+        block_sync_tc();
+        if (t == 0 && ok) {
             umma_gemm(tmem, s_x, s_w1, kCacheIn, kCacheHidden, false);
             umma_commit(&bar);
         }
-        {
-            const bool w = mbar_wait(&bar, phase);
-            if (w) phase ^= 1u;
-            ok = __all_sync(0xffffffffu, w);
-        }
+        done(true);
         tc_fence_after_sync();
-        if (ok) tmem_relu_to_tile(tlane, 0, smem + kInfSmemH, t);
+        if (mlp && ok) tmem_relu_to_tile(tlane, 0, smem + kInfSmemH, t);
         // layer 2: D[64:128) = H1 W2^T
-        fence_smem_async();
-        tc_fence_before_sync();
-        __syncthreads();
-        tc_fence_after_sync();
+        block_sync_tc();
         if (t == 0 && ok) {
             umma_gemm(tmem + 64u, s_h, s_w2, kCacheHidden, kCacheHidden, false);
             umma_commit(&bar);
         }
-        {
-            const bool w = ok && mbar_wait(&bar, phase);
-            if (w) phase ^= 1u;
-            ok = __all_sync(0xffffffffu, w);
-        }
+        done(true);
         tc_fence_after_sync();
-        if (ok) tmem_relu_to_tile(tlane, 64u, smem + kInfSmemH, t);
+        if (mlp && ok) tmem_relu_to_tile(tlane, 64u, smem + kInfSmemH, t);
         // layer 3: D[0:16) = H2 W3^T
-        fence_smem_async();
-        tc_fence_before_sync();
-        __syncthreads();
-        tc_fence_after_sync();
+        block_sync_tc();
         if (t == 0 && ok) {
             umma_gemm(tmem, s_h, s_w3, kCacheHidden, kCacheOutPad, false);
             umma_commit(&bar);
         }
-        {
-            const bool w = ok && mbar_wait(&bar, phase);
-            if (w) phase ^= 1u;
-            ok = __all_sync(0xffffffffu, w);
-        }
+        done(true);
         tc_fence_after_sync();
-        if (ok) {
+        if (mlp && ok) {
             float v[16];
             tmem_ld16(tlane, v);
             if (q < n) {
@@ -251,7 +276,7 @@ __global__ void __launch_bounds__(128, 1) k_cache_infer(const __grid_constant__ 
         // a wait timed out: record it, give an MMA still in flight a bounded time to land, and
         // release TMEM only then
         if (t == 0) atomicOr(c.status, 4);
-        mbar_wait(&bar, phase);
+        if (mlp) mbar_wait(&bar, phase);
     }
     tc_fence_before_sync();
     __syncthreads();
@@ -297,12 +322,6 @@ struct TcSync {
     }
 };
 
-S2D void block_sync_tc() {
-    fence_smem_async();
-    tc_fence_before_sync();
-    __syncthreads();
-    tc_fence_after_sync();
-}
 
 // One pass over n training records (position, target radiance): forward, relative L2 loss
 // sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / 3 per record (denominator not differentiated), backward
