@@ -485,7 +485,25 @@ def main():
                     help="render one frame of the workload with SPP samples and exit (profiling)")
     ap.add_argument("--cache-kernels", type=int, default=0, metavar="STEPS",
                     help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
+    ap.add_argument("--cached-frames", type=int, default=0, metavar="N",
+                    help="render N 1-spp frames of the workload in the radiance-cache form and exit (profiling)")
     args = ap.parse_args()
+    if args.cached_frames:
+        from stratum2_b200 import Device, _abi
+        from stratum2_b200.scenegen import terrain_scene
+        dev = Device(0)
+        wl = terrain_scene()
+        dev.upload_scene(wl.scene)
+        dev.cache_init()
+        out = []
+        for k in range(args.cached_frames):
+            p = params(dev, 1, 50000 + k, _abi.FLAG_RADIANCE_CACHE | (_abi.FLAG_ACCUMULATE if k else 0))
+            p.cache_bounces = 1
+            r = dev.render(wl.view, wl.width, wl.height, params=p)
+            out.append({"gpu_ms": r.stats.gpu_ms, "launches": r.stats.kernel_launches,
+                        "extension_rays": r.stats.extension_rays, "shadow_rays": r.stats.shadow_rays})
+        print(json.dumps(out))
+        return
     if args.cache_kernels:
         from stratum2_b200 import Device
         print(json.dumps(cache_kernel_line(Device(0), args.cache_kernels)))
