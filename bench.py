@@ -187,6 +187,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     def seed(step: int) -> int:
         return frame_seed(step, rank, world, SPP)  # disjoint frame seeds per rank and step
 
+    # autotuning (untimed set-up): wave size and traversal knobs for this workload
+    tuning = None
+    if not args.no_autotune:
+        from stratum2_b200 import autotune
+        tuning = autotune.autotune(dev, wl.view, params(dev, SPP, 7777), path=Path(tempfile.gettempdir()) / "s2_bench_tuning.json",
+                                   force=True)
     # fetch counts for the algorithmic-byte model (untimed run, same seeds as timed step 0)
     cnt = dev.render_device(wl.view, params(dev, SPP, seed(0), _abi.FLAG_COUNT_FETCHES), aovs)
     for w in range(args.warmup):
@@ -255,7 +261,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "min_path_length": MIN_LEN,
                        "max_path_length": MAX_LEN, "triangles": int(dev.bvh_stats.triangle_count),
                        "bvh8_nodes": int(dev.bvh_stats.node_count), "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"{world} rank(s), disjoint sample seeds"},
+                       "parallelism": f"{world} rank(s), disjoint sample seeds",
+                       "tuning": (tuning or {}).get("tuning", "defaults"),
+                       "autotune_trials": (tuning or {}).get("trials", 0)},
             "mpaths_per_s": paths / ms / 1e3,
             "kernel_ms_per_step": {"k_extend": ext_ms / args.steps, "k_shade": sh_ms / args.steps,
                                    "k_occlude": oc_ms / args.steps},
@@ -479,6 +487,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the batched and time-to-relMSE measurements")
+    ap.add_argument("--no-autotune", action="store_true", help="render with the default tuning")
     ap.add_argument("--quality-spp", type=int, default=2048,
                     help="sample budget of the time-to-relMSE runs (extrapolated beyond it)")
     ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",

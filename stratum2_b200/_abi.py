@@ -50,6 +50,7 @@ EXPORTED_SYMBOLS = [
     "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
+    "s2_set_tuning", "s2_get_tuning", "s2_autotune",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -134,6 +135,11 @@ class S2CacheParams(C.Structure):
                 ("reserved", C.c_uint32 * 6)]
 
 
+class S2Tuning(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint32), ("trav_tris_per_step", C.c_uint32), ("trav_vote8", C.c_uint32),
+                ("refill_min", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+
 class S2RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
                 ("nan_count", C.c_uint64), ("gpu_ms", C.c_double), ("kernel_launches", C.c_uint64),
@@ -178,6 +184,9 @@ def lib() -> C.CDLL:
     L.s2_default_render_params.argtypes = [P(S2RenderParams)]
     L.s2_default_render_params.restype = None
     L.s2_update_image.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+    L.s2_set_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
+    L.s2_get_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
+    L.s2_autotune.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Tuning), P(C.c_uint32)]
     L.s2_render_diff.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, P(S2RenderStats)]
     L.s2_render_adjoint.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, C.c_void_p,
                                     P(S2RenderStats)]

@@ -284,3 +284,19 @@ class Device:
         loss = C.c_float(0)
         self._check(self._lib.s2_cache_train(self._h, C.c_void_p(pos_ptr), C.c_void_p(target_ptr), n, C.byref(loss), 1))
         return loss.value
+
+    # ---- tuning
+    def set_tuning(self, tuning: _abi.S2Tuning | None):
+        self._check(self._lib.s2_set_tuning(self._h, C.byref(tuning) if tuning is not None else None))
+
+    def get_tuning(self) -> _abi.S2Tuning:
+        t = _abi.S2Tuning()
+        self._check(self._lib.s2_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def autotune(self, view, params: _abi.S2RenderParams) -> tuple[_abi.S2Tuning, int]:
+        """Measures tuning candidates on this scene/view/params and applies the fastest."""
+        t = _abi.S2Tuning()
+        n = C.c_uint32(0)
+        self._check(self._lib.s2_autotune(self._h, C.byref(view), C.byref(params), C.byref(t), C.byref(n)))
+        return t, n.value

@@ -53,6 +53,7 @@ struct S2Context {
 
     s2::RenderState* render = nullptr;
     s2::CacheState* cache = nullptr;
+    S2Tuning tuning{};                      // wavefront renderer tuning (zeros = defaults)
     int* status_dev = nullptr;              // device status word (stack/queue overflow, timeouts)
 };
 

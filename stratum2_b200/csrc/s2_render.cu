@@ -210,7 +210,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         return set_error(ctx, S2_ERR_INVALID, "invalid ReSTIR hash-grid parameters");
     cudaSetDevice(ctx->device);
     const uint32_t pixels = (uint32_t)W * (uint32_t)H;
-    uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 25);
+    uint64_t target = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (1u << 25));
     uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, target / pixels));
     const uint32_t capacity = slots * pixels;
     int rc = ensure_state(ctx, (uint32_t)W, (uint32_t)H, capacity);
@@ -234,6 +234,9 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     P.frame_seed = prm->frame_seed;
     P.restir_m = prm->restir_candidates ? prm->restir_candidates : 32;
     P.exposure = prm->exposure;
+    P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;
+    P.trav.vote8 = ctx->tuning.trav_vote8;
+    P.refill_min = ctx->tuning.refill_min;
     P.q[0] = st->q[0]; P.q[1] = st->q[1];
     P.hits = st->hits; P.sh_o = st->sh_o; P.sh_d = st->sh_d; P.sh_c = st->sh_c;
     P.accum = st->accum;
@@ -509,7 +512,8 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     BatchState* B = g_batch_for(ctx);
     if (!B) return set_error(ctx, S2_ERR_OOM, "batch state allocation failed");
     cudaStream_t s = ctx->stream;
-    const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(prm->wave_paths ? prm->wave_paths : (1u << 25), paths));
+    const uint64_t wave = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (1u << 25));
+    const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(wave, paths));
     if (B->capacity < capacity) {
         free_bufs(B->qbufs);
         B->capacity = 0;
@@ -579,6 +583,9 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     P.flags = prm->flags;
     P.frame_seed = prm->frame_seed;
     P.restir_m = prm->restir_candidates ? prm->restir_candidates : 32;
+    P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;
+    P.trav.vote8 = ctx->tuning.trav_vote8;
+    P.refill_min = ctx->tuning.refill_min;
     P.exposure = prm->exposure;
     P.q[0] = B->q[0]; P.q[1] = B->q[1];
     P.hits = B->hits; P.sh_o = B->sh_o; P.sh_d = B->sh_d; P.sh_c = B->sh_c;
@@ -695,5 +702,79 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         stats_out->shadow_node_fetches = sv[S_SH_NODES];
         stats_out->shadow_tri_fetches = sv[S_SH_TRIS];
     }
+    return S2_OK;
+}
+
+// ============================================================================== tuning
+extern "C" int s2_set_tuning(S2Context* ctx, const S2Tuning* t) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!t) { std::memset(&ctx->tuning, 0, sizeof(ctx->tuning)); return S2_OK; }
+    if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024))
+        return set_error(ctx, S2_ERR_INVALID, "tuning out of range (tris_per_step <= 32, vote8 <= 9, refill_min <= 32, "
+                                              "wave_paths 0 or >= 1024)");
+    ctx->tuning = *t;
+    return S2_OK;
+}
+
+extern "C" int s2_get_tuning(S2Context* ctx, S2Tuning* t) {
+    if (!ctx || !t) return S2_ERR_INVALID;
+    *t = ctx->tuning;
+    return S2_OK;
+}
+
+extern "C" int s2_autotune(S2Context* ctx, const S2View* view, const S2RenderParams* prm, S2Tuning* out,
+                           uint32_t* trials_out) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!view || !prm) return set_error(ctx, S2_ERR_INVALID, "view and params are required");
+    S2RenderParams p = *prm;
+    p.flags &= ~(S2_FLAG_ACCUMULATE | S2_FLAG_PROFILE_KERNELS | S2_FLAG_COUNT_FETCHES);
+    p.wave_paths = 0;
+    const S2Tuning saved = ctx->tuning;
+    uint32_t trials = 0;
+    uint32_t seed = p.frame_seed;
+    // ray throughput of the current tuning: best of two renders (the first also warms caches)
+    auto measure = [&](double& mrays) -> int {
+        double best = 0.0;
+        for (int k = 0; k < 2; ++k) {
+            p.frame_seed = seed;
+            seed += std::max(1u, p.spp);
+            S2RenderStats st;
+            const int rc = s2_render(ctx, view, &p, nullptr, 0, &st);
+            if (rc != S2_OK) return rc;
+            trials++;
+            if (st.gpu_ms > 0) best = std::max(best, (double)(st.extension_rays + st.shadow_rays) / st.gpu_ms / 1e3);
+        }
+        mrays = best;
+        return S2_OK;
+    };
+    S2Tuning best = saved;
+    double best_rate = 0.0;
+    int rc = measure(best_rate);
+    if (rc != S2_OK) { ctx->tuning = saved; return rc; }
+    const uint32_t waves[] = {1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26};
+    const uint32_t tris[] = {1, 2, 4, 8};
+    const uint32_t votes[] = {2, 3, 4, 5, 6};
+    const uint32_t refills[] = {4, 8, 12, 16};
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int knob = 0; knob < 4; ++knob) {
+            const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : refills;
+            const int nv = knob == 0 ? 5 : knob == 1 ? 4 : knob == 2 ? 5 : 4;
+            for (int v = 0; v < nv; ++v) {
+                S2Tuning t = best;
+                uint32_t* field = knob == 0 ? &t.wave_paths : knob == 1 ? &t.trav_tris_per_step
+                                : knob == 2 ? &t.trav_vote8 : &t.refill_min;
+                if (*field == vals[v]) continue;
+                *field = vals[v];
+                ctx->tuning = t;
+                double rate = 0.0;
+                rc = measure(rate);
+                if (rc != S2_OK) { ctx->tuning = saved; return rc; }
+                if (rate > best_rate * 1.01) { best_rate = rate; best = t; }
+            }
+        }
+    }
+    ctx->tuning = best;
+    if (out) *out = best;
+    if (trials_out) *trials_out = trials;
     return S2_OK;
 }

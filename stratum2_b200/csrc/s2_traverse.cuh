@@ -162,10 +162,11 @@ struct TravState {
     uint32_t node;
     int sp;
     bool ok;    // false if the stack overflowed
+    uint32_t tbase, tmask;  // pending leaf triangles (trav_step_pp)
 };
 
 S2D void trav_begin(TravState& st, TravHit& hit, float tmax) {
-    st.node = 0; st.sp = 0; st.ok = true;
+    st.node = 0; st.sp = 0; st.ok = true; st.tbase = 0; st.tmask = 0;
     hit.t = tmax; hit.tri = 0xffffffffu; hit.instance = 0xffffffffu; hit.primitive = 0xffffffffu;
     hit.b1 = hit.b2 = 0.f;
 }
@@ -234,6 +235,104 @@ S2D bool trav_step(const TravRay& r, TravState& st, const uint4* __restrict__ no
         st.sp--;
     }
     return false;
+}
+
+// Step of the warp-cooperative traversal with postponed triangle tests (the "while-while" order of
+// Aila and Laine, HPG 2009, decided per step by a warp vote).  A lane alternates between node steps
+// and triangle steps: a node step visits st.node, records the node's leaf triangles as pending
+// (st.tbase, st.tmask) and moves to the next node; a lane with pending triangles takes no node step
+// until they are tested, one per triangle step.  `do_tri` (warp-uniform) selects the step kind, so
+// lanes in one step run the same code.  Returns true when the ray is finished (no node left and no
+// triangle pending, or an accepted any-hit).
+constexpr uint32_t kTravDone = 0xffffffffu;
+// Tuning of the warp-cooperative traversal (runtime, chosen by s2_autotune): triangle tests per
+// triangle step, and the vote: a triangle step when vote8 / 8 of the lanes with work have
+// triangles pending (or no lane can take a node step).  Zero selects the defaults, measured on B200
+// (terrain workload): 4 triangles, 4/8.
+struct TravTuning {
+    uint32_t tris_per_step;
+    uint32_t vote8;
+};
+
+template <bool ANYHIT, bool COUNT, class Alpha = NoAlphaTest>
+S2D bool trav_step_pp(const TravRay& r, TravState& st, const uint4* __restrict__ nodes4, const float4* __restrict__ tris4,
+                      uint2* __restrict__ smem_stack, uint32_t lane_stride, uint2* lstack, TravHit& hit, TravCounters& ctr,
+                      bool do_tri, uint32_t tris_per_step, const Alpha& alpha = Alpha()) {
+    if (do_tri) {
+        const uint32_t nt = tris_per_step ? tris_per_step : 4u;  // 0: the default
+#pragma unroll 1
+        for (uint32_t rep = 0; rep < nt && st.tmask; ++rep) {
+            const uint32_t k = __ffs(st.tmask) - 1;
+            st.tmask &= st.tmask - 1;
+            const uint32_t ti = st.tbase + k;
+            const float4 a = __ldg(tris4 + 3 * (size_t)ti + 0);
+            const float4 b = __ldg(tris4 + 3 * (size_t)ti + 1);
+            const float4 c = __ldg(tris4 + 3 * (size_t)ti + 2);
+            if (COUNT) ctr.tris++;
+            float t, b1, b2;
+            if (intersect_triangle(r, ld3(a), ld3(b), ld3(c), hit.t, t, b1, b2)) {
+                const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+                if (!((__float_as_uint(c.w) & S2_TRI_ALPHA_TESTED) && !alpha(inst, prim, b1, b2))) {
+                    if (ANYHIT) {
+                        hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+                        st.tmask = 0;
+                        st.node = kTravDone;
+                        return true;
+                    }
+                    if (t < hit.t || inst < hit.instance || (inst == hit.instance && prim < hit.primitive)) {
+                        hit.t = t; hit.tri = ti; hit.instance = inst; hit.primitive = prim; hit.b1 = b1; hit.b2 = b2;
+                    }
+                }
+            }
+        }
+    } else if (st.tmask == 0 && st.node != kTravDone) {
+        uint32_t child_base, imask, hits, tri_base, trimask;
+        intersect_node(r, nodes4, st.node, hit.t, child_base, imask, hits, tri_base, trimask);
+        if (COUNT) ctr.nodes++;
+        st.tbase = tri_base;
+        st.tmask = trimask;
+        if (hits) {
+            const uint32_t b = __ffs(hits) - 1;
+            hits &= hits - 1;
+            const uint32_t s = b ^ r.oct;
+            const uint32_t next = child_base + __popc(imask & ((1u << s) - 1u));
+            if (hits) {
+                const uint2 g = make_uint2(child_base, imask | (hits << 8));
+                if (st.sp < S2_STACK_SMEM) smem_stack[st.sp * lane_stride] = g;
+                else if (st.sp < S2_STACK_DEPTH) lstack[st.sp - S2_STACK_SMEM] = g;
+                else st.ok = false;
+                if (st.sp < S2_STACK_DEPTH) st.sp++;
+            }
+            st.node = next;
+        } else if (st.sp == 0) {
+            st.node = kTravDone;
+        } else {
+            uint2 g = (st.sp - 1 < S2_STACK_SMEM) ? smem_stack[(st.sp - 1) * lane_stride] : lstack[st.sp - 1 - S2_STACK_SMEM];
+            uint32_t gh = g.y >> 8;
+            const uint32_t b = __ffs(gh) - 1;
+            gh &= gh - 1;
+            const uint32_t gi = g.y & 0xffu;
+            const uint32_t s = b ^ r.oct;
+            st.node = g.x + __popc(gi & ((1u << s) - 1u));
+            if (gh) {
+                g.y = gi | (gh << 8);
+                if (st.sp - 1 < S2_STACK_SMEM) smem_stack[(st.sp - 1) * lane_stride] = g;
+                else lstack[st.sp - 1 - S2_STACK_SMEM] = g;
+            } else {
+                st.sp--;
+            }
+        }
+    }
+    return st.tmask == 0 && st.node == kTravDone;
+}
+
+// Warp vote for trav_step_pp: a triangle step when at least vote8 / 8 of the lanes with work have
+// triangles pending, or when no lane can take a node step.
+S2D bool trav_vote_tri(bool active, const TravState& st, uint32_t vote8) {
+    const uint32_t tri = __ballot_sync(0xffffffffu, active && st.tmask != 0);
+    const uint32_t node = __ballot_sync(0xffffffffu, active && st.tmask == 0 && st.node != kTravDone);
+    const uint32_t v = vote8 ? vote8 : 4u;  // 0: the default
+    return node == 0u || 8u * (uint32_t)__popc(tri) >= v * (uint32_t)__popc(tri | node);
 }
 
 // Whole traversal of one ray.  ANYHIT: stop at the first accepted triangle.  COUNT: count node and

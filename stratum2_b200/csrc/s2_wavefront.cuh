@@ -97,6 +97,9 @@ struct PTParams {
     uint32_t cq_cap;
     float4 *tr_pos, *tr_thr, *tr_rad;
     uint32_t tr_cap;
+    // traversal tuning (s2_autotune / s2_set_tuning; 0 = default)
+    TravTuning trav;
+    uint32_t refill_min;  // refill a warp's idle lanes once this many are idle
 };
 
 // fixed-point scale of the batched accumulators: integer sums are independent of the order of the
@@ -285,7 +288,7 @@ __global__ void k_resolve_fx(const unsigned long long* __restrict__ total_fx, ui
 // all have), the warp fetches that many new rays from the global work counter with one atomic.
 // Lanes therefore stay busy while long rays finish, instead of the whole warp waiting for its
 // slowest ray (dynamic ray fetch in the manner of Aila and Laine, HPG 2009).
-constexpr uint32_t kRefillMin = 8;
+constexpr uint32_t kRefillMin = 8;  // default of PTParams::refill_min
 constexpr uint32_t kNoRay = 0xffffffffu;
 
 // Warp-sum of the fetch counters, one 64-bit atomic per warp (counting runs only).
@@ -296,11 +299,11 @@ S2D void add_fetches(unsigned long long* stats, uint32_t node_stat, const TravCo
 }
 
 // Gives idle lanes new work items [0, count) from `work`; returns the lane's item or kNoRay.
-S2D uint32_t refill(uint32_t* work, uint32_t count, uint32_t item, bool& exhausted) {
+S2D uint32_t refill(uint32_t* work, uint32_t count, uint32_t item, bool& exhausted, uint32_t refill_min) {
     const bool need = item == kNoRay && !exhausted;
     const uint32_t needm = __ballot_sync(0xffffffffu, need);
     const uint32_t activem = __ballot_sync(0xffffffffu, item != kNoRay);
-    if (needm && (__popc(needm) >= kRefillMin || activem == 0)) {
+    if (needm && ((uint32_t)__popc(needm) >= (refill_min ? refill_min : kRefillMin) || activem == 0)) {
         const uint32_t lane = threadIdx.x & 31u;
         const uint32_t leader = __ffs(needm) - 1;
         uint32_t base = 0;
@@ -330,16 +333,17 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
     bool exhausted = false;
     while (true) {
         const uint32_t prev = ray;
-        ray = refill(&P.counters[C_WORK_EXT], count, ray, exhausted);
+        ray = refill(&P.counters[C_WORK_EXT], count, ray, exhausted, P.refill_min);
         if (!__any_sync(0xffffffffu, ray != kNoRay)) break;
         if (ray != kNoRay && prev == kNoRay) {
             const float4 a = q.s0[ray], b = q.s1[ray];
             r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
             trav_begin(st, h, S2_INF);
         }
+        const bool tri_step = trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
         if (ray != kNoRay) {
-            if (trav_step<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
-                                        SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
+            if (trav_step_pp<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                           tri_step, P.trav.tris_per_step, SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
                 if (!st.ok) atomicOr(P.status, 1);
                 P.hits[ray] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
                 ray = kNoRay;
@@ -364,16 +368,17 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ 
     bool exhausted = false;
     while (true) {
         const uint32_t prev = ray;
-        ray = refill(&P.counters[C_WORK_OCC], count, ray, exhausted);
+        ray = refill(&P.counters[C_WORK_OCC], count, ray, exhausted, P.refill_min);
         if (!__any_sync(0xffffffffu, ray != kNoRay)) break;
         if (ray != kNoRay && prev == kNoRay) {
             const float4 o = P.sh_o[ray], d = P.sh_d[ray];
             r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
             trav_begin(st, h, o.w);
         }
+        const bool tri_step = trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
         if (ray != kNoRay) {
-            if (trav_step<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
-                                       SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
+            if (trav_step_pp<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                          tri_step, P.trav.tris_per_step, SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
                 if (!st.ok) atomicOr(P.status, 1);
                 if (h.tri == 0xffffffffu) {
                     const float4 cc = P.sh_c[ray];
