@@ -282,17 +282,23 @@ int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams*
  * defaults.  s2_autotune measures candidates on the caller's scene, view and parameters and
  * applies the fastest; s2_set_tuning applies a stored result (stratum2_b200/autotune.py keeps them
  * as JSON keyed by GPU and workload). */
+#define S2_SHADE_ORDER_MATERIAL 0u
+#define S2_SHADE_ORDER_QUEUE 1u
+
 typedef struct S2Tuning {
     uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^25) */
     uint32_t trav_tris_per_step;  /* triangle tests per triangle step of the traversal (0 = 4) */
     uint32_t trav_vote8;          /* triangle step when vote8/8 of the busy lanes have triangles (0 = 4) */
     uint32_t refill_min;          /* traversal lanes refilled once this many are idle (0 = 8) */
-    uint32_t reserved[4];
+    uint32_t shade_order;         /* S2_SHADE_ORDER_MATERIAL (0, default): counting-sort the path queue by
+                                     hit material before shading; S2_SHADE_ORDER_QUEUE (1): shade in queue
+                                     order.  Images are bit-identical either way. */
+    uint32_t reserved[3];
 } S2Tuning;
 
 int  s2_set_tuning(S2Context* ctx, const S2Tuning* tuning);
 int  s2_get_tuning(S2Context* ctx, S2Tuning* tuning);
-/* Coordinate search over wave size, triangle batch, vote and refill threshold: every candidate
+/* Coordinate search over wave size, triangle batch, vote, refill threshold and shading order: every candidate
  * renders `params` (its spp; frame seeds advance per trial) and the highest ray throughput wins.
  * The result is applied to `ctx` and written to `out` (may be NULL); `trials_out` (may be NULL)
  * receives the number of timed renders. */

@@ -1,6 +1,6 @@
 """Autotuner front end: runs s2_autotune (a coordinate search over the wavefront renderer's wave
 size, traversal triangle batch, triangle-step vote and lane-refill threshold, timed on the caller's
-own scene, view and render parameters) and keeps the results in a JSON file keyed by GPU and
+own scene, view and render parameters; and whether to shade in material-sorted or queue order) and keeps the results in a JSON file keyed by GPU and
 workload, so later runs of the same workload apply them without searching."""
 from __future__ import annotations
 
@@ -10,7 +10,7 @@ from pathlib import Path
 
 from . import _abi
 
-FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min")
+FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min", "shade_order")
 
 
 def default_path() -> Path:

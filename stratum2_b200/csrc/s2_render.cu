@@ -39,6 +39,12 @@ struct RenderState {
     } grid[2];
     uint32_t grid_cur = 0;
     bool grid_prev_valid = false;
+    // material-key sort buffers (S2Tuning::shade_order)
+    std::vector<DevBuf> sort_bufs;
+    uint32_t* sort_keys = nullptr;
+    uint32_t* sort_perm = nullptr;
+    uint32_t* sort_hist = nullptr;
+    uint32_t sort_cap = 0;
     // radiance cache queues: terminal-vertex queries and training vertices
     std::vector<DevBuf> cache_bufs;
     float4 *cq_pos = nullptr, *cq_thr = nullptr, *tr_pos = nullptr, *tr_thr = nullptr, *tr_rad = nullptr;
@@ -53,6 +59,7 @@ void destroy_render_state(S2Context* ctx) {
     for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
     for (auto& g : ctx->render->grid) free_bufs(g.bufs);
     free_bufs(ctx->render->cache_bufs);
+    free_bufs(ctx->render->sort_bufs);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -122,6 +129,27 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
         cudaMemsetAsync(st->accum, 0, sizeof(float4) * capacity, ctx->stream);
         st->capacity = capacity;
     }
+    return S2_OK;
+}
+
+// Counting sort of the live queue by material key into P.sort_perm (histogram, scan, scatter).
+void launch_sort(const PTParams& P, uint32_t parity, uint32_t blocks, cudaStream_t s) {
+    cudaMemsetAsync(P.sort_hist, 0, sizeof(uint32_t) * kSortBuckets, s);
+    k_sort_hist<<<blocks, 256, 0, s>>>(P, parity);
+    k_sort_scan<<<1, 1024, 0, s>>>(P);
+    k_sort_scatter<<<blocks, 256, 0, s>>>(P, parity);
+}
+
+// Material-sort buffers for `cap` paths.
+int ensure_sort(S2Context* ctx, RenderState* st, uint32_t cap) {
+    if (st->sort_cap >= cap) return S2_OK;
+    free_bufs(st->sort_bufs);
+    st->sort_cap = 0;
+    st->sort_keys = alloc<uint32_t>(ctx, st->sort_bufs, cap);
+    st->sort_perm = alloc<uint32_t>(ctx, st->sort_bufs, cap);
+    st->sort_hist = alloc<uint32_t>(ctx, st->sort_bufs, kSortBuckets);
+    if (!st->sort_keys || !st->sort_perm || !st->sort_hist) { free_bufs(st->sort_bufs); return S2_ERR_OOM; }
+    st->sort_cap = cap;
     return S2_OK;
 }
 
@@ -237,6 +265,12 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;
     P.trav.vote8 = ctx->tuning.trav_vote8;
     P.refill_min = ctx->tuning.refill_min;
+    const bool sort = ctx->tuning.shade_order == S2_SHADE_ORDER_MATERIAL;
+    if (sort) {
+        rc = ensure_sort(ctx, st, capacity);
+        if (rc != S2_OK) return set_error(ctx, rc, "material-sort buffer allocation failed");
+        P.sort_on = 1; P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
+    }
     P.q[0] = st->q[0]; P.q[1] = st->q[1];
     P.hits = st->hits; P.sh_o = st->sh_o; P.sh_d = st->sh_d; P.sh_c = st->sh_c;
     P.accum = st->accum;
@@ -324,6 +358,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             ev_end();
+            if (sort) { launch_sort(P, parity, st->shade_blocks, s); launches += 3; }
             ev_begin(1);
             if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
             else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
@@ -586,6 +621,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;
     P.trav.vote8 = ctx->tuning.trav_vote8;
     P.refill_min = ctx->tuning.refill_min;
+    const bool sort = ctx->tuning.shade_order == S2_SHADE_ORDER_MATERIAL;
     P.exposure = prm->exposure;
     P.q[0] = B->q[0]; P.q[1] = B->q[1];
     P.hits = B->hits; P.sh_o = B->sh_o; P.sh_d = B->sh_d; P.sh_c = B->sh_c;
@@ -606,14 +642,21 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         if (rc != S2_OK) return rc;
         st = ctx->render;
     }
+    if (sort) {
+        const int rc = ensure_sort(ctx, st, capacity);
+        if (rc != S2_OK) return set_error(ctx, rc, "material-sort buffer allocation failed");
+        P.sort_on = 1; P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
+    }
     const bool lam = (prm->flags & S2_FLAG_LAMBERTIAN) != 0, restir = (prm->flags & S2_FLAG_RESTIR_DI) != 0;
     const bool count = (prm->flags & S2_FLAG_COUNT_FETCHES) != 0;
-    // one graph = two iterations (parity 0 and 1) of setup, regeneration, extend, shade, occlude
+    // one graph = two iterations (parity 0 and 1) of setup, regeneration, extend, [material sort,]
+    // shade, occlude
     auto iteration = [&](uint32_t parity, int first) {
         k_stream_setup<<<1, 32, 0, s>>>(P, parity, first);
         k_regen<<<std::min<uint32_t>((capacity + 255) / 256, 148u * 16u), 256, 0, s>>>(P, parity);
         if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
         else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+        if (sort) launch_sort(P, parity, st->shade_blocks, s);
         if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
         else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
         if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
@@ -630,7 +673,8 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     rc = check_cuda(ctx, cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
     if (rc == S2_OK) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
     if (rc != S2_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
-    uint64_t launches = 5;
+    const uint64_t per_iter = sort ? 8 : 5;
+    uint64_t launches = per_iter;
     // replay until the device reports every path finished; the check trails one group behind so
     // the host never waits on the group it just queued
     const uint64_t lower = (paths + capacity - 1) / capacity;
@@ -641,7 +685,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     cudaEventCreateWithFlags(&pending, cudaEventDisableTiming);
     bool done = false, have_pending = false;
     while (!done && iters < cap_iters + 2) {
-        for (uint32_t g = 0; g < group; ++g) { cudaGraphLaunch(exec, s); iters += 2; launches += 10; }
+        for (uint32_t g = 0; g < group; ++g) { cudaGraphLaunch(exec, s); iters += 2; launches += 2 * per_iter; }
         if (have_pending) {
             cudaEventSynchronize(pending);
             done = *B->done_host != 0;
@@ -709,9 +753,10 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
 extern "C" int s2_set_tuning(S2Context* ctx, const S2Tuning* t) {
     if (!ctx) return S2_ERR_INVALID;
     if (!t) { std::memset(&ctx->tuning, 0, sizeof(ctx->tuning)); return S2_OK; }
-    if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024))
+    if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024) ||
+        t->shade_order > S2_SHADE_ORDER_QUEUE)
         return set_error(ctx, S2_ERR_INVALID, "tuning out of range (tris_per_step <= 32, vote8 <= 9, refill_min <= 32, "
-                                              "wave_paths 0 or >= 1024)");
+                                              "wave_paths 0 or >= 1024, shade_order 0 or 1)");
     ctx->tuning = *t;
     return S2_OK;
 }
@@ -755,14 +800,15 @@ extern "C" int s2_autotune(S2Context* ctx, const S2View* view, const S2RenderPar
     const uint32_t tris[] = {1, 2, 4, 8};
     const uint32_t votes[] = {2, 3, 4, 5, 6};
     const uint32_t refills[] = {4, 8, 12, 16};
+    const uint32_t sorts[] = {S2_SHADE_ORDER_MATERIAL, S2_SHADE_ORDER_QUEUE};
     for (int pass = 0; pass < 2; ++pass) {
-        for (int knob = 0; knob < 4; ++knob) {
-            const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : refills;
-            const int nv = knob == 0 ? 5 : knob == 1 ? 4 : knob == 2 ? 5 : 4;
+        for (int knob = 0; knob < 5; ++knob) {
+            const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : knob == 3 ? refills : sorts;
+            const int nv = knob == 0 ? 5 : knob == 1 ? 4 : knob == 2 ? 5 : knob == 3 ? 4 : 2;
             for (int v = 0; v < nv; ++v) {
                 S2Tuning t = best;
                 uint32_t* field = knob == 0 ? &t.wave_paths : knob == 1 ? &t.trav_tris_per_step
-                                : knob == 2 ? &t.trav_vote8 : &t.refill_min;
+                                : knob == 2 ? &t.trav_vote8 : knob == 3 ? &t.refill_min : &t.shade_order;
                 if (*field == vals[v]) continue;
                 *field = vals[v];
                 ctx->tuning = t;

@@ -223,9 +223,10 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
         so.valid = false;
         uint32_t slot = 0;
         if (i < count) {
-            const float4 a = qi.s0[i], b = qi.s1[i], c = qi.s2[i];
-            const uint4 rs = qi.s3[i];
-            const float4 h = P.hits[i];
+            const uint32_t pi = P.sort_on ? P.sort_perm[i] : i;  // material-sorted order
+            const float4 a = qi.s0[pi], b = qi.s1[pi], c = qi.s2[pi];
+            const uint4 rs = qi.s3[pi];
+            const float4 h = P.hits[pi];
             float3 org = f3(a.x, a.y, a.z);
             float dir_pdf = a.w;
             const float3 dir = f3(b.x, b.y, b.z);

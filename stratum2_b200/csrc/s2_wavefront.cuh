@@ -100,7 +100,15 @@ struct PTParams {
     // traversal tuning (s2_autotune / s2_set_tuning; 0 = default)
     TravTuning trav;
     uint32_t refill_min;  // refill a warp's idle lanes once this many are idle
+    // material-key sorting before shading (S2Tuning::shade_order): k_extend writes a key per
+    // path (hit material, misses last), a counting sort builds sort_perm, k_shade reads through it
+    uint32_t sort_on;
+    uint32_t* sort_keys;
+    uint32_t* sort_perm;
+    uint32_t* sort_hist;   // kSortBuckets counters / offsets
 };
+
+constexpr uint32_t kSortBuckets = 4096;  // k_sort_scan: 1024 threads x 4 buckets
 
 // fixed-point scale of the batched accumulators: integer sums are independent of the order of the
 // (atomic) additions, so batched renders are deterministic
@@ -346,6 +354,8 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
                                            tri_step, P.trav.tris_per_step, SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
                 if (!st.ok) atomicOr(P.status, 1);
                 P.hits[ray] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
+                if (P.sort_on)  // key: the instance's material word (material address | instance type), misses last
+                    P.sort_keys[ray] = h.tri == 0xffffffffu ? kSortBuckets - 1u : P.scene.instances[h.instance].x % (kSortBuckets - 1u);
                 ray = kNoRay;
             }
         }
@@ -430,6 +440,59 @@ __global__ void k_cache_targets(PTParams P) {
         const float ty = t.y > 1e-8f ? (fin.y - r0.y) / t.y : 0.f;
         const float tz = t.z > 1e-8f ? (fin.z - r0.z) / t.z : 0.f;
         P.tr_rad[i] = make_float4(fmaxf(tx, 0.f), fmaxf(ty, 0.f), fmaxf(tz, 0.f), 0.f);
+    }
+}
+}  // namespace s2
+
+namespace s2 {
+// ---------------------------------------------------------------- material-key counting sort
+// Histogram of the live queue's keys (per-block shared histogram, then global).
+__global__ void __launch_bounds__(256) k_sort_hist(PTParams P, uint32_t parity) {
+    __shared__ uint32_t h[kSortBuckets];
+    for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const uint32_t n = P.counters[parity];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&h[P.sort_keys[i]], 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x)
+        if (h[b]) atomicAdd(&P.sort_hist[b], h[b]);
+}
+
+// Exclusive scan of the histogram in place (one block of 1024 threads, four buckets each).
+__global__ void __launch_bounds__(1024) k_sort_scan(PTParams P) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x;
+    uint32_t v[4], sum = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { v[k] = P.sort_hist[4 * t + k]; sum += v[k]; }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        const uint32_t x = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += x;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { P.sort_hist[4 * t + k] = run; run += v[k]; }
+}
+
+// Scatter: sort_perm[offset[key] + rank] = i, ranks taken per warp group of equal keys.
+__global__ void __launch_bounds__(256) k_sort_scatter(PTParams P, uint32_t parity) {
+    const uint32_t n = P.counters[parity];
+    const uint32_t rounded = (n + 31u) & ~31u;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
+        const bool live = i < n;
+        const uint32_t key = live ? P.sort_keys[i] : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (live && lane == leader) base = atomicAdd(&P.sort_hist[key], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (live) P.sort_perm[base + __popc(peers & ((1u << lane) - 1u))] = i;
     }
 }
 }  // namespace s2
