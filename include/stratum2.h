@@ -284,6 +284,8 @@ int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams*
  * as JSON keyed by GPU and workload). */
 #define S2_SHADE_ORDER_MATERIAL 0u
 #define S2_SHADE_ORDER_QUEUE 1u
+#define S2_TRACE_ORDER_QUEUE 0u
+#define S2_TRACE_ORDER_COHERENT 1u
 
 typedef struct S2Tuning {
     uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^25) */
@@ -293,7 +295,10 @@ typedef struct S2Tuning {
     uint32_t shade_order;         /* S2_SHADE_ORDER_MATERIAL (0, default): counting-sort the path queue by
                                      hit material before shading; S2_SHADE_ORDER_QUEUE (1): shade in queue
                                      order.  Images are bit-identical either way. */
-    uint32_t reserved[3];
+    uint32_t trace_order;         /* S2_TRACE_ORDER_QUEUE (0, default): trace continuation rays in queue
+                                     order; S2_TRACE_ORDER_COHERENT (1): counting-sort them by origin cell
+                                     and direction octant first.  Images are bit-identical either way. */
+    uint32_t reserved[2];
 } S2Tuning;
 
 int  s2_set_tuning(S2Context* ctx, const S2Tuning* tuning);

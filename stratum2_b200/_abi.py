@@ -44,6 +44,8 @@ FLAG_NORMAL_MAPS_OFF = 1 << 13
 FLAG_RADIANCE_CACHE = 1 << 14
 SHADE_ORDER_MATERIAL = 0
 SHADE_ORDER_QUEUE = 1
+TRACE_ORDER_QUEUE = 0
+TRACE_ORDER_COHERENT = 1
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -139,7 +141,8 @@ class S2CacheParams(C.Structure):
 
 class S2Tuning(C.Structure):
     _fields_ = [("wave_paths", C.c_uint32), ("trav_tris_per_step", C.c_uint32), ("trav_vote8", C.c_uint32),
-                ("refill_min", C.c_uint32), ("shade_order", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("refill_min", C.c_uint32), ("shade_order", C.c_uint32), ("trace_order", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class S2RenderStats(C.Structure):

@@ -10,7 +10,7 @@ from pathlib import Path
 
 from . import _abi
 
-FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min", "shade_order")
+FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min", "shade_order", "trace_order")
 
 
 def default_path() -> Path:

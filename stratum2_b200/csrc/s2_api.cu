@@ -506,6 +506,14 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
     ctx->scene.tris = (const float4*)upload(ctx, ctx->bvh_bufs, out.tris.data(), out.tris.size());
     ctx->scene.tri_count = (uint32_t)out.tris.size();
     if (!ctx->scene.nodes || !ctx->scene.tris) return S2_ERR_OOM;
+    ctx->scene.key_lo = ctx->scene.key_scale = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!out.nodes.empty()) {  // root box: p + [0, 256) * 2^(e-127) per axis
+        const S2BvhNode& root = out.nodes[0];
+        const float sc[3] = {std::ldexp(256.f, (int)root.e[0] - 127), std::ldexp(256.f, (int)root.e[1] - 127),
+                             std::ldexp(256.f, (int)root.e[2] - 127)};
+        ctx->scene.key_lo = make_float4(root.p[0], root.p[1], root.p[2], 0.f);
+        ctx->scene.key_scale = make_float4(8.f / sc[0], 8.f / sc[1], 8.f / sc[2], 0.f);
+    }
     S2_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "BVH upload"));
     if (stats) {
         stats->node_count = out.nodes.size();

@@ -266,10 +266,12 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     P.trav.vote8 = ctx->tuning.trav_vote8;
     P.refill_min = ctx->tuning.refill_min;
     const bool sort = ctx->tuning.shade_order == S2_SHADE_ORDER_MATERIAL;
-    if (sort) {
+    const bool ray_sort = ctx->tuning.trace_order == S2_TRACE_ORDER_COHERENT;
+    if (sort || ray_sort) {
         rc = ensure_sort(ctx, st, capacity);
-        if (rc != S2_OK) return set_error(ctx, rc, "material-sort buffer allocation failed");
-        P.sort_on = 1; P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
+        if (rc != S2_OK) return set_error(ctx, rc, "sort buffer allocation failed");
+        P.sort_on = sort; P.ray_sort_on = ray_sort;
+        P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
     }
     P.q[0] = st->q[0]; P.q[1] = st->q[1];
     P.hits = st->hits; P.sh_o = st->sh_o; P.sh_d = st->sh_d; P.sh_c = st->sh_c;
@@ -354,6 +356,8 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         for (uint32_t b = 0; b < prm->max_path_length; ++b) {
             const uint32_t parity = b & 1u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
+            P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
+            if (P.ray_sorted) { launch_sort(P, parity, st->shade_blocks, s); launches += 3; }
             ev_begin(0);
             if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
@@ -754,9 +758,9 @@ extern "C" int s2_set_tuning(S2Context* ctx, const S2Tuning* t) {
     if (!ctx) return S2_ERR_INVALID;
     if (!t) { std::memset(&ctx->tuning, 0, sizeof(ctx->tuning)); return S2_OK; }
     if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024) ||
-        t->shade_order > S2_SHADE_ORDER_QUEUE)
+        t->shade_order > S2_SHADE_ORDER_QUEUE || t->trace_order > S2_TRACE_ORDER_COHERENT)
         return set_error(ctx, S2_ERR_INVALID, "tuning out of range (tris_per_step <= 32, vote8 <= 9, refill_min <= 32, "
-                                              "wave_paths 0 or >= 1024, shade_order 0 or 1)");
+                                              "wave_paths 0 or >= 1024, shade_order and trace_order 0 or 1)");
     ctx->tuning = *t;
     return S2_OK;
 }
@@ -801,14 +805,16 @@ extern "C" int s2_autotune(S2Context* ctx, const S2View* view, const S2RenderPar
     const uint32_t votes[] = {2, 3, 4, 5, 6};
     const uint32_t refills[] = {4, 8, 12, 16};
     const uint32_t sorts[] = {S2_SHADE_ORDER_MATERIAL, S2_SHADE_ORDER_QUEUE};
+    const uint32_t traces[] = {S2_TRACE_ORDER_QUEUE, S2_TRACE_ORDER_COHERENT};
     for (int pass = 0; pass < 2; ++pass) {
-        for (int knob = 0; knob < 5; ++knob) {
-            const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : knob == 3 ? refills : sorts;
+        for (int knob = 0; knob < 6; ++knob) {
+            const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : knob == 3 ? refills
+                                 : knob == 4 ? sorts : traces;
             const int nv = knob == 0 ? 5 : knob == 1 ? 4 : knob == 2 ? 5 : knob == 3 ? 4 : 2;
             for (int v = 0; v < nv; ++v) {
                 S2Tuning t = best;
                 uint32_t* field = knob == 0 ? &t.wave_paths : knob == 1 ? &t.trav_tris_per_step
-                                : knob == 2 ? &t.trav_vote8 : knob == 3 ? &t.refill_min : &t.shade_order;
+                                : knob == 2 ? &t.trav_vote8 : knob == 3 ? &t.refill_min : knob == 4 ? &t.shade_order : &t.trace_order;
                 if (*field == vals[v]) continue;
                 *field = vals[v];
                 ctx->tuning = t;

@@ -55,7 +55,21 @@ struct DevScene {
     const DevImage* images;
     uint32_t image_count;
     float4 scene_sphere;
+    // ray-coherence keys: the BVH root box as origin and 8 / extent per axis (zero: no BVH)
+    float4 key_lo, key_scale;
 };
+
+// Ray-coherence key: Morton code of the origin's cell in an 8^3 grid over the BVH root box
+// (9 bits) above the direction octant (3 bits), 12 bits in all.
+S2D uint32_t ray_key(const DevScene& s, float3 o, float3 d) {
+    const int cx = min(max((int)((o.x - s.key_lo.x) * s.key_scale.x), 0), 7);
+    const int cy = min(max((int)((o.y - s.key_lo.y) * s.key_scale.y), 0), 7);
+    const int cz = min(max((int)((o.z - s.key_lo.z) * s.key_scale.z), 0), 7);
+    uint32_t m = 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) m |= (((cx >> b) & 1) << (3 * b + 2)) | (((cy >> b) & 1) << (3 * b + 1)) | (((cz >> b) & 1) << (3 * b));
+    return (m << 3) | (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+}
 
 // ---- transforms (TransformData: row-major 3x4)
 S2D float3 xform_point(const float4* m, float3 p) {

@@ -367,7 +367,10 @@ __global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
             shadow = so.valid;
         }
         const uint32_t qi_out = warp_append(&P.counters[1 - parity], alive);
-        if (alive) { qo.s0[qi_out] = n0; qo.s1[qi_out] = n1; qo.s2[qi_out] = n2; qo.s3[qi_out] = n3; }
+        if (alive) {
+            qo.s0[qi_out] = n0; qo.s1[qi_out] = n1; qo.s2[qi_out] = n2; qo.s3[qi_out] = n3;
+            if (P.ray_sort_on) P.sort_keys[qi_out] = ray_key(s, f3(n0.x, n0.y, n0.z), f3(n1.x, n1.y, n1.z));
+        }
         const uint32_t si = warp_append(&P.counters[C_SHADOW], shadow);
         if (shadow) {
             P.sh_o[si] = make_float4(so.o.x, so.o.y, so.o.z, so.tmax);

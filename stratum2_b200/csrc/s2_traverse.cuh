@@ -95,6 +95,21 @@ struct TravCounters { uint32_t nodes, tris; };
 
 S2D uint32_t extract_byte(uint32_t w, uint32_t i) { return (w >> (8 * i)) & 0xffu; }
 
+// Byte i of w as a float.  The node test spreads the 48 conversions of a node over two pipes:
+// x planes by integer-to-float conversion, y and z planes through the mantissa (2^23 + b is
+// exact, and so is the subtraction), measured 2.4 % faster on B200 than converting all six.
+S2D float byte_f_prmt(uint32_t w, uint32_t i) {
+    return __uint_as_float(__byte_perm(w, 0x4Bu, i | 0x4550u)) - 8388608.f;
+}
+S2D float byte_f_cvt(uint32_t w, uint32_t i) { return (float)extract_byte(w, i); }
+// three-input min / max (sm_100)
+S2D float max3f(float a, float b, float c) {
+    float d; asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c)); return d;
+}
+S2D float min3f(float a, float b, float c) {
+    float d; asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c)); return d;
+}
+
 // Intersect the 8 children of `node` with [tmin, tmax].  Returns the hit mask in bit-position
 // space (bit b = slot b ^ oct) for internal children, and the triangle mask for leaf slots.
 S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint32_t node_idx, float tmax,
@@ -125,20 +140,20 @@ S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint
     const uint32_t xn0 = nx ? xhi0 : xlo0, xn1 = nx ? xhi1 : xlo1, xf0 = nx ? xlo0 : xhi0, xf1 = nx ? xlo1 : xhi1;
     const uint32_t yn0 = ny ? yhi0 : ylo0, yn1 = ny ? yhi1 : ylo1, yf0 = ny ? ylo0 : yhi0, yf1 = ny ? ylo1 : yhi1;
     const uint32_t zn0 = nz ? zhi0 : zlo0, zn1 = nz ? zhi1 : zlo1, zf0 = nz ? zlo0 : zhi0, zf1 = nz ? zlo1 : zhi1;
-    const float tfar_lim = tmax * 1.0000004f;
     hits = 0; trimask = 0;
 #pragma unroll
     for (uint32_t s = 0; s < 8; ++s) {
         const uint32_t w = s < 4 ? 0 : 1, i = s & 3;
-        const float qnx = (float)extract_byte(w ? xn1 : xn0, i), qfx = (float)extract_byte(w ? xf1 : xf0, i);
-        const float qny = (float)extract_byte(w ? yn1 : yn0, i), qfy = (float)extract_byte(w ? yf1 : yf0, i);
-        const float qnz = (float)extract_byte(w ? zn1 : zn0, i), qfz = (float)extract_byte(w ? zf1 : zf0, i);
+        const float qnx = byte_f_cvt(w ? xn1 : xn0, i), qfx = byte_f_cvt(w ? xf1 : xf0, i);
+        const float qny = byte_f_prmt(w ? yn1 : yn0, i), qfy = byte_f_prmt(w ? yf1 : yf0, i);
+        const float qnz = byte_f_prmt(w ? zn1 : zn0, i), qfz = byte_f_prmt(w ? zf1 : zf0, i);
         const float tnx = fmaf(qnx, sx, ax), tfx = fmaf(qfx, sx, ax);
         const float tny = fmaf(qny, sy, ay), tfy = fmaf(qfy, sy, ay);
         const float tnz = fmaf(qnz, sz, az), tfz = fmaf(qfz, sz, az);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
-        const float tf = fminf(fminf(tfx, tfy), tfz) * 1.0000004f;
-        if (tn <= fminf(tf, tfar_lim)) {
+        // min(tf, tmax) * c == min(tf * c, tmax * c): the padding also covers tmax
+        const float tn = max3f(tnx, tny, fmaxf(tnz, r.tmin));
+        const float tf = min3f(tfx, tfy, fminf(tfz, tmax)) * 1.0000004f;
+        if (tn <= tf) {
             if ((imask >> s) & 1u) {
                 hits |= 1u << (s ^ r.oct);
             } else {

@@ -103,6 +103,10 @@ struct PTParams {
     // material-key sorting before shading (S2Tuning::shade_order): k_extend writes a key per
     // path (hit material, misses last), a counting sort builds sort_perm, k_shade reads through it
     uint32_t sort_on;
+    // ray-coherence sorting before traversal (S2Tuning::trace_order): k_shade writes ray_key() of
+    // each continuation ray (ray_sort_on), a counting sort builds sort_perm, and k_extend takes its
+    // rays through it (ray_sorted, set per launch)
+    uint32_t ray_sort_on, ray_sorted;
     uint32_t* sort_keys;
     uint32_t* sort_perm;
     uint32_t* sort_hist;   // kSortBuckets counters / offsets
@@ -143,6 +147,7 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_CACHE (1u << 14)
 
 constexpr int kTravBlock = 128;
+
 
 // ---------------------------------------------------------------- camera rays
 // InitializeCameraPath (testrenderer.slang:938-957): ViewData::toWorld (compat/scene.h:152-157)
@@ -344,6 +349,7 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
         ray = refill(&P.counters[C_WORK_EXT], count, ray, exhausted, P.refill_min);
         if (!__any_sync(0xffffffffu, ray != kNoRay)) break;
         if (ray != kNoRay && prev == kNoRay) {
+            if (P.ray_sorted) ray = P.sort_perm[ray];  // coherence order; results stay per queue slot
             const float4 a = q.s0[ray], b = q.s1[ray];
             r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
             trav_begin(st, h, S2_INF);

@@ -42,11 +42,11 @@ def test_autotune_applies_a_tuning_that_keeps_the_image(device, tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("flags", [_abi.FLAG_LAMBERTIAN, 0, _abi.FLAG_RESTIR_DI])
-def test_material_sort_keeps_the_image_bitwise(device, flags):
-    """Sorting paths by material before shading only reorders the queue: each path keeps its own
-    random state and accumulator slot, so the image is bit-identical in material-sorted (default)
-    and queue order, also across several waves (wave_paths below the path count) and in the
-    batched streaming entry point."""
+def test_queue_orders_keep_the_image_bitwise(device, flags):
+    """Sorting paths by material before shading, and continuation rays by origin cell and octant
+    before tracing, only reorders the queue: each path keeps its own random state and accumulator
+    slot, so the image is bit-identical in every order, also across several waves (wave_paths
+    below the path count) and in the batched streaming entry point."""
     from stratum2_b200.scenegen import textured_box_scene
     wl = textured_box_scene(seed=4, width=48, height=48, spheres=3)
     device.upload_scene(wl.scene)
@@ -58,11 +58,12 @@ def test_material_sort_keeps_the_image_bitwise(device, flags):
     device.set_tuning(queue)
     ref = device.render(wl.view, 48, 48, params=p).radiance
     for wave in (0, 4096):
-        t = _abi.S2Tuning()
-        t.wave_paths = wave
-        device.set_tuning(t)
-        out = device.render(wl.view, 48, 48, params=p).radiance
-        np.testing.assert_array_equal(out, ref)
+        for trace in (_abi.TRACE_ORDER_QUEUE, _abi.TRACE_ORDER_COHERENT):
+            t = _abi.S2Tuning()
+            t.wave_paths, t.trace_order = wave, trace
+            device.set_tuning(t)
+            out = device.render(wl.view, 48, 48, params=p).radiance
+            np.testing.assert_array_equal(out, ref)
     # batched streaming: fixed-point accumulation, so also independent of the shading order
     device.set_tuning(queue)
     a, _ = device.render_views([wl.view], p)
