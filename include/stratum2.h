@@ -181,7 +181,7 @@ typedef struct S2RenderParams {
     float environment_sample_probability; /* default 0.9 (TestRenderer.cpp:41) */
     uint32_t restir_candidates;      /* mCandidateSamples (default 32) */
     float restir_max_m;              /* mMaxM (default 3) */
-    uint32_t wave_paths;             /* paths in flight per wave / queue (0 = 2^25) */
+    uint32_t wave_paths;             /* paths in flight per wave / queue (0 = 2^26) */
     uint32_t restir_grid_cells;      /* hash-grid cell count (0 = 100000, TestRenderer.cpp:52) */
     float restir_grid_cell_size;     /* minimum cell size (0 = 0.5, TestRenderer.cpp:52) */
     float restir_grid_pixel_radius;  /* mCellPixelRadius: 0 = constant cell size */
@@ -231,6 +231,10 @@ int  s2_set_stream(S2Context* ctx, void* stream);
 int  s2_scene_upload(S2Context* ctx, const S2SceneDesc* scene);
 /* Builds the BVH8 over all mesh instances (flattened to world space). */
 int  s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStats* stats_out);
+/* Copies the built BVH8 to host memory: `nodes` receives counts_out[0] 128-byte nodes and `tris`
+ * counts_out[1] 48-byte triangle records (layouts: stratum2_b200/csrc/s2_bvh.h).  Either pointer
+ * may be NULL (call once with both NULL to size the buffers). */
+int  s2_get_bvh(S2Context* ctx, void* nodes, void* tris, uint64_t* counts_out);
 
 /* ---- queries (replace traceRay / traceVisibilityRay) ------------------------------------- */
 /* rays/hits are DEVICE pointers when on_device != 0, else host pointers.
@@ -288,7 +292,7 @@ int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams*
 #define S2_TRACE_ORDER_COHERENT 1u
 
 typedef struct S2Tuning {
-    uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^25) */
+    uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^26) */
     uint32_t trav_tris_per_step;  /* triangle tests per triangle step of the traversal (0 = 4) */
     uint32_t trav_vote8;          /* triangle step when vote8/8 of the busy lanes have triangles (0 = 4) */
     uint32_t refill_min;          /* traversal lanes refilled once this many are idle (0 = 8) */

@@ -580,3 +580,125 @@ template <class R> Hit<R> trace(const Scene<R>& s, const V3<R>& o, const V3<R>& 
 }  // namespace orc
 
 #include "oracle_pt.inl"
+
+// ============================================================================ BVH8 reference walker
+// Sequential nearest-first walk of the library's compressed BVH8 (node and triangle-record layouts
+// of stratum2_b200/csrc/s2_bvh.h, downloaded with s2_get_bvh), counting node and triangle fetches.
+// It restates, in plain C++ on the CPU, the traversal order of the library's counted query
+// (trav_step: visit a node, test its leaf triangles, descend into the nearest hit child, keep the
+// others as one stack group of hit bits): the FP32 slab test of the 8-bit planes with the
+// 1.0000004 far-plane padding, the watertight triangle test (isect_tri<float>), closest-hit ties
+// to the lowest (instance, primitive).  No alpha test: for scenes without alpha-tested triangles.
+// The fetch counts it returns are the algorithmic work of one closest-hit query on this BVH8.
+namespace orc {
+namespace bvh8 {
+
+struct Group { uint32_t base, bits; };  // child_base, imask | (remaining hit bits << 8)
+
+inline float safe_inv(float d) {
+    const float dd = std::fabs(d) < 1e-30f ? std::copysign(1e-30f, d) : d;
+    return 1.f / dd;
+}
+inline float exp2_byte(uint32_t e) { uint32_t b = e << 23; float f; std::memcpy(&f, &b, 4); return f; }
+inline float word_f(const uint8_t* p) { float f; std::memcpy(&f, p, 4); return f; }
+inline uint32_t word_u(const uint8_t* p) { uint32_t u; std::memcpy(&u, p, 4); return u; }
+
+struct Walk {
+    float t, b1, b2;
+    uint32_t tri, inst, prim;
+    uint32_t nodes, tris;
+};
+
+Walk walk(const uint8_t* nodes, const float* tris, const float* ray, bool anyhit) {
+    const V3<float> o(ray[0], ray[1], ray[2]), d(ray[4], ray[5], ray[6]);
+    const float tmin = ray[3], tmax = ray[7];
+    const WRay<float> r = make_wray(o, d, tmin);
+    const float inv[3] = {safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+    const uint32_t oct = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    Walk w{tmax, 0.f, 0.f, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0, 0};
+    std::vector<Group> stack;
+    uint32_t node = 0;
+    while (true) {
+        const uint8_t* n = nodes + 128 * (size_t)node;
+        w.nodes++;
+        const float p[3] = {word_f(n), word_f(n + 4), word_f(n + 8)};
+        const uint32_t imask = n[15], child_base = word_u(n + 16), tri_base = word_u(n + 20);
+        const uint8_t* meta = n + 24;
+        const uint8_t* qlo = n + 32;   // [axis][slot]
+        const uint8_t* qhi = n + 56;
+        float sc[3], a[3];
+        for (int k = 0; k < 3; ++k) { sc[k] = exp2_byte(n[12 + k]) * inv[k]; a[k] = (p[k] - o[k]) * inv[k]; }
+        uint32_t hits = 0, trimask = 0;
+        for (uint32_t s = 0; s < 8; ++s) {
+            float tn[3], tf[3];
+            for (int k = 0; k < 3; ++k) {
+                const bool neg = inv[k] < 0;
+                const float qn = (float)(neg ? qhi[8 * k + s] : qlo[8 * k + s]);
+                const float qf = (float)(neg ? qlo[8 * k + s] : qhi[8 * k + s]);
+                tn[k] = std::fma(qn, sc[k], a[k]);
+                tf[k] = std::fma(qf, sc[k], a[k]);
+            }
+            const float lo = std::fmax(std::fmax(tn[0], tn[1]), std::fmax(tn[2], tmin));
+            const float hi = std::fmin(std::fmin(tf[0], tf[1]), std::fmin(tf[2], w.t)) * 1.0000004f;
+            if (lo <= hi) {
+                if ((imask >> s) & 1u) hits |= 1u << (s ^ oct);
+                else trimask |= ((1u << (meta[s] >> 5)) - 1u) << (meta[s] & 31u);
+            }
+        }
+        for (uint32_t k = 0; k < 32; ++k) {
+            if (!((trimask >> k) & 1u)) continue;
+            const uint32_t ti = tri_base + k;
+            const float* tr = tris + 12 * (size_t)ti;
+            const float v[9] = {tr[0], tr[1], tr[2], tr[4], tr[5], tr[6], tr[8], tr[9], tr[10]};
+            uint32_t inst, prim;
+            std::memcpy(&inst, tr + 3, 4);
+            std::memcpy(&prim, tr + 7, 4);
+            w.tris++;
+            float t, b1, b2;
+            if (!isect_tri(r, v, w.t, t, b1, b2)) continue;
+            if (anyhit) { w.t = t; w.b1 = b1; w.b2 = b2; w.tri = ti; w.inst = inst; w.prim = prim; return w; }
+            if (t < w.t || inst < w.inst || (inst == w.inst && prim < w.prim)) {
+                w.t = t; w.b1 = b1; w.b2 = b2; w.tri = ti; w.inst = inst; w.prim = prim;
+            }
+        }
+        auto slot_node = [&](uint32_t base, uint32_t im, uint32_t bit) {
+            const uint32_t s = bit ^ oct;
+            return base + (uint32_t)__builtin_popcount(im & ((1u << s) - 1u));
+        };
+        if (hits) {
+            const uint32_t b = (uint32_t)__builtin_ctz(hits);
+            hits &= hits - 1;
+            if (hits) stack.push_back(Group{child_base, imask | (hits << 8)});
+            node = slot_node(child_base, imask, b);
+            continue;
+        }
+        if (stack.empty()) return w;
+        Group& g = stack.back();
+        uint32_t gh = g.bits >> 8;
+        const uint32_t b = (uint32_t)__builtin_ctz(gh);
+        gh &= gh - 1;
+        node = slot_node(g.base, g.bits & 0xffu, b);
+        if (gh) g.bits = (g.bits & 0xffu) | (gh << 8);
+        else stack.pop_back();
+    }
+}
+
+}  // namespace bvh8
+}  // namespace orc
+
+// rays: n x 8 floats (origin, tmin, direction, tmax); hits: n x 5 words (S2Hit: t, instance,
+// primitive, b1, b2); counts: n x 2 (node fetches, triangle fetches).  Returns 0.
+extern "C" int oracle_bvh8_trace(const uint8_t* nodes, const float* tris, const float* rays, uint32_t n, int anyhit,
+                                 uint32_t* hits, uint32_t* counts) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        const orc::bvh8::Walk w = orc::bvh8::walk(nodes, tris, rays + 8 * i, anyhit != 0);
+        uint32_t* h = hits + 5 * i;
+        std::memcpy(&h[0], &w.t, 4);
+        h[1] = w.inst; h[2] = w.prim;
+        std::memcpy(&h[3], &w.b1, 4);
+        std::memcpy(&h[4], &w.b2, 4);
+        counts[2 * i] = w.nodes; counts[2 * i + 1] = w.tris;
+    }
+    return 0;
+}

@@ -50,7 +50,7 @@ TRACE_ORDER_COHERENT = 1
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
     "s2_get_abi_version", "s2_create", "s2_destroy", "s2_last_error", "s2_sync", "s2_set_stream",
-    "s2_scene_upload", "s2_build_bvh", "s2_trace", "s2_trace_counted", "s2_render",
+    "s2_scene_upload", "s2_build_bvh", "s2_get_bvh", "s2_trace", "s2_trace_counted", "s2_render",
     "s2_default_render_params", "s2_render_noalloc", "s2_render_views",
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
@@ -182,6 +182,7 @@ def lib() -> C.CDLL:
     L.s2_build_bvh.argtypes = [C.c_void_p, P(S2BvhParams), P(S2BvhStats)]
     L.s2_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_int]
     L.s2_trace_counted.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    L.s2_get_bvh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_render.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Aovs), C.c_int, P(S2RenderStats)]
     L.s2_render_views.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, P(S2RenderParams), C.c_void_p, C.c_int,
                                   P(S2RenderStats)]

@@ -97,6 +97,16 @@ class Device:
         self._check(self._lib.s2_trace(self._h, rays.ctypes.data, n, int(anyhit), out.ctypes.data, 0))
         return hits_from_bytes(out)
 
+    def get_bvh(self):
+        """The built BVH8 as host arrays: nodes (n, 128) uint8 and triangle records (m, 12) float32
+        (layouts in csrc/s2_bvh.h)."""
+        counts = np.zeros(2, np.uint64)
+        self._check(self._lib.s2_get_bvh(self._h, None, None, counts.ctypes.data))
+        nodes = np.zeros((int(counts[0]), 128), np.uint8)
+        tris = np.zeros((int(counts[1]), 12), np.float32)
+        self._check(self._lib.s2_get_bvh(self._h, nodes.ctypes.data, tris.ctypes.data, counts.ctypes.data))
+        return nodes, tris
+
     def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, anyhit: bool = False):
         """Same query with device pointers (e.g. torch tensors' data_ptr())."""
         self._check(self._lib.s2_trace(self._h, C.c_void_p(rays_ptr), n, int(anyhit), C.c_void_p(hits_ptr), 1))

@@ -505,6 +505,7 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
     ctx->scene.nodes = (const uint4*)upload(ctx, ctx->bvh_bufs, out.nodes.data(), out.nodes.size());
     ctx->scene.tris = (const float4*)upload(ctx, ctx->bvh_bufs, out.tris.data(), out.tris.size());
     ctx->scene.tri_count = (uint32_t)out.tris.size();
+    ctx->bvh_node_count = out.nodes.size();
     if (!ctx->scene.nodes || !ctx->scene.tris) return S2_ERR_OOM;
     ctx->scene.key_lo = ctx->scene.key_scale = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!out.nodes.empty()) {  // root box: p + [0, 256) * 2^(e-127) per axis
@@ -525,6 +526,21 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
     }
     ctx->has_bvh = true;
     return S2_OK;
+}
+
+extern "C" int s2_get_bvh(S2Context* ctx, void* nodes, void* tris, uint64_t* counts_out) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!ctx->has_bvh) return set_error(ctx, S2_ERR_NO_SCENE, "s2_get_bvh before s2_build_bvh");
+    if (!counts_out) return set_error(ctx, S2_ERR_INVALID, "counts_out is required");
+    counts_out[0] = ctx->bvh_node_count;
+    counts_out[1] = ctx->scene.tri_count;
+    cudaSetDevice(ctx->device);
+    if (nodes && ctx->bvh_node_count)
+        cudaMemcpyAsync(nodes, ctx->scene.nodes, sizeof(S2BvhNode) * ctx->bvh_node_count, cudaMemcpyDeviceToHost, ctx->stream);
+    if (tris && ctx->scene.tri_count)
+        cudaMemcpyAsync(tris, ctx->scene.tris, sizeof(S2TriRecord) * (size_t)ctx->scene.tri_count, cudaMemcpyDeviceToHost,
+                        ctx->stream);
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "BVH download");
 }
 
 // ============================================================================== ray queries

@@ -36,6 +36,7 @@ struct S2Context {
     std::vector<s2::DevBuf> scene_bufs;  // freed on re-upload / destroy
     std::vector<s2::DevBuf> bvh_bufs;
     bool has_scene = false, has_bvh = false;
+    uint64_t bvh_node_count = 0;           // 128-byte BVH8 nodes in bvh_bufs
 
     // host copies needed by the BVH build
     std::vector<float> tri_v0, tri_v1, tri_v2;

@@ -11,6 +11,10 @@
 
 namespace s2 {
 
+// Paths per wave (and batched queue capacity) when neither the call nor the tuning sets one: 2^26
+// paths hold about 14 GB of queues, hits and shadow rays.
+constexpr uint32_t kDefaultWavePaths = 1u << 26;
+
 struct RenderState {
     uint32_t capacity = 0;      // paths per wave
     uint32_t pixels = 0, width = 0, height = 0;
@@ -238,7 +242,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         return set_error(ctx, S2_ERR_INVALID, "invalid ReSTIR hash-grid parameters");
     cudaSetDevice(ctx->device);
     const uint32_t pixels = (uint32_t)W * (uint32_t)H;
-    uint64_t target = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (1u << 25));
+    uint64_t target = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : kDefaultWavePaths);
     uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, target / pixels));
     const uint32_t capacity = slots * pixels;
     int rc = ensure_state(ctx, (uint32_t)W, (uint32_t)H, capacity);
@@ -551,7 +555,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     BatchState* B = g_batch_for(ctx);
     if (!B) return set_error(ctx, S2_ERR_OOM, "batch state allocation failed");
     cudaStream_t s = ctx->stream;
-    const uint64_t wave = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (1u << 25));
+    const uint64_t wave = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : kDefaultWavePaths);
     const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(wave, paths));
     if (B->capacity < capacity) {
         free_bufs(B->qbufs);
@@ -800,7 +804,7 @@ extern "C" int s2_autotune(S2Context* ctx, const S2View* view, const S2RenderPar
     double best_rate = 0.0;
     int rc = measure(best_rate);
     if (rc != S2_OK) { ctx->tuning = saved; return rc; }
-    const uint32_t waves[] = {1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26};
+    const uint32_t waves[] = {1u << 23, 1u << 24, 1u << 25, 1u << 26, 1u << 27};
     const uint32_t tris[] = {1, 2, 4, 8};
     const uint32_t votes[] = {2, 3, 4, 5, 6};
     const uint32_t refills[] = {4, 8, 12, 16};

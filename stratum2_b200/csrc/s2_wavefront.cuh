@@ -354,10 +354,15 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
             r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
             trav_begin(st, h, S2_INF);
         }
-        const bool tri_step = trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
+        // counting runs take the sequential nearest-first walk, the order the CPU BVH8 walker
+        // restates.  The postponed-triangle order visits the same nodes: a lane tests its pending
+        // triangles before its next box test, and the next node is chosen from box tests alone.
+        const bool tri_step = COUNT ? false : trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
         if (ray != kNoRay) {
-            if (trav_step_pp<false, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
-                                           tri_step, P.trav.tris_per_step, SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
+            const SceneAlphaTest alpha{&P.scene, !(P.flags & S2F_NO_ALPHA)};
+            if (COUNT ? trav_step<false, true>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c, alpha)
+                      : trav_step_pp<false, false>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                                   tri_step, P.trav.tris_per_step, alpha)) {
                 if (!st.ok) atomicOr(P.status, 1);
                 P.hits[ray] = make_float4(h.t, __uint_as_float(h.tri), h.b1, h.b2);
                 if (P.sort_on)  // key: the instance's material word (material address | instance type), misses last
@@ -391,10 +396,12 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ 
             r = make_trav_ray(f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0.f);
             trav_begin(st, h, o.w);
         }
-        const bool tri_step = trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
+        const bool tri_step = COUNT ? false : trav_vote_tri(ray != kNoRay, st, P.trav.vote8);
         if (ray != kNoRay) {
-            if (trav_step_pp<true, COUNT>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
-                                          tri_step, P.trav.tris_per_step, SceneAlphaTest{&P.scene, !(P.flags & S2F_NO_ALPHA)})) {
+            const SceneAlphaTest alpha{&P.scene, !(P.flags & S2F_NO_ALPHA)};
+            if (COUNT ? trav_step<true, true>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c, alpha)
+                      : trav_step_pp<true, false>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
+                                                  tri_step, P.trav.tris_per_step, alpha)) {
                 if (!st.ok) atomicOr(P.status, 1);
                 if (h.tri == 0xffffffffu) {
                     const float4 cc = P.sh_c[ray];

@@ -98,3 +98,29 @@ def test_empty_and_degenerate_inputs(device):
     o = osc.trace(r, precision=32)
     np.testing.assert_array_equal(g["instance"], o["instance"])
     np.testing.assert_array_equal(g["primitive"], o["primitive"])
+
+
+def test_counted_trace_matches_cpu_bvh8_walker(device, scene_case):
+    """The counted query's per-ray node and triangle fetches (the algorithmic work behind the
+    traversal roofline) equal those of the CPU BVH8 reference walker on the downloaded BVH8, and
+    both walks return bit-identical hits."""
+    import ctypes as C
+    from oracle_lib import oracle
+    name, wl, osc, rays = scene_case
+    sub = np.ascontiguousarray(rays[::7][:40_000], np.float32)
+    nodes, tris = device.get_bvh()
+    L = oracle()
+    L.oracle_bvh8_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]
+    for anyhit in (False, True):
+        h, cnt = device.trace(sub, anyhit=anyhit, counted=True)
+        oh = np.zeros((len(sub), 5), np.uint32)
+        oc = np.zeros((len(sub), 2), np.uint32)
+        L.oracle_bvh8_trace(nodes.ctypes.data, tris.ctypes.data, sub.ctypes.data, len(sub), int(anyhit),
+                            oh.ctypes.data, oc.ctypes.data)
+        np.testing.assert_array_equal(cnt, oc)
+        np.testing.assert_array_equal(h["instance"], oh[:, 1])
+        if not anyhit:
+            np.testing.assert_array_equal(h["primitive"], oh[:, 2])
+            np.testing.assert_array_equal(h["t"].view(np.uint32), oh[:, 0])
+            np.testing.assert_array_equal(h["b1"].view(np.uint32), oh[:, 3])
+            np.testing.assert_array_equal(h["b2"].view(np.uint32), oh[:, 4])
