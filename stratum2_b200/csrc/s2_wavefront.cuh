@@ -415,16 +415,27 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------- accumulation
-// Sum the wave's per-sample slots into the per-pixel total in a fixed order and clear them.
+// Sum the wave's per-sample slots into the per-pixel total in a fixed order (sample 0 first) and
+// clear them.  Loads are issued eight samples at a time so each thread keeps eight 16-byte reads
+// in flight; the additions stay in sample order, so the sums do not depend on the batching.
 __global__ void k_reduce(PTParams P, float4* __restrict__ total) {
+    constexpr uint32_t kBatch = 8;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.pixels) return;
     float4 t = total[p];
-    for (uint32_t k = 0; k < P.wave_samples; ++k) {
-        const size_t idx = (size_t)k * P.pixels + p;
-        const float4 a = P.accum[idx];
-        t.x += a.x; t.y += a.y; t.z += a.z;
-        P.accum[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t k0 = 0; k0 < P.wave_samples; k0 += kBatch) {
+        float4 a[kBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kBatch; ++j)
+            a[j] = k0 + j < P.wave_samples ? __ldcs(P.accum + (size_t)(k0 + j) * P.pixels + p) : zero;
+#pragma unroll
+        for (uint32_t j = 0; j < kBatch; ++j) {
+            if (k0 + j < P.wave_samples) {
+                t.x += a[j].x; t.y += a[j].y; t.z += a[j].z;
+                P.accum[(size_t)(k0 + j) * P.pixels + p] = zero;
+            }
+        }
     }
     total[p] = t;
 }
@@ -459,14 +470,22 @@ __global__ void k_cache_targets(PTParams P) {
 
 namespace s2 {
 // ---------------------------------------------------------------- material-key counting sort
-// Histogram of the live queue's keys (per-block shared histogram, then global).
+// Histogram of the live queue's keys: per-block shared histogram with one shared atomic per group
+// of equal keys in a warp (queues are spatially coherent, so most lanes of a warp share a key),
+// then one global atomic per non-empty bucket and block.
 __global__ void __launch_bounds__(256) k_sort_hist(PTParams P, uint32_t parity) {
     __shared__ uint32_t h[kSortBuckets];
     for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x) h[b] = 0;
     __syncthreads();
     const uint32_t n = P.counters[parity];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        atomicAdd(&h[P.sort_keys[i]], 1u);
+    const uint32_t rounded = (n + 31u) & ~31u;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
+        const bool live = i < n;
+        const uint32_t key = live ? P.sort_keys[i] : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (live && lane == (uint32_t)__ffs(peers) - 1u) atomicAdd(&h[key], (uint32_t)__popc(peers));
+    }
     __syncthreads();
     for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x)
         if (h[b]) atomicAdd(&P.sort_hist[b], h[b]);
@@ -492,18 +511,36 @@ __global__ void __launch_bounds__(1024) k_sort_scan(PTParams P) {
     for (int k = 0; k < 4; ++k) { P.sort_hist[4 * t + k] = run; run += v[k]; }
 }
 
-// Scatter: sort_perm[offset[key] + rank] = i, ranks taken per warp group of equal keys.
+// Scatter: sort_perm[offset[key] + rank] = i.  Each block takes one contiguous chunk of the
+// queue: it counts its keys in shared memory, reserves its range of every non-empty bucket with
+// one global atomic, and ranks its items inside those ranges with shared atomics (one per group of
+// equal keys in a warp).  The order inside a bucket is not fixed; shading results do not depend on
+// it (every path keeps its own random state and accumulator slot).
 __global__ void __launch_bounds__(256) k_sort_scatter(PTParams P, uint32_t parity) {
+    __shared__ uint32_t h[kSortBuckets];
+    for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x) h[b] = 0;
+    __syncthreads();
     const uint32_t n = P.counters[parity];
-    const uint32_t rounded = (n + 31u) & ~31u;
+    const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 255u) & ~255u;
+    const uint32_t begin = min(n, blockIdx.x * chunk), end = min(n, begin + chunk);
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
-        const bool live = i < n;
+    for (uint32_t i = begin + threadIdx.x; i < begin + chunk; i += blockDim.x) {  // warp-uniform trip count
+        const bool live = i < end;
         const uint32_t key = live ? P.sort_keys[i] : 0xffffffffu;
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        const uint32_t leader = __ffs(peers) - 1;
+        if (live && lane == (uint32_t)__ffs(peers) - 1u) atomicAdd(&h[key], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < kSortBuckets; b += blockDim.x)
+        if (h[b]) h[b] = atomicAdd(&P.sort_hist[b], h[b]);
+    __syncthreads();
+    for (uint32_t i = begin + threadIdx.x; i < begin + chunk; i += blockDim.x) {
+        const bool live = i < end;
+        const uint32_t key = live ? P.sort_keys[i] : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = __ffs(peers) - 1u;
         uint32_t base = 0;
-        if (live && lane == leader) base = atomicAdd(&P.sort_hist[key], (uint32_t)__popc(peers));
+        if (live && lane == leader) base = atomicAdd(&h[key], (uint32_t)__popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
         if (live) P.sort_perm[base + __popc(peers & ((1u << lane) - 1u))] = i;
     }
