@@ -35,6 +35,8 @@ struct RenderState {
     unsigned long long* stats = nullptr;
     uint64_t accumulated_spp = 0;
     int ext_blocks = 0, occ_blocks = 0, shade_blocks = 0;
+    int shade_blocks_rc = 0;   // ReSTIR / radiance-cache shade variants (more registers)
+    int sort_blocks = 0;
     std::vector<cudaEvent_t> events;  // reusable start/stop pairs for S2_FLAG_PROFILE_KERNELS
     // ReSTIR DI reuse: the grid appended to by this call and the previous call's grid
     struct Grid {
@@ -91,6 +93,9 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
         st->occ_blocks = std::max(1, b) * prop.multiProcessorCount;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, false>, 128, 0);
         st->shade_blocks = std::max(1, b) * prop.multiProcessorCount;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, true, true>, 128, 0);
+        st->shade_blocks_rc = std::max(1, b) * prop.multiProcessorCount;
+        st->sort_blocks = 8 * prop.multiProcessorCount;
     }
     const uint32_t pixels = width * height;
     if (st->pixels != pixels || st->width != width) {
@@ -198,9 +203,9 @@ int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t s
 }
 
 template <bool L, bool R>
-void launch_shade(const PTParams& P, uint32_t parity, int blocks, cudaStream_t s) {
-    if (P.cache_on) k_shade<L, R, true><<<blocks, 128, 0, s>>>(P, parity);
-    else k_shade<L, R><<<blocks, 128, 0, s>>>(P, parity);
+void launch_shade(const PTParams& P, uint32_t parity, const RenderState* st, cudaStream_t s) {
+    if (P.cache_on) k_shade<L, R, true><<<st->shade_blocks_rc, 128, 0, s>>>(P, parity);
+    else k_shade<L, R><<<R ? st->shade_blocks_rc : st->shade_blocks, 128, 0, s>>>(P, parity);
 }
 
 }  // namespace
@@ -361,15 +366,15 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             const uint32_t parity = b & 1u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
             P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
-            if (P.ray_sorted) { launch_sort(P, parity, st->shade_blocks, s); launches += 3; }
+            if (P.ray_sorted) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(0);
             if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             ev_end();
-            if (sort) { launch_sort(P, parity, st->shade_blocks, s); launches += 3; }
+            if (sort) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(1);
-            if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
-            else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
+            if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
+            else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
             ev_end();
             if (cache && b + 1 == cache_len) {
                 rc = cache_apply_device(ctx, st->cq_pos, st->cq_thr, st->cq_cap, st->counters + C_CACHEQ, st->accum);
@@ -664,9 +669,9 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         k_regen<<<std::min<uint32_t>((capacity + 255) / 256, 148u * 16u), 256, 0, s>>>(P, parity);
         if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
         else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
-        if (sort) launch_sort(P, parity, st->shade_blocks, s);
-        if (lam) { if (restir) launch_shade<true, true>(P, parity, st->shade_blocks, s); else launch_shade<true, false>(P, parity, st->shade_blocks, s); }
-        else { if (restir) launch_shade<false, true>(P, parity, st->shade_blocks, s); else launch_shade<false, false>(P, parity, st->shade_blocks, s); }
+        if (sort) launch_sort(P, parity, st->sort_blocks, s);
+        if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
+        else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
         if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
         else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
     };

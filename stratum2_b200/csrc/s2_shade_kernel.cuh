@@ -204,8 +204,14 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
     return so;
 }
 
+// Resident 128-thread blocks per SM the shade variants are compiled for: the plain NEE variants at
+// 64 registers (8 blocks; measured 2-3 % faster on B200 than 128 registers and 4 blocks despite
+// the spills); the ReSTIR and radiance-cache variants, which need more live state, at 3 blocks
+// (up to 170 registers).
+template <bool RESTIR, bool CACHE> constexpr int kShadeMinBlocks = (RESTIR || CACHE) ? 3 : 8;
+
 template <bool LAMBERT, bool RESTIR, bool CACHE = false>
-__global__ void __launch_bounds__(128) k_shade(PTParams P, uint32_t parity) {
+__global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(PTParams P, uint32_t parity) {
     const uint32_t count = P.counters[parity];
     const PathQueue qi = P.q[parity];
     const PathQueue qo = P.q[1 - parity];
