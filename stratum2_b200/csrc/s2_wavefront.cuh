@@ -186,8 +186,14 @@ __global__ void k_raygen(PTParams P) {
         P.counters[C_TRAIN] = 0;
     }
     if (i >= n) return;
-    const uint32_t k = i / P.pixels, pix = i - k * P.pixels;
-    const uint32_t px = pix % P.width, py = pix / P.width;
+    // Queue order: image row, then sample, then column.  All samples of a row are traced together,
+    // so the BVH region under a few rows stays in L2 instead of every sample sweeping the whole
+    // image (and the whole visible BVH) again; a warp still takes 32 neighbouring pixels.  The
+    // accumulator slot keeps the sample-major layout that k_reduce sums.
+    const uint32_t row_rays = P.wave_samples * P.width;
+    const uint32_t py = i / row_rays, rem = i - py * row_rays;
+    const uint32_t k = rem / P.width, px = rem - k * P.width;
+    const uint32_t slot = k * P.pixels + py * P.width + px;
     const uint32_t sample = P.wave_base_sample + k;
     Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
     float ox = 0.5f, oy = 0.5f;
@@ -208,11 +214,11 @@ __global__ void k_raygen(PTParams P) {
                                    c[8] * ld.x + c[9] * ld.y + c[10] * ld.z));
     const float3 d = unpack_normal(pack_normal(wd));
     uint32_t meta = (sample == 0 ? 0x100u : 0u);  // path length 0; bit 8: write AOVs
-    if (P.cache_on && pcg_hash(i ^ pcg_hash(P.frame_seed + sample)) % P.train_mod == 0u) meta |= 0x200u;  // training path
+    if (P.cache_on && pcg_hash(slot ^ pcg_hash(P.frame_seed + sample)) % P.train_mod == 0u) meta |= 0x200u;  // training path
     const PathQueue& q = P.q[0];
     q.s0[i] = make_float4(c[3], c[7], c[11], 0.f);
     q.s1[i] = make_float4(d.x, d.y, d.z, 1.f);
-    q.s2[i] = make_float4(1.f, 1.f, __uint_as_float(i), __uint_as_float(meta));
+    q.s2[i] = make_float4(1.f, 1.f, __uint_as_float(slot), __uint_as_float(meta));
     q.s3[i] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
 }
 
