@@ -296,6 +296,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world == 1 and not args.no_quality:
         line["radiance_cache_kernels"] = cache_kernel_line(dev, args.steps)
         line["adjoint"] = adjoint_line(dev)
+        line["restir_many_lights"] = restir_line(dev)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         osc = cpu_oracle(wl)
@@ -480,6 +481,60 @@ def adjoint_line(dev, steps: int = 2) -> dict:
             "gradient_texels": int(sum(t.shape[0] * t.shape[1] for t in grads))}
 
 
+def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
+    """Many-lights ReSTIR DI: the cfg2 terrain carrying 100k small emissive triangles of lognormal(0, 2)
+    power, camera animated over `frames` frames along a seeded Catmull-Rom loop, 1920x1080, 1 spp per
+    frame, 32 RIS candidates, screen-space reuse (1 temporal + 5 spatial neighbours within 30 px,
+    M-cap 20), direct illumination at the primary vertex (path length 2).  Plain NEE at equal GPU
+    time renders the last view with as many samples as one ReSTIR frame's time buys; both last
+    frames are scored by relMSE against `ref_spp`-spp plain NEE of that view."""
+    import torch
+
+    from stratum2_b200 import _abi, metrics
+    from stratum2_b200.scenegen import catmull_rom_views, terrain_scene
+    wl = terrain_scene(emissive_triangles=100_000, emissive_sigma=2.0)
+    dev.upload_scene(wl.scene)
+    W, H = wl.width, wl.height
+    views = catmull_rom_views(W, H, frames=frames, seed=11, looping=True)
+    rad = torch.zeros((H, W, 4), device="cuda")
+    aov = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+
+    def prm(seed, flags, spp=1):
+        p = _abi.S2RenderParams()
+        _abi.lib().s2_default_render_params(p)
+        p.spp, p.min_path_length, p.max_path_length, p.frame_seed = spp, 2, 2, seed
+        p.flags = flags | _abi.FLAG_PIXEL_JITTER
+        p.restir_candidates, p.restir_spatial, p.restir_spatial_radius, p.restir_max_m = 32, 5, 30.0, 20.0
+        return p
+
+    restir = _abi.FLAG_RESTIR_DI | _abi.FLAG_RESTIR_SCREEN
+    for v in views[:4]:  # warm-up
+        dev.render_device(v, prm(1, restir), aov)
+    dev.render_device(views[0], prm(2, 0), aov)  # a call without reuse drops the reservoirs
+    ms = rays = 0.0
+    for f, v in enumerate(views):
+        st = dev.render_device(v, prm(1000 + f, restir), aov)
+        ms += st.gpu_ms
+        rays += st.extension_rays + st.shadow_rays
+    last_restir = rad[..., :3].double().cpu().numpy()
+    restir_ms = ms / frames
+    nee_1 = min(dev.render_device(views[-1], prm(5000 + k, 0), aov).gpu_ms for k in range(3))
+    spp_eq = max(1, int(round(restir_ms / nee_1)))
+    st = dev.render_device(views[-1], prm(6000, 0, spp_eq), aov)
+    last_nee = rad[..., :3].double().cpu().numpy()
+    nee_ms = st.gpu_ms
+    dev.render_device(views[-1], prm(7000, 0, ref_spp), aov)
+    ref = rad[..., :3].double().cpu().numpy()
+    return {"workload": "cfg2 terrain + 100k emissive triangles (power lognormal(0,2)), 32-frame Catmull-Rom camera "
+                        "loop, 1920x1080, 1 spp per frame, direct illumination at the primary vertex",
+            "restir": "32 RIS candidates, screen-space reuse: 1 temporal + 5 spatial neighbours within 30 px, M-cap 20",
+            "restir_ms_per_frame": restir_ms, "restir_mrays_per_s": rays / ms / 1e3,
+            "nee_1spp_ms": nee_1, "nee_equal_time_spp": spp_eq, "nee_equal_time_ms": nee_ms,
+            "relmse_restir_last_frame": metrics.relmse(last_restir, ref),
+            "relmse_nee_equal_time": metrics.relmse(last_nee, ref),
+            "reference": f"plain NEE, {ref_spp} spp, last view (GPU)"}
+
+
 def C_sizeof_view_params() -> int:
     import ctypes
     from stratum2_b200 import _abi
@@ -504,6 +559,8 @@ def main():
                     help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
     ap.add_argument("--cached-frames", type=int, default=0, metavar="N",
                     help="render N 1-spp frames of the workload in the radiance-cache form and exit (profiling)")
+    ap.add_argument("--restir-only", action="store_true",
+                    help="run only the many-lights ReSTIR DI versus equal-time NEE comparison and print it")
     args = ap.parse_args()
     if args.cached_frames:
         from stratum2_b200 import Device, _abi
@@ -524,6 +581,10 @@ def main():
     if args.cache_kernels:
         from stratum2_b200 import Device
         print(json.dumps(cache_kernel_line(Device(0), args.cache_kernels)))
+        return
+    if args.restir_only:
+        from stratum2_b200 import Device
+        print(json.dumps(restir_line(Device(0))))
         return
     if args.single_frame:
         from stratum2_b200 import Device

@@ -170,6 +170,16 @@ typedef struct S2View {
                                                   scattered radiance there, and one path in
                                                   (paths / cache_train_paths) runs to its end and
                                                   trains the cache after each wave (s2_render only) */
+#define S2_FLAG_RESTIR_SCREEN       (1u << 15) /* screen-space ReSTIR DI reuse (no counterpart in the
+                                                  reference, which reuses through the hash grid of
+                                                  S2_FLAG_RESTIR_REUSE; exclusive with it): with
+                                                  S2_FLAG_RESTIR_DI, the primary vertex of every path
+                                                  combines its RIS reservoir with the previous
+                                                  s2_render call's reservoirs at its reprojected
+                                                  pixel (temporal) and at restir_spatial random pixels
+                                                  within restir_spatial_radius of it (spatial); each
+                                                  pixel's sample-0 path stores its reservoir for the
+                                                  next call (s2_render only) */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */
@@ -187,7 +197,9 @@ typedef struct S2RenderParams {
     float restir_grid_pixel_radius;  /* mCellPixelRadius: 0 = constant cell size */
     uint32_t cache_bounces;          /* S2_FLAG_RADIANCE_CACHE: bounces before the cache (0 = 2) */
     uint32_t cache_train_paths;      /* training paths per wave (0 = 65536) */
-    uint32_t reserved[5];
+    uint32_t restir_spatial;         /* S2_FLAG_RESTIR_SCREEN: spatial neighbours (0 = 5, at most 32) */
+    float restir_spatial_radius;     /* S2_FLAG_RESTIR_SCREEN: neighbour radius in pixels (0 = 30) */
+    uint32_t reserved[3];
 } S2RenderParams;
 
 /* Output AOVs (caller-allocated, device or host pointers per s2_render's `out_on_host`).

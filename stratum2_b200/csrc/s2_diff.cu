@@ -28,7 +28,7 @@ using s2::set_error;
 
 namespace {
 
-constexpr uint32_t kDiffUnsupported = S2_FLAG_RESTIR_DI | S2_FLAG_RESTIR_REUSE | S2_FLAG_RADIANCE_CACHE | S2_FLAG_ACCUMULATE |
+constexpr uint32_t kDiffUnsupported = S2_FLAG_RESTIR_DI | S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE | S2_FLAG_ACCUMULATE |
                                       S2_FLAG_PROFILE_KERNELS | S2_FLAG_COUNT_FETCHES;
 
 int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, DiffArgs& A) {

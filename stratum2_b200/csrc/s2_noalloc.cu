@@ -115,8 +115,9 @@ extern "C" int s2_render_noalloc(S2Context* ctx, const S2View* view, const S2Ren
                                                   std::to_string(S2_NOALLOC_MAX_PIXELS) + " pixels (64 MiB scratch array)");
     if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
-    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RADIANCE_CACHE))
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RADIANCE_CACHE are supported by s2_render only");
+    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE, S2_FLAG_RESTIR_SCREEN and S2_FLAG_RADIANCE_CACHE are "
+                                                  "supported by s2_render only");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     cudaSetDevice(ctx->device);

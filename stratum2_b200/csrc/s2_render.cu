@@ -45,6 +45,11 @@ struct RenderState {
     } grid[2];
     uint32_t grid_cur = 0;
     bool grid_prev_valid = false;
+    // screen-space ReSTIR DI reuse: per-pixel reservoirs of this call and of the previous one
+    std::vector<DevBuf> ss_bufs;
+    ReservoirRecord* ss[2] = {nullptr, nullptr};
+    uint32_t ss_cur = 0, ss_pixels = 0, ss_width = 0;
+    bool ss_prev_valid = false;
     // material-key sort buffers (S2Tuning::shade_order)
     std::vector<DevBuf> sort_bufs;
     uint32_t* sort_keys = nullptr;
@@ -66,6 +71,7 @@ void destroy_render_state(S2Context* ctx) {
     for (auto& g : ctx->render->grid) free_bufs(g.bufs);
     free_bufs(ctx->render->cache_bufs);
     free_bufs(ctx->render->sort_bufs);
+    free_bufs(ctx->render->ss_bufs);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -239,6 +245,13 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
+    const bool screen = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_SCREEN);
+    if ((prm->flags & S2_FLAG_RESTIR_REUSE) && (prm->flags & S2_FLAG_RESTIR_SCREEN))
+        return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RESTIR_SCREEN are exclusive");
+    if (screen && (prm->restir_spatial > 32 || !(prm->restir_spatial_radius >= 0.f) || !std::isfinite(prm->restir_spatial_radius) ||
+                   !(prm->restir_max_m > 0.f)))
+        return set_error(ctx, S2_ERR_INVALID, "invalid screen-space ReSTIR parameters (restir_spatial <= 32, "
+                                              "restir_spatial_radius >= 0, restir_max_m > 0)");
     const bool cache = (prm->flags & S2_FLAG_RADIANCE_CACHE) != 0;
     if (cache && !ctx->cache) return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RADIANCE_CACHE needs s2_cache_init");
     if (reuse && (prm->restir_grid_cells > (1u << 26) || prm->restir_grid_cell_size < 0.f ||
@@ -325,6 +338,29 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     } else {
         st->grid_prev_valid = false;  // TestRenderer.cpp:495-498 drops the grids when reuse is off
     }
+    if (screen) {
+        if (st->ss_pixels != pixels || st->ss_width != (uint32_t)W) {
+            free_bufs(st->ss_bufs);
+            st->ss_pixels = 0;
+            st->ss_prev_valid = false;
+            st->ss[0] = alloc<ReservoirRecord>(ctx, st->ss_bufs, pixels);
+            st->ss[1] = alloc<ReservoirRecord>(ctx, st->ss_bufs, pixels);
+            if (!st->ss[0] || !st->ss[1]) { free_bufs(st->ss_bufs); return set_error(ctx, S2_ERR_OOM, "reservoir buffer allocation failed"); }
+            st->ss_pixels = pixels;
+            st->ss_width = (uint32_t)W;
+        }
+        ReservoirRecord* cur = st->ss[st->ss_cur];
+        cudaMemsetAsync(cur, 0, sizeof(ReservoirRecord) * pixels, s);  // pixels without a primary vertex: W = 0
+        P.ss_on = 1;
+        P.ss_cur = cur;
+        P.ss_prev = st->ss[st->ss_cur ^ 1u];
+        P.ss_prev_valid = st->ss_prev_valid ? 1u : 0u;
+        P.ss_spatial = prm->restir_spatial ? prm->restir_spatial : 5u;
+        P.ss_radius = prm->restir_spatial_radius > 0.f ? prm->restir_spatial_radius : 30.f;
+        P.max_m = prm->restir_max_m;
+    } else {
+        st->ss_prev_valid = false;
+    }
     const uint32_t cache_len = (prm->cache_bounces ? prm->cache_bounces : 2u) + 1u;
     const uint32_t train_paths = prm->cache_train_paths ? prm->cache_train_paths : 65536u;
     if (cache) {
@@ -407,6 +443,10 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         launches += 2;
         st->grid_cur ^= 1u;
         st->grid_prev_valid = true;
+    }
+    if (screen) {  // this call's reservoirs become the previous ones
+        st->ss_cur ^= 1u;
+        st->ss_prev_valid = true;
     }
     launches += 1;  // resolve
     st->accumulated_spp += prm->spp;
@@ -533,8 +573,9 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
-    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RADIANCE_CACHE))
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RADIANCE_CACHE are supported by s2_render only");
+    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE, S2_FLAG_RESTIR_SCREEN and S2_FLAG_RADIANCE_CACHE are "
+                                                  "supported by s2_render only");
     cudaSetDevice(ctx->device);
     std::vector<ViewEntry> ve(nviews);
     std::vector<uint32_t> layout;

@@ -111,10 +111,31 @@ S2D void reservoir_reuse(const PTParams& P, const Mat& m, const SD& sd, float3 i
     iw = cur.target() > 0.f ? total / cur.target() : 0.f;
 }
 
-// One NEE connection: plain light sample, or RIS over restir_m candidates (+ hash-grid reuse).
+// Previous-frame camera-space position of world point pw (row-major 3x4 world-to-camera).
+S2D float3 prev_camera_point(const float* pv, float3 pw) {
+    return f3(pv[0] * pw.x + pv[1] * pw.y + pv[2] * pw.z + pv[3], pv[4] * pw.x + pv[5] * pw.y + pv[6] * pw.z + pv[7],
+              pv[8] * pw.x + pv[9] * pw.y + pv[10] * pw.z + pv[11]);
+}
+
+// ViewData::toRaster (compat/scene.h:158-165), perspective projectPoint: raster position (pixels,
+// image_min included) of camera-space point pc; leaves `out` unchanged and returns false when pc is
+// behind the camera or outside the frustum.
+S2D bool camera_to_raster(const float* proj, const int* imin, const int* imax, float3 pc, float2& out) {
+    const float nr = proj[4];
+    if (!((pc.z > 0.f) == (nr > 0.f) && pc.z != 0.f)) return false;
+    const float x4 = pc.x * proj[0] + pc.z * proj[2], y4 = pc.y * proj[1] + pc.z * proj[3];
+    const float z4 = fabsf(nr), w4 = pc.z * (nr > 0.f ? 1.f : -1.f);
+    if (fabsf(x4) >= fabsf(w4) || fabsf(y4) >= fabsf(w4) || fabsf(z4) >= fabsf(w4)) return false;
+    const float W = (float)(imax[0] - imin[0]), H = (float)(imax[1] - imin[1]);
+    out = make_float2(imin[0] + W * (x4 / w4 * 0.5f + 0.5f), imin[1] + H * (-y4 / w4 * 0.5f + 0.5f));
+    return true;
+}
+
+// One NEE connection: plain light sample, or RIS over restir_m candidates (+ hash-grid or
+// screen-space reuse).
 template <bool LAMBERT, bool RESTIR>
 S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, float3 in, float3 thr, Rng& rng, uint32_t len,
-                               bool sn, uint32_t inst, uint32_t prim) {
+                               bool sn, uint32_t inst, uint32_t prim, uint32_t pixel, bool store_pixel) {
     ShadowOut so;
     so.valid = false;
     const DevScene& s = P.scene;
@@ -136,6 +157,43 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
             if (rng.next_float().x <= risw / wsum) best = c;
         }
         float iw = best.target() > 0.f ? wsum / ((float)P.restir_m * best.target()) : 0.f;
+        if (P.ss_on && len == 1) {
+            // screen-space reuse at the primary vertex: the previous call's reservoirs at the
+            // reprojected pixel and at ss_spatial random pixels within ss_radius of it, each
+            // combined with the running reservoir by ReservoirReuse's two-domain resampling
+            float M = (float)P.restir_m;
+            float2 pr;
+            if (P.ss_prev_valid &&
+                camera_to_raster(P.proj, P.imin, P.imax,
+                                 prev_camera_point(P.prev_inv, xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos)), pr)) {
+                for (uint32_t j = 0; j <= P.ss_spatial; ++j) {
+                    float2 q = pr;
+                    if (j > 0) {
+                        const float4 u = rng.next_float();
+                        const float2 d = sample_concentric_disc(u.x, u.y);
+                        q = make_float2(pr.x + d.x * P.ss_radius, pr.y + d.y * P.ss_radius);
+                    }
+                    const float fx = floorf(q.x - (float)P.imin[0]), fy = floorf(q.y - (float)P.imin[1]);
+                    if (!(fx >= 0.f && fy >= 0.f && fx < (float)P.width && fy < (float)P.height)) continue;
+                    const ReservoirRecord rq = P.ss_prev[(uint32_t)fy * P.width + (uint32_t)fx];
+                    if (!(rq.W > 0.f)) continue;
+                    reservoir_reuse<LAMBERT>(P, m, sd, in, cp, rq, best, iw, M, rng, sn);
+                }
+            }
+            if (store_pixel) {
+                ReservoirRecord rec;
+                rec.local_pos = xform_point(s.inv_transforms + 3 * (size_t)inst, sd.pos);
+                rec.instance = inst;
+                rec.primitive = prim;
+                rec.rnd = best.rnd;
+                rec.target_pdf = best.target();
+                rec.W = iw > 0.f ? iw : 0.f;
+                rec.M = fminf(M, P.max_m * (float)P.restir_m);
+                rec.local_dir_in = in;
+                rec.pad = 0.f;
+                P.ss_cur[pixel] = rec;
+            }
+        }
         if (P.reuse) {
             float M = (float)P.restir_m;
             if (P.prev_valid) {
@@ -288,24 +346,12 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                     if (A.vis) A.vis[pix] = make_uint2((inst & 0xffffu) | (prim << 16), sd.ns);
                     if (A.ids) A.ids[pix] = make_uint2(inst, prim);
                     const float3 pw = xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos);
-                    const float* pv = A.prev_inv;
-                    const float3 pc = f3(pv[0] * pw.x + pv[1] * pw.y + pv[2] * pw.z + pv[3],
-                                         pv[4] * pw.x + pv[5] * pw.y + pv[6] * pw.z + pv[7],
-                                         pv[8] * pw.x + pv[9] * pw.y + pv[10] * pw.z + pv[11]);
+                    const float3 pc = prev_camera_point(A.prev_inv, pw);
                     const uint32_t px = pix % A.width, py = pix / A.width;
                     const float W = (float)(A.imax[0] - A.imin[0]), H = (float)(A.imax[1] - A.imin[1]);
-                    float ppx = (float)px + 0.5f, ppy = (float)py + 0.5f;
-                    const float nr = A.proj[4];
-                    if ((pc.z > 0.f) == (nr > 0.f) && pc.z != 0.f) {
-                        // ViewData::toRaster (compat/scene.h:158-165), perspective projectPoint
-                        const float x4 = pc.x * A.proj[0] + pc.z * A.proj[2], y4 = pc.y * A.proj[1] + pc.z * A.proj[3];
-                        const float z4 = fabsf(nr), w4 = pc.z * (nr > 0.f ? 1.f : -1.f);
-                        if (!(fabsf(x4) >= fabsf(w4) || fabsf(y4) >= fabsf(w4) || fabsf(z4) >= fabsf(w4))) {
-                            ppx = A.imin[0] + W * (x4 / w4 * 0.5f + 0.5f);
-                            ppy = A.imin[1] + H * (-y4 / w4 * 0.5f + 0.5f);
-                        }
-                    }
-                    if (A.prev_uv) A.prev_uv[pix] = make_float2(ppx / W, ppy / H);
+                    float2 pr = make_float2((float)px + 0.5f, (float)py + 0.5f);
+                    camera_to_raster(A.proj, A.imin, A.imax, pc, pr);
+                    if (A.prev_uv) A.prev_uv[pix] = make_float2(pr.x / W, pr.y / H);
                     if (A.depth) A.depth[pix] = make_float4(isect_dist, length(pc), 1.f, 1.f);
                 }
                 // ---- emission (surface lights are one-sided)
@@ -338,7 +384,9 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                 }
                 if (!cached && len < P.max_len && any_pos(m.base())) {
                     const bool sing = mat_singular<LAMBERT>(m);
-                    if (!sing && nee) so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim);
+                    if (!sing && nee)
+                        so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim, slot % P.pixels,
+                                                               aov && !P.views);
                     const float cp = fminf(1.f, cont_prob(m));
                     bool cont = true;
                     if (!(P.flags & S2F_NO_RR)) {

@@ -89,6 +89,12 @@ struct PTParams {
     HashGridDev grid_cur, grid_prev;
     uint32_t reuse, prev_valid;
     float max_m;
+    // screen-space ReSTIR DI reuse (S2_FLAG_RESTIR_SCREEN): per-pixel reservoirs of the previous
+    // call (read) and of this call (written by each pixel's sample-0 primary vertex)
+    const ReservoirRecord* ss_prev;
+    ReservoirRecord* ss_cur;
+    uint32_t ss_on, ss_prev_valid, ss_spatial;
+    float ss_radius;
     // learned radiance cache (S2_FLAG_RADIANCE_CACHE): non-training paths end at vertex cache_len
     // with a query {position, slot} + throughput; training paths (meta bit 9, one in train_mod)
     // record every vertex {position, slot}, throughput, accumulated radiance
@@ -142,6 +148,7 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_NO_RR (1u << 6)
 #define S2F_NO_SN (1u << 8)
 #define S2F_REUSE (1u << 11)
+#define S2F_SCREEN (1u << 15)
 #define S2F_NO_ALPHA (1u << 12)
 #define S2F_NO_NORMAL_MAPS (1u << 13)
 #define S2F_CACHE (1u << 14)

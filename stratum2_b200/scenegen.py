@@ -340,3 +340,34 @@ def terrain_scene(seed: int = 2, grid: int = 1024, spheres: int = 64, sphere_lev
     pos = (0.0, 0.9, 1.9)
     view = make_view(pos, width, height, 45.0, look_at_rotation(pos, (0.0, 0.0, 0.0)))
     return Workload(s, view, width, height, spp, 3, 12, False, f"terrain{grid}_{width}x{height}")
+
+
+# ------------------------------------------------------------------------------ animated camera
+def catmull_rom_views(width: int, height: int, frames: int = 32, seed: int = 5, center=(0.0, 0.9, 1.9),
+                      spread=(0.3, 0.1, 0.2), target=(0.0, 0.0, 0.0), control_points: int = 6, vfov_degrees: float = 45.0,
+                      looping: bool = False):
+    """Camera animation along a seeded closed Catmull-Rom spline: `control_points` positions drawn
+    uniformly within `spread` of `center`, the camera looking at `target`; one view per frame, each
+    carrying the previous frame's camera transform for reprojection.  The first view's previous
+    transform is its own, or with `looping` the last view's (for playing the loop repeatedly)."""
+    rng = np.random.default_rng(seed)
+    ctrl = np.asarray(center, np.float64) + rng.uniform(-1, 1, (control_points, 3)) * np.asarray(spread, np.float64)
+
+    def position(t):
+        seg = int(np.floor(t)) % control_points
+        u = t - np.floor(t)
+        p0, p1, p2, p3 = (ctrl[(seg + k - 1) % control_points] for k in range(4))
+        # uniform Catmull-Rom: tangents (p2 - p0) / 2 and (p3 - p1) / 2
+        return 0.5 * ((2 * p1) + (-p0 + p2) * u + (2 * p0 - 5 * p1 + 4 * p2 - p3) * u * u + (-p0 + 3 * p1 - 3 * p2 + p3) * u ** 3)
+
+    views, prev = [], None
+    for f in range(frames):
+        pos = position(control_points * f / frames)
+        rot = look_at_rotation(pos, target)
+        m = transform_trs(pos, rot)
+        views.append(make_view(pos, width, height, vfov_degrees, rot, prev_camera_to_world=prev if prev is not None else m))
+        prev = m
+    if looping:
+        views[0] = make_view(position(0.0), width, height, vfov_degrees, look_at_rotation(position(0.0), target),
+                             prev_camera_to_world=prev)
+    return views
