@@ -485,9 +485,11 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
     """Many-lights ReSTIR DI: the cfg2 terrain carrying 100k small emissive triangles of lognormal(0, 2)
     power, camera animated over `frames` frames along a seeded Catmull-Rom loop, 1920x1080, 1 spp per
     frame, 32 RIS candidates, screen-space reuse (1 temporal + 5 spatial neighbours within 30 px,
-    M-cap 20), direct illumination at the primary vertex (path length 2).  Plain NEE at equal GPU
-    time renders the last view with as many samples as one ReSTIR frame's time buys; both last
-    frames are scored by relMSE against `ref_spp`-spp plain NEE of that view."""
+    M-cap 20), direct illumination at the primary vertex (path length 2), lights picked in
+    proportion to their power (both estimators; the uniform pick leaves even the reference
+    unconverged at these power ratios).  Plain NEE at equal GPU time renders the last view with as
+    many samples as one ReSTIR frame's time buys; both last frames are scored by relMSE against
+    `ref_spp`-spp plain NEE of that view."""
     import torch
 
     from stratum2_b200 import _abi, metrics
@@ -503,7 +505,7 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
         p = _abi.S2RenderParams()
         _abi.lib().s2_default_render_params(p)
         p.spp, p.min_path_length, p.max_path_length, p.frame_seed = spp, 2, 2, seed
-        p.flags = flags | _abi.FLAG_PIXEL_JITTER
+        p.flags = flags | _abi.FLAG_PIXEL_JITTER | _abi.FLAG_LIGHT_POWER_PICK
         p.restir_candidates, p.restir_spatial, p.restir_spatial_radius, p.restir_max_m = 32, 5, 30.0, 20.0
         return p
 
@@ -519,20 +521,24 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
     last_restir = rad[..., :3].double().cpu().numpy()
     restir_ms = ms / frames
     nee_1 = min(dev.render_device(views[-1], prm(5000 + k, 0), aov).gpu_ms for k in range(3))
+    relmse_nee_1 = rad[..., :3].double().cpu().numpy()
     spp_eq = max(1, int(round(restir_ms / nee_1)))
     st = dev.render_device(views[-1], prm(6000, 0, spp_eq), aov)
     last_nee = rad[..., :3].double().cpu().numpy()
     nee_ms = st.gpu_ms
     dev.render_device(views[-1], prm(7000, 0, ref_spp), aov)
     ref = rad[..., :3].double().cpu().numpy()
+    relmse_nee_1 = metrics.relmse(relmse_nee_1, ref)
     return {"workload": "cfg2 terrain + 100k emissive triangles (power lognormal(0,2)), 32-frame Catmull-Rom camera "
                         "loop, 1920x1080, 1 spp per frame, direct illumination at the primary vertex",
             "restir": "32 RIS candidates, screen-space reuse: 1 temporal + 5 spatial neighbours within 30 px, M-cap 20",
+            "light_pick": "power-proportional (alias table), both estimators",
             "restir_ms_per_frame": restir_ms, "restir_mrays_per_s": rays / ms / 1e3,
             "nee_1spp_ms": nee_1, "nee_equal_time_spp": spp_eq, "nee_equal_time_ms": nee_ms,
             "relmse_restir_last_frame": metrics.relmse(last_restir, ref),
             "relmse_nee_equal_time": metrics.relmse(last_nee, ref),
-            "reference": f"plain NEE, {ref_spp} spp, last view (GPU)"}
+            "relmse_nee_1spp": relmse_nee_1,
+            "reference": f"plain NEE, {ref_spp} spp, last view (GPU, power-proportional pick)"}
 
 
 def C_sizeof_view_params() -> int:

@@ -180,6 +180,12 @@ typedef struct S2View {
                                                   within restir_spatial_radius of it (spatial); each
                                                   pixel's sample-0 path stores its reservoir for the
                                                   next call (s2_render only) */
+#define S2_FLAG_LIGHT_POWER_PICK    (1u << 16) /* pick emissive lights in proportion to their power
+                                                  (emission luminance x area, from an alias table built
+                                                  at s2_scene_upload) instead of uniformly as the
+                                                  reference does (lights.hlsli:200); no counterpart in
+                                                  the reference.  Same expected image, less noise with
+                                                  many lights of unequal power */
 
 typedef struct S2RenderParams {
     uint32_t min_path_length;        /* VCM --minPathLength (vcm.slang:922,960,977) */

@@ -43,6 +43,7 @@ FLAG_ALPHA_TEST_OFF = 1 << 12
 FLAG_NORMAL_MAPS_OFF = 1 << 13
 FLAG_RADIANCE_CACHE = 1 << 14
 FLAG_RESTIR_SCREEN = 1 << 15
+FLAG_LIGHT_POWER_PICK = 1 << 16
 SHADE_ORDER_MATERIAL = 0
 SHADE_ORDER_QUEUE = 1
 TRACE_ORDER_QUEUE = 0

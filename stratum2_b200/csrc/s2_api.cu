@@ -427,6 +427,70 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     if (d->instance_light_map) std::memcpy(ilm.data(), d->instance_light_map, 4 * (size_t)ni);
     else for (uint32_t l = 0; l < d->light_count; ++l) ilm[d->light_instance_map[l]] = l;
     s.instance_light_map = upload(ctx, ctx->scene_bufs, ilm.data(), ni);
+    {
+        // power-proportional pick: weight = emission luminance (material factor, textures ignored)
+        // x world-space area of the light instance, floored at 1e-3 of the mean so every light
+        // keeps a nonzero probability; Walker alias table (Vose's construction)
+        const uint32_t L = d->light_count;
+        std::vector<double> wgt(L, 0.0);
+        double total = 0.0;
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint32_t li = d->light_instance_map[l];
+            const uint32_t mat = d->instances[2 * li] >> 4;
+            double lum = 0.0;
+            if ((size_t)mat + 36 <= d->material_bytes) {
+                uint32_t w1; float esc;
+                std::memcpy(&w1, (const uint8_t*)d->material_data + mat + 4, 4);
+                std::memcpy(&esc, (const uint8_t*)d->material_data + mat + 32, 4);
+                lum = (0.2126 * (w1 & 0xffu) + 0.7152 * ((w1 >> 8) & 0xffu) + 0.0722 * ((w1 >> 16) & 0xffu)) / 255.0 * esc;
+            }
+            double area = 0.0;
+            for (uint32_t t = ctx->inst_tri_offset[li], e = t + prim_counts[li]; t < e && t < ctx->tri_inst.size(); ++t) {
+                const float* a = &ctx->tri_v0[3 * (size_t)t]; const float* b = &ctx->tri_v1[3 * (size_t)t]; const float* c = &ctx->tri_v2[3 * (size_t)t];
+                const double u[3] = {b[0] - (double)a[0], b[1] - (double)a[1], b[2] - (double)a[2]};
+                const double v[3] = {c[0] - (double)a[0], c[1] - (double)a[1], c[2] - (double)a[2]};
+                const double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2], z = u[0] * v[1] - u[1] * v[0];
+                area += 0.5 * std::sqrt(x * x + y * y + z * z);
+            }
+            wgt[l] = std::isfinite(lum * area) && lum * area > 0.0 ? lum * area : 0.0;
+            total += wgt[l];
+        }
+        std::vector<float> pick(L), thr(L);
+        std::vector<uint32_t> alias(L);
+        if (L) {
+            const double floor_w = total > 0.0 ? 1e-3 * total / L : 1.0;
+            total = 0.0;
+            for (uint32_t l = 0; l < L; ++l) { wgt[l] = std::max(wgt[l], floor_w); total += wgt[l]; }
+            std::vector<double> q(L);
+            std::vector<uint32_t> small, large;
+            for (uint32_t l = 0; l < L; ++l) {
+                pick[l] = (float)(wgt[l] / total);
+                q[l] = wgt[l] / total * L;
+                (q[l] < 1.0 ? small : large).push_back(l);
+                alias[l] = l;
+                thr[l] = 1.f;
+            }
+            while (!small.empty() && !large.empty()) {
+                const uint32_t a = small.back(); small.pop_back();
+                const uint32_t g = large.back();
+                thr[a] = (float)q[a];
+                alias[a] = g;
+                q[g] -= 1.0 - q[a];
+                if (q[g] < 1.0) { large.pop_back(); small.push_back(g); }
+            }
+            // leftovers (rounding) keep threshold 1 and alias themselves
+        }
+        // the sampled probability of light l is (thr[l] + sum of (1 - thr[a]) over columns a aliasing
+        // to l) / L; store that exactly so pdfs match the sampling with float thresholds
+        std::vector<double> eff(L, 0.0);
+        for (uint32_t a = 0; a < L; ++a) { eff[a] += (double)thr[a] / L; eff[alias[a]] += (1.0 - (double)thr[a]) / L; }
+        std::vector<float2> tab(std::max(1u, L));
+        for (uint32_t l = 0; l < L; ++l) { uint32_t ab = alias[l]; float af; std::memcpy(&af, &ab, 4); tab[l] = make_float2(thr[l], af); pick[l] = (float)eff[l]; }
+        s.light_alias = upload(ctx, ctx->scene_bufs, tab.data(), tab.size());
+        if (pick.empty()) pick.push_back(0.f);
+        s.light_pick_pdf = upload(ctx, ctx->scene_bufs, pick.data(), pick.size());
+        s.light_power_pick = 0;
+    }
     s.env_address = d->environment_material_address;
     if (s.env_address != S2_NO_ENVIRONMENT && (size_t)s.env_address + 16 > d->material_bytes)
         return set_error(ctx, S2_ERR_INVALID, "environment material address out of range");

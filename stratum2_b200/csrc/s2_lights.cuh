@@ -165,8 +165,19 @@ S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_n
         if (L > 0) rnd.w = (rnd.w - envp) / (1.f - envp);
     }
     if (L == 0) return r;
-    const uint32_t inst = s.light_instance_map[(uint32_t)(rnd.z * L) % L];
-    float pdf = 1.f / (float)L;
+    uint32_t light;
+    float pdf;
+    if (s.light_power_pick) {  // alias table: one uniform number picks a column and its threshold
+        const float u = rnd.z * (float)L;
+        const uint32_t col = min((uint32_t)u, L - 1u);
+        const float2 a = s.light_alias[col];
+        light = (u - (float)col) < a.x ? col : __float_as_uint(a.y);
+        pdf = s.light_pick_pdf[light];
+    } else {
+        light = (uint32_t)(rnd.z * L) % L;
+        pdf = 1.f / (float)L;
+    }
+    const uint32_t inst = s.light_instance_map[light];
     if (has_env(s)) pdf *= 1.f - envp;
     if ((s.instances[inst].x & 0xfu) != 0u) return r;
     const uint32_t pc = s.prim_counts[inst];
@@ -189,7 +200,13 @@ S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_n
 // IntersectionResult::LightSamplePdfA (lights.hlsli:264-272)
 S2D float light_pdfa(const DevScene& s, uint32_t inst, float area) {
     if (s.light_count == 0) return 0.f;
-    float pdf = (1.f / (float)s.prim_counts[inst]) / (area * (float)s.light_count);
+    float pdf;
+    if (s.light_power_pick) {  // instances outside the light list are never picked
+        const uint32_t light = s.instance_light_map[inst];
+        pdf = light < s.light_count ? s.light_pick_pdf[light] / ((float)s.prim_counts[inst] * area) : 0.f;
+    } else {
+        pdf = (1.f / (float)s.prim_counts[inst]) / (area * (float)s.light_count);
+    }
     if (has_env(s)) pdf *= 1.f - s.env_sample_prob;
     return pdf;
 }

@@ -49,6 +49,12 @@ struct DevScene {
     const uint32_t* light_instance_map;
     const uint32_t* instance_light_map;
     uint32_t light_count;
+    // power-proportional light pick (S2_FLAG_LIGHT_POWER_PICK; no counterpart in the reference, whose
+    // pick is uniform): Walker alias table over the lights {threshold, alias index as float bits}
+    // and each light's pick probability; light_power_pick is set per render call
+    const float2* light_alias;
+    const float* light_pick_pdf;
+    uint32_t light_power_pick;
     uint32_t env_address;              // 0xffffffff = none
     float env_sample_prob;
     // images
