@@ -490,6 +490,41 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
         if (pick.empty()) pick.push_back(0.f);
         s.light_pick_pdf = upload(ctx, ctx->scene_bufs, pick.data(), pick.size());
         s.light_power_pick = 0;
+        // baked light triangles (world space, from the flattened copy): the geometric normal and
+        // area follow make_shading (cross(v0 - v2, v1 - v2)), the emission LoadMaterial's 8-bit
+        // colour x scale; instances with a normal stream or an emission texture are not baked
+        std::vector<uint2> range(std::max(1u, L), make_uint2(0u, 0u));
+        std::vector<float4> tris;
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint32_t li = d->light_instance_map[l];
+            const uint32_t mat = d->instances[2 * li] >> 4;
+            const uint32_t vinfo = d->instances[2 * li + 1] & 0xffffu;
+            const uint32_t nb = d->vertex_infos[8 * (size_t)vinfo + 1] & 0xffffu;
+            uint32_t w1, eimg; float esc;
+            std::memcpy(&w1, (const uint8_t*)d->material_data + mat + 4, 4);
+            std::memcpy(&eimg, (const uint8_t*)d->material_data + mat + 20, 4);
+            std::memcpy(&esc, (const uint8_t*)d->material_data + mat + 32, 4);
+            const bool bake = nb >= d->vertex_buffer_count && eimg >= d->image_count;
+            const float er = (float)(w1 & 0xffu) / 255.f * esc, eg = (float)((w1 >> 8) & 0xffu) / 255.f * esc,
+                        eb = (float)((w1 >> 16) & 0xffu) / 255.f * esc;
+            range[l] = make_uint2((uint32_t)(tris.size() / 4), prim_counts[li]);
+            for (uint32_t p = 0; p < prim_counts[li]; ++p) {
+                const size_t t = (size_t)ctx->inst_tri_offset[li] + p;
+                const float* a = &ctx->tri_v0[3 * t]; const float* b = &ctx->tri_v1[3 * t]; const float* c = &ctx->tri_v2[3 * t];
+                const float ds[3] = {a[0] - c[0], a[1] - c[1], a[2] - c[2]}, dt[3] = {b[0] - c[0], b[1] - c[1], b[2] - c[2]};
+                float gn[3] = {ds[1] * dt[2] - ds[2] * dt[1], ds[2] * dt[0] - ds[0] * dt[2], ds[0] * dt[1] - ds[1] * dt[0]};
+                const float area2 = std::sqrt(gn[0] * gn[0] + gn[1] * gn[1] + gn[2] * gn[2]);
+                const bool ok = bake && area2 > 0.f && std::isfinite(area2);
+                for (float& g : gn) g = ok ? g / area2 : 0.f;
+                tris.push_back(make_float4(a[0], a[1], a[2], ok ? 0.5f * area2 : -1.f));
+                tris.push_back(make_float4(b[0] - a[0], b[1] - a[1], b[2] - a[2], er));
+                tris.push_back(make_float4(c[0] - a[0], c[1] - a[1], c[2] - a[2], eg));
+                tris.push_back(make_float4(gn[0], gn[1], gn[2], eb));
+            }
+        }
+        if (tris.empty()) for (int k = 0; k < 4; ++k) tris.push_back(make_float4(0.f, 0.f, 0.f, -1.f));
+        s.light_tri_range = upload(ctx, ctx->scene_bufs, range.data(), range.size());
+        s.light_tris = upload(ctx, ctx->scene_bufs, tris.data(), tris.size());
     }
     s.env_address = d->environment_material_address;
     if (s.env_address != S2_NO_ENVIRONMENT && (size_t)s.env_address + 16 > d->material_bytes)

@@ -173,6 +173,24 @@ S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_n
         const float2 a = s.light_alias[col];
         light = (u - (float)col) < a.x ? col : __float_as_uint(a.y);
         pdf = s.light_pick_pdf[light];
+        const uint2 range = s.light_tri_range[light];
+        const uint32_t prim = (uint32_t)(rnd.w * range.y) % max(range.y, 1u);
+        const float4* lt = s.light_tris + 4 * (size_t)(range.x + prim);
+        const float4 t0 = lt[0];
+        if (t0.w > 0.f) {  // baked triangle: one 64-byte record instead of make_shading's gathers
+            const float4 t1 = lt[1], t2 = lt[2], t3 = lt[3];
+            const float2 b = sample_uniform_triangle(rnd.x, rnd.y);
+            const float3 pos = f3(t0.x + t1.x * b.x + t2.x * b.y, t0.y + t1.y * b.x + t2.y * b.y, t0.z + t1.z * b.x + t2.z * b.y);
+            if (has_env(s)) pdf *= 1.f - envp;
+            r.radiance = f3(t1.w, t2.w, t3.w);
+            r.dir = pos - ref;
+            r.dist = length(r.dir);
+            r.dir = r.dir / r.dist;
+            r.cos_light = -dot(f3(t3.x, t3.y, t3.z), r.dir);
+            r.pdf = pdf / ((float)range.y * t0.w);
+            if (r.cos_light <= 0.f) { r.radiance = f3(0.f); r.pdf = 0.f; }
+            return r;
+        }
     } else {
         light = (uint32_t)(rnd.z * L) % L;
         pdf = 1.f / (float)L;

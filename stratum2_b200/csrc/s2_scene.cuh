@@ -55,6 +55,12 @@ struct DevScene {
     const float2* light_alias;
     const float* light_pick_pdf;
     uint32_t light_power_pick;
+    // baked light triangles for that mode: per light {first record, triangle count}; per triangle
+    // four float4 {v0, area}, {v1 - v0, emission r}, {v2 - v0, emission g}, {geometric normal,
+    // emission b}, world space; area <= 0 marks a triangle sampled through make_shading instead
+    // (vertex normals, which may flip the geometric normal, or an emission texture)
+    const uint2* light_tri_range;
+    const float4* light_tris;
     uint32_t env_address;              // 0xffffffff = none
     float env_sample_prob;
     // images
