@@ -686,6 +686,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     P.status = ctx->status_dev;
     P.views = B->views_dev;
     P.nviews = nviews;
+    P.view_spp = prm->spp;
     P.total_fx = B->total_fx;
     P.total_paths = paths;
     P.capacity = capacity;

@@ -80,7 +80,7 @@ struct PTParams {
     // batched streaming mode (s2_render_views): view table, fixed-point per-pixel accumulators,
     // path-space size and queue capacity; null / 0 in wave mode
     const ViewEntry* views;
-    uint32_t nviews;
+    uint32_t nviews, view_spp;
     unsigned long long* total_fx;   // 4 x u64 per pixel: r, g, b fixed point (2^-24), unused
     unsigned long long total_paths;
     uint32_t capacity;
@@ -276,8 +276,13 @@ S2D void regen_one(const PTParams& P, uint32_t parity, uint32_t fill, uint32_t i
     while (v + 1 < P.nviews && P.views[v + 1].path_offset <= id) ++v;
     const ViewEntry& V = P.views[v];
     const unsigned long long local = id - V.path_offset;
-    const uint32_t sample = (uint32_t)(local / V.pixels), pix = (uint32_t)(local - (unsigned long long)sample * V.pixels);
-    const uint32_t px = pix % V.width, py = pix / V.width;
+    // path order inside a view: image row, then sample, then column (as k_raygen), so the samples
+    // of a row are traced together and the BVH under a few rows stays in L2
+    const unsigned long long row_paths = (unsigned long long)P.view_spp * V.width;
+    const uint32_t py = (uint32_t)(local / row_paths);
+    const uint32_t rem = (uint32_t)(local - (unsigned long long)py * row_paths);
+    const uint32_t sample = rem / V.width, px = rem - sample * V.width;
+    const uint32_t pix = py * V.width + px;
     Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
     float ox = 0.5f, oy = 0.5f;
     if (P.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
