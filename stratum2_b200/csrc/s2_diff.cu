@@ -37,6 +37,8 @@ int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, Di
     const int W = view->image_max[0] - view->image_min[0], H = view->image_max[1] - view->image_min[1];
     if (W <= 0 || H <= 0 || (int64_t)W * H > (1ll << 26)) return set_error(ctx, S2_ERR_INVALID, "invalid view extent");
     if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
+    if ((uint64_t)W * H * prm->spp > 0xffffffffull)
+        return set_error(ctx, S2_ERR_INVALID, "pixels x spp must stay below 2^32 (one thread per path)");
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if (prm->flags & kDiffUnsupported)
         return set_error(ctx, S2_ERR_UNSUPPORTED, "differentiable rendering supports plain NEE path tracing only "
@@ -62,13 +64,14 @@ int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, Di
 
 template <bool ADJ>
 void launch(const DiffArgs& A, cudaStream_t s) {
-    const uint32_t blocks = (A.pixels + 127) / 128;
+    const uint32_t blocks = (uint32_t)(((uint64_t)A.pixels * A.spp + 127) / 128);
     if (A.flags & S2_FLAG_LAMBERTIAN) dk::k_diff<true, ADJ><<<blocks, 128, 0, s>>>(A);
     else dk::k_diff<false, ADJ><<<blocks, 128, 0, s>>>(A);
+    if (!ADJ) dk::k_diff_resolve<<<(A.pixels + 255) / 256, 256, 0, s>>>(A);
 }
 
 int finish(S2Context* ctx, std::vector<DevBuf>& tmp, unsigned long long* rays_dev, float ms_unused, S2RenderStats* st,
-           uint64_t paths) {
+           uint64_t paths, uint64_t launches) {
     (void)ms_unused;
     unsigned long long rays[2] = {0, 0};
     int status = 0;
@@ -87,7 +90,7 @@ int finish(S2Context* ctx, std::vector<DevBuf>& tmp, unsigned long long* rays_de
         st->shadow_rays = rays[1];
         st->paths = paths;
         st->gpu_ms = ms;
-        st->kernel_launches = 1;
+        st->kernel_launches = launches;
     }
     return S2_OK;
 }
@@ -105,7 +108,8 @@ extern "C" int s2_render_diff(S2Context* ctx, const S2View* view, const S2Render
     std::vector<DevBuf> tmp;
     A.rays = (unsigned long long*)dev_alloc(ctx, tmp, 2 * sizeof(unsigned long long));
     A.image = out_on_host ? (float4*)dev_alloc(ctx, tmp, sizeof(float4) * A.pixels) : (float4*)radiance;
-    if (!A.rays || !A.image) { free_bufs(tmp); return S2_ERR_OOM; }
+    A.path_l = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)A.pixels * A.spp);
+    if (!A.rays || !A.image || !A.path_l) { free_bufs(tmp); return S2_ERR_OOM; }
     cudaMemsetAsync(A.rays, 0, 2 * sizeof(unsigned long long), ctx->stream);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaEventRecord(ctx->ev0, ctx->stream);
@@ -113,7 +117,7 @@ extern "C" int s2_render_diff(S2Context* ctx, const S2View* view, const S2Render
     rc = check_cuda(ctx, cudaGetLastError(), "differentiable render launch");
     if (rc != S2_OK) { cudaStreamSynchronize(ctx->stream); free_bufs(tmp); return rc; }
     if (out_on_host) cudaMemcpyAsync(radiance, A.image, sizeof(float4) * A.pixels, cudaMemcpyDeviceToHost, ctx->stream);
-    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp);
+    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, 2);
 }
 
 extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2RenderParams* prm, const float* d_radiance,
@@ -152,5 +156,5 @@ extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2Ren
         cudaMemcpyAsync(d_images[k], A.grad + off[k], bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                         ctx->stream);
     }
-    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp);
+    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, 1);
 }

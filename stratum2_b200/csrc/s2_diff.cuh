@@ -110,6 +110,7 @@ struct DiffArgs {
     uint32_t min_len, max_len, flags, frame_seed;
     float out_scale;                  // 2^exposure / spp
     float4* image;                    // forward: mean radiance * 2^exposure per pixel
+    float4* path_l;                   // forward: radiance of every path, [sample][pixel]
     const float4* d_image;            // adjoint: dLoss / d image
     float4* grad;                     // adjoint: texel gradients of every image, concatenated
     const uint32_t* grad_offset;      // first texel of image k in `grad`
@@ -314,34 +315,50 @@ __device__ __noinline__ float3 diff_path(const DiffArgs& A, uint32_t px, uint32_
     return L;
 }
 
-// Forward (ADJ = false): image[pixel] = mean path radiance * 2^exposure.  Adjoint: texel gradients
-// of sum(d_image * image).  One thread per pixel, looping over its samples (deterministic image).
+// One thread per path (sample-major: a warp takes 32 neighbouring pixels of one sample, so its
+// lanes start in phase).  Forward (ADJ = false): path_l[path] = the path's radiance, summed per
+// pixel by k_diff_resolve.  Adjoint: the thread replays its path twice, the second time adding the
+// texel gradients of sum(d_image * image).
+S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow) {
+    // warp sums of the ray counts, one 64-bit atomic pair per warp
+    for (int o = 16; o > 0; o >>= 1) { ext += __shfl_xor_sync(0xffffffffu, ext, o); shd += __shfl_xor_sync(0xffffffffu, shd, o); }
+    if ((threadIdx.x & 31u) == 0) { atomicAdd(A.rays, (unsigned long long)ext); atomicAdd(A.rays + 1, (unsigned long long)shd); }
+    if (overflow) atomicOr(A.status, 1);
+}
+
 template <bool LAMBERT, bool ADJ>
 __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs A) {
     __shared__ uint2 stack[S2_STACK_SMEM * 128];
-    const uint32_t pix = blockIdx.x * 128u + threadIdx.x;
-    if (pix >= A.pixels) return;
-    const uint32_t px = pix % A.width, py = pix / A.width;
-    float3 sum = f3(0.f), delta = f3(0.f);
-    if (ADJ) {
-        const float4 d = A.d_image[pix];
-        delta = f3(d.x, d.y, d.z) * A.out_scale;
-    }
+    const uint32_t path = blockIdx.x * 128u + threadIdx.x;
+    const uint32_t n = A.pixels * A.spp;
     uint32_t ext = 0, shd = 0;
     bool overflow = false;
-    for (uint32_t k = 0; k < A.spp; ++k) {
+    if (path < n) {
+        const uint32_t k = path / A.pixels, pix = path - k * A.pixels;
+        const uint32_t px = pix % A.width, py = pix / A.width;
         const float3 l = diff_path<LAMBERT>(A, px, py, k, false, f3(0.f), f3(0.f), stack + threadIdx.x, 128u, ext, shd, overflow);
         if (ADJ) {
+            const float4 d = A.d_image[pix];
+            const float3 delta = f3(d.x, d.y, d.z) * A.out_scale;
             if (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f)
                 diff_path<LAMBERT>(A, px, py, k, true, l, delta, stack + threadIdx.x, 128u, ext, shd, overflow);
         } else {
-            sum = sum + l;
+            A.path_l[path] = make_float4(l.x, l.y, l.z, 0.f);
         }
     }
-    if (!ADJ) A.image[pix] = make_float4(sum.x * A.out_scale, sum.y * A.out_scale, sum.z * A.out_scale, 1.f);
-    atomicAdd(A.rays, (unsigned long long)ext);
-    atomicAdd(A.rays + 1, (unsigned long long)shd);
-    if (overflow) atomicOr(A.status, 1);
+    diff_count(A, ext, shd, overflow);
+}
+
+// image[pixel] = sum of the pixel's path radiances in sample order * 2^exposure / spp.
+__global__ void k_diff_resolve(const __grid_constant__ DiffArgs A) {
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= A.pixels) return;
+    float3 sum = f3(0.f);
+    for (uint32_t k = 0; k < A.spp; ++k) {
+        const float4 l = A.path_l[(size_t)k * A.pixels + pix];
+        sum = sum + f3(l.x, l.y, l.z);
+    }
+    A.image[pix] = make_float4(sum.x * A.out_scale, sum.y * A.out_scale, sum.z * A.out_scale, 1.f);
 }
 
 }  // namespace s2
