@@ -289,10 +289,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "batched": time_to_quality(dev, wl, True, 50000, max_spp=args.quality_spp),
                 "cached_1_bounce": time_to_quality(dev, wl, False, 50000, chunk=1, max_spp=1024, cache_bounces=1),
                 "cached_2_bounces": time_to_quality(dev, wl, False, 50000, chunk=1, max_spp=1024, cache_bounces=2),
+                "batched_cached_1_bounce": time_to_quality(dev, wl, True, 50000, chunk=1, max_spp=1024, cache_bounces=1),
                 "reference_image": f"FP64 oracle, {int(np.load(GOLDEN_CFG2)['spp'])} spp, 64x36 pixel subset (stride 30)",
                 "note": "GPU time of progressive calls (plain/batched: independent 128-spp calls averaged, past the "
                         "budget the expected time from the mean single-call relMSE as relMSE ~ 1/spp; cached: 1 spp "
-                        "frames of the radiance-cache form with online training, measured)"}
+                        "frames of the radiance-cache form with online training, measured; batched_cached: the same "
+                        "through the batched streaming entry point s2_render_views)"}
     if world == 1 and not args.no_quality:
         line["radiance_cache_kernels"] = cache_kernel_line(dev, args.steps)
         line["adjoint"] = adjoint_line(dev)

@@ -208,15 +208,19 @@ void set_infer_attributes(S2Context* ctx) {
     }
 }
 
+// Sets the inference kernel's attributes (once per device); callers that capture
+// cache_apply_device into a CUDA graph call it first.
+void cache_prepare_device(S2Context* ctx) { set_infer_attributes(ctx); }
+
 // Path-tracer terminal vertices: accum[slot] += tput * cache(pos) for up to `cap` queries, the
 // count read from n_dev.
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
-                       float4* accum) {
+                       float4* accum, unsigned long long* total_fx) {
     CacheState* c = ctx->cache;
     set_infer_attributes(ctx);
     const uint32_t tiles = (cap + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
-    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum, total_fx);
     return check_cuda(ctx, cudaGetLastError(), "cache apply launch");
 }
 
@@ -227,7 +231,7 @@ int cache_infer_device(S2Context* ctx, const float4* pos, uint32_t n, float4* ou
     set_infer_attributes(ctx);
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
-    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr, nullptr);
     return check_cuda(ctx, cudaGetLastError(), "cache inference launch");
 }
 }  // namespace s2

@@ -11,6 +11,7 @@
 #pragma once
 #include <cuda_fp16.h>
 
+#include "s2_math.cuh"
 #include "s2_tc.cuh"
 
 namespace s2 {
@@ -169,12 +170,14 @@ S2D void tmem_relu_to_tile(uint32_t tlane, uint32_t col, uint8_t* dst, uint32_t 
 
 // Radiance cache inference: out[i] = MLP(encode(pos[i])), raw (unclamped) outputs.  With `tput`
 // (the path tracer's terminal vertices) the result is instead added to the path's accumulator:
-// accum[slot] += tput[i] * max(y, 0), slot in pos[i].w.  n_dev (optional) caps n with a device count.
+// accum[slot] += tput[i] * max(y, 0), slot in pos[i].w, or with `total_fx` (the batched renderer)
+// to the pixel's fixed-point totals.  n_dev (optional) caps n with a device count.
 // Persistent: grid-stride over tiles of 128 queries; 128 threads; kInfSmemBytes dynamic smem.
 __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
                                                                 uint32_t n, const uint32_t* __restrict__ n_dev,
                                                                 float4* __restrict__ out, const float4* __restrict__ tput,
-                                                                float4* __restrict__ accum) {
+                                                                float4* __restrict__ accum,
+                                                                unsigned long long* __restrict__ total_fx) {
     if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar;
@@ -258,9 +261,16 @@ __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_con
                     const uint32_t slot = __float_as_uint(pos[q].w);
                     const float r = fmaxf(v[0], 0.f) * tp.x, g = fmaxf(v[1], 0.f) * tp.y, b = fmaxf(v[2], 0.f) * tp.z;
                     if (isfinite(r) && isfinite(g) && isfinite(b)) {
-                        float4 a = accum[slot];
-                        a.x += r; a.y += g; a.z += b;
-                        accum[slot] = a;
+                        if (total_fx) {
+                            unsigned long long* tf = total_fx + 4 * (size_t)slot;
+                            if (r > 0.f) atomicAdd(tf + 0, (unsigned long long)__float2ull_rn(r * S2_FX_SCALE));
+                            if (g > 0.f) atomicAdd(tf + 1, (unsigned long long)__float2ull_rn(g * S2_FX_SCALE));
+                            if (b > 0.f) atomicAdd(tf + 2, (unsigned long long)__float2ull_rn(b * S2_FX_SCALE));
+                        } else {
+                            float4 a = accum[slot];
+                            a.x += r; a.y += g; a.z += b;
+                            accum[slot] = a;
+                        }
                     }
                 } else {
                     out[q] = make_float4(v[0], v[1], v[2], 0.f);

@@ -67,7 +67,8 @@ void destroy_render_state(S2Context* ctx);
 void destroy_cache_state(S2Context* ctx);
 // radiance cache entry points used by the renderer (s2_cache.cu)
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
-                       float4* accum);
+                       float4* accum, unsigned long long* total_fx = nullptr);
+void cache_prepare_device(S2Context* ctx);
 int cache_backward_device(S2Context* ctx, const float4* pos, const float4* target, uint32_t n, const uint32_t* n_dev);
 int cache_adam_device(S2Context* ctx, uint32_t n, const uint32_t* n_dev);
 }  // namespace s2

@@ -2,6 +2,10 @@
 // Each function states the reference shader function it restates (paths relative to the
 // Stratum2 source tree).
 #pragma once
+
+// fixed-point scale of the batched accumulators: integer sums are independent of the order of the
+// (atomic) additions, so batched renders are deterministic
+#define S2_FX_SCALE 16777216.0f
 #include <cuda_runtime.h>
 #include <stdint.h>
 

@@ -524,6 +524,9 @@ struct BatchState {
     unsigned long long* done_host = nullptr;  // pinned
     float4* stage_rad = nullptr;
     uint64_t accumulated_spp = 0;
+    std::vector<DevBuf> tbufs;     // radiance-cache training-path accumulators
+    float4* train_accum = nullptr;
+    uint32_t train_cap = 0;
 };
 
 BatchState* g_batch_for(S2Context* ctx);
@@ -574,9 +577,12 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
-    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE))
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE, S2_FLAG_RESTIR_SCREEN and S2_FLAG_RADIANCE_CACHE are "
-                                                  "supported by s2_render only");
+    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RESTIR_SCREEN are supported by s2_render only");
+    const bool cache = (prm->flags & S2_FLAG_RADIANCE_CACHE) != 0;
+    if (cache && !ctx->cache) return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RADIANCE_CACHE needs s2_cache_init");
+    // radiance cache: training paths are extra paths after the views' (their own accumulators)
+    const uint32_t train_paths = cache ? (prm->cache_train_paths ? prm->cache_train_paths : 65536u) : 0u;
     cudaSetDevice(ctx->device);
     std::vector<ViewEntry> ve(nviews);
     std::vector<uint32_t> layout;
@@ -603,7 +609,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (!B) return set_error(ctx, S2_ERR_OOM, "batch state allocation failed");
     cudaStream_t s = ctx->stream;
     const uint64_t wave = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : kDefaultWavePaths);
-    const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(wave, paths));
+    const uint32_t capacity = (uint32_t)std::max<uint64_t>(1024, std::min<uint64_t>(wave, paths + train_paths));
     if (B->capacity < capacity) {
         free_bufs(B->qbufs);
         B->capacity = 0;
@@ -688,7 +694,9 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     P.nviews = nviews;
     P.view_spp = prm->spp;
     P.total_fx = B->total_fx;
-    P.total_paths = paths;
+    P.total_paths = paths + train_paths;
+    P.image_paths = paths;
+    P.batch_pixels = (uint32_t)pixels;
     P.capacity = capacity;
     P.stream_state = B->stream_state;
     P.pixels = 1;  // unused in batched mode
@@ -704,10 +712,32 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         if (rc != S2_OK) return set_error(ctx, rc, "material-sort buffer allocation failed");
         P.sort_on = 1; P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
     }
+    if (cache) {
+        // terminal-vertex queries of one iteration (at most a queue) and the training vertices of the
+        // call; training paths accumulate into train_accum (zeroed per call)
+        const uint64_t tr_cap64 = std::min<uint64_t>((uint64_t)train_paths * std::max(1u, prm->max_path_length), 1u << 26);
+        int rc = ensure_cache_queues(ctx, st, capacity, (uint32_t)tr_cap64);
+        if (rc != S2_OK) return set_error(ctx, rc, "radiance cache queue allocation failed");
+        if (B->train_cap < train_paths) {
+            free_bufs(B->tbufs);
+            B->train_cap = 0;
+            B->train_accum = (float4*)dev_alloc(ctx, B->tbufs, sizeof(float4) * (size_t)train_paths);
+            if (!B->train_accum) return set_error(ctx, S2_ERR_OOM, "training accumulator allocation failed");
+            B->train_cap = train_paths;
+        }
+        cudaMemsetAsync(B->train_accum, 0, sizeof(float4) * (size_t)train_paths, s);
+        cache_prepare_device(ctx);  // kernel attributes, outside the graph capture
+        P.accum = B->train_accum;
+        P.cache_on = 1;
+        P.cache_len = (prm->cache_bounces ? prm->cache_bounces : 2u) + 1u;
+        P.cq_pos = st->cq_pos; P.cq_thr = st->cq_thr; P.cq_cap = st->cq_cap;
+        P.tr_pos = st->tr_pos; P.tr_thr = st->tr_thr; P.tr_rad = st->tr_rad; P.tr_cap = st->tr_cap;
+    }
     const bool lam = (prm->flags & S2_FLAG_LAMBERTIAN) != 0, restir = (prm->flags & S2_FLAG_RESTIR_DI) != 0;
     const bool count = (prm->flags & S2_FLAG_COUNT_FETCHES) != 0;
+    int apply_rc = S2_OK;
     // one graph = two iterations (parity 0 and 1) of setup, regeneration, extend, [material sort,]
-    // shade, occlude
+    // shade, [radiance-cache inference for the terminal vertices,] occlude
     auto iteration = [&](uint32_t parity, int first) {
         k_stream_setup<<<1, 32, 0, s>>>(P, parity, first);
         k_regen<<<std::min<uint32_t>((capacity + 255) / 256, 148u * 16u), 256, 0, s>>>(P, parity);
@@ -716,6 +746,10 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         if (sort) launch_sort(P, parity, st->sort_blocks, s);
         if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
         else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
+        if (cache) {
+            const int r = cache_apply_device(ctx, st->cq_pos, st->cq_thr, st->cq_cap, B->counters + C_CACHEQ, nullptr, B->total_fx);
+            if (r != S2_OK) apply_rc = r;
+        }
         if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
         else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
     };
@@ -730,12 +764,14 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     rc = check_cuda(ctx, cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
     if (rc == S2_OK) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
     if (rc != S2_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
-    const uint64_t per_iter = sort ? 8 : 5;
+    if (apply_rc != S2_OK) { cudaGraphExecDestroy(exec); cudaGraphDestroy(graph); return apply_rc; }
+    const uint64_t per_iter = (sort ? 8 : 5) + (cache ? 1 : 0);
     uint64_t launches = per_iter;
     // replay until the device reports every path finished; the check trails one group behind so
     // the host never waits on the group it just queued
-    const uint64_t lower = (paths + capacity - 1) / capacity;
-    const uint64_t cap_iters = paths * (uint64_t)std::max(1u, prm->max_path_length) / std::max<uint64_t>(1, capacity) + prm->max_path_length + 4;
+    const uint64_t lower = (paths + train_paths + capacity - 1) / capacity;
+    const uint64_t cap_iters = (paths + train_paths) * (uint64_t)std::max(1u, prm->max_path_length) / std::max<uint64_t>(1, capacity) +
+                               prm->max_path_length + 4;
     const uint32_t group = 4;  // graph launches (8 iterations) per done check
     uint64_t iters = 1;
     cudaEvent_t pending = nullptr;
@@ -758,6 +794,14 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     if (!*B->done_host) return set_error(ctx, S2_ERR_DEVICE, "batched render did not finish within its iteration bound");
+    if (cache) {
+        // online training on this call's training paths (as after each wave of s2_render)
+        k_cache_targets<<<std::max(1, st->shade_blocks / 2), 256, 0, s>>>(P);
+        rc = cache_backward_device(ctx, st->tr_pos, st->tr_rad, st->tr_cap, B->counters + C_TRAIN);
+        if (rc == S2_OK) rc = cache_adam_device(ctx, st->tr_cap, B->counters + C_TRAIN);
+        if (rc != S2_OK) return rc;
+        launches += 4;
+    }
     B->accumulated_spp += prm->spp;
     const float scale = (float)(1.0 / (double)B->accumulated_spp) * exp2f(prm->exposure);
     for (uint32_t v = 0; v < nviews; ++v) {
@@ -787,6 +831,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     rc = check_cuda(ctx, cudaStreamSynchronize(s), "batched render");
     free_bufs(stage);
     if (rc != S2_OK) return rc;
+    if (status & 4) return set_error(ctx, S2_ERR_TIMEOUT, "tensor-core wait timed out in the radiance cache");
     if (status) return set_error(ctx, S2_ERR_DEVICE, "traversal stack overflow during render");
     if (stats_out) {
         std::memset(stats_out, 0, sizeof(*stats_out));

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                         tr = true;
                         c_pos = pw;
                         c_thr = make_float4(thr.x, thr.y, thr.z, 0.f);
-                        c_rad = P.accum[slot];
+                        c_rad = P.accum[slot & ~kTrainSlot];
                     }
                 }
                 if (!cached && len < P.max_len && any_pos(m.base())) {

@@ -81,6 +81,8 @@ struct PTParams {
     // path-space size and queue capacity; null / 0 in wave mode
     const ViewEntry* views;
     uint32_t nviews, view_spp;
+    unsigned long long image_paths;  // batched: paths of the views; ids beyond are training paths
+    uint32_t batch_pixels;
     unsigned long long* total_fx;   // 4 x u64 per pixel: r, g, b fixed point (2^-24), unused
     unsigned long long total_paths;
     uint32_t capacity;
@@ -120,13 +122,19 @@ struct PTParams {
 
 constexpr uint32_t kSortBuckets = 4096;  // k_sort_scan: 1024 threads x 4 buckets
 
-// fixed-point scale of the batched accumulators: integer sums are independent of the order of the
-// (atomic) additions, so batched renders are deterministic
-#define S2_FX_SCALE 16777216.0f
 
 // Adds a contribution to a path's accumulator: an exclusive float slot in wave mode, or an atomic
 // fixed-point add into the pixel's total in batched mode.
+// Batched mode: pixel slots accumulate in fixed point; slots with bit 31 set are radiance-cache
+// training paths, which accumulate their own radiance in accum[slot & 0x7fffffff] (the training
+// targets need it per path) and add nothing to the image.
+constexpr uint32_t kTrainSlot = 0x80000000u;
 S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
+    if (P.total_fx && (slot & kTrainSlot)) {
+        float* a = (float*)(P.accum + (slot & ~kTrainSlot));
+        atomicAdd(a + 0, v.x); atomicAdd(a + 1, v.y); atomicAdd(a + 2, v.z);
+        return;
+    }
     if (P.total_fx) {
         unsigned long long* t = P.total_fx + 4 * (size_t)slot;
         if (v.x > 0.f) atomicAdd(t + 0, (unsigned long long)__float2ull_rn(v.x * S2_FX_SCALE));
@@ -267,11 +275,33 @@ __global__ void k_stream_setup(PTParams P, uint32_t parity, int first) {
     P.counters[C_SHADOW] = 0;
     P.counters[C_WORK_EXT] = 0;
     P.counters[C_WORK_OCC] = 0;
+    P.counters[C_CACHEQ] = 0;
 }
 
 // New camera paths for path ids [base, base + fill), appended after the live paths.
 S2D void regen_one(const PTParams& P, uint32_t parity, uint32_t fill, uint32_t i) {
     const unsigned long long id = P.stream_state[1] + i;
+    const uint32_t q = P.counters[parity] - fill + i;
+    const PathQueue& Q = P.q[parity];
+    if (id >= P.image_paths) {
+        // radiance-cache training path: a seeded pixel of the batch, its own sample seed, slot =
+        // its training accumulator (bit 31), meta bit 9 (runs to its end and records its vertices)
+        const uint32_t ti = (uint32_t)(id - P.image_paths);
+        const uint32_t g = pcg_hash(ti ^ pcg_hash(P.frame_seed ^ 0x9e3779b9u)) % P.batch_pixels;
+        uint32_t v = 0;
+        while (v + 1 < P.nviews && P.views[v + 1].pixel_offset <= g) ++v;
+        const ViewEntry& V = P.views[v];
+        const uint32_t pix = g - V.pixel_offset, px = pix % V.width, py = pix / V.width;
+        Rng rng = make_rng(px, py, P.frame_seed + P.view_spp + ti, (P.flags & S2F_PCG32) != 0);
+        float ox = 0.5f, oy = 0.5f;
+        if (P.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
+        const float3 d = camera_dir(V.proj, V.imin, V.imax, V.cam, px, py, ox, oy);
+        Q.s0[q] = make_float4(V.cam[3], V.cam[7], V.cam[11], 0.f);
+        Q.s1[q] = make_float4(d.x, d.y, d.z, 1.f);
+        Q.s2[q] = make_float4(1.f, 1.f, __uint_as_float(kTrainSlot | ti), __uint_as_float(0x200u | (v << 16)));
+        Q.s3[q] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+        return;
+    }
     uint32_t v = 0;
     while (v + 1 < P.nviews && P.views[v + 1].path_offset <= id) ++v;
     const ViewEntry& V = P.views[v];
@@ -289,8 +319,6 @@ S2D void regen_one(const PTParams& P, uint32_t parity, uint32_t fill, uint32_t i
     const float3 d = camera_dir(V.proj, V.imin, V.imax, V.cam, px, py, ox, oy);
     // meta: path length 0, bit 8 = write AOVs, bits 16..23 = view
     const uint32_t meta = (sample == 0 ? 0x100u : 0u) | (v << 16);
-    const uint32_t q = P.counters[parity] - fill + i;
-    const PathQueue& Q = P.q[parity];
     Q.s0[q] = make_float4(V.cam[3], V.cam[7], V.cam[11], 0.f);
     Q.s1[q] = make_float4(d.x, d.y, d.z, 1.f);
     Q.s2[q] = make_float4(1.f, 1.f, __uint_as_float(V.pixel_offset + pix), __uint_as_float(meta));
@@ -476,7 +504,7 @@ namespace s2 {
 __global__ void k_cache_targets(PTParams P) {
     const uint32_t n = min(P.counters[C_TRAIN], P.tr_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = __float_as_uint(P.tr_pos[i].w);
+        const uint32_t slot = __float_as_uint(P.tr_pos[i].w) & ~kTrainSlot;
         const float4 fin = P.accum[slot], r0 = P.tr_rad[i], t = P.tr_thr[i];
         const float tx = t.x > 1e-8f ? (fin.x - r0.x) / t.x : 0.f;
         const float ty = t.y > 1e-8f ? (fin.y - r0.y) / t.y : 0.f;
