@@ -169,7 +169,10 @@ typedef struct S2View {
                                                   vertex cache_bounces + 1 with the cache's
                                                   scattered radiance there, and one path in
                                                   (paths / cache_train_paths) runs to its end and
-                                                  trains the cache after each wave (s2_render only) */
+                                                  trains the cache after each wave; in
+                                                  s2_render_views the cache_train_paths training
+                                                  paths are extra paths with their own
+                                                  accumulators, and training follows each call */
 #define S2_FLAG_RESTIR_SCREEN       (1u << 15) /* screen-space ReSTIR DI reuse (no counterpart in the
                                                   reference, which reuses through the hash grid of
                                                   S2_FLAG_RESTIR_REUSE; exclusive with it): with
