@@ -399,6 +399,67 @@ int  s2_cache_train(S2Context* ctx, const float* positions, const float* targets
 int  s2_cache_gradients(S2Context* ctx, const float* positions, const float* targets, uint32_t n,
                         float* grad_weights, float* grad_table, float* loss, int on_device);
 
+/* ---- post-processing (replaces the Denoiser's temporal accumulation and the Tonemapper) ---- */
+/* Temporal accumulation (src/Shaders/kernels/svgf/temporal_accumulation.slang:34-129, driven by
+ * Denoiser.cpp:121-201): a running average of the frames rendered by s2_render, reprojected
+ * through the prev_uv AOV with per-tap instance / normal / depth rejection.  The context keeps the
+ * history (previous accumulated colour and moments, visibility and depth). */
+#define S2_TEMPORAL_REPROJECT          (1u << 0)  /* gReprojection (default on, Denoiser.cpp:24) */
+#define S2_TEMPORAL_CHECK_NORMAL       (1u << 1)  /* gCheckNormal (default on) */
+#define S2_TEMPORAL_CHECK_DEPTH        (1u << 2)  /* gCheckDepth (default on) */
+#define S2_TEMPORAL_DEMODULATE_ALBEDO  (1u << 3)  /* gDemodulateAlbedo */
+#define S2_TEMPORAL_SHADOW_HYSTERESIS  (1u << 4)  /* gShadowHysteresis */
+#define S2_TEMPORAL_RESET              (1u << 5)  /* drop the history first (mResetAccumulation) */
+
+typedef struct S2TemporalParams {
+    uint32_t flags;                  /* S2_TEMPORAL_* */
+    uint32_t history_limit;          /* mHistoryLimit: cap of the accumulated count, 0 = none */
+    float shadow_preserve_offset;    /* mShadowPreserveOffset (0.1) */
+    float shadow_preserve_scale;     /* mShadowPreserveScale (1) */
+} S2TemporalParams;
+
+/* The reference's defaults: reprojection with normal and depth checks, no history limit. */
+void s2_default_temporal_params(S2TemporalParams* p);
+/* One frame: `frame` holds the DEVICE AOVs of one s2_render call of `view` (radiance and, with
+ * reprojection, visibility, depth and prev_uv; albedo when demodulating).  instance_index_map
+ * (device, may be NULL = identity) maps this frame's instance ids to the previous frame's
+ * (mInstanceIndexMap).  Writes the accumulated colour (float4: rgb, sample count) and, when not
+ * NULL, the luminance moments (float2) to DEVICE buffers of the view's extent.  The first call, a
+ * reset or a change of extent starts a new history. */
+int  s2_temporal_accumulate(S2Context* ctx, const S2View* view, const S2TemporalParams* params, const S2Aovs* frame,
+                            const uint32_t* instance_index_map, float* accum_color, float* accum_moments);
+
+/* Tonemapping (src/Shaders/kernels/tonemap.slang:113-192, Tonemapper.cpp:49-97): maximum reduce,
+ * radiance x 2^exposure, one operator, optional gamma.  Modes follow TonemapMode
+ * (compat/tonemap.h). */
+#define S2_TONEMAP_RAW                       0u
+#define S2_TONEMAP_REINHARD                  1u
+#define S2_TONEMAP_REINHARD_EXTENDED         2u
+#define S2_TONEMAP_REINHARD_LUMINANCE        3u
+#define S2_TONEMAP_REINHARD_LUMINANCE_EXT    4u
+#define S2_TONEMAP_UNCHARTED2                5u
+#define S2_TONEMAP_FILMIC                    6u
+#define S2_TONEMAP_ACES                      7u
+#define S2_TONEMAP_ACES_APPROX               8u
+#define S2_TONEMAP_VIRIDIS_R                 9u
+#define S2_TONEMAP_VIRIDIS_LENGTH_RGB       10u
+#define S2_TONEMAP_GAMMA            (1u << 0)  /* standard sRGB encoding of the result */
+#define S2_TONEMAP_GAMMA_REFERENCE  (1u << 1)  /* the reference's rgbToSrgb (compat/common.h:88-93),
+                                                  pow(1.055 x, 1/2.4) - 0.055, which is not sRGB:
+                                                  compatibility mode */
+
+typedef struct S2TonemapParams {
+    uint32_t mode;                   /* S2_TONEMAP_RAW .. S2_TONEMAP_VIRIDIS_LENGTH_RGB */
+    float exposure;                  /* mExposure: radiance x 2^exposure */
+    uint32_t flags;                  /* S2_TONEMAP_GAMMA / S2_TONEMAP_GAMMA_REFERENCE */
+    uint32_t reserved;
+} S2TonemapParams;
+
+/* DEVICE float4 images of width x height; `albedo` (may be NULL) modulates the input
+ * (gModulateAlbedo: radiance x (0.01 + albedo), and albedo x radiance in the maximum). */
+int  s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2TonemapParams* params, const float* input,
+                const float* albedo, float* output);
+
 #ifdef __cplusplus
 }
 #endif

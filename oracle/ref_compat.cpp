@@ -6,6 +6,7 @@
 
 namespace stm2 { class Node; }
 
+#include <Shaders/compat/common.h>
 #include <Shaders/compat/material_data.h>
 #include <Shaders/compat/scene.h>
 #include <Shaders/compat/transform.h>
@@ -81,6 +82,17 @@ void ref_back_project(const float* proj, float cx, float cy, float* out) {
     const float3 r = p.backProject(float2(cx, cy));
     out[0] = r[0]; out[1] = r[1]; out[2] = r[2];
 }
+
+// colour helpers of compat/common.h (51, 88-104): rgbToSrgb, viridisQuintic, luminance
+void ref_rgb_to_srgb(const float* rgb, float* out) {
+    const float3 r = rgbToSrgb(float3(rgb[0], rgb[1], rgb[2]));
+    out[0] = r[0]; out[1] = r[1]; out[2] = r[2];
+}
+void ref_viridis(float x, float* out) {
+    const float3 r = viridisQuintic(x);
+    out[0] = r[0]; out[1] = r[1]; out[2] = r[2];
+}
+float ref_luminance(const float* rgb) { return luminance(float3(rgb[0], rgb[1], rgb[2])); }
 
 // sizes of the shared structs
 void ref_sizes(uint32_t* out) {

@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = [
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
     "s2_set_tuning", "s2_get_tuning", "s2_autotune",
+    "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -148,6 +149,23 @@ class S2Tuning(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
 
+TEMPORAL_REPROJECT, TEMPORAL_CHECK_NORMAL, TEMPORAL_CHECK_DEPTH = 1 << 0, 1 << 1, 1 << 2
+TEMPORAL_DEMODULATE_ALBEDO, TEMPORAL_SHADOW_HYSTERESIS, TEMPORAL_RESET = 1 << 3, 1 << 4, 1 << 5
+(TONEMAP_RAW, TONEMAP_REINHARD, TONEMAP_REINHARD_EXTENDED, TONEMAP_REINHARD_LUMINANCE, TONEMAP_REINHARD_LUMINANCE_EXT,
+ TONEMAP_UNCHARTED2, TONEMAP_FILMIC, TONEMAP_ACES, TONEMAP_ACES_APPROX, TONEMAP_VIRIDIS_R,
+ TONEMAP_VIRIDIS_LENGTH_RGB) = range(11)
+TONEMAP_GAMMA, TONEMAP_GAMMA_REFERENCE = 1 << 0, 1 << 1
+
+
+class S2TemporalParams(C.Structure):
+    _fields_ = [("flags", C.c_uint32), ("history_limit", C.c_uint32), ("shadow_preserve_offset", C.c_float),
+                ("shadow_preserve_scale", C.c_float)]
+
+
+class S2TonemapParams(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("exposure", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class S2RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
                 ("nan_count", C.c_uint64), ("gpu_ms", C.c_double), ("kernel_launches", C.c_uint64),
@@ -194,6 +212,11 @@ def lib() -> C.CDLL:
     L.s2_default_render_params.restype = None
     L.s2_update_image.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
     L.s2_set_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
+    L.s2_default_temporal_params.restype = None
+    L.s2_default_temporal_params.argtypes = [P(S2TemporalParams)]
+    L.s2_temporal_accumulate.argtypes = [C.c_void_p, P(S2View), P(S2TemporalParams), P(S2Aovs), C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+    L.s2_tonemap.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(S2TonemapParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_get_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
     L.s2_autotune.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Tuning), P(C.c_uint32)]
     L.s2_render_diff.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, P(S2RenderStats)]

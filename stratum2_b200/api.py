@@ -296,6 +296,27 @@ class Device:
         return loss.value
 
     # ---- tuning
+    # ---- post-processing (device buffers, e.g. torch tensors' data_ptr())
+    @staticmethod
+    def default_temporal_params() -> _abi.S2TemporalParams:
+        p = _abi.S2TemporalParams()
+        _abi.lib().s2_default_temporal_params(C.byref(p))
+        return p
+
+    def temporal_accumulate(self, view, params: _abi.S2TemporalParams, frame: _abi.S2Aovs, accum_color_ptr: int,
+                            accum_moments_ptr: int | None = None, instance_index_map_ptr: int | None = None):
+        """One frame of temporal accumulation (s2_temporal_accumulate) over the device AOVs in `frame`."""
+        self._check(self._lib.s2_temporal_accumulate(self._h, C.byref(view), C.byref(params), C.byref(frame),
+                                                     C.c_void_p(instance_index_map_ptr) if instance_index_map_ptr else None,
+                                                     C.c_void_p(accum_color_ptr),
+                                                     C.c_void_p(accum_moments_ptr) if accum_moments_ptr else None))
+
+    def tonemap(self, width: int, height: int, params: _abi.S2TonemapParams, input_ptr: int, output_ptr: int,
+                albedo_ptr: int | None = None):
+        """Tonemaps a device float4 image (s2_tonemap)."""
+        self._check(self._lib.s2_tonemap(self._h, width, height, C.byref(params), C.c_void_p(input_ptr),
+                                         C.c_void_p(albedo_ptr) if albedo_ptr else None, C.c_void_p(output_ptr)))
+
     def set_tuning(self, tuning: _abi.S2Tuning | None):
         self._check(self._lib.s2_set_tuning(self._h, C.byref(tuning) if tuning is not None else None))
 

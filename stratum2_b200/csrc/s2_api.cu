@@ -255,6 +255,7 @@ extern "C" void s2_destroy(S2Context* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     destroy_render_state(ctx);
     destroy_cache_state(ctx);
+    destroy_post_state(ctx);
     free_bufs(ctx->scene_bufs);
     free_bufs(ctx->bvh_bufs);
     if (ctx->status_dev) cudaFree(ctx->status_dev);

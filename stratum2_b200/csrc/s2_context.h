@@ -19,6 +19,7 @@ struct DevBuf {
 
 struct RenderState;  // wavefront queues and accumulators (s2_render.cu)
 struct CacheState;   // learned radiance cache parameters and optimiser state (s2_cache.cu)
+struct PostState;    // temporal-accumulation history and tonemap scratch (s2_post.cu)
 
 struct HostImage {
     uint32_t w = 0, h = 0;
@@ -54,6 +55,7 @@ struct S2Context {
 
     s2::RenderState* render = nullptr;
     s2::CacheState* cache = nullptr;
+    s2::PostState* post = nullptr;
     S2Tuning tuning{};                      // wavefront renderer tuning (zeros = defaults)
     int* status_dev = nullptr;              // device status word (stack/queue overflow, timeouts)
 };
@@ -65,6 +67,7 @@ void* dev_alloc(S2Context* ctx, std::vector<DevBuf>& owner, size_t bytes);
 void free_bufs(std::vector<DevBuf>& bufs);
 void destroy_render_state(S2Context* ctx);
 void destroy_cache_state(S2Context* ctx);
+void destroy_post_state(S2Context* ctx);
 // radiance cache entry points used by the renderer (s2_cache.cu)
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
                        float4* accum, unsigned long long* total_fx = nullptr);
