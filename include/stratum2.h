@@ -429,6 +429,36 @@ void s2_default_temporal_params(S2TemporalParams* p);
 int  s2_temporal_accumulate(S2Context* ctx, const S2View* view, const S2TemporalParams* params, const S2Aovs* frame,
                             const uint32_t* instance_index_map, float* accum_color, float* accum_moments);
 
+/* SVGF filter over the context's accumulation history (Denoiser.cpp:202-241:
+ * svgf/estimate_variance.slang, then `iterations` passes of svgf/atrous.slang with step 2^i).
+ * Call after s2_temporal_accumulate for the same view and frame. */
+#define S2_SVGF_KERNEL_ATROUS            0u  /* FilterKernelType (compat/filter_type.h) */
+#define S2_SVGF_KERNEL_BOX3              1u  /* the reference's default */
+#define S2_SVGF_KERNEL_BOX5              2u
+#define S2_SVGF_KERNEL_SUBSAMPLED        3u
+#define S2_SVGF_KERNEL_BOX3_SUBSAMPLED   4u
+#define S2_SVGF_KERNEL_BOX5_SUBSAMPLED   5u
+
+typedef struct S2SvgfParams {
+    uint32_t iterations;             /* mAtrousIterations (1..16) */
+    uint32_t kernel;                 /* S2_SVGF_KERNEL_* */
+    uint32_t history_tap;            /* mHistoryTap: after this iteration (1-based) the filtered colour
+                                        replaces the history's colour (0 = never) */
+    uint32_t flags;                  /* S2_TEMPORAL_CHECK_NORMAL / S2_TEMPORAL_CHECK_DEPTH edge stops */
+    uint32_t history_limit;          /* mHistoryLimit: histories shorter than it get a spatial
+                                        variance estimate (0: never, as in the reference default) */
+    float variance_boost_length;     /* mVarianceBoostLength (4) */
+    float sigma_luminance_boost;     /* mSigmaLuminanceBoost (3) */
+    uint32_t reserved;
+} S2SvgfParams;
+
+/* The reference's Denoiser defaults with 5 iterations (mAtrousIterations is 0 = off there). */
+void s2_default_svgf_params(S2SvgfParams* p);
+/* `frame` holds the same DEVICE visibility and depth AOVs as the accumulation call; output is a
+ * DEVICE float4 image of the view's extent (rgb filtered, a = filtered variance). */
+int  s2_svgf_filter(S2Context* ctx, const S2View* view, const S2SvgfParams* params, const S2Aovs* frame,
+                    const uint32_t* instance_index_map, float* output);
+
 /* Tonemapping (src/Shaders/kernels/tonemap.slang:113-192, Tonemapper.cpp:49-97): maximum reduce,
  * radiance x 2^exposure, one operator, optional gamma.  Modes follow TonemapMode
  * (compat/tonemap.h). */

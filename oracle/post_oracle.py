@@ -198,3 +198,96 @@ def tonemap(img, mode, exposure=0.0, gamma=False, gamma_reference=False, albedo=
     elif gamma:
         c = rgb_to_srgb(c)
     return np.concatenate([c, np.ones(c.shape[:-1] + (1,))], -1)
+
+
+# ------------------------------------------------------------------------------ SVGF
+def svgf_variance(color, moments, vis, depth, flags, history_limit=0, boost=4.0, instance_map=None):
+    """estimate_variance.slang main (:26-74): (H, W, 4) of (rgb, variance)."""
+    H, W = color.shape[:2]
+    out = np.zeros((H, W, 4))
+    for y in range(H):
+        for x in range(W):
+            c = color[y, x].astype(np.float64).copy()
+            m = moments[y, x].astype(np.float64).copy()
+            inst = int(vis[y, x, 0]) & 0xFFFF
+            if inst == 0xFFFF or c[3] >= history_limit:
+                out[y, x] = (*c[:3], abs(m[1] - m[0] ** 2))
+                continue
+            n = unpack_normal(vis[y, x, 1])
+            mapped = instance_map[inst] if instance_map is not None else inst
+            d = depth[y, x]
+            sw = 1.0
+            r = 2 if c[3] > 1 else 3
+            for yy in range(-r, r + 1):
+                for xx in range(-r, r + 1):
+                    if xx == 0 and yy == 0:
+                        continue
+                    px, py = x + xx, y + yy
+                    if not (0 <= px < W and 0 <= py < H) or (int(vis[py, px, 0]) & 0xFFFF) != mapped:
+                        continue
+                    wz = abs(depth[py, px, 0] - d[0]) / (np.hypot(d[2] * xx, d[3] * yy) + 1e-2) if flags & CHECK_DEPTH else 0.0
+                    wn = min(max(float(np.dot(unpack_normal(vis[py, px, 1]), n)), 0.0), 1.0) ** 128 if flags & CHECK_NORMAL else 1.0
+                    w = np.exp(-wz) * wn
+                    if not np.isfinite(w):
+                        continue
+                    m = m + moments[py, px] * w
+                    c[:3] = c[:3] + color[py, px, :3] * w
+                    sw += w
+            m, c[:3] = m / sw, c[:3] / sw
+            v = abs(m[1] - m[0] ** 2)
+            if boost > 0:
+                v *= max(1.0, boost / (1 + c[3]))
+            out[y, x] = (*c[:3], v)
+    return out
+
+
+def _svgf_taps(kernel, it, st):
+    if kernel == 4:
+        kernel = 1 if st == 1 else 3
+    if kernel == 5:
+        kernel = 2 if st == 1 else 3
+    if kernel == 0:  # atrous (atrous.slang:136-170)
+        k1 = [1.0, 2 / 3, 1 / 6]
+        return [(xx * st, yy * st, k1[abs(xx) + abs(yy)] if xx == 0 or yy == 0 else k1[abs(xx)] * k1[abs(yy)])
+                for yy in range(-2, 3) for xx in range(-2, 3) if xx or yy]
+    if kernel == 3:  # subsampled (:84-118)
+        pair = [(-2 * st, 0, 1.0), (2 * st, 0, 1.0)] if it % 2 == 0 else [(0, -2 * st, 1.0), (0, 2 * st, 1.0)]
+        return pair + [(-st, st, 1.0), (st, st, 1.0), (-st, -st, 1.0), (st, -st, 1.0)]
+    r = 2 if kernel == 2 else 1
+    return [(xx * st, yy * st, 1.0) for yy in range(-r, r + 1) for xx in range(-r, r + 1) if xx or yy]
+
+
+def svgf_atrous(img, vis, depth, it, kernel, flags, sigma_boost=3.0):
+    """One atrous.slang pass (:180-227), step 2^it."""
+    H, W = img.shape[:2]
+    st = 1 << it
+    out = np.zeros((H, W, 4))
+    for y in range(H):
+        for x in range(W):
+            c = img[y, x].astype(np.float64)
+            s = c[3] / 16.0
+            for yy in (-1, 0, 1):
+                for xx in (-1, 0, 1):
+                    if (xx or yy) and 0 <= x + xx < W and 0 <= y + yy < H:
+                        s += img[y + yy, x + xx, 3] * (1 / 8 if xx == 0 or yy == 0 else 1 / 16)
+            sigma = np.sqrt(max(s, 0.0)) * sigma_boost
+            lc = float(c[:3] @ LUM)
+            nc = unpack_normal(vis[y, x, 1])
+            zc, dz = depth[y, x, 0], depth[y, x, 2:4]
+            acc, sw = c.copy(), 1.0
+            if np.isfinite(zc):
+                for ox, oy, kw in _svgf_taps(kernel, it, st):
+                    px, py = x + ox, y + oy
+                    if not (0 <= px < W and 0 <= py < H):
+                        continue
+                    cp = img[py, px].astype(np.float64)
+                    wl = abs(float(cp[:3] @ LUM) - lc) / max(sigma, 1e-10)
+                    wz = abs(depth[py, px, 0] - zc) / (np.hypot(dz[0] * ox * st, dz[1] * oy * st) + 1e-2) if flags & CHECK_DEPTH else 0.0
+                    wn = max(0.0, float(np.dot(unpack_normal(vis[py, px, 1]), nc))) ** 256 if flags & CHECK_NORMAL else 1.0
+                    w = np.exp(-wl * wl - wz) * kw * wn
+                    if not np.isfinite(w):
+                        continue
+                    acc = acc + cp * np.array([w, w, w, w * w])
+                    sw += w
+            out[y, x] = acc * np.array([1 / sw, 1 / sw, 1 / sw, 1 / sw ** 2])
+    return out

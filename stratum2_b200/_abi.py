@@ -57,7 +57,7 @@ EXPORTED_SYMBOLS = [
     "s2_cache_default_params", "s2_cache_init", "s2_cache_get_params", "s2_cache_set_params", "s2_cache_query",
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
     "s2_set_tuning", "s2_get_tuning", "s2_autotune",
-    "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap",
+    "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap", "s2_default_svgf_params", "s2_svgf_filter",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -162,6 +162,16 @@ class S2TemporalParams(C.Structure):
                 ("shadow_preserve_scale", C.c_float)]
 
 
+(SVGF_KERNEL_ATROUS, SVGF_KERNEL_BOX3, SVGF_KERNEL_BOX5, SVGF_KERNEL_SUBSAMPLED, SVGF_KERNEL_BOX3_SUBSAMPLED,
+ SVGF_KERNEL_BOX5_SUBSAMPLED) = range(6)
+
+
+class S2SvgfParams(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("kernel", C.c_uint32), ("history_tap", C.c_uint32), ("flags", C.c_uint32),
+                ("history_limit", C.c_uint32), ("variance_boost_length", C.c_float), ("sigma_luminance_boost", C.c_float),
+                ("reserved", C.c_uint32)]
+
+
 class S2TonemapParams(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("exposure", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
 
@@ -216,6 +226,9 @@ def lib() -> C.CDLL:
     L.s2_default_temporal_params.argtypes = [P(S2TemporalParams)]
     L.s2_temporal_accumulate.argtypes = [C.c_void_p, P(S2View), P(S2TemporalParams), P(S2Aovs), C.c_void_p, C.c_void_p,
                                          C.c_void_p]
+    L.s2_default_svgf_params.restype = None
+    L.s2_default_svgf_params.argtypes = [P(S2SvgfParams)]
+    L.s2_svgf_filter.argtypes = [C.c_void_p, P(S2View), P(S2SvgfParams), P(S2Aovs), C.c_void_p, C.c_void_p]
     L.s2_tonemap.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(S2TonemapParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_get_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
     L.s2_autotune.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Tuning), P(C.c_uint32)]

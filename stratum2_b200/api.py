@@ -311,6 +311,19 @@ class Device:
                                                      C.c_void_p(accum_color_ptr),
                                                      C.c_void_p(accum_moments_ptr) if accum_moments_ptr else None))
 
+    @staticmethod
+    def default_svgf_params() -> _abi.S2SvgfParams:
+        p = _abi.S2SvgfParams()
+        _abi.lib().s2_default_svgf_params(C.byref(p))
+        return p
+
+    def svgf_filter(self, view, params: _abi.S2SvgfParams, frame: _abi.S2Aovs, output_ptr: int,
+                    instance_index_map_ptr: int | None = None):
+        """SVGF variance estimate + a-trous passes over the accumulation history (s2_svgf_filter)."""
+        self._check(self._lib.s2_svgf_filter(self._h, C.byref(view), C.byref(params), C.byref(frame),
+                                             C.c_void_p(instance_index_map_ptr) if instance_index_map_ptr else None,
+                                             C.c_void_p(output_ptr)))
+
     def tonemap(self, width: int, height: int, params: _abi.S2TonemapParams, input_ptr: int, output_ptr: int,
                 albedo_ptr: int | None = None):
         """Tonemaps a device float4 image (s2_tonemap)."""

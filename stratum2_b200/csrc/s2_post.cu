@@ -29,12 +29,16 @@ struct PostState {
     bool valid = false;
     unsigned int* max_buf = nullptr;  // tonemap maximum (4 x u32)
     std::vector<DevBuf> max_bufs;
+    float4* filter[2] = {nullptr, nullptr};  // SVGF ping-pong images (rgb, variance)
+    std::vector<DevBuf> fbufs;
+    uint32_t filter_pixels = 0;
 };
 
 void destroy_post_state(S2Context* ctx) {
     if (!ctx->post) return;
     free_bufs(ctx->post->bufs);
     free_bufs(ctx->post->max_bufs);
+    free_bufs(ctx->post->fbufs);
     delete ctx->post;
     ctx->post = nullptr;
 }
@@ -154,6 +158,164 @@ __global__ void k_temporal(const __grid_constant__ TemporalArgs A) {
         A.color[ip] = cur;
         A.moments[ip] = make_float2(l, l * l);
     }
+}
+
+// ---------------------------------------------------------------- SVGF
+struct SvgfArgs {
+    uint32_t width, height, flags, history_limit, kernel, iteration;
+    int step;
+    float variance_boost, sigma_boost;
+    const float4* color;      // accumulated colour (rgb, history length)
+    const float2* moments;
+    const uint2* vis;
+    const float4* depth;
+    const uint32_t* instance_map;
+    const float4* in;
+    float4* out;
+};
+
+// estimate_variance.slang main (:26-74): temporal variance from the moments, or for short
+// histories a spatial estimate over a 5x5 (7x7 for one sample) neighbourhood of the same instance.
+__global__ void k_svgf_variance(const __grid_constant__ SvgfArgs A) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= (int)A.width || y >= (int)A.height) return;
+    const uint32_t ip = (uint32_t)y * A.width + (uint32_t)x;
+    float4 c = A.color[ip];
+    float2 m = A.moments[ip];
+    const uint2 vis = A.vis[ip];
+    const uint32_t inst = vis.x & 0xffffu;
+    const float histlen = c.w;
+    if (inst == kInvalidInstance16 || histlen >= (float)A.history_limit) {
+        A.out[ip] = make_float4(c.x, c.y, c.z, fabsf(m.y - m.x * m.x));
+        return;
+    }
+    const float4 dep = A.depth[ip];
+    const float3 n = unpack_normal(vis.y);
+    const uint32_t mapped = A.instance_map ? A.instance_map[inst] : inst;
+    float sum_w = 1.f;
+    const int r = histlen > 1.f ? 2 : 3;
+    for (int yy = -r; yy <= r; ++yy)
+        for (int xx = -r; xx <= r; ++xx) {
+            if (xx == 0 && yy == 0) continue;
+            const int px = x + xx, py = y + yy;
+            if (px < 0 || py < 0 || px >= (int)A.width || py >= (int)A.height) continue;
+            const uint32_t q = (uint32_t)py * A.width + (uint32_t)px;
+            const uint2 vp = A.vis[q];
+            if (mapped != (vp.x & 0xffffu)) continue;
+            const float dzl = sqrtf(dep.z * dep.z * (float)(xx * xx) + dep.w * dep.w * (float)(yy * yy));
+            const float w_z = (A.flags & S2_TEMPORAL_CHECK_DEPTH) ? fabsf(A.depth[q].x - dep.x) / (dzl + 1e-2f) : 0.f;
+            const float w_n = (A.flags & S2_TEMPORAL_CHECK_NORMAL) ? powf(fminf(fmaxf(dot(unpack_normal(vp.y), n), 0.f), 1.f), 128.f) : 1.f;
+            const float w = expf(-w_z) * w_n;
+            if (isnan(w) || isinf(w)) continue;
+            const float2 mp = A.moments[q];
+            const float4 cp = A.color[q];
+            m = make_float2(m.x + mp.x * w, m.y + mp.y * w);
+            c = make_float4(c.x + cp.x * w, c.y + cp.y * w, c.z + cp.z * w, c.w);
+            sum_w += w;
+        }
+    const float inv = 1.f / sum_w;
+    m = make_float2(m.x * inv, m.y * inv);
+    c = make_float4(c.x * inv, c.y * inv, c.z * inv, c.w);
+    float v = fabsf(m.y - m.x * m.x);
+    if (A.variance_boost > 0.f) v *= fmaxf(1.f, A.variance_boost / (1.f + c.w));
+    A.out[ip] = make_float4(c.x, c.y, c.z, v);
+}
+
+struct SvgfTap {
+    float3 n_c;
+    float z_c;
+    float2 dz_c;
+    float l_c, sigma_l;
+    float4 sum;
+    float sum_w;
+};
+
+// TapData::tap (atrous.slang:63-81); `off` is the offset already scaled by the step, and the depth
+// term scales it by the step once more, as the shader does.
+S2D void svgf_tap(const SvgfArgs& A, SvgfTap& t, int x, int y, int ox, int oy, float kw) {
+    const int px = x + ox, py = y + oy;
+    if (px < 0 || py < 0 || px >= (int)A.width || py >= (int)A.height) return;
+    const uint32_t q = (uint32_t)py * A.width + (uint32_t)px;
+    const float4 cp = A.in[q];
+    const float w_l = fabsf(lum3(f3(cp.x, cp.y, cp.z)) - t.l_c) / fmaxf(t.sigma_l, 1e-10f);
+    float w_z = 0.f;
+    if (A.flags & S2_TEMPORAL_CHECK_DEPTH) {
+        const float sx = t.dz_c.x * (float)(ox * A.step), sy = t.dz_c.y * (float)(oy * A.step);
+        w_z = fabsf(A.depth[q].x - t.z_c) / (sqrtf(sx * sx + sy * sy) + 1e-2f);
+    }
+    const float w_n = (A.flags & S2_TEMPORAL_CHECK_NORMAL) ? powf(fmaxf(0.f, dot(unpack_normal(A.vis[q].y), t.n_c)), 256.f) : 1.f;
+    const float w = expf(-w_l * w_l - w_z) * kw * w_n;
+    if (isinf(w) || isnan(w)) return;
+    t.sum = make_float4(t.sum.x + cp.x * w, t.sum.y + cp.y * w, t.sum.z + cp.z * w, t.sum.w + cp.w * w * w);
+    t.sum_w += w;
+}
+
+// atrous.slang main (:180-227) for one iteration: edge-stopping wavelet filter of `in` into `out`.
+__global__ void k_svgf_atrous(const __grid_constant__ SvgfArgs A) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= (int)A.width || y >= (int)A.height) return;
+    const uint32_t ip = (uint32_t)y * A.width + (uint32_t)x;
+    const uint2 vis = A.vis[ip];
+    const float4 dep = A.depth[ip];
+    SvgfTap t;
+    t.n_c = unpack_normal(vis.y);
+    t.z_c = dep.x;
+    t.dz_c = make_float2(dep.z, dep.w);
+    t.sum_w = 1.f;
+    t.sum = A.in[ip];
+    t.l_c = lum3(f3(t.sum.x, t.sum.y, t.sum.z));
+    {   // compute_sigma_luminance (:48-61): the centre term is weighted by kernel[1][1] as written
+        float s = t.sum.w * (1.f / 16.f);
+        for (int yy = -1; yy <= 1; ++yy)
+            for (int xx = -1; xx <= 1; ++xx) {
+                if (xx == 0 && yy == 0) continue;
+                const int px = x + xx, py = y + yy;
+                if (px < 0 || py < 0 || px >= (int)A.width || py >= (int)A.height) continue;
+                const float k = (xx == 0 || yy == 0) ? (1.f / 8.f) : (1.f / 16.f);
+                s += A.in[(uint32_t)py * A.width + (uint32_t)px].w * k;
+            }
+        t.sigma_l = sqrtf(fmaxf(s, 0.f)) * A.sigma_boost;
+    }
+    if (!isinf(t.z_c)) {  // only foreground pixels
+        const int st = A.step;
+        uint32_t kernel = A.kernel;
+        if (kernel == S2_SVGF_KERNEL_BOX3_SUBSAMPLED) kernel = st == 1 ? S2_SVGF_KERNEL_BOX3 : S2_SVGF_KERNEL_SUBSAMPLED;
+        if (kernel == S2_SVGF_KERNEL_BOX5_SUBSAMPLED) kernel = st == 1 ? S2_SVGF_KERNEL_BOX5 : S2_SVGF_KERNEL_SUBSAMPLED;
+        if (kernel == S2_SVGF_KERNEL_ATROUS) {
+            // 5x5 B3-spline taps (:136-170): 2/3 at distance 1 on the axes, 1/6 at 2, products off-axis
+            const float k1[3] = {1.f, 2.f / 3.f, 1.f / 6.f};
+            for (int yy = -2; yy <= 2; ++yy)
+                for (int xx = -2; xx <= 2; ++xx) {
+                    if (xx == 0 && yy == 0) continue;
+                    const int ax = xx < 0 ? -xx : xx, ay = yy < 0 ? -yy : yy;
+                    const float kw = (ax == 0 || ay == 0) ? k1[ax + ay] : k1[ax] * k1[ay];
+                    svgf_tap(A, t, x, y, xx * st, yy * st, kw);
+                }
+        } else if (kernel == S2_SVGF_KERNEL_SUBSAMPLED) {
+            // (:84-118): alternating horizontal / vertical pair plus the four diagonals
+            if ((A.iteration & 1u) == 0) { svgf_tap(A, t, x, y, -2 * st, 0, 1.f); svgf_tap(A, t, x, y, 2 * st, 0, 1.f); }
+            else { svgf_tap(A, t, x, y, 0, -2 * st, 1.f); svgf_tap(A, t, x, y, 0, 2 * st, 1.f); }
+            svgf_tap(A, t, x, y, -st, st, 1.f);
+            svgf_tap(A, t, x, y, st, st, 1.f);
+            svgf_tap(A, t, x, y, -st, -st, 1.f);
+            svgf_tap(A, t, x, y, st, -st, 1.f);
+        } else {
+            const int r = kernel == S2_SVGF_KERNEL_BOX5 ? 2 : 1;  // box3 (default) / box5
+            for (int yy = -r; yy <= r; ++yy)
+                for (int xx = -r; xx <= r; ++xx)
+                    if (xx != 0 || yy != 0) svgf_tap(A, t, x, y, xx * st, yy * st, 1.f);
+        }
+    }
+    const float inv = 1.f / t.sum_w;
+    A.out[ip] = make_float4(t.sum.x * inv, t.sum.y * inv, t.sum.z * inv, t.sum.w * inv * inv);
+}
+
+// copy_rgb (:229-236): the filtered colour of filter image 0 becomes the history's colour.
+__global__ void k_svgf_copy_rgb(float4* __restrict__ color, const float4* __restrict__ filtered, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 f = filtered[i];
+    color[i] = make_float4(f.x, f.y, f.z, color[i].w);
 }
 
 // ---------------------------------------------------------------- tonemapping
@@ -361,6 +523,71 @@ extern "C" int s2_temporal_accumulate(S2Context* ctx, const S2View* view, const 
     ps->cur ^= 1u;
     ps->valid = true;
     return S2_OK;
+}
+
+extern "C" void s2_default_svgf_params(S2SvgfParams* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->iterations = 5;
+    p->kernel = S2_SVGF_KERNEL_BOX3;              // Denoiser.hpp:50
+    p->history_tap = 0;                           // Denoiser.hpp:49
+    p->flags = S2_TEMPORAL_CHECK_NORMAL | S2_TEMPORAL_CHECK_DEPTH;
+    p->history_limit = 0;
+    p->variance_boost_length = 4.f;               // Denoiser.hpp:55
+    p->sigma_luminance_boost = 3.f;               // Denoiser.hpp:56
+}
+
+extern "C" int s2_svgf_filter(S2Context* ctx, const S2View* view, const S2SvgfParams* prm, const S2Aovs* frame,
+                              const uint32_t* instance_index_map, float* output) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!view || !prm || !frame || !output) return set_error(ctx, S2_ERR_INVALID, "view, params, frame and output are required");
+    if (!frame->visibility || !frame->depth) return set_error(ctx, S2_ERR_INVALID, "the SVGF filter needs the visibility and depth AOVs");
+    if (prm->iterations == 0 || prm->iterations > 16) return set_error(ctx, S2_ERR_INVALID, "iterations must be in 1..16");
+    if (prm->kernel > S2_SVGF_KERNEL_BOX5_SUBSAMPLED) return set_error(ctx, S2_ERR_INVALID, "unknown SVGF kernel");
+    const int W = view->image_max[0] - view->image_min[0], H = view->image_max[1] - view->image_min[1];
+    PostState* ps = ctx->post;
+    if (!ps || !ps->valid || ps->width != (uint32_t)W || ps->height != (uint32_t)H)
+        return set_error(ctx, S2_ERR_INVALID, "s2_svgf_filter needs a preceding s2_temporal_accumulate of the same extent");
+    cudaSetDevice(ctx->device);
+    const uint32_t n = (uint32_t)W * (uint32_t)H;
+    if (ps->filter_pixels != n) {
+        free_bufs(ps->fbufs);
+        ps->filter_pixels = 0;
+        ps->filter[0] = (float4*)dev_alloc(ctx, ps->fbufs, sizeof(float4) * n);
+        ps->filter[1] = (float4*)dev_alloc(ctx, ps->fbufs, sizeof(float4) * n);
+        if (!ps->filter[0] || !ps->filter[1]) { free_bufs(ps->fbufs); return set_error(ctx, S2_ERR_OOM, "filter allocation failed"); }
+        ps->filter_pixels = n;
+    }
+    const uint32_t last = ps->cur ^ 1u;  // the latest accumulation result
+    SvgfArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.width = (uint32_t)W; A.height = (uint32_t)H;
+    A.flags = prm->flags;
+    A.history_limit = prm->history_limit;
+    A.kernel = prm->kernel;
+    A.variance_boost = prm->variance_boost_length;
+    A.sigma_boost = prm->sigma_luminance_boost;
+    A.color = ps->color[last];
+    A.moments = ps->moments[last];
+    A.vis = (const uint2*)frame->visibility;
+    A.depth = (const float4*)frame->depth;
+    A.instance_map = instance_index_map;
+    A.out = ps->filter[0];
+    cudaStream_t s = ctx->stream;
+    const dim3 block(16, 16), grid((W + 15) / 16, (H + 15) / 16);
+    k_svgf_variance<<<grid, block, 0, s>>>(A);
+    for (uint32_t i = 0; i < prm->iterations; ++i) {
+        A.iteration = i;
+        A.step = 1 << i;
+        A.in = ps->filter[i % 2];
+        A.out = ps->filter[(i + 1) % 2];
+        k_svgf_atrous<<<grid, block, 0, s>>>(A);
+        if (i + 1 == prm->history_tap) k_svgf_copy_rgb<<<(n + 255) / 256, 256, 0, s>>>(ps->color[last], ps->filter[0], n);
+    }
+    cudaMemcpyAsync(output, ps->filter[prm->iterations % 2], sizeof(float4) * n, cudaMemcpyDeviceToDevice, s);
+    int rc = check_cuda(ctx, cudaGetLastError(), "SVGF launch");
+    if (rc != S2_OK) return rc;
+    return check_cuda(ctx, cudaStreamSynchronize(s), "SVGF filter");
 }
 
 extern "C" int s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2TonemapParams* prm, const float* input,

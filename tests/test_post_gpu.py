@@ -106,3 +106,42 @@ def test_post_argument_errors(device):
         device.temporal_accumulate(view, tp, bad, t["radiance"].data_ptr())
     with pytest.raises(_abi.S2Error):
         device.tonemap(8, 8, _abi.S2TonemapParams(99, 0.0, 0, 0), t["radiance"].data_ptr(), t["albedo"].data_ptr())
+
+
+@pytest.mark.parametrize("kernel,iterations,tap", [(_abi.SVGF_KERNEL_BOX3, 3, 0), (_abi.SVGF_KERNEL_ATROUS, 2, 1),
+                                                   (_abi.SVGF_KERNEL_BOX5_SUBSAMPLED, 3, 2)])
+def test_svgf_matches_oracle(device, kernel, iterations, tap):
+    """s2_svgf_filter after two accumulated frames against the oracle's estimate_variance and
+    atrous passes (and the history tap's colour copy)."""
+    frames = _frames(device, n=2, W=24, H=20)
+    H, W = 20, 24
+    color = torch.zeros((H, W, 4), device="cuda")
+    moments = torch.zeros((H, W, 2), device="cuda")
+    tp = device.default_temporal_params()
+    for k, (view, t, aov) in enumerate(frames):
+        tp.flags = (tp.flags | _abi.TEMPORAL_RESET) if k == 0 else (tp.flags & ~_abi.TEMPORAL_RESET)
+        device.temporal_accumulate(view, tp, aov, color.data_ptr(), moments.data_ptr())
+    view, t, aov = frames[-1]
+    sp = device.default_svgf_params()
+    sp.kernel, sp.iterations, sp.history_tap, sp.history_limit = kernel, iterations, tap, 2
+    out = torch.zeros((H, W, 4), device="cuda")
+    device.svgf_filter(view, sp, aov, out.data_ptr())
+    host = {name: v.cpu().numpy() for name, v in t.items()}
+    vis = host["vis"].view(np.uint32)
+    c, m = color.cpu().numpy().astype(np.float64), moments.cpu().numpy().astype(np.float64)
+    img = [po.svgf_variance(c, m, vis, host["depth"], sp.flags, history_limit=2, boost=sp.variance_boost_length), None]
+    tapped = None
+    for i in range(iterations):
+        img[(i + 1) % 2] = po.svgf_atrous(img[i % 2], vis, host["depth"], i, kernel, sp.flags, sp.sigma_luminance_boost)
+        if i + 1 == tap:
+            tapped = img[0].copy()  # copy_rgb reads filter image 0 whichever image the pass wrote
+    _close(out.cpu().numpy(), img[iterations % 2], rtol=2e-3, atol=1e-5)
+    if tap:
+        # the history's colour now holds filter image 0's rgb (the next accumulation reads it)
+        h2 = torch.zeros((H, W, 4), device="cuda")
+        tp.flags = 0  # no reprojection: the next frame blends with the history in place
+        device.temporal_accumulate(view, tp, aov, h2.data_ptr())
+        prev_rgb = tapped[..., :3]
+        cur = host["radiance"][..., :3].astype(np.float64)
+        n = c[..., 3:4] + 1
+        _close(h2.cpu().numpy()[..., :3], prev_rgb + (cur - prev_rgb) / n, rtol=2e-3, atol=1e-5)
