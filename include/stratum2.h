@@ -183,6 +183,12 @@ typedef struct S2View {
                                                   within restir_spatial_radius of it (spatial); each
                                                   pixel's sample-0 path stores its reservoir for the
                                                   next call (s2_render only) */
+#define S2_FLAG_LIGHT_TRACE         (1u << 17) /* TestRenderer's light tracing mode (mLightTrace,
+                                                  testrenderer.slang:441-512, 983-1020): light
+                                                  subpaths connect every non-singular vertex to the
+                                                  camera; no NEE, ReSTIR or cache; the radiance AOV
+                                                  is written, the others are cleared to zero
+                                                  (s2_render only) */
 #define S2_FLAG_LIGHT_POWER_PICK    (1u << 16) /* pick emissive lights in proportion to their power
                                                   (emission luminance x area, from an alias table built
                                                   at s2_scene_upload) instead of uniformly as the
@@ -208,7 +214,9 @@ typedef struct S2RenderParams {
     uint32_t cache_train_paths;      /* training paths per wave (0 = 65536) */
     uint32_t restir_spatial;         /* S2_FLAG_RESTIR_SCREEN: spatial neighbours (0 = 5, at most 32) */
     float restir_spatial_radius;     /* S2_FLAG_RESTIR_SCREEN: neighbour radius in pixels (0 = 30) */
-    uint32_t reserved[3];
+    float light_subpaths;            /* S2_FLAG_LIGHT_TRACE: light subpaths per sample pass =
+                                        max(1, pixels x light_subpaths) (mLightSubpathCount, 0 = 1) */
+    uint32_t reserved[2];
 } S2RenderParams;
 
 /* Output AOVs (caller-allocated, device or host pointers per s2_render's `out_on_host`).

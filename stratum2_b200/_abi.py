@@ -44,6 +44,7 @@ FLAG_NORMAL_MAPS_OFF = 1 << 13
 FLAG_RADIANCE_CACHE = 1 << 14
 FLAG_RESTIR_SCREEN = 1 << 15
 FLAG_LIGHT_POWER_PICK = 1 << 16
+FLAG_LIGHT_TRACE = 1 << 17
 SHADE_ORDER_MATERIAL = 0
 SHADE_ORDER_QUEUE = 1
 TRACE_ORDER_QUEUE = 0
@@ -127,7 +128,8 @@ class S2RenderParams(C.Structure):
         ("restir_max_m", C.c_float), ("wave_paths", C.c_uint32), ("restir_grid_cells", C.c_uint32),
         ("restir_grid_cell_size", C.c_float), ("restir_grid_pixel_radius", C.c_float),
         ("cache_bounces", C.c_uint32), ("cache_train_paths", C.c_uint32), ("restir_spatial", C.c_uint32),
-        ("restir_spatial_radius", C.c_float), ("reserved", C.c_uint32 * 3),
+        ("restir_spatial_radius", C.c_float), ("light_subpaths", C.c_float),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 

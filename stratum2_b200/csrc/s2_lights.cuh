@@ -215,6 +215,56 @@ S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_n
     return r;
 }
 
+// A point on a light to start a light subpath from (InitializeLightPath, testrenderer.slang:
+// 983-1001): the light pick and triangle sampling of sample_illum, without its one-sidedness test
+// against a reference point.  Area lights give the point, its geometric normal (the emitting side),
+// the emission and the area pdf; the environment gives the direction toward it and its solid-angle
+// pdf, from sample_illum's own environment branch.
+struct LightPoint {
+    float3 pos, n, radiance, dir;
+    float pdf;
+    bool finite, ok;
+};
+S2D LightPoint sample_light_point(const DevScene& s, float4 rnd, bool shading_normals) {
+    LightPoint p;
+    p.pos = p.n = p.radiance = p.dir = f3(0.f);
+    p.pdf = 0.f; p.finite = true; p.ok = false;
+    const uint32_t L = s.light_count;
+    const float envp = s.env_sample_prob;
+    if (has_env(s) && (L == 0 || rnd.w < envp)) {
+        const Illum r = sample_illum(s, rnd, f3(0.f), shading_normals);
+        p.finite = false; p.dir = r.dir; p.radiance = r.radiance; p.pdf = r.pdf;
+        p.ok = r.pdf > 0.f && any_pos(r.radiance);
+        return p;
+    }
+    if (L == 0) return p;
+    if (has_env(s)) rnd.w = (rnd.w - envp) / (1.f - envp);
+    uint32_t light;
+    float pdf;
+    if (s.light_power_pick) {
+        const float u = rnd.z * (float)L;
+        const uint32_t col = min((uint32_t)u, L - 1u);
+        const float2 a = s.light_alias[col];
+        light = (u - (float)col) < a.x ? col : __float_as_uint(a.y);
+        pdf = s.light_pick_pdf[light];
+    } else {
+        light = (uint32_t)(rnd.z * L) % L;
+        pdf = 1.f / (float)L;
+    }
+    if (has_env(s)) pdf *= 1.f - envp;
+    const uint32_t inst = s.light_instance_map[light];
+    if ((s.instances[inst].x & 0xfu) != 0u) return p;
+    const uint32_t pc = s.prim_counts[inst];
+    const uint32_t prim = (uint32_t)(rnd.w * pc) % pc;
+    const float2 b = sample_uniform_triangle(rnd.x, rnd.y);
+    const SD sd = make_shading(s, inst, prim, b.x, b.y, shading_normals);
+    const Mat m = load_material(s, sd.mat, sd.uv);
+    p.pos = sd.pos; p.n = sd.gn; p.radiance = m.emission();
+    p.pdf = pdf / (float)pc / sd.area;
+    p.ok = p.pdf > 0.f && any_pos(p.radiance);
+    return p;
+}
+
 // IntersectionResult::LightSamplePdfA (lights.hlsli:264-272)
 S2D float light_pdfa(const DevScene& s, uint32_t inst, float area) {
     if (s.light_count == 0) return 0.f;

@@ -8,6 +8,7 @@
 
 #include "s2_context.h"
 #include "s2_shade_kernel.cuh"
+#include "s2_light_trace.cuh"
 
 namespace s2 {
 
@@ -45,6 +46,10 @@ struct RenderState {
     } grid[2];
     uint32_t grid_cur = 0;
     bool grid_prev_valid = false;
+    // light tracing: fixed-point per-pixel totals of the camera connections
+    std::vector<DevBuf> lt_bufs;
+    unsigned long long* lt_fx = nullptr;
+    uint32_t lt_pixels = 0;
     // screen-space ReSTIR DI reuse: per-pixel reservoirs of this call and of the previous one
     std::vector<DevBuf> ss_bufs;
     ReservoirRecord* ss[2] = {nullptr, nullptr};
@@ -72,6 +77,7 @@ void destroy_render_state(S2Context* ctx) {
     free_bufs(ctx->render->cache_bufs);
     free_bufs(ctx->render->sort_bufs);
     free_bufs(ctx->render->ss_bufs);
+    free_bufs(ctx->render->lt_bufs);
     free_bufs(ctx->render->bufs);
     free_bufs(ctx->render->pixel_bufs);
     delete ctx->render;
@@ -145,6 +151,29 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
         st->capacity = capacity;
     }
     return S2_OK;
+}
+
+// Inverse of a row-major 3x4 affine transform (the world-to-camera matrix of a view), in double.
+void invert_affine(const float* m, float* out) {
+    double a[3][3], t[3];
+    for (int r = 0; r < 3; ++r) { for (int c = 0; c < 3; ++c) a[r][c] = m[4 * r + c]; t[r] = m[4 * r + 3]; }
+    const double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                       a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    const double id = det != 0.0 ? 1.0 / det : 0.0;
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) * id;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) * id;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) * id;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) out[4 * r + c] = (float)inv[r][c];
+        out[4 * r + 3] = (float)-(inv[r][0] * t[0] + inv[r][1] * t[1] + inv[r][2] * t[2]);
+    }
 }
 
 // Counting sort of the live queue by material key into P.sort_perm (histogram, scan, scatter).
@@ -246,6 +275,13 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
     const bool screen = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_SCREEN);
+    const bool light_trace = (prm->flags & S2_FLAG_LIGHT_TRACE) != 0;
+    if (light_trace) {
+        if (prm->flags & (S2_FLAG_RESTIR_DI | S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE))
+            return set_error(ctx, S2_ERR_UNSUPPORTED, "light tracing takes no ReSTIR or radiance-cache flags");
+        if (!(prm->light_subpaths >= 0.f) || !std::isfinite(prm->light_subpaths))
+            return set_error(ctx, S2_ERR_INVALID, "light_subpaths must be finite and >= 0");
+    }
     if ((prm->flags & S2_FLAG_RESTIR_REUSE) && (prm->flags & S2_FLAG_RESTIR_SCREEN))
         return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RESTIR_SCREEN are exclusive");
     if (screen && (prm->restir_spatial > 32 || !(prm->restir_spatial_radius >= 0.f) || !std::isfinite(prm->restir_spatial_radius) ||
@@ -262,7 +298,10 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     const uint32_t pixels = (uint32_t)W * (uint32_t)H;
     uint64_t target = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : kDefaultWavePaths);
     uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, target / pixels));
-    const uint32_t capacity = slots * pixels;
+    // light tracing: one queue of max(1, pixels x light_subpaths) light subpaths per sample pass
+    const uint32_t lt_paths = (uint32_t)std::max(1.0, std::min(4294967040.0, (double)pixels *
+                                                 (prm->light_subpaths > 0.f ? (double)prm->light_subpaths : 1.0)));
+    const uint32_t capacity = light_trace ? lt_paths : slots * pixels;
     int rc = ensure_state(ctx, (uint32_t)W, (uint32_t)H, capacity);
     if (rc != S2_OK) return rc;
     RenderState* st = ctx->render;
@@ -377,6 +416,30 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         cudaMemsetAsync(st->total, 0, sizeof(float4) * pixels, s);
         st->accumulated_spp = 0;
     }
+    if (light_trace) {
+        if (st->lt_pixels != pixels) {
+            free_bufs(st->lt_bufs);
+            st->lt_pixels = 0;
+            st->lt_fx = (unsigned long long*)dev_alloc(ctx, st->lt_bufs, 32ull * pixels);
+            if (!st->lt_fx) return set_error(ctx, S2_ERR_OOM, "light-tracing accumulator allocation failed");
+            st->lt_pixels = pixels;
+            cudaMemsetAsync(st->lt_fx, 0, 32ull * pixels, s);
+        }
+        if (!(prm->flags & S2_FLAG_ACCUMULATE)) cudaMemsetAsync(st->lt_fx, 0, 32ull * pixels, s);
+        P.total_fx = st->lt_fx;
+        // light tracing has no first camera hit: the other AOVs are cleared to zero
+        if (P.aov_albedo) cudaMemsetAsync(P.aov_albedo, 0, 16ull * pixels, s);
+        if (P.aov_vis) cudaMemsetAsync(P.aov_vis, 0, 8ull * pixels, s);
+        if (P.aov_depth) cudaMemsetAsync(P.aov_depth, 0, 16ull * pixels, s);
+        if (P.aov_prev_uv) cudaMemsetAsync(P.aov_prev_uv, 0, 8ull * pixels, s);
+        if (P.aov_ids) cudaMemsetAsync(P.aov_ids, 0, 8ull * pixels, s);
+        P.aov_albedo = nullptr; P.aov_vis = nullptr; P.aov_depth = nullptr; P.aov_prev_uv = nullptr; P.aov_ids = nullptr;
+        P.sort_on = 0; P.ray_sort_on = 0;
+        P.lt_paths = lt_paths;
+        // ViewData::imagePlaneDist: |image height| / (2 tan(vfov / 2))
+        P.lt_image_plane_dist = std::fabs((float)(view->image_max[1] - view->image_min[1])) / (2.f * std::tan(view->projection[7] * 0.5f));
+        invert_affine(view->camera_to_world, P.cam_inv);
+    }
     cudaMemsetAsync(st->stats, 0, sizeof(unsigned long long) * S_COUNT, s);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), s);
     cudaEventRecord(ctx->ev0, s);
@@ -393,7 +456,32 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         prof_kind.push_back(kind);
     };
     auto ev_end = [&]() { if (prof) cudaEventRecord(st->events[2 * prof_kind.size() - 1], s); };
-    for (uint32_t done = 0; done < prm->spp; done += slots) {
+    for (uint32_t sample = 0; light_trace && sample < prm->spp; ++sample) {
+        // one light pass: light subpaths, then per vertex the camera connections and continuation
+        cudaMemsetAsync(st->counters, 0, sizeof(uint32_t) * C_COUNT, s);
+        k_light_gen<<<std::min<uint32_t>((lt_paths + 255) / 256, 148u * 16u), 256, 0, s>>>(P, sample);
+        launches += 1;
+        for (uint32_t b = 0; b < prm->max_path_length; ++b) {
+            const uint32_t parity = b & 1u;
+            k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
+            ev_begin(0);
+            if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            ev_end();
+            ev_begin(1);
+            if (lam) k_light_shade<true><<<st->shade_blocks, 128, 0, s>>>(P, parity);
+            else k_light_shade<false><<<st->shade_blocks, 128, 0, s>>>(P, parity);
+            ev_end();
+            ev_begin(2);
+            if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            ev_end();
+            launches += 4;
+        }
+        k_wave_finish<<<1, 32, 0, s>>>(P);
+        launches += 1;
+    }
+    for (uint32_t done = 0; !light_trace && done < prm->spp; done += slots) {
         P.wave_base_sample = done;
         P.wave_samples = std::min(slots, prm->spp - done);
         const uint32_t n = P.wave_samples * pixels;
@@ -452,8 +540,12 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     launches += 1;  // resolve
     st->accumulated_spp += prm->spp;
     float4* rad = (out && out->radiance) ? (host ? st->out_radiance : (float4*)out->radiance) : st->out_radiance;
-    k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(st->total, pixels, (float)(1.0 / (double)st->accumulated_spp),
-                                                   exp2f(prm->exposure), rad);
+    if (light_trace)
+        k_resolve_fx<<<(pixels + 255) / 256, 256, 0, s>>>(st->lt_fx, 0, pixels,
+                                                          (float)(1.0 / (double)st->accumulated_spp) * exp2f(prm->exposure), rad);
+    else
+        k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(st->total, pixels, (float)(1.0 / (double)st->accumulated_spp),
+                                                       exp2f(prm->exposure), rad);
     cudaEventRecord(ctx->ev1, s);
     rc = check_cuda(ctx, cudaGetLastError(), "render kernel launch");
     if (rc != S2_OK) return rc;

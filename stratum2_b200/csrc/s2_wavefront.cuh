@@ -110,6 +110,11 @@ struct PTParams {
     uint32_t refill_min;  // refill a warp's idle lanes once this many are idle
     // material-key sorting before shading (S2Tuning::shade_order): k_extend writes a key per
     // path (hit material, misses last), a counting sort builds sort_perm, k_shade reads through it
+    // light tracing (S2_FLAG_LIGHT_TRACE): world-to-camera transform, light subpaths per pass and
+    // the image-plane distance of ViewData::imagePlaneDist
+    float cam_inv[12];
+    uint32_t lt_paths;
+    float lt_image_plane_dist;
     uint32_t sort_on;
     // ray-coherence sorting before traversal (S2Tuning::trace_order): k_shade writes ray_key() of
     // each continuation ray (ray_sort_on), a counting sort builds sort_perm, and k_extend takes its
