@@ -498,6 +498,57 @@ typedef struct S2TonemapParams {
 int  s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2TonemapParams* params, const float* input,
                 const float* albedo, float* output);
 
+/* ---------------------------------------------------------------- vertex connection and merging
+ * Replaces the reference's VCM renderer (VCM.cpp:370-620, vcm.slang:880-1238: SmallVCM's
+ * bidirectional techniques with the MIS quantities dVCM / dVC / dVM).  Each iteration traces
+ * n_light = max(1, pixels x light_path_fraction) light subpaths, then one camera path per pixel.
+ * Camera samples are jittered over their pixel (the reference uses pixel centres), so camera paths
+ * and camera connections estimate the same box-filtered image.  The environment is black and never
+ * sampled, as in the reference (GetBackgroundRadiance returns zero radiance); only area lights
+ * emit.  The merge radius of iteration i is max(1e-7, merge_radius_factor x scene radius /
+ * (i + 1)^(0.5 (1 - merge_radius_alpha))), i = first_iteration + the iteration's index
+ * (VCM.cpp:454-457). */
+#define S2_VCM_PATH_TRACE   0u  /* VcmAlgorithmType (compat/vcm.h:103-132) */
+#define S2_VCM_LIGHT_TRACE  1u
+#define S2_VCM_PPM          2u
+#define S2_VCM_BPM          3u
+#define S2_VCM_BPT          4u
+#define S2_VCM_VCM          5u
+#define S2_VCM_FLAG_LIGHT_VERTEX_CACHE  (1u << 0)  /* BPT: one connection to a random cached light
+                                                      vertex (mUseLightVertexCache, the reference's
+                                                      default) instead of all vertices of one subpath */
+#define S2_VCM_FLAG_DEBUG_PATHS         (1u << 1)  /* gDebugPaths: keep only the technique with
+                                                      debug_camera_vertices / debug_light_vertices */
+#define S2_VCM_FLAG_DEBUG_UNWEIGHTED    (1u << 2)  /* with DEBUG_PATHS and not gDebugPathWeights: every
+                                                      MIS weight 1 */
+
+typedef struct S2VcmParams {
+    uint32_t algorithm;              /* S2_VCM_PATH_TRACE .. S2_VCM_VCM (default S2_VCM_BPT, VCM.hpp:66) */
+    uint32_t min_path_length;        /* mMinPathLength (default 0) */
+    uint32_t max_path_length;        /* mMaxPathLength (default 6), 1..64 */
+    uint32_t iterations;             /* light pass + camera pass per iteration; the image is their mean */
+    uint32_t frame_seed;             /* mRandomSeed of the first iteration (+1 per iteration) */
+    uint32_t first_iteration;        /* index of the first iteration in the merge-radius schedule */
+    uint32_t flags;                  /* S2_FLAG_LAMBERTIAN, PCG32, NO_RR, SHADING_NORMALS_OFF,
+                                        ALPHA_TEST_OFF, NORMAL_MAPS_OFF, LIGHT_POWER_PICK */
+    uint32_t vcm_flags;              /* S2_VCM_FLAG_* */
+    float light_path_fraction;       /* mLightPathPercent (default 1) */
+    float merge_radius_factor;       /* mVmRadiusFactor (default 0.025) */
+    float merge_radius_alpha;        /* mVmRadiusAlpha (default 0.01) */
+    float exposure;                  /* output x 2^exposure */
+    uint16_t debug_camera_vertices;  /* mDebugPathLengths (compat/vcm.h:49-55) */
+    uint16_t debug_light_vertices;
+    uint32_t reserved[3];
+} S2VcmParams;
+
+void s2_default_vcm_params(S2VcmParams* p);
+/* One call renders `iterations` iterations of the view.  AOVs (albedo 0 on a miss, as in the VCM
+ * renderer) come from the first iteration's camera paths.  stats_out: extension and shadow rays of
+ * both passes, paths = pixels x iterations.  S2_ERR_UNSUPPORTED for flags outside the list above or
+ * the light vertex cache with an algorithm other than BPT. */
+int  s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmParams* params, const S2Aovs* out, int out_on_host,
+                   S2RenderStats* stats_out);
+
 #ifdef __cplusplus
 }
 #endif

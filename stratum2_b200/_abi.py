@@ -59,6 +59,7 @@ EXPORTED_SYMBOLS = [
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
     "s2_set_tuning", "s2_get_tuning", "s2_autotune",
     "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap", "s2_default_svgf_params", "s2_svgf_filter",
+    "s2_default_vcm_params", "s2_render_vcm",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -178,6 +179,20 @@ class S2TonemapParams(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("exposure", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+# vertex connection and merging (S2_VCM_*)
+VCM_PATH_TRACE, VCM_LIGHT_TRACE, VCM_PPM, VCM_BPM, VCM_BPT, VCM_VCM = range(6)
+VCM_FLAG_LIGHT_VERTEX_CACHE, VCM_FLAG_DEBUG_PATHS, VCM_FLAG_DEBUG_UNWEIGHTED = 1 << 0, 1 << 1, 1 << 2
+
+
+class S2VcmParams(C.Structure):
+    _fields_ = [("algorithm", C.c_uint32), ("min_path_length", C.c_uint32), ("max_path_length", C.c_uint32),
+                ("iterations", C.c_uint32), ("frame_seed", C.c_uint32), ("first_iteration", C.c_uint32),
+                ("flags", C.c_uint32), ("vcm_flags", C.c_uint32), ("light_path_fraction", C.c_float),
+                ("merge_radius_factor", C.c_float), ("merge_radius_alpha", C.c_float), ("exposure", C.c_float),
+                ("debug_camera_vertices", C.c_uint16), ("debug_light_vertices", C.c_uint16),
+                ("reserved", C.c_uint32 * 3)]
+
+
 class S2RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
                 ("nan_count", C.c_uint64), ("gpu_ms", C.c_double), ("kernel_launches", C.c_uint64),
@@ -190,6 +205,7 @@ class S2RenderStats(C.Structure):
 assert C.sizeof(S2Ray) == 32 and C.sizeof(S2Hit) == 20
 assert C.sizeof(S2RenderParams) == 80
 assert C.sizeof(S2CacheParams) == 80
+assert C.sizeof(S2VcmParams) == 64
 
 _lib = None
 
@@ -234,6 +250,9 @@ def lib() -> C.CDLL:
     L.s2_tonemap.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(S2TonemapParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.s2_get_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
     L.s2_autotune.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), P(S2Tuning), P(C.c_uint32)]
+    L.s2_default_vcm_params.restype = None
+    L.s2_default_vcm_params.argtypes = [P(S2VcmParams)]
+    L.s2_render_vcm.argtypes = [C.c_void_p, P(S2View), P(S2VcmParams), P(S2Aovs), C.c_int, P(S2RenderStats)]
     L.s2_render_diff.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, P(S2RenderStats)]
     L.s2_render_adjoint.argtypes = [C.c_void_p, P(S2View), P(S2RenderParams), C.c_void_p, C.c_int, C.c_void_p,
                                     P(S2RenderStats)]

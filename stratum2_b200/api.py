@@ -147,6 +147,29 @@ class Device:
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(p), C.byref(aov), 1, C.byref(st)))
         return RenderResult(rad, alb, vis, dep, puv, ids, st)
 
+    # ---- vertex connection and merging (the reference's VCM renderer)
+    @staticmethod
+    def default_vcm_params() -> _abi.S2VcmParams:
+        p = _abi.S2VcmParams()
+        _abi.lib().s2_default_vcm_params(C.byref(p))
+        return p
+
+    def render_vcm(self, view: _abi.S2View, width: int, height: int,
+                   params: _abi.S2VcmParams | None = None) -> RenderResult:
+        """s2_render_vcm: `params.iterations` light + camera passes of one view (host arrays)."""
+        p = params if params is not None else self.default_vcm_params()
+        rad = np.zeros((height, width, 4), np.float32)
+        alb = np.zeros((height, width, 4), np.float32)
+        vis = np.zeros((height, width, 2), np.uint32)
+        dep = np.zeros((height, width, 4), np.float32)
+        puv = np.zeros((height, width, 2), np.float32)
+        ids = np.zeros((height, width, 2), np.uint32)
+        aov = _abi.S2Aovs(rad.ctypes.data, alb.ctypes.data, vis.ctypes.data, dep.ctypes.data, puv.ctypes.data,
+                          ids.ctypes.data)
+        st = _abi.S2RenderStats()
+        self._check(self._lib.s2_render_vcm(self._h, C.byref(view), C.byref(p), C.byref(aov), 1, C.byref(st)))
+        return RenderResult(rad, alb, vis, dep, puv, ids, st)
+
     def render_views(self, views, params: _abi.S2RenderParams, aovs: bool = True):
         """Batched render of several views (any resolutions) in one call (s2_render_views).
         Returns one RenderResult per view (host arrays) and the call's statistics."""
