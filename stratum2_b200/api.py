@@ -123,9 +123,26 @@ class Device:
         _abi.lib().s2_default_render_params(C.byref(p))
         return p
 
+    @staticmethod
+    def host_result(width: int, height: int, pinned: bool = False) -> RenderResult:
+        """Host arrays for every output of one view, to pass as render(out=...) frame after frame.
+        pinned=True page-locks them (through torch), so the library's device-to-host copies run
+        asynchronously at full link speed and overlap the render."""
+        def arr(shape, dt):
+            if not pinned:
+                return np.zeros(shape, dt)
+            import torch
+            t = torch.zeros(shape, dtype=torch.float32 if dt == np.float32 else torch.int32, pin_memory=True)
+            return t.numpy().view(dt)  # the array keeps the pinned tensor alive
+        return RenderResult(arr((height, width, 4), np.float32), arr((height, width, 4), np.float32),
+                            arr((height, width, 2), np.uint32), arr((height, width, 4), np.float32),
+                            arr((height, width, 2), np.float32), arr((height, width, 2), np.uint32),
+                            _abi.S2RenderStats())
+
     def render(self, view: _abi.S2View, width: int, height: int, spp: int = 1, min_path_length: int = 0,
                max_path_length: int = 5, exposure: float = 0.0, frame_seed: int = 0, flags: int = 0,
-               params: _abi.S2RenderParams | None = None) -> RenderResult:
+               params: _abi.S2RenderParams | None = None, out: RenderResult | None = None) -> RenderResult:
+        """s2_render into host arrays: new ones, or `out` (from host_result) reused in place."""
         p = params if params is not None else self.default_params()
         if params is None:
             p.min_path_length = min_path_length
@@ -134,18 +151,16 @@ class Device:
             p.spp = spp
             p.frame_seed = frame_seed
             p.flags = flags
-        n = width * height
-        rad = np.zeros((height, width, 4), np.float32)
-        alb = np.zeros((height, width, 4), np.float32)
-        vis = np.zeros((height, width, 2), np.uint32)
-        dep = np.zeros((height, width, 4), np.float32)
-        puv = np.zeros((height, width, 2), np.float32)
-        ids = np.zeros((height, width, 2), np.uint32)
-        aov = _abi.S2Aovs(rad.ctypes.data, alb.ctypes.data, vis.ctypes.data, dep.ctypes.data, puv.ctypes.data,
-                          ids.ctypes.data)
+        r = out if out is not None else self.host_result(width, height)
+        for a, c in ((r.radiance, 4), (r.albedo, 4), (r.visibility, 2), (r.depth, 4), (r.prev_uv, 2), (r.ids32, 2)):
+            if a.shape != (height, width, c) or not a.flags.c_contiguous:
+                raise ValueError("output arrays do not match the view")
+        aov = _abi.S2Aovs(r.radiance.ctypes.data, r.albedo.ctypes.data, r.visibility.ctypes.data, r.depth.ctypes.data,
+                          r.prev_uv.ctypes.data, r.ids32.ctypes.data)
         st = _abi.S2RenderStats()
         self._check(self._lib.s2_render(self._h, C.byref(view), C.byref(p), C.byref(aov), 1, C.byref(st)))
-        return RenderResult(rad, alb, vis, dep, puv, ids, st)
+        r.stats = st
+        return r
 
     # ---- vertex connection and merging (the reference's VCM renderer)
     @staticmethod

@@ -39,6 +39,9 @@ struct RenderState {
     int shade_blocks_rc = 0;   // ReSTIR / radiance-cache shade variants (more registers)
     int sort_blocks = 0;
     std::vector<cudaEvent_t> events;  // reusable start/stop pairs for S2_FLAG_PROFILE_KERNELS
+    // host outputs: the first-hit AOVs are copied on a side stream while the later bounces render
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t aov_ready = nullptr, copies_done = nullptr;
     // ReSTIR DI reuse: the grid appended to by this call and the previous call's grid
     struct Grid {
         std::vector<DevBuf> bufs;
@@ -73,6 +76,9 @@ void destroy_render_state(S2Context* ctx) {
     destroy_batch_state(ctx);
     if (!ctx->render) return;
     for (cudaEvent_t e : ctx->render->events) cudaEventDestroy(e);
+    if (ctx->render->copy_stream) cudaStreamDestroy(ctx->render->copy_stream);
+    if (ctx->render->aov_ready) cudaEventDestroy(ctx->render->aov_ready);
+    if (ctx->render->copies_done) cudaEventDestroy(ctx->render->copies_done);
     for (auto& g : ctx->render->grid) free_bufs(g.bufs);
     free_bufs(ctx->render->cache_bufs);
     free_bufs(ctx->render->sort_bufs);
@@ -456,6 +462,17 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         prof_kind.push_back(kind);
     };
     auto ev_end = [&]() { if (prof) cudaEventRecord(st->events[2 * prof_kind.size() - 1], s); };
+    // Host outputs: the first-hit AOVs are written by wave 0's first shade only, so their copies can
+    // run on a side stream while the later bounces render.  They are issued after every kernel of the
+    // call is queued, since a copy to pageable memory holds the host until it completes.
+    const bool early_aov = host && out && !light_trace &&
+                           (out->albedo || out->visibility || out->depth || out->prev_uv || out->ids32);
+    if (early_aov) {
+        if (!st->copy_stream) cudaStreamCreateWithFlags(&st->copy_stream, cudaStreamNonBlocking);
+        if (!st->aov_ready) cudaEventCreateWithFlags(&st->aov_ready, cudaEventDisableTiming);
+        if (!st->copies_done) cudaEventCreateWithFlags(&st->copies_done, cudaEventDisableTiming);
+        if (!st->copy_stream || !st->aov_ready || !st->copies_done) return set_error(ctx, S2_ERR_CUDA, "copy stream creation failed");
+    }
     for (uint32_t sample = 0; light_trace && sample < prm->spp; ++sample) {
         // one light pass: light subpaths, then per vertex the camera connections and continuation
         cudaMemsetAsync(st->counters, 0, sizeof(uint32_t) * C_COUNT, s);
@@ -501,6 +518,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
             else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
             ev_end();
+            if (early_aov && done == 0 && b == 0) cudaEventRecord(st->aov_ready, s);  // first-hit AOVs are final
             if (cache && b + 1 == cache_len) {
                 rc = cache_apply_device(ctx, st->cq_pos, st->cq_thr, st->cq_cap, st->counters + C_CACHEQ, st->accum);
                 if (rc != S2_OK) return rc;
@@ -550,12 +568,18 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     rc = check_cuda(ctx, cudaGetLastError(), "render kernel launch");
     if (rc != S2_OK) return rc;
     if (host && out) {
+        cudaStream_t as = early_aov ? st->copy_stream : s;
+        if (early_aov) cudaStreamWaitEvent(as, st->aov_ready, 0);
+        if (out->albedo) cudaMemcpyAsync(out->albedo, st->aov_albedo, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, as);
+        if (out->visibility) cudaMemcpyAsync(out->visibility, st->aov_vis, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, as);
+        if (out->depth) cudaMemcpyAsync(out->depth, st->aov_depth, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, as);
+        if (out->prev_uv) cudaMemcpyAsync(out->prev_uv, st->aov_prev_uv, sizeof(float2) * pixels, cudaMemcpyDeviceToHost, as);
+        if (out->ids32) cudaMemcpyAsync(out->ids32, st->aov_ids, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, as);
+        if (early_aov) {  // the call's stream waits for the side copies, so its synchronisation covers them
+            cudaEventRecord(st->copies_done, as);
+            cudaStreamWaitEvent(s, st->copies_done, 0);
+        }
         if (out->radiance) cudaMemcpyAsync(out->radiance, st->out_radiance, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
-        if (out->albedo) cudaMemcpyAsync(out->albedo, st->aov_albedo, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
-        if (out->visibility) cudaMemcpyAsync(out->visibility, st->aov_vis, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, s);
-        if (out->depth) cudaMemcpyAsync(out->depth, st->aov_depth, sizeof(float4) * pixels, cudaMemcpyDeviceToHost, s);
-        if (out->prev_uv) cudaMemcpyAsync(out->prev_uv, st->aov_prev_uv, sizeof(float2) * pixels, cudaMemcpyDeviceToHost, s);
-        if (out->ids32) cudaMemcpyAsync(out->ids32, st->aov_ids, sizeof(uint2) * pixels, cudaMemcpyDeviceToHost, s);
     }
     if (stats_out || host) {
         unsigned long long sv[S_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
