@@ -183,6 +183,13 @@ typedef struct S2View {
                                                   within restir_spatial_radius of it (spatial); each
                                                   pixel's sample-0 path stores its reservoir for the
                                                   next call (s2_render only) */
+#define S2_FLAG_RESTIR_REUSE_VISIBILITY (1u << 18) /* gReSTIR_DI_Reuse_Visibility (TestRenderer.cpp:34,
+                                                   testrenderer.slang:611-742): with reuse on, the
+                                                   canonical sample's visibility is traced before
+                                                   reuse (occluded: W = 0), a reused sample's in the
+                                                   current domain before resampling, and the result
+                                                   is added without a deferred shadow ray; ignored
+                                                   without S2_FLAG_RESTIR_REUSE / _SCREEN */
 #define S2_FLAG_LIGHT_TRACE         (1u << 17) /* TestRenderer's light tracing mode (mLightTrace,
                                                   testrenderer.slang:441-512, 983-1020): light
                                                   subpaths connect every non-singular vertex to the

@@ -18,7 +18,7 @@ namespace orc {
 constexpr uint32_t FLAG_PIXEL_JITTER = 1u << 0, FLAG_LAMBERTIAN = 1u << 1, FLAG_PCG32 = 1u << 2, FLAG_NO_NEE = 1u << 3,
                    FLAG_RESTIR = 1u << 4, FLAG_REF_ENV_MIS = 1u << 5, FLAG_NO_RR = 1u << 6, FLAG_NO_SHADING_NORMALS = 1u << 8,
                    FLAG_RESTIR_REUSE = 1u << 11, FLAG_NO_ALPHA = 1u << 12,
-                   FLAG_NO_NORMAL_MAPS = 1u << 13,
+                   FLAG_NO_NORMAL_MAPS = 1u << 13, FLAG_RESTIR_REUSE_VIS = 1u << 18,
                    FLAG_F32_MATERIALS = 1u << 30;  // oracle only: the materials of s2_render_diff
 
 template <class R> R un8(uint32_t w, int shift) { return R((w >> shift) & 0xffu) / R(255); }
@@ -816,6 +816,7 @@ template <class R> struct Tracer {
         float x[4] = {0, 0, 0, 0};
         R src_pdf = 0, wtoa = 0, misw = 0, dist = 0;
         V3<R> contrib = V3<R>(0), dir = V3<R>(0);
+        R vis = 1;  // visibility traced in the reuse-visibility mode
         R target() const { return luminance(contrib) * wtoa; }
     };
     DI eval_di(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, const float x[4], R cp) const {
@@ -840,8 +841,12 @@ template <class R> struct Tracer {
     // ReservoirReuse (testrenderer.slang:608-663): pairwise MIS between the current reservoir
     // and the stored one
     void reservoir_reuse(const Mat<R>& m, const SD<R>& sd, const V3<R>& in, R cp, const GridRecord<R>& q, DI& cur,
-                         R& iw, R& M, Rng& rng) const {
-        const DI nw = eval_di(m, sd, in, q.rnd, cp);
+                         R& iw, R& M, Rng& rng, bool vis_on) {
+        DI nw = eval_di(m, sd, in, q.rnd, cp);
+        // gReSTIR_DI_Reuse_Visibility (testrenderer.slang:611-616): q's sample in the current domain
+        // carries its visibility in the contribution; the target pdf stays unshadowed
+        if (vis_on && nw.target() > 0 && occluded(ray_offset(sd.pos, sd.gn, nw.dir), nw.dir, adjust_distance(nw.dist)))
+            nw.vis = 0;
         R phat_q = 0;
         {
             SD<R> sdq = shading_local(q.inst, q.prim, q.local_pos);
@@ -878,6 +883,13 @@ template <class R> struct Tracer {
                 if ((R)u[0] <= risw / wsum) best = c;
             }
             R iw = best.target() > 0 ? wsum / ((R)p.restir_m * best.target()) : R(0);
+            // gReSTIR_DI_Reuse_Visibility (testrenderer.slang:689-694): canonical visibility first
+            const bool vis_on = grid_cur && (p.flags & FLAG_RESTIR_REUSE_VIS);
+            if (vis_on) {
+                if (best.target() > 0 && occluded(ray_offset(sd.pos, sd.gn, best.dir), best.dir, adjust_distance(best.dist)))
+                    best.vis = 0;
+                if (!(best.vis > 0)) iw = 0;
+            }
             if (grid_cur) {
                 R M = (R)p.restir_m;
                 if (grid_prev) {
@@ -889,7 +901,7 @@ template <class R> struct Tracer {
                     if (cell != 0xffffffffu && grid_prev->counter[cell] > 0) {
                         const uint32_t k = rng.next().x % grid_prev->counter[cell];
                         const GridRecord<R>& q = grid_prev->data[grid_prev->data_index[grid_prev->offset[cell] + k]];
-                        reservoir_reuse(m, sd, in, cp, q, best, iw, M, rng);
+                        reservoir_reuse(m, sd, in, cp, q, best, iw, M, rng, vis_on);
                     }
                 }
                 if (iw > 0) {
@@ -906,11 +918,11 @@ template <class R> struct Tracer {
             }
             if (!(iw > 0)) return;
             iw *= best.wtoa;
-            const V3<R> contrib = thr * best.contrib * iw;
+            const V3<R> contrib = thr * best.contrib * (iw * best.vis);
             if (!(best.misw > 0) || all_nonpos(contrib)) return;
             if (len + 1 < p.min_len) return;
             const V3<R> o = ray_offset(sd.pos, sd.gn, best.dir);
-            if (occluded(o, best.dir, adjust_distance(best.dist))) return;
+            if (!vis_on && occluded(o, best.dir, adjust_distance(best.dist))) return;  // AddRadiance when traced
             add(contrib, best.misw, len + 1);
             return;
         }

@@ -49,7 +49,8 @@ S2D AovTarget aov_target(const PTParams& P, uint32_t slot, uint32_t meta) {
     return t;
 }
 
-struct ShadowOut { float3 o, d, c; float tmax; bool valid; };
+// A deferred shadow ray, or (direct) a contribution whose visibility is already known.
+struct ShadowOut { float3 o, d, c; float tmax; bool valid, direct; };
 
 // A light sample evaluated at one vertex: ReservoirSampleDataDI (testrenderer.slang:568-606).
 struct DISample {
@@ -60,13 +61,26 @@ struct DISample {
     float dist;
     float3 contrib;    // f * Le (shading-normal corrected)
     float3 dir;
+    float vis;         // traced visibility (1 unless a reuse-visibility ray found the light occluded)
     S2D float target() const { return luminance(contrib) * wtoa; }
 };
+
+// traceVisibilityRay for a light sample, traced inline (S2_FLAG_RESTIR_REUSE_VISIBILITY).
+S2D bool di_visible(const PTParams& P, const SD& sd, const DISample& c, uint2* vstack) {
+    const SceneAlphaTest alpha{&P.scene, !(P.flags & S2F_NO_ALPHA)};
+    TravHit h;
+    TravCounters ctr{0, 0};
+    if (!traverse<true, false>(make_trav_ray(ray_offset(sd.pos, sd.gn, c.dir), c.dir, 0.f), adjust_distance(c.dist),
+                               P.scene.nodes, P.scene.tris, vstack, 128u, h, ctr, alpha))
+        atomicOr(P.status, 1);
+    atomicAdd(&P.stats[S_SHADOW], 1ull);
+    return h.tri == 0xffffffffu;
+}
 
 template <bool LAMBERT>
 S2D DISample eval_di(const DevScene& s, const Mat& m, const SD& sd, float3 in, float4 x, bool sn, float cp) {
     DISample c;
-    c.rnd = x; c.contrib = f3(0.f); c.wtoa = 0.f; c.mis = 0.f; c.dist = 0.f; c.dir = f3(0.f);
+    c.rnd = x; c.contrib = f3(0.f); c.wtoa = 0.f; c.mis = 0.f; c.dist = 0.f; c.dir = f3(0.f); c.vis = 1.f;
     const Illum r = sample_illum(s, x, sd.pos, sn);
     c.src_pdf = r.pdf;
     if (luminance(r.radiance) > 0.f && r.pdf > 0.f) {
@@ -89,9 +103,13 @@ S2D DISample eval_di(const DevScene& s, const Mat& m, const SD& sd, float3 in, f
 // (q) with pairwise power-heuristic MIS over the two domains' target pdfs.
 template <bool LAMBERT>
 S2D void reservoir_reuse(const PTParams& P, const Mat& m, const SD& sd, float3 in, float cp, const ReservoirRecord& q,
-                         DISample& cur, float& iw, float& M, Rng& rng, bool sn) {
+                         DISample& cur, float& iw, float& M, Rng& rng, bool sn, uint2* vstack) {
     const DevScene& s = P.scene;
-    const DISample nw = eval_di<LAMBERT>(s, m, sd, in, q.rnd, sn, cp);  // q's sample in the current domain
+    DISample nw = eval_di<LAMBERT>(s, m, sd, in, q.rnd, sn, cp);  // q's sample in the current domain
+    // reuse visibility (testrenderer.slang:611-616): the reused sample's contribution carries its
+    // visibility here, its target pdf stays unshadowed.  The reference also traces the current
+    // sample's visibility in q's domain, but only that sample's target pdf is used there.
+    if (vstack && nw.target() > 0.f && !di_visible(P, sd, nw, vstack)) nw.vis = 0.f;
     float phat_q = 0.f;                                                 // current sample in q's domain
     {
         SD sdq = make_shading_local(s, q.instance, q.primitive, q.local_pos, sn);
@@ -135,9 +153,10 @@ S2D bool camera_to_raster(const float* proj, const int* imin, const int* imax, f
 // screen-space reuse).
 template <bool LAMBERT, bool RESTIR>
 S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, float3 in, float3 thr, Rng& rng, uint32_t len,
-                               bool sn, uint32_t inst, uint32_t prim, uint32_t pixel, bool store_pixel) {
+                               bool sn, uint32_t inst, uint32_t prim, uint32_t pixel, bool store_pixel, uint2* vstack) {
     ShadowOut so;
     so.valid = false;
+    so.direct = false;
     const DevScene& s = P.scene;
     const float cp = (P.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
     float3 dir, contrib;
@@ -157,6 +176,13 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
             if (rng.next_float().x <= risw / wsum) best = c;
         }
         float iw = best.target() > 0.f ? wsum / ((float)P.restir_m * best.target()) : 0.f;
+        // gReSTIR_DI_Reuse_Visibility (testrenderer.slang:689-694): the canonical sample's visibility
+        // before reuse; an occluded one gets W = 0
+        uint2* vs = (vstack && (P.reuse || (P.ss_on && len == 1))) ? vstack : nullptr;
+        if (vs) {
+            if (best.target() > 0.f && !di_visible(P, sd, best, vs)) best.vis = 0.f;
+            if (!(best.vis > 0.f)) iw = 0.f;
+        }
         if (P.ss_on && len == 1) {
             // screen-space reuse at the primary vertex: the previous call's reservoirs at the
             // reprojected pixel and at ss_spatial random pixels within ss_radius of it, each
@@ -177,7 +203,7 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
                     if (!(fx >= 0.f && fy >= 0.f && fx < (float)P.width && fy < (float)P.height)) continue;
                     const ReservoirRecord rq = P.ss_prev[(uint32_t)fy * P.width + (uint32_t)fx];
                     if (!(rq.W > 0.f)) continue;
-                    reservoir_reuse<LAMBERT>(P, m, sd, in, cp, rq, best, iw, M, rng, sn);
+                    reservoir_reuse<LAMBERT>(P, m, sd, in, cp, rq, best, iw, M, rng, sn, vs);
                 }
             }
             if (store_pixel) {
@@ -208,7 +234,7 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
                         const uint32_t off = P.grid_prev.indices[cell];
                         const uint32_t k = rng.next().x % count;
                         const ReservoirRecord q = P.grid_prev.data[P.grid_prev.data_indices[off + k]];
-                        reservoir_reuse<LAMBERT>(P, m, sd, in, cp, q, best, iw, M, rng, sn);
+                        reservoir_reuse<LAMBERT>(P, m, sd, in, cp, q, best, iw, M, rng, sn, vs);
                     }
                 }
             }
@@ -228,7 +254,8 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
         }
         if (!(iw > 0.f)) return so;
         iw *= best.wtoa;  // 1/pdfA -> 1/pdfW
-        contrib = thr * best.contrib * iw;
+        contrib = thr * best.contrib * (iw * best.vis);
+        so.direct = vs != nullptr;  // visibility already traced: AddRadiance without a shadow ray (:742-743)
         w = best.mis;
         dir = best.dir;
         dist = best.dist;
@@ -270,6 +297,8 @@ template <bool RESTIR, bool CACHE> constexpr int kShadeMinBlocks = (RESTIR || CA
 
 template <bool LAMBERT, bool RESTIR, bool CACHE = false>
 __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(PTParams P, uint32_t parity) {
+    // traversal stacks of the inline reuse-visibility rays (ReSTIR variants only)
+    __shared__ uint2 vstack[RESTIR ? S2_STACK_SMEM * 128 : 1];
     const uint32_t count = P.counters[parity];
     const PathQueue qi = P.q[parity];
     const PathQueue qo = P.q[1 - parity];
@@ -386,7 +415,8 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                     const bool sing = mat_singular<LAMBERT>(m);
                     if (!sing && nee)
                         so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim, slot % P.pixels,
-                                                               aov && !P.views);
+                                                               aov && !P.views,
+                                                               (RESTIR && (P.flags & S2F_REUSE_VIS)) ? vstack + threadIdx.x : nullptr);
                     const float cp = fminf(1.f, cont_prob(m));
                     bool cont = true;
                     if (!(P.flags & S2F_NO_RR)) {
@@ -417,6 +447,10 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                         }
                     }
                 }
+            }
+            if (so.valid && so.direct) {
+                add_contrib(P, slot, so.c);
+                so.valid = false;
             }
             shadow = so.valid;
         }

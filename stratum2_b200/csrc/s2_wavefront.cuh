@@ -165,6 +165,7 @@ S2D void add_contrib(const PTParams& P, uint32_t slot, float3 v) {
 #define S2F_NO_ALPHA (1u << 12)
 #define S2F_NO_NORMAL_MAPS (1u << 13)
 #define S2F_CACHE (1u << 14)
+#define S2F_REUSE_VIS (1u << 18)
 
 constexpr int kTravBlock = 128;
 

@@ -107,3 +107,23 @@ def test_oracle_reuse_converges_to_nee(box):
     z = (m - gm) / np.sqrt(v + gv + (1e-5 * np.abs(gm) + 1e-9) ** 2)
     assert np.mean(np.abs(z) > 5) <= 0.01, np.sort(np.abs(z).ravel())[-5:]
     assert abs(z.mean()) < 0.25, z.mean()
+
+
+def test_oracle_reuse_visibility_first_call_and_second_call(box):
+    """gReSTIR_DI_Reuse_Visibility (testrenderer.slang:611-616, 689-694, 742-743) in the oracle:
+    without a previous grid the traced visibility changes nothing (an occluded canonical sample
+    contributes zero either way), so the first call equals plain reuse's bit for bit; with a grid
+    the reused samples differ."""
+    wl, osc = box
+    rect = (0, 0, 64, 64)
+    V = _abi.FLAG_RESTIR_REUSE_VISIBILITY
+    osc.render(wl.view, params(1, FLAGS), 64, 64, rect=rect, stride=8)
+    a = osc.render(wl.view, params(2, FLAGS | _abi.FLAG_RESTIR_REUSE), 64, 64, rect=rect, stride=8)["mean"]
+    osc.render(wl.view, params(1, FLAGS), 64, 64, rect=rect, stride=8)
+    b = osc.render(wl.view, params(2, FLAGS | _abi.FLAG_RESTIR_REUSE | V), 64, 64, rect=rect, stride=8)["mean"]
+    np.testing.assert_array_equal(a, b)
+    c = osc.render(wl.view, params(3, FLAGS | _abi.FLAG_RESTIR_REUSE | V), 64, 64, rect=rect, stride=8)["mean"]
+    osc.render(wl.view, params(1, FLAGS), 64, 64, rect=rect, stride=8)
+    osc.render(wl.view, params(2, FLAGS | _abi.FLAG_RESTIR_REUSE), 64, 64, rect=rect, stride=8)
+    d = osc.render(wl.view, params(3, FLAGS | _abi.FLAG_RESTIR_REUSE), 64, 64, rect=rect, stride=8)["mean"]
+    assert np.isfinite(c).all() and not np.array_equal(c, d)

@@ -136,3 +136,55 @@ def test_reuse_argument_errors(device, lights):
     with pytest.raises(_abi.S2Error) as e:
         render(device, wl, p)
     assert e.value.code == _abi.S2_ERR_INVALID
+
+
+VIS = _abi.FLAG_RESTIR_REUSE_VISIBILITY
+
+
+def test_reuse_visibility_first_call_equals_plain_reuse(device, lights):
+    """gReSTIR_DI_Reuse_Visibility without a previous grid: zeroing W of an occluded canonical
+    sample and adding the traced result directly change nothing, so the first call equals plain
+    reuse's first call (the RIS-only render)."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    render(device, wl, params(1, RIS | J, 4))  # drop any previous grid
+    a = render(device, wl, params(31, REUSE | LAM | J, 4, 2, 4)).radiance
+    render(device, wl, params(1, RIS | J, 4))
+    b = render(device, wl, params(31, REUSE | VIS | LAM | J, 4, 2, 4)).radiance
+    np.testing.assert_allclose(b, a, rtol=1e-6, atol=1e-9)
+
+
+def test_reuse_visibility_matches_the_oracle(device, lights):
+    """The reuse-visibility estimator (testrenderer.slang:611-616, 689-694, 742-743) is biased near
+    shadow boundaries (reused samples are weighted with unshadowed target pdfs), so the check is
+    against the oracle's restatement of the same estimator, not against plain NEE: 16 sequences
+    of 64 frames each, batch means compared by the z-test, and the per-frame error ratio to RIS
+    alone within 15 % of the oracle's."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    osc = OracleScene(wl.scene, 1)
+    ref = render(device, wl, params(700000, J | LAM, minl=2, maxl=2, spp=65536)).radiance[..., :3].astype(np.float64)
+
+    def err(imgs):
+        return float(np.mean((imgs - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    g, o = [], []
+    for b in range(16):
+        s0 = 300000 + 1000 * b
+        render(device, wl, params(s0 - 1, RIS | J, 4))  # drop the grid: a new sequence
+        g.append(frames(device, wl, REUSE | VIS | LAM, 4, s0, 64, 2, 2))
+        osc.render(wl.view, params(s0 - 1, RIS | LAM | J, 4, 2, 2), wl.width, wl.height)
+        o.append(np.stack([osc.render(wl.view, params(s0 + k, REUSE | VIS | LAM | J, 4, 2, 2), wl.width, wl.height)["mean"]
+                           for k in range(64)]))
+    g, o = np.stack(g), np.stack(o)
+    gm, om = g.mean(1), o.mean(1)
+    z = (gm.mean(0) - om.mean(0)) / np.sqrt(gm.var(0, ddof=1) / 16 + om.var(0, ddof=1) / 16 + 1e-12)
+    assert np.mean(np.abs(z) > 5) <= 2e-3, f"{np.mean(np.abs(z) > 5):.4%} of pixel channels with |z| > 5"
+    assert abs(z.mean()) < 0.15, z.mean()
+    ris = frames(device, wl, RIS | LAM, 4, 90000, 1024, 2, 2)
+    gpu_ratio = err(g.reshape(-1, *g.shape[2:])) / err(ris)
+    ris_o = np.stack([osc.render(wl.view, params(90000 + k, RIS | LAM | J, 4, 2, 2), wl.width, wl.height)["mean"]
+                      for k in range(1024)])
+    oracle_ratio = err(o.reshape(-1, *o.shape[2:])) / err(ris_o)
+    assert gpu_ratio < 0.92, gpu_ratio
+    assert abs(gpu_ratio - oracle_ratio) < 0.15 * oracle_ratio, (gpu_ratio, oracle_ratio)

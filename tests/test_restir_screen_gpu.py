@@ -148,3 +148,21 @@ def test_screen_reuse_argument_errors(device, lights):
     with pytest.raises(_abi.S2Error) as e:
         device.render(wl.view, wl.width, wl.height, params=p)
     assert e.value.code == _abi.S2_ERR_INVALID
+
+
+def test_screen_reuse_with_visibility_first_call_and_reproducible(device, lights):
+    """S2_FLAG_RESTIR_REUSE_VISIBILITY on the screen-space reuse: the first call equals the plain
+    screen-space first call (no previous reservoirs), and sequences reproduce bit for bit."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    V = _abi.FLAG_RESTIR_REUSE_VISIBILITY
+    img(device, wl.view, wl, params(1, RIS | J))  # drop previous reservoirs
+    a = img(device, wl.view, wl, params(40, SCREEN | LAM | J))
+    img(device, wl.view, wl, params(1, RIS | J))
+    b = img(device, wl.view, wl, params(40, SCREEN | V | LAM | J))
+    np.testing.assert_allclose(b, a, rtol=1e-6, atol=1e-9)
+    seqs = []
+    for _ in range(2):
+        img(device, wl.view, wl, params(1, RIS | J))
+        seqs.append(np.stack([img(device, wl.view, wl, params(50 + k, SCREEN | V | LAM | J)) for k in range(4)]))
+    np.testing.assert_array_equal(seqs[0], seqs[1])
