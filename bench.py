@@ -303,6 +303,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line["radiance_cache_kernels"] = cache_kernel_line(dev, args.steps)
         line["adjoint"] = adjoint_line(dev)
         line["restir_many_lights"] = restir_line(dev)
+        line["vcm_many_lights"] = vcm_line(dev)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         osc = cpu_oracle(wl)
@@ -502,6 +503,38 @@ def adjoint_line(dev, steps: int = 2) -> dict:
             "gradient_texels": int(sum(t.shape[0] * t.shape[1] for t in grads))}
 
 
+def vcm_line(dev, iterations: int = 3) -> dict:
+    """The VCM renderer (s2_render_vcm) on the many-lights frame: the cfg2 terrain carrying 100k
+    emissive triangles (the environment is black in this renderer), 1920x1080, paths of up to 6
+    segments (the VCM renderer's default), one light subpath per pixel, power-proportional light
+    pick.  Device time per iteration (a light pass and a camera pass) and rays traced per second,
+    for path tracing, BPT with the light vertex cache (the reference's default algorithm), BPT
+    connecting to whole light subpaths, and VCM."""
+    from stratum2_b200 import _abi
+    from stratum2_b200.scenegen import terrain_scene
+    wl = terrain_scene(emissive_triangles=100_000, emissive_sigma=2.0)
+    dev.upload_scene(wl.scene)
+    out = {"workload": "cfg2 terrain + 100k emissive triangles, 1920x1080, max path length 6, "
+                       "1 light subpath per pixel, Disney BSDF",
+           "kernels": "thread-per-path light and camera megakernels on the shared BVH8 traversal"}
+    for name, algo, fl in (("path_trace", _abi.VCM_PATH_TRACE, 0),
+                           ("bpt_light_vertex_cache", _abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE),
+                           ("bpt", _abi.VCM_BPT, 0), ("vcm", _abi.VCM_VCM, 0)):
+        p = dev.default_vcm_params()
+        p.algorithm, p.vcm_flags, p.iterations = algo, fl, 1
+        p.flags = _abi.FLAG_LIGHT_POWER_PICK
+        p.frame_seed = 7
+        dev.render_vcm(wl.view, wl.width, wl.height, p)  # warm-up
+        ms = rays = 0.0
+        for k in range(iterations):
+            p.frame_seed = 100 + k
+            st = dev.render_vcm(wl.view, wl.width, wl.height, p).stats
+            ms += st.gpu_ms
+            rays += st.extension_rays + st.shadow_rays
+        out[name] = {"ms_per_iteration": ms / iterations, "mrays_per_s": rays / ms / 1e3}
+    return out
+
+
 def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
     """Many-lights ReSTIR DI: the cfg2 terrain carrying 100k small emissive triangles of lognormal(0, 2)
     power, camera animated over `frames` frames along a seeded Catmull-Rom loop, 1920x1080, 1 spp per
@@ -586,6 +619,8 @@ def main():
                     help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
     ap.add_argument("--cached-frames", type=int, default=0, metavar="N",
                     help="render N 1-spp frames of the workload in the radiance-cache form and exit (profiling)")
+    ap.add_argument("--vcm-only", action="store_true",
+                    help="run only the VCM renderer measurement on the many-lights frame and print it")
     ap.add_argument("--restir-only", action="store_true",
                     help="run only the many-lights ReSTIR DI versus equal-time NEE comparison and print it")
     args = ap.parse_args()
@@ -608,6 +643,10 @@ def main():
     if args.cache_kernels:
         from stratum2_b200 import Device
         print(json.dumps(cache_kernel_line(Device(0), args.cache_kernels)))
+        return
+    if args.vcm_only:
+        from stratum2_b200 import Device
+        print(json.dumps(vcm_line(Device(0))))
         return
     if args.restir_only:
         from stratum2_b200 import Device
