@@ -693,8 +693,13 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
-    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN))
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RESTIR_SCREEN are supported by s2_render only");
+    if (prm->flags & S2_FLAG_RESTIR_SCREEN)
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_SCREEN is supported by s2_render only");
+    const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
+    if (reuse && (prm->restir_grid_cells > (1u << 26) || prm->restir_grid_cell_size < 0.f ||
+                  !std::isfinite(prm->restir_grid_cell_size) || !(prm->restir_grid_pixel_radius >= 0.f) ||
+                  !std::isfinite(prm->restir_grid_pixel_radius) || !(prm->restir_max_m > 0.f)))
+        return set_error(ctx, S2_ERR_INVALID, "invalid ReSTIR hash-grid parameters");
     const bool cache = (prm->flags & S2_FLAG_RADIANCE_CACHE) != 0;
     if (cache && !ctx->cache) return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RADIANCE_CACHE needs s2_cache_init");
     // radiance cache: training paths are extra paths after the views' (their own accumulators)
@@ -828,6 +833,38 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         if (rc != S2_OK) return set_error(ctx, rc, "material-sort buffer allocation failed");
         P.sort_on = 1; P.sort_keys = st->sort_keys; P.sort_perm = st->sort_perm; P.sort_hist = st->sort_hist;
     }
+    if (reuse) {
+        // ReSTIR DI hash-grid reuse across the views of the call, as TestRenderer renders all its
+        // views into one world-space grid (TestRenderer.cpp:488-493): the grid holds
+        // pixels x min(2, maxDepth-1) records per sample pass over all views, and its cell sizes
+        // follow view 0's camera.  This call appends to one grid of the pair and reads the other,
+        // the previous call's (s2_render's grids: either entry point continues the sequence).
+        const uint32_t cells = prm->restir_grid_cells ? prm->restir_grid_cells : 100000u;
+        const uint64_t per_pass = (uint64_t)pixels * std::max(1u, std::min(2u, prm->max_path_length ? prm->max_path_length - 1 : 1u));
+        const uint32_t size = (uint32_t)std::min<uint64_t>(per_pass * prm->spp, 1u << 24);
+        RenderState::Grid& cur = st->grid[st->grid_cur];
+        RenderState::Grid& prev = st->grid[st->grid_cur ^ 1];
+        const int rc = ensure_grid(ctx, cur, cells, size);
+        if (rc != S2_OK) return set_error(ctx, rc, "hash grid allocation failed");
+        HashGridDev& g = cur.g;
+        const S2View& v0 = views[0];
+        const int W0 = v0.image_max[0] - v0.image_min[0], H0 = v0.image_max[1] - v0.image_min[1];
+        g.min_cell_size = prm->restir_grid_cell_size > 0.f ? prm->restir_grid_cell_size : 0.5f;
+        g.cell_pixel_radius = prm->restir_grid_pixel_radius;
+        g.camera_position = make_float3(v0.camera_to_world[3], v0.camera_to_world[7], v0.camera_to_world[11]);
+        g.distance_scale = tanf(g.cell_pixel_radius * v0.projection[7] *
+                                std::max(1.f / (float)H0, (float)H0 / ((float)W0 * (float)W0)));
+        cudaMemsetAsync(g.checksums, 0, sizeof(uint32_t) * cells, s);
+        cudaMemsetAsync(g.cell_counters, 0, sizeof(uint32_t) * cells, s);
+        cudaMemsetAsync(g.other, 0, sizeof(uint32_t) * 4, s);
+        P.grid_cur = g;
+        P.grid_prev = prev.g;
+        P.prev_valid = st->grid_prev_valid && prev.g.checksums ? 1u : 0u;
+        P.reuse = 1;
+        P.max_m = prm->restir_max_m;
+    } else {
+        st->grid_prev_valid = false;  // a call without reuse drops the grids, as s2_render does
+    }
     if (cache) {
         // terminal-vertex queries of one iteration (at most a queue) and the training vertices of the
         // call; training paths accumulate into train_accum (zeroed per call)
@@ -910,6 +947,15 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     if (!*B->done_host) return set_error(ctx, S2_ERR_DEVICE, "batched render did not finish within its iteration bound");
+    if (reuse) {
+        // GpuHashGrid::build (GpuHashGrid.cpp:84-111), then this grid becomes the previous one
+        const HashGridDev& g = st->grid[st->grid_cur].g;
+        k_hg_compute_indices<<<(g.cell_count + 255) / 256, 256, 0, s>>>(g);
+        k_hg_swizzle<<<(g.max_size + 255) / 256, 256, 0, s>>>(g);
+        launches += 2;
+        st->grid_cur ^= 1u;
+        st->grid_prev_valid = true;
+    }
     if (cache) {
         // online training on this call's training paths (as after each wave of s2_render)
         k_cache_targets<<<std::max(1, st->shade_blocks / 2), 256, 0, s>>>(P);

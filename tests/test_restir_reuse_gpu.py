@@ -129,13 +129,48 @@ def test_reuse_argument_errors(device, lights):
     wl = lights
     device.upload_scene(wl.scene)
     p = params(1, REUSE | J, 4)
-    with pytest.raises(_abi.S2Error) as e:
-        device.render_views([wl.view], p)
-    assert e.value.code == _abi.S2_ERR_UNSUPPORTED
     p.restir_grid_cell_size = float("nan")
     with pytest.raises(_abi.S2Error) as e:
         render(device, wl, p)
     assert e.value.code == _abi.S2_ERR_INVALID
+    with pytest.raises(_abi.S2Error) as e:
+        device.render_views([wl.view], p)
+    assert e.value.code == _abi.S2_ERR_INVALID
+
+
+def batched(device, views, flags, m, seed, minl=1, maxl=6):
+    res, _ = device.render_views(views, params(seed, flags | J, m, minl, maxl))
+    return np.stack([r.radiance[..., :3].astype(np.float64) for r in res])
+
+
+def test_batched_reuse_first_call_is_ris(device, lights):
+    """s2_render_views with hash-grid reuse: without a previous grid the call is the RIS-only
+    batched render, bit for bit (fixed-point pixel totals)."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    views = [wl.view, wl.view]
+    a = batched(device, views, RIS | LAM, 4, 77, 2, 4)
+    b = batched(device, views, REUSE | LAM, 4, 77, 2, 4)  # the RIS-only call dropped the grids
+    np.testing.assert_array_equal(a, b)
+
+
+def test_batched_reuse_sequence_unbiased(device, lights):
+    """Several views reuse one world-space grid per call, as TestRenderer's views do: a sequence
+    of batched reuse calls over two views converges to plain NEE in both views."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    ref = np.stack([render(device, wl, params(600000 + 4096 * b, J | LAM, minl=2, maxl=4, spp=4096))
+                    .radiance[..., :3].astype(np.float64) for b in range(16)])
+    views = [wl.view, wl.view]
+    means = []
+    for b in range(16):
+        batched(device, views, RIS | LAM, 4, 40000 + 1000 * b - 1, 2, 4)  # new sequence
+        means.append(np.stack([batched(device, views, REUSE | LAM, 4, 40000 + 1000 * b + k, 2, 4)
+                               for k in range(128)]).mean(0))
+    means = np.stack(means)  # [batch, view, H, W, 3]
+    for v in range(2):
+        z_check(means[:, v].mean(0), means[:, v].var(0, ddof=1) / 16, ref.mean(0), ref.var(0, ddof=1) / 16,
+                f"batched reuse, view {v}")
 
 
 VIS = _abi.FLAG_RESTIR_REUSE_VISIBILITY
