@@ -693,8 +693,15 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
-    if (prm->flags & S2_FLAG_RESTIR_SCREEN)
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_SCREEN is supported by s2_render only");
+    if ((prm->flags & S2_FLAG_RESTIR_REUSE) && (prm->flags & S2_FLAG_RESTIR_SCREEN))
+        return set_error(ctx, S2_ERR_INVALID, "S2_FLAG_RESTIR_REUSE and S2_FLAG_RESTIR_SCREEN are exclusive");
+    const bool screen = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_SCREEN);
+    if (screen && (prm->flags & S2_FLAG_RADIANCE_CACHE))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "batched screen-space ReSTIR reuse takes no radiance cache");
+    if (screen && (prm->restir_spatial > 32 || !(prm->restir_spatial_radius >= 0.f) || !std::isfinite(prm->restir_spatial_radius) ||
+                   !(prm->restir_max_m > 0.f)))
+        return set_error(ctx, S2_ERR_INVALID, "invalid screen-space ReSTIR parameters (restir_spatial <= 32, "
+                                              "restir_spatial_radius >= 0, restir_max_m > 0)");
     const bool reuse = (prm->flags & S2_FLAG_RESTIR_DI) && (prm->flags & S2_FLAG_RESTIR_REUSE);
     if (reuse && (prm->restir_grid_cells > (1u << 26) || prm->restir_grid_cell_size < 0.f ||
                   !std::isfinite(prm->restir_grid_cell_size) || !(prm->restir_grid_pixel_radius >= 0.f) ||
@@ -865,6 +872,34 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     } else {
         st->grid_prev_valid = false;  // a call without reuse drops the grids, as s2_render does
     }
+    if (screen) {
+        // one reservoir per pixel of every view (views at their pixel offsets), kept for the next
+        // call with the same view layout
+        uint32_t key = 2166136261u;  // FNV-1a of the view extents
+        for (uint32_t x : layout) { key ^= x; key *= 16777619u; }
+        key |= 0x80000000u;
+        if (st->ss_pixels != (uint32_t)pixels || st->ss_width != key) {
+            free_bufs(st->ss_bufs);
+            st->ss_pixels = 0;
+            st->ss_prev_valid = false;
+            st->ss[0] = (ReservoirRecord*)dev_alloc(ctx, st->ss_bufs, sizeof(ReservoirRecord) * pixels);
+            st->ss[1] = (ReservoirRecord*)dev_alloc(ctx, st->ss_bufs, sizeof(ReservoirRecord) * pixels);
+            if (!st->ss[0] || !st->ss[1]) { free_bufs(st->ss_bufs); return set_error(ctx, S2_ERR_OOM, "reservoir buffer allocation failed"); }
+            st->ss_pixels = (uint32_t)pixels;
+            st->ss_width = key;
+        }
+        ReservoirRecord* cur = st->ss[st->ss_cur];
+        cudaMemsetAsync(cur, 0, sizeof(ReservoirRecord) * pixels, s);
+        P.ss_on = 1;
+        P.ss_cur = cur;
+        P.ss_prev = st->ss[st->ss_cur ^ 1u];
+        P.ss_prev_valid = st->ss_prev_valid ? 1u : 0u;
+        P.ss_spatial = prm->restir_spatial ? prm->restir_spatial : 5u;
+        P.ss_radius = prm->restir_spatial_radius > 0.f ? prm->restir_spatial_radius : 30.f;
+        P.max_m = prm->restir_max_m;
+    } else {
+        st->ss_prev_valid = false;
+    }
     if (cache) {
         // terminal-vertex queries of one iteration (at most a queue) and the training vertices of the
         // call; training paths accumulate into train_accum (zeroed per call)
@@ -963,6 +998,10 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         if (rc == S2_OK) rc = cache_adam_device(ctx, st->tr_cap, B->counters + C_TRAIN);
         if (rc != S2_OK) return rc;
         launches += 4;
+    }
+    if (screen) {  // this call's reservoirs become the previous ones
+        st->ss_cur ^= 1u;
+        st->ss_prev_valid = true;
     }
     B->accumulated_spp += prm->spp;
     const float scale = (float)(1.0 / (double)B->accumulated_spp) * exp2f(prm->exposure);

@@ -153,7 +153,8 @@ S2D bool camera_to_raster(const float* proj, const int* imin, const int* imax, f
 // screen-space reuse).
 template <bool LAMBERT, bool RESTIR>
 S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, float3 in, float3 thr, Rng& rng, uint32_t len,
-                               bool sn, uint32_t inst, uint32_t prim, uint32_t pixel, bool store_pixel, uint2* vstack) {
+                               bool sn, uint32_t inst, uint32_t prim, const ViewEntry* V, uint32_t pixel, bool store_pixel,
+                               uint2* vstack) {
     ShadowOut so;
     so.valid = false;
     so.direct = false;
@@ -178,20 +179,29 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
         float iw = best.target() > 0.f ? wsum / ((float)P.restir_m * best.target()) : 0.f;
         // gReSTIR_DI_Reuse_Visibility (testrenderer.slang:689-694): the canonical sample's visibility
         // before reuse; an occluded one gets W = 0
-        uint2* vs = (vstack && (P.reuse || (P.ss_on && len == 1))) ? vstack : nullptr;
+        // screen-space reuse at the primary vertex of an image path; V: its view in a batched call
+        const bool ss_here = P.ss_on && len == 1 && (!P.views || V != nullptr);
+        uint2* vs = (vstack && (P.reuse || ss_here)) ? vstack : nullptr;
         if (vs) {
             if (best.target() > 0.f && !di_visible(P, sd, best, vs)) best.vis = 0.f;
             if (!(best.vis > 0.f)) iw = 0.f;
         }
-        if (P.ss_on && len == 1) {
+        if (ss_here) {
             // screen-space reuse at the primary vertex: the previous call's reservoirs at the
             // reprojected pixel and at ss_spatial random pixels within ss_radius of it, each
-            // combined with the running reservoir by ReservoirReuse's two-domain resampling
+            // combined with the running reservoir by ReservoirReuse's two-domain resampling.  A
+            // batched call keeps one reservoir per pixel of every view, views at their pixel offsets.
+            const float* vproj = V ? V->proj : P.proj;
+            const int* vimin = V ? V->imin : P.imin;
+            const int* vimax = V ? V->imax : P.imax;
+            const uint32_t vw = V ? V->width : P.width, vh = V ? V->height : P.height;
+            const uint32_t base = V ? V->pixel_offset : 0u;
             float M = (float)P.restir_m;
             float2 pr;
             if (P.ss_prev_valid &&
-                camera_to_raster(P.proj, P.imin, P.imax,
-                                 prev_camera_point(P.prev_inv, xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos)), pr)) {
+                camera_to_raster(vproj, vimin, vimax,
+                                 prev_camera_point(V ? V->prev_inv : P.prev_inv,
+                                                   xform_point(s.motion_transforms + 3 * (size_t)inst, sd.pos)), pr)) {
                 for (uint32_t j = 0; j <= P.ss_spatial; ++j) {
                     float2 q = pr;
                     if (j > 0) {
@@ -199,9 +209,9 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
                         const float2 d = sample_concentric_disc(u.x, u.y);
                         q = make_float2(pr.x + d.x * P.ss_radius, pr.y + d.y * P.ss_radius);
                     }
-                    const float fx = floorf(q.x - (float)P.imin[0]), fy = floorf(q.y - (float)P.imin[1]);
-                    if (!(fx >= 0.f && fy >= 0.f && fx < (float)P.width && fy < (float)P.height)) continue;
-                    const ReservoirRecord rq = P.ss_prev[(uint32_t)fy * P.width + (uint32_t)fx];
+                    const float fx = floorf(q.x - (float)vimin[0]), fy = floorf(q.y - (float)vimin[1]);
+                    if (!(fx >= 0.f && fy >= 0.f && fx < (float)vw && fy < (float)vh)) continue;
+                    const ReservoirRecord rq = P.ss_prev[base + (uint32_t)fy * vw + (uint32_t)fx];
                     if (!(rq.W > 0.f)) continue;
                     reservoir_reuse<LAMBERT>(P, m, sd, in, cp, rq, best, iw, M, rng, sn, vs);
                 }
@@ -217,7 +227,7 @@ S2D ShadowOut connect_to_light(const PTParams& P, const Mat& m, const SD& sd, fl
                 rec.M = fminf(M, P.max_m * (float)P.restir_m);
                 rec.local_dir_in = in;
                 rec.pad = 0.f;
-                P.ss_cur[pixel] = rec;
+                P.ss_cur[base + pixel] = rec;
             }
         }
         if (P.reuse) {
@@ -413,9 +423,11 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                 }
                 if (!cached && len < P.max_len && any_pos(m.base())) {
                     const bool sing = mat_singular<LAMBERT>(m);
+                    // the path's view and pixel within it (batched training paths have neither)
+                    const ViewEntry* sview = (P.views && !(slot & kTrainSlot)) ? &P.views[(meta >> 16) & 0xffu] : nullptr;
+                    const uint32_t spix = sview ? slot - sview->pixel_offset : slot % P.pixels;
                     if (!sing && nee)
-                        so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim, slot % P.pixels,
-                                                               aov && !P.views,
+                        so = connect_to_light<LAMBERT, RESTIR>(P, m, sd, in, thr, rng, len, sn, inst, prim, sview, spix, aov,
                                                                (RESTIR && (P.flags & S2F_REUSE_VIS)) ? vstack + threadIdx.x : nullptr);
                     const float cp = fminf(1.f, cont_prob(m));
                     bool cont = true;

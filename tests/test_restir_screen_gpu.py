@@ -136,10 +136,11 @@ def test_many_lights_moving_camera_unbiased_and_lower_error(device, lights):
 def test_screen_reuse_argument_errors(device, lights):
     wl = lights
     device.upload_scene(wl.scene)
-    p = params(1, SCREEN | J)
+    p = params(1, SCREEN | J | _abi.FLAG_RADIANCE_CACHE)
     with pytest.raises(_abi.S2Error) as e:
         device.render_views([wl.view], p)
     assert e.value.code == _abi.S2_ERR_UNSUPPORTED
+    p = params(1, SCREEN | J)
     p.flags |= _abi.FLAG_RESTIR_REUSE
     with pytest.raises(_abi.S2Error) as e:
         device.render(wl.view, wl.width, wl.height, params=p)
@@ -166,3 +167,43 @@ def test_screen_reuse_with_visibility_first_call_and_reproducible(device, lights
         img(device, wl.view, wl, params(1, RIS | J))
         seqs.append(np.stack([img(device, wl.view, wl, params(50 + k, SCREEN | V | LAM | J)) for k in range(4)]))
     np.testing.assert_array_equal(seqs[0], seqs[1])
+
+
+def views_img(device, views, p):
+    res, _ = device.render_views(views, p)
+    return np.stack([r.radiance[..., :3].astype(np.float64) for r in res])
+
+
+def test_batched_screen_reuse_first_call_and_reproducible(device, lights):
+    """s2_render_views with screen-space reuse: one reservoir per pixel of every view.  Without
+    previous reservoirs the call is the RIS-only batched render bit for bit, and sequences
+    reproduce bit for bit."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    views = [wl.view, wl.view]
+    a = views_img(device, views, params(60, RIS | LAM | J))
+    b = views_img(device, views, params(60, SCREEN | LAM | J))  # the RIS-only call dropped the reservoirs
+    np.testing.assert_array_equal(a, b)
+    seqs = []
+    for _ in range(2):
+        views_img(device, views, params(1, RIS | J))
+        seqs.append(np.stack([views_img(device, views, params(70 + k, SCREEN | LAM | J)) for k in range(4)]))
+    np.testing.assert_array_equal(seqs[0], seqs[1])
+
+
+def test_batched_screen_reuse_converges_to_nee(device, lights):
+    """A sequence of batched screen-space reuse calls over two views converges to plain NEE in
+    both views (16 sequences of 64 calls against a 16 x 4096 spp NEE image)."""
+    wl = lights
+    device.upload_scene(wl.scene)
+    ref = np.stack([img(device, wl.view, wl, params(800000 + 4096 * b, J | LAM, spp=4096)) for b in range(16)])
+    views = [wl.view, wl.view]
+    means = []
+    for b in range(16):
+        views_img(device, views, params(60000 + 1000 * b - 1, RIS | J))  # new sequence
+        means.append(np.stack([views_img(device, views, params(60000 + 1000 * b + k, SCREEN | LAM | J))
+                               for k in range(64)]).mean(0))
+    means = np.stack(means)
+    for v in range(2):
+        z_check(means[:, v].mean(0), means[:, v].var(0, ddof=1) / 16, ref.mean(0), ref.var(0, ddof=1) / 16,
+                f"batched screen reuse, view {v}")
