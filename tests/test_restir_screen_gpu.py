@@ -191,19 +191,20 @@ def test_batched_screen_reuse_first_call_and_reproducible(device, lights):
     np.testing.assert_array_equal(seqs[0], seqs[1])
 
 
-def test_batched_screen_reuse_converges_to_nee(device, lights):
-    """A sequence of batched screen-space reuse calls over two views converges to plain NEE in
-    both views (16 sequences of 64 calls against a 16 x 4096 spp NEE image)."""
-    wl = lights
+def test_batched_screen_reuse_converges_to_fp64_golden(device):
+    """A sequence of batched screen-space reuse calls over two views of the box converges to the
+    FP64 golden image in both views, by the same z-test and sequence lengths as the single-view
+    box test (16 sequences of 256 calls)."""
+    wl = box_scene(seed=1, width=64, height=64)
     device.upload_scene(wl.scene)
-    ref = np.stack([img(device, wl.view, wl, params(800000 + 4096 * b, J | LAM, spp=4096)) for b in range(16)])
+    gold = np.load(GOLDEN / "box_64x64_fp64_16384spp.npz")
     views = [wl.view, wl.view]
     means = []
     for b in range(16):
-        views_img(device, views, params(60000 + 1000 * b - 1, RIS | J))  # new sequence
-        means.append(np.stack([views_img(device, views, params(60000 + 1000 * b + k, SCREEN | LAM | J))
-                               for k in range(64)]).mean(0))
+        views_img(device, views, params(1, RIS | J | LAM, minl=2, maxl=5))  # new sequence
+        means.append(np.mean([views_img(device, views, params(50000 + 256 * b + k, SCREEN | J | LAM, minl=2, maxl=5))
+                              for k in range(256)], axis=0))
     means = np.stack(means)
     for v in range(2):
-        z_check(means[:, v].mean(0), means[:, v].var(0, ddof=1) / 16, ref.mean(0), ref.var(0, ddof=1) / 16,
-                f"batched screen reuse, view {v}")
+        z_check(means[:, v].mean(0), means[:, v].var(0, ddof=1) / 16, gold["mean"], gold["var_of_mean"],
+                f"batched box screen reuse, view {v}")
