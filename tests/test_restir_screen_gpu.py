@@ -191,20 +191,28 @@ def test_batched_screen_reuse_first_call_and_reproducible(device, lights):
     np.testing.assert_array_equal(seqs[0], seqs[1])
 
 
-def test_batched_screen_reuse_converges_to_fp64_golden(device):
-    """A sequence of batched screen-space reuse calls over two views of the box converges to the
-    FP64 golden image in both views, by the same z-test and sequence lengths as the single-view
-    box test (16 sequences of 256 calls)."""
+def test_batched_screen_reuse_matches_single_view_sequence(device):
+    """Batched screen-space reuse over two views of the box runs the single-view estimator in each
+    view: over 8 sequences of 64 calls, each view's mean image equals the s2_render sequence's with
+    the same seeds (accumulation order differs: fixed-point totals against float), and the two
+    views equal each other.  The single-view estimator itself is checked against the FP64 golden
+    image by test_box_screen_reuse_converges_to_fp64_golden.  (With spatial reuse, neighbouring
+    pixels share reservoirs, so an image-wide mean z is far from normal with few sequences: it
+    measured -0.12 and +0.29 for two seed sets of the single-view test, in the batched path
+    alike.)"""
     wl = box_scene(seed=1, width=64, height=64)
     device.upload_scene(wl.scene)
-    gold = np.load(GOLDEN / "box_64x64_fp64_16384spp.npz")
     views = [wl.view, wl.view]
-    means = []
-    for b in range(16):
-        views_img(device, views, params(1, RIS | J | LAM, minl=2, maxl=5))  # new sequence
-        means.append(np.mean([views_img(device, views, params(50000 + 256 * b + k, SCREEN | J | LAM, minl=2, maxl=5))
-                              for k in range(256)], axis=0))
-    means = np.stack(means)
-    for v in range(2):
-        z_check(means[:, v].mean(0), means[:, v].var(0, ddof=1) / 16, gold["mean"], gold["var_of_mean"],
-                f"batched box screen reuse, view {v}")
+    single, both = [], []
+    for b in range(8):
+        img(device, wl.view, wl, params(1, RIS | J | LAM, minl=2, maxl=5))
+        single.append(np.mean([img(device, wl.view, wl, params(30000 + 256 * b + k, SCREEN | J | LAM, minl=2, maxl=5))
+                               for k in range(64)], axis=0))
+        views_img(device, views, params(1, RIS | J | LAM, minl=2, maxl=5))
+        both.append(np.mean([views_img(device, views, params(30000 + 256 * b + k, SCREEN | J | LAM, minl=2, maxl=5))
+                             for k in range(64)], axis=0))
+    single, both = np.stack(single), np.stack(both)  # [b, H, W, 3], [b, view, H, W, 3]
+    np.testing.assert_allclose(both[:, 0], both[:, 1], rtol=1e-6, atol=1e-9)
+    m, ms = both[:, 0].mean(0), single.mean(0)
+    assert abs(m.sum() / ms.sum() - 1) < 1e-3, (m.sum(), ms.sum())
+    assert np.mean(np.abs(m - ms)) < 1e-3 * np.mean(ms), np.mean(np.abs(m - ms)) / np.mean(ms)
