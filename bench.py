@@ -18,7 +18,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import tempfile
@@ -38,6 +37,10 @@ WORKLOAD = ("terrain 1024^2 grid (2.09M tris) + 64 icospheres (1.31M tris), GLTF
 # fetch + one 48-byte record per triangle fetch, with the fetch counts of the sequential
 # nearest-first BVH8 walk (the counting run).  NODE_PAYLOAD is the node's 80 bytes of content.
 NODE_BYTES, NODE_PAYLOAD, TRI_BYTES, RAY_BYTES, HIT_BYTES = 128, 80, 48, 32, 16
+# Algorithmic bytes of shading: a path's 64-byte state read, the 64-byte material record, 3 x (4-byte
+# index + 32 bytes of position/normal/uv), the 64-byte state written for a continuation ray, and a
+# 48-byte shadow-ray record per NEE sample.
+SHADE_IN_BYTES, SHADE_MAT_BYTES, SHADE_ATTR_BYTES, SHADE_OUT_BYTES, SHADOW_REC_BYTES = 64, 64, 3 * (4 + 32), 64, 48
 GOLDEN_CFG2 = ROOT / "tests" / "golden" / "cfg2_1920x1080_subset30_fp64_262144spp.npz"
 RELMSE_TARGET = 0.01
 
@@ -50,13 +53,11 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-def extend_traffic_per_ray() -> float | None:
-    """DRAM bytes per extension ray of k_extend from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "k_extend_terrain.md"
-    if not p.exists():
-        return None
-    m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+-]+)", p.read_text())
-    return float(m.group(1)) if m else None
+def bench_config(world: int, triangles: int) -> dict:
+    """The `config` object of both arms' JSON lines (identical keys and values)."""
+    return {"workload": WORKLOAD, "width": 1920, "height": 1080, "spp": SPP, "min_path_length": MIN_LEN,
+            "max_path_length": MAX_LEN, "triangles": int(triangles), "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"dp{world}: disjoint sample seeds per rank, images summed into rank 0"}
 
 
 class ClockSampler:
@@ -139,11 +140,11 @@ def run_reference(args, rank: int, world: int):
     Vulkan/Slang implementation cannot be built or run here)."""
     if rank != 0:
         return
-    from stratum2_b200 import _abi
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import default_render_params  # noqa: E402 (the oracle's defaults: no product library)
     from stratum2_b200.scenegen import terrain_scene
     wl = terrain_scene()
-    p = _abi.S2RenderParams()
-    _abi.lib().s2_default_render_params(p)
+    p = default_render_params()
     p.spp, p.min_path_length, p.max_path_length = SPP, MIN_LEN, MAX_LEN
     threads = os.cpu_count() or 1
     osc = cpu_oracle(wl)
@@ -160,8 +161,7 @@ def run_reference(args, rank: int, world: int):
     line = {"metric": "Mrays/s", "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "min_path_length": MIN_LEN,
-                                                     "max_path_length": MAX_LEN, "spp": SPP},
+            "data": "synthetic (seeded scene generator, no datasets)", "config": bench_config(world, wl.scene.triangle_count()),
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port",
                              "sample": f"pixel subset (stride {r['stride']}, {r['pixels']} pixels) x {SPP} spp per step"},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -251,12 +251,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     avg_launch_s = ext_ms / 1e3 / max(ext_launches, 1)
     achieved = bytes_per_ray * rays_per_launch / avg_launch_s / 1e9
     pk = peaks()
-    tpr = extend_traffic_per_ray()
     dominant = max([("k_extend", ext_ms), ("k_shade", sh_ms), ("k_occlude", oc_ms)], key=lambda x: x[1])[0]
     roof = {"kernel": "k_extend", "dominant_kernel": dominant, "bound": "hbm", "achieved": achieved,
             "peak": pk["hbm_gbs"], "peak_source": pk["source"] + " copy bandwidth", "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"],
-            "traffic": (tpr * rays_per_launch) if tpr is not None else None,
+            "traffic": None,
+            "traffic_note": "DRAM bytes are not measurable inside the timed run; the ncu figures per launch are "
+                            "in profiles/k_extend_terrain.md",
             "algorithmic_bytes_per_launch": bytes_per_ray * rays_per_launch,
             "bytes_per_ray": bytes_per_ray,
             "byte_model": "32 ray + 16 hit + 128 per node fetch + 48 per triangle fetch; fetch counts of the "
@@ -265,20 +266,30 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "node_fetches_per_ray": n_node,
             "tri_fetches_per_ray": n_tri,
             "avg_launch_ms": avg_launch_s * 1e3}
+    # shading: the measurement plan's byte model per shaded path vertex (state in, hit, material
+    # record, three indices + attributes), per continuation (state out) and per shadow ray record
+    sh_launches = sum(s.shade_launches for s in stats)
+    shade_bytes = ext_rays * (SHADE_IN_BYTES + HIT_BYTES + SHADE_MAT_BYTES + SHADE_ATTR_BYTES) + \
+        (ext_rays - sum(s.paths for s in stats)) * SHADE_OUT_BYTES + sum(s.shadow_rays for s in stats) * SHADOW_REC_BYTES
+    sh_achieved = shade_bytes / max(sh_ms, 1e-9) / 1e6
+    roof_shade = {"kernel": "k_shade", "bound": "hbm", "achieved": sh_achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                  "frac": sh_achieved / pk["hbm_gbs"], "traffic": None,
+                  "algorithmic_bytes_per_launch": shade_bytes / max(sh_launches, 1),
+                  "avg_launch_ms": sh_ms / max(sh_launches, 1),
+                  "byte_model": "per shaded vertex 64 state in + 16 hit + 64 material + 108 indices/attributes; "
+                                "64 per continuation ray written; 48 per shadow-ray record (misses counted as hits)"}
     line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, no datasets)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "min_path_length": MIN_LEN,
-                       "max_path_length": MAX_LEN, "triangles": int(dev.bvh_stats.triangle_count),
-                       "bvh8_nodes": int(dev.bvh_stats.node_count), "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"{world} rank(s), disjoint sample seeds",
-                       "tuning": (tuning or {}).get("tuning", "defaults"),
-                       "autotune_trials": (tuning or {}).get("trials", 0)},
+            "config": bench_config(world, wl.scene.triangle_count()),
+            "bvh8_nodes": int(dev.bvh_stats.node_count),
+            "tuning": {"values": (tuning or {}).get("tuning", "defaults"), "autotune_trials": (tuning or {}).get("trials", 0)},
             "mpaths_per_s": paths / ms / 1e3,
             "kernel_ms_per_step": {"k_extend": ext_ms / args.steps, "k_shade": sh_ms / args.steps,
                                    "k_occlude": oc_ms / args.steps},
             "gpu_launches": int(sum(s.kernel_launches for s in stats)),
             "roofline": roof,
+            "roofline_shade": roof_shade,
             "e2e": {"value": e2e_rays / e2e_s / 1e6, "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(C_sizeof_view_params()),
                     "d2h_bytes_per_step": int(W * H * (16 + 16 + 8 + 16 + 8 + 8)),
@@ -662,9 +673,20 @@ def main():
         print(json.dumps({"gpu_ms": r.stats.gpu_ms, "extension_rays": r.stats.extension_rays,
                           "shadow_rays": r.stats.shadow_rays}))
         return
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: relaunch this command under torchrun with --gpus ranks
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} disagrees with WORLD_SIZE={world} from the launcher")
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

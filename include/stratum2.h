@@ -223,7 +223,13 @@ typedef struct S2RenderParams {
     float restir_spatial_radius;     /* S2_FLAG_RESTIR_SCREEN: neighbour radius in pixels (0 = 30) */
     float light_subpaths;            /* S2_FLAG_LIGHT_TRACE: light subpaths per sample pass =
                                         max(1, pixels x light_subpaths) (mLightSubpathCount, 0 = 1) */
-    uint32_t reserved[2];
+    float cache_min_roughness;       /* S2_FLAG_RADIANCE_CACHE: path regularisation (no counterpart in
+                                        the reference).  Once a path has left a vertex of roughness >=
+                                        this value, every later vertex's roughness is raised to at least
+                                        it, so glossy reflections of small bright lights seen through a
+                                        rough bounce (caustics) are blurred instead of sampled as rare
+                                        fireflies.  Biased; 0 = off (default) */
+    uint32_t reserved;
 } S2RenderParams;
 
 /* Output AOVs (caller-allocated, device or host pointers per s2_render's `out_on_host`).
@@ -310,9 +316,11 @@ void s2_default_render_params(S2RenderParams* p);
  * library, held on every GPU that loads it until the process exits, and radiance accumulates in
  * the caller's output.  Allocates nothing.
  *   - `out` holds DEVICE pointers; out->radiance is required; other AOVs may be NULL.
- *   - Views above 322,618 pixels (64 MiB / 208 bytes per path, e.g. 512x512 fits, 1920x1080 does
- *     not) are rejected with S2_ERR_INVALID.  S2_FLAG_ACCUMULATE and S2_FLAG_PROFILE_KERNELS are
- *     rejected.
+ *   - Views above 322,603 pixels (64 MiB less a 4 KiB header and 13 x 256 bytes of stream
+ *     alignment, / 208 bytes per path; e.g. 512x512 fits, 1920x1080 does not) are rejected with
+ *     S2_ERR_INVALID.  S2_FLAG_ACCUMULATE and S2_FLAG_PROFILE_KERNELS are rejected, and so are
+ *     the modes with buffers of their own (ReSTIR reuse, radiance cache, light tracing:
+ *     S2_ERR_UNSUPPORTED).
  *   - The first call on a device looks up the array's address; make it before any stream capture.
  *   - Calls share the array: calls whose GPU work overlaps race; serialise them. */
 int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams* params,

@@ -131,7 +131,7 @@ class S2RenderParams(C.Structure):
         ("restir_grid_cell_size", C.c_float), ("restir_grid_pixel_radius", C.c_float),
         ("cache_bounces", C.c_uint32), ("cache_train_paths", C.c_uint32), ("restir_spatial", C.c_uint32),
         ("restir_spatial_radius", C.c_float), ("light_subpaths", C.c_float),
-        ("reserved", C.c_uint32 * 2),
+        ("cache_min_roughness", C.c_float), ("reserved", C.c_uint32),
     ]
 
 

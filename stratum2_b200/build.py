@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -48,6 +49,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "stratum2.h"]
     objs = []
     log = []
+    jobs = []
     for src in CUDA_SOURCES + CXX_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
@@ -59,7 +61,11 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         else:
             cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-fopenmp",
                    "-I", str(CSRC), "-c", str(s), "-o", str(o)]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append(cmd)
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda c: (c, subprocess.run(c, capture_output=True, text=True)), jobs))
+    for cmd, r in results:
         log.append(r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

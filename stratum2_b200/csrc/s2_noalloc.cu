@@ -19,7 +19,9 @@
 //    must start at zero.  Calls whose GPU work overlaps (other streams, other host threads) race
 //    on the array: serialise them.
 //  * Outputs are device pointers; the radiance buffer is required.  S2_FLAG_ACCUMULATE and
-//    S2_FLAG_PROFILE_KERNELS are rejected (they need state or events this variant does not keep).
+//    S2_FLAG_PROFILE_KERNELS are rejected (they need state or events this variant does not keep),
+//    and so are the modes that need buffers of their own: ReSTIR reuse, the radiance cache and
+//    light tracing.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -42,9 +44,13 @@ namespace nak = s2_noalloc_impl;
 
 #define S2_NOALLOC_SCRATCH_BYTES (64ull << 20)
 #define S2_NOALLOC_HEADER_BYTES 4096ull
-// per path: two path queues (2 x 64 B), hit (16 B), shadow ray (48 B), accumulator (16 B)
+// per path: two path queues (2 x 64 B), hit (16 B), shadow ray (48 B), accumulator (16 B), in 13
+// streams of 16 bytes per path, each stream's start rounded up to 256 bytes
 #define S2_NOALLOC_PATH_BYTES 208ull
-#define S2_NOALLOC_MAX_PIXELS ((S2_NOALLOC_SCRATCH_BYTES - S2_NOALLOC_HEADER_BYTES) / S2_NOALLOC_PATH_BYTES)
+#define S2_NOALLOC_STREAMS 13ull
+#define S2_NOALLOC_MAX_PIXELS \
+    ((S2_NOALLOC_SCRATCH_BYTES - S2_NOALLOC_HEADER_BYTES - 256ull * S2_NOALLOC_STREAMS) / S2_NOALLOC_PATH_BYTES)
+static_assert(S2_NOALLOC_MAX_PIXELS == 322603ull, "documented pixel limit of s2_render_noalloc");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[S2_NOALLOC_SCRATCH_BYTES];
 
@@ -53,11 +59,11 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
-int g_blocks[kMaxDevices][3] = {};  // persistent grid sizes: extend, occlude, shade
+int g_blocks[kMaxDevices][4] = {};  // persistent grid sizes: extend, occlude, shade, ReSTIR shade
 
 // Once per device, with that device current: the device address of the scratch array and the
 // occupancy-derived grid sizes.
-int noalloc_setup(S2Context* ctx, unsigned char** scratch, int blocks[3]) {
+int noalloc_setup(S2Context* ctx, unsigned char** scratch, int blocks[4]) {
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return s2::set_error(ctx, S2_ERR_UNSUPPORTED, "device index too large");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_ptr[ctx->device]) {
@@ -78,10 +84,13 @@ int noalloc_setup(S2Context* ctx, unsigned char** scratch, int blocks[3]) {
         g_blocks[ctx->device][1] = std::max(1, b) * prop.multiProcessorCount;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, nak::k_shade<false, false>, 128, 0);
         g_blocks[ctx->device][2] = std::max(1, b) * prop.multiProcessorCount;
+        // the ReSTIR variants keep more state live and are compiled for fewer blocks per SM
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, nak::k_shade<false, true>, 128, 0);
+        g_blocks[ctx->device][3] = std::max(1, b) * prop.multiProcessorCount;
         g_scratch_ptr[ctx->device] = (unsigned char*)p;
     }
     *scratch = g_scratch_ptr[ctx->device];
-    std::memcpy(blocks, g_blocks[ctx->device], sizeof(int) * 3);
+    std::memcpy(blocks, g_blocks[ctx->device], sizeof(int) * 4);
     return S2_OK;
 }
 
@@ -115,20 +124,20 @@ extern "C" int s2_render_noalloc(S2Context* ctx, const S2View* view, const S2Ren
                                                   std::to_string(S2_NOALLOC_MAX_PIXELS) + " pixels (64 MiB scratch array)");
     if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
-    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE))
-        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE, S2_FLAG_RESTIR_SCREEN and S2_FLAG_RADIANCE_CACHE are "
-                                                  "supported by s2_render only");
+    if (prm->flags & (S2_FLAG_RESTIR_REUSE | S2_FLAG_RESTIR_SCREEN | S2_FLAG_RADIANCE_CACHE | S2_FLAG_LIGHT_TRACE))
+        return set_error(ctx, S2_ERR_UNSUPPORTED, "S2_FLAG_RESTIR_REUSE, S2_FLAG_RESTIR_SCREEN, S2_FLAG_RADIANCE_CACHE and "
+                                                  "S2_FLAG_LIGHT_TRACE are supported by s2_render only");
     if ((prm->flags & S2_FLAG_RESTIR_DI) && (prm->restir_candidates == 0 || prm->restir_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "restir_candidates must be in 1..1024");
     cudaSetDevice(ctx->device);
     unsigned char* scratch = nullptr;
-    int blocks[3];
+    int blocks[4];
     int rc = noalloc_setup(ctx, &scratch, blocks);
     if (rc != S2_OK) return rc;
     cudaStream_t s = ctx->stream;
 
     const uint32_t pixels = (uint32_t)pixels64;
-    const uint64_t target = prm->wave_paths ? prm->wave_paths : (1u << 22);
+    const uint64_t target = prm->wave_paths ? prm->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (1u << 22));
     const uint64_t max_paths = std::min<uint64_t>(target, S2_NOALLOC_MAX_PIXELS);
     const uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(prm->spp, max_paths / pixels));
     const size_t cap = (size_t)slots * pixels;
@@ -172,6 +181,9 @@ extern "C" int s2_render_noalloc(S2Context* ctx, const S2View* view, const S2Ren
     P.frame_seed = prm->frame_seed;
     P.restir_m = prm->restir_candidates ? prm->restir_candidates : 32;
     P.exposure = prm->exposure;
+    P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;  // traversal tuning, as s2_render takes it
+    P.trav.vote8 = ctx->tuning.trav_vote8;
+    P.refill_min = ctx->tuning.refill_min;
     P.counters = counters;
     P.stats = stats;
     P.status = ctx->status_dev;
@@ -202,10 +214,10 @@ extern "C" int s2_render_noalloc(S2Context* ctx, const S2View* view, const S2Ren
             if (count) k_extend<true><<<blocks[0], kTravBlock, 0, s>>>(P, parity);
             else k_extend<false><<<blocks[0], kTravBlock, 0, s>>>(P, parity);
             if (lam) {
-                if (restir) k_shade<true, true><<<blocks[2], 128, 0, s>>>(P, parity);
+                if (restir) k_shade<true, true><<<blocks[3], 128, 0, s>>>(P, parity);
                 else k_shade<true, false><<<blocks[2], 128, 0, s>>>(P, parity);
             } else {
-                if (restir) k_shade<false, true><<<blocks[2], 128, 0, s>>>(P, parity);
+                if (restir) k_shade<false, true><<<blocks[3], 128, 0, s>>>(P, parity);
                 else k_shade<false, false><<<blocks[2], 128, 0, s>>>(P, parity);
             }
             if (count) k_occlude<true><<<blocks[1], kTravBlock, 0, s>>>(P);

@@ -415,6 +415,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         if (rc != S2_OK) return set_error(ctx, rc, "radiance cache queue allocation failed");
         P.cache_on = 1;
         P.cache_len = cache_len;
+        P.cache_rough = std::min(1.f, std::max(0.f, prm->cache_min_roughness));
         P.cq_pos = st->cq_pos; P.cq_thr = st->cq_thr; P.cq_cap = st->cq_cap;
         P.tr_pos = st->tr_pos; P.tr_thr = st->tr_thr; P.tr_rad = st->tr_rad; P.tr_cap = st->tr_cap;
     }
@@ -918,6 +919,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
         P.accum = B->train_accum;
         P.cache_on = 1;
         P.cache_len = (prm->cache_bounces ? prm->cache_bounces : 2u) + 1u;
+        P.cache_rough = std::min(1.f, std::max(0.f, prm->cache_min_roughness));
         P.cq_pos = st->cq_pos; P.cq_thr = st->cq_thr; P.cq_cap = st->cq_cap;
         P.tr_pos = st->tr_pos; P.tr_thr = st->tr_thr; P.tr_rad = st->tr_rad; P.tr_cap = st->tr_cap;
     }

@@ -373,7 +373,13 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                 if (!(P.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
                 const float isect_dist = half_round(h.x);
                 const float isect_pdfa = half_round(light_pdfa(s, inst, sd.area));
-                const Mat m = load_material(s, sd.mat, sd.uv);
+                Mat m = load_material(s, sd.mat, sd.uv);
+                uint32_t rough_path = 0u;  // meta bit 10 of the continuation: cache-form regularisation
+                if (CACHE && P.cache_on && P.cache_rough > 0.f) {
+                    if ((meta & 0x400u) && m.roughness() < P.cache_rough)
+                        m.w[2] = (m.w[2] & ~0xff00u) | (pk8(P.cache_rough) << 8);
+                    if ((meta & 0x400u) || LAMBERT || m.roughness() >= P.cache_rough) rough_path = 0x400u;
+                }
                 const float3 in = sd.to_local(-dir);
                 const float cos_in = fabsf(in.z);
                 if (aov) {
@@ -454,7 +460,8 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                             alive = true;
                             n0 = make_float4(org.x, org.y, org.z, dir_pdf);
                             n1 = make_float4(nd.x, nd.y, nd.z, thr.x);
-                            n2 = make_float4(thr.y, thr.z, __uint_as_float(slot), __uint_as_float((meta & ~0xffu) | len));
+                            n2 = make_float4(thr.y, thr.z, __uint_as_float(slot),
+                                             __uint_as_float((meta & ~0xffu) | len | rough_path));
                             n3 = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
                         }
                     }

@@ -69,9 +69,21 @@ def cfg2_case():
     return wl, p
 
 
-SUBSET = {"cfg2_1920x1080_subset30": ((15, 15, 1920, 1080), 30)}
+def cfg5_case():
+    """The learned-cache workload: the benchmark terrain with 8 area lights (1920x1080, 5e3 sun,
+    path length 3..12, pixel centres), on the same pixel subset as cfg2_case."""
+    wl = terrain_scene(seed=2, area_lights=8)
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length = 3, 12
+    p.flags = 0
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    return wl, p
+
+
+SUBSET = {"cfg2_1920x1080_subset30": ((15, 15, 1920, 1080), 30), "cfg5_1920x1080_subset30": ((15, 15, 1920, 1080), 30)}
 CASES = {"box_64x64": (box_case, 16384), "terrain_64x36": (terrain_case, 131072), "cutout_64x64": (cutout_case, 16384),
-         "cfg2_1920x1080_subset30": (cfg2_case, 262144)}
+         "cfg2_1920x1080_subset30": (cfg2_case, 262144), "cfg5_1920x1080_subset30": (cfg5_case, 262144)}
 
 
 def make(name: str, out_dir: Path = HERE):

@@ -62,6 +62,21 @@ def ref_compat() -> C.CDLL | None:
     return _r
 
 
+def default_render_params():
+    """Render parameters with the reference's defaults (TestRenderer.cpp:38-43, 52: maxDepth 5,
+    environment sample probability 0.9, 32 RIS candidates, M cap 3, 100,000 hash-grid cells of size
+    0.5), filled on the host without loading the product library."""
+    from stratum2_b200 import _abi
+    p = _abi.S2RenderParams()
+    p.min_path_length, p.max_path_length, p.exposure, p.spp = 0, 5, 0.0, 1
+    p.environment_sample_probability = 0.9
+    p.restir_candidates = 32
+    p.restir_max_m = 3.0
+    p.restir_grid_cells = 100000
+    p.restir_grid_cell_size = 0.5
+    return p
+
+
 class OracleScene:
     """An oracle copy of a packed scene (precision_mask: 1 = FP64, 2 = FP32-exact, 3 = both)."""
 

@@ -59,5 +59,57 @@ def test_no_alloc_render_matches_s2_render_on_two_calls():
         rc = lib.s2_render_noalloc(dev._h, C.byref(big), C.byref(p), C.byref(aovs), None)
         assert rc == _abi.S2_ERR_INVALID
         assert b"scratch limit" in lib.s2_last_error(dev._h)
+        # modes that need buffers of their own are refused, not rendered as plain path tracing
+        for flag in (_abi.FLAG_LIGHT_TRACE, _abi.FLAG_RESTIR_REUSE, _abi.FLAG_RESTIR_SCREEN, _abi.FLAG_RADIANCE_CACHE):
+            q = _params(1, 7)
+            q.flags |= flag
+            rc = lib.s2_render_noalloc(dev._h, C.byref(wl.view), C.byref(q), C.byref(aovs), None)
+            assert rc == _abi.S2_ERR_UNSUPPORTED, hex(flag)
+    finally:
+        dev.close()
+
+
+def test_no_alloc_restir_matches_s2_render():
+    """RIS (S2_FLAG_RESTIR_DI without reuse) through the allocation-free entry point, whose ReSTIR
+    shade variant runs on its own grid, equals s2_render's image on two calls in a row."""
+    wl = box_scene(seed=1, width=48, height=40)
+    dev = Device(0)
+    try:
+        dev.upload_scene(wl.scene)
+        p = _params(8, 11)
+        p.flags |= _abi.FLAG_RESTIR_DI
+        p.restir_candidates = 8
+        ref = dev.render(wl.view, wl.width, wl.height, params=p)
+        rad = torch.empty((wl.height, wl.width, 4), dtype=torch.float32, device="cuda")
+        aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+        lib = _abi.lib()
+        for call in range(2):
+            rad.fill_(-1.0)
+            rc = lib.s2_render_noalloc(dev._h, C.byref(wl.view), C.byref(p), C.byref(aovs), None)
+            assert rc == _abi.S2_OK, lib.s2_last_error(dev._h).decode()
+            torch.cuda.synchronize()
+            np.testing.assert_allclose(rad.cpu().numpy(), ref.radiance, rtol=1e-6, atol=1e-7, err_msg=f"call {call}")
+    finally:
+        dev.close()
+
+
+def test_no_alloc_view_at_the_pixel_limit():
+    """A view of exactly 322,603 pixels (the documented limit) renders; one pixel more is refused."""
+    limit = 322_603
+    wl = box_scene(seed=1, n_random=50, width=limit, height=1)
+    dev = Device(0)
+    try:
+        dev.upload_scene(wl.scene)
+        p = _params(1, 3)
+        rad = torch.empty((1, limit, 4), dtype=torch.float32, device="cuda")
+        aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+        lib = _abi.lib()
+        rc = lib.s2_render_noalloc(dev._h, C.byref(wl.view), C.byref(p), C.byref(aovs), None)
+        assert rc == _abi.S2_OK, lib.s2_last_error(dev._h).decode()
+        torch.cuda.synchronize()
+        assert torch.isfinite(rad).all()
+        over = box_scene(seed=1, n_random=50, width=limit + 1, height=1).view
+        rc = lib.s2_render_noalloc(dev._h, C.byref(over), C.byref(p), C.byref(aovs), None)
+        assert rc == _abi.S2_ERR_INVALID and b"scratch limit" in lib.s2_last_error(dev._h)
     finally:
         dev.close()
