@@ -41,8 +41,13 @@ NODE_BYTES, NODE_PAYLOAD, TRI_BYTES, RAY_BYTES, HIT_BYTES = 128, 80, 48, 32, 16
 # index + 32 bytes of position/normal/uv), the 64-byte state written for a continuation ray, and a
 # 48-byte shadow-ray record per NEE sample.
 SHADE_IN_BYTES, SHADE_MAT_BYTES, SHADE_ATTR_BYTES, SHADE_OUT_BYTES, SHADOW_REC_BYTES = 64, 64, 3 * (4 + 32), 64, 48
-GOLDEN_CFG2 = ROOT / "tests" / "golden" / "cfg2_1920x1080_subset30_fp64_262144spp.npz"
+GOLDEN_CFG5 = ROOT / "tests" / "golden" / "cfg5_1920x1080_subset30_fp64_262144spp.npz"
 RELMSE_TARGET = 0.01
+CACHE_WARMUP_FRAMES = 64      # radiance-cache forms: training frames before accumulation starts
+CACHE_MIN_ROUGHNESS = 0.35    # path regularisation of the 2-bounce cache form
+# environment sampling of every estimator on the learned-cache scene: the bilinear-footprint pdf,
+# whose expected image equals the texel pdf's (the sun of one texel otherwise leaves its bilinear
+# halo to BSDF sampling)
 
 
 def peaks() -> dict:
@@ -298,18 +303,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "clocks": ck}
     if world == 1 and not args.no_quality:
         line["batched_16_views"] = batched_line(dev, args.steps)
-        if GOLDEN_CFG2.exists():
-            line["time_to_relmse_0.01"] = {
-                "plain": time_to_quality(dev, wl, False, 50000, max_spp=args.quality_spp),
-                "batched": time_to_quality(dev, wl, True, 50000, max_spp=args.quality_spp),
-                "cached_1_bounce": time_to_quality(dev, wl, False, 50000, chunk=1, max_spp=1024, cache_bounces=1),
-                "cached_2_bounces": time_to_quality(dev, wl, False, 50000, chunk=1, max_spp=1024, cache_bounces=2),
-                "batched_cached_1_bounce": time_to_quality(dev, wl, True, 50000, chunk=1, max_spp=1024, cache_bounces=1),
-                "reference_image": f"FP64 oracle, {int(np.load(GOLDEN_CFG2)['spp'])} spp, 64x36 pixel subset (stride 30)",
-                "note": "GPU time of progressive calls (plain/batched: independent 128-spp calls averaged, past the "
-                        "budget the expected time from the mean single-call relMSE as relMSE ~ 1/spp; cached: 1 spp "
-                        "frames of the radiance-cache form with online training, measured; batched_cached: the same "
-                        "through the batched streaming entry point s2_render_views)"}
+        if GOLDEN_CFG5.exists():
+            line["time_to_relmse_0.01"] = quality_line(dev, args)
     if world == 1 and not args.no_quality:
         line["radiance_cache_kernels"] = cache_kernel_line(dev, args.steps)
         line["adjoint"] = adjoint_line(dev)
@@ -339,64 +334,111 @@ def batched_views(seed: int = 7, n: int = 16):
     return views
 
 
-def time_to_quality(dev, wl, batched: bool, seed0: int, chunk: int = 128, max_spp: int = 2048,
-                    cache_bounces: int = 0) -> dict:
-    """GPU milliseconds of progressive rendering (`chunk` spp per call, S2_FLAG_ACCUMULATE) until the
-    relMSE (eps 1e-2) of the 64x36 pixel subset (x = 15 + 30 i, y = 15 + 30 j) against the FP64
-    oracle image reaches 0.01, or until `max_spp`.  The oracle image's own noise (its variance of
-    the mean, relMSE ~1e-3 at 262144 spp) is subtracted.  When the budget ends first, the time is
-    the expected time of an unbiased estimator (relMSE proportional to 1/spp), predicted from the
-    mean relMSE of the independent `chunk`-spp renders (a statistic of every chunk, where the
-    cumulative image's relMSE swings with single fireflies), and marked so.
-    `batched` uses the streaming entry point s2_render_views.  cache_bounces > 0: the radiance-cache
-    form (S2_FLAG_RADIANCE_CACHE, freshly initialised cache trained online; `chunk` spp per frame),
-    not extrapolated (it is biased)."""
+def quality_line(dev, args) -> dict:
+    """Time to relMSE 0.01 on the learned-cache scene (the terrain workload with 8 area lights,
+    1920x1080, path length 3..12, against its FP64 oracle image on a 64x36 pixel subset): the plain
+    unbiased path tracer against the radiance-cache forms (paths end in the cache after 1 or 2
+    bounces, online training, in the wave entry point and in the batched streaming entry point)."""
+    from stratum2_b200.scenegen import terrain_scene
+    wl = terrain_scene(area_lights=8)
+    dev.upload_scene(wl.scene)
+    g = np.load(GOLDEN_CFG5)
+    out = {"workload": "terrain 1024^2 + 64 icospheres + 8 area lights, 512x256 sky with 5e3 sun; 1920x1080, path "
+                       "length 3..12, Russian roulette",
+           "reference_image": f"FP64 oracle, {int(g['spp'])} spp, 64x36 pixel subset (stride 30)",
+           "plain": plain_quality(dev, wl, g, args.quality_chunks),
+           "cached_1_bounce": cached_quality(dev, wl, g, False, 1, 0.0),
+           "cached_2_bounces_unregularised": cached_quality(dev, wl, g, False, 2, 0.0, max_ms=6000.0),
+           "cached_2_bounces": cached_quality(dev, wl, g, False, 2, CACHE_MIN_ROUGHNESS),
+           "batched_cached_2_bounces": cached_quality(dev, wl, g, True, 2, CACHE_MIN_ROUGHNESS),
+           "note": "plain: expected GPU time of the unbiased estimator from the mean relMSE of independent 64-spp "
+                   "calls (relMSE ~ 1/spp); cached: measured GPU time of 1-spp frames with online training "
+                   f"({CACHE_WARMUP_FRAMES} training frames, then progressive accumulation), including the training "
+                   f"frames; regularised forms raise roughness to >= {CACHE_MIN_ROUGHNESS} after the first bounce; "
+                   "every estimator samples the environment by its bilinear footprint (S2_FLAG_ENV_FOOTPRINT_PDF)"}
+    plain_ms = out["plain"]["ms"]
+    for k in ("cached_1_bounce", "cached_2_bounces", "batched_cached_2_bounces"):
+        if out[k]["ms"] is not None:
+            out[k]["fraction_of_plain_time"] = out[k]["ms"] / plain_ms
+    return out
+
+
+def _subset(rad, g):
+    x0, y0, st = int(g["rect"][0]), int(g["rect"][1]), int(g["stride"])
+    ref = g["mean"]
+    return rad[y0::st, x0::st, :3].double().cpu().numpy()[:ref.shape[0], :ref.shape[1]]
+
+
+def _ref_noise(g):
+    ref = g["mean"].astype(np.float64)
+    return ref, float(np.mean(g["var_of_mean"].astype(np.float64) / (ref ** 2 + 1e-2)))
+
+
+def quality_flags():
+    from stratum2_b200 import _abi
+    return _abi.FLAG_ENV_FOOTPRINT_PDF
+
+
+def plain_quality(dev, wl, g, chunks: int, chunk: int = 64) -> dict:
+    """Plain unbiased path tracing: `chunks` independent `chunk`-spp renders; the expected GPU time
+    to relMSE 0.01 is (mean single-chunk relMSE x chunk / 0.01) spp at the measured time per spp (the
+    estimator's relMSE falls as 1/spp); the cumulative image's relMSE is reported beside it."""
     import torch
 
     from stratum2_b200 import _abi
     from stratum2_b200.metrics import relmse
-    g = np.load(GOLDEN_CFG2)
-    ref = g["mean"].astype(np.float64)
-    noise = float(np.mean(g["var_of_mean"].astype(np.float64) / (ref ** 2 + 1e-2)))
-    x0, y0, st = int(g["rect"][0]), int(g["rect"][1]), int(g["stride"])
-    W, H = wl.width, wl.height
-    rad = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    ref, noise = _ref_noise(g)
+    rad = torch.zeros((wl.height, wl.width, 4), dtype=torch.float32, device="cuda")
     aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
-    total_ms, spp, rm, curve = 0.0, 0, float("inf"), []
-    acc, chunk_rm = None, []
-    if cache_bounces:
-        dev.cache_init()
-    while spp < max_spp:
-        # unbiased forms: independent chunks averaged here (so each chunk's own error is known);
-        # the cache form accumulates its 1-spp frames on the device
-        p = params(dev, chunk, seed0 + spp, ((_abi.FLAG_ACCUMULATE if spp else 0) | _abi.FLAG_RADIANCE_CACHE)
-                   if cache_bounces else 0)
-        p.cache_bounces = cache_bounces
+    ms, rms, acc = 0.0, [], None
+    for k in range(chunks):
+        s = dev.render_device(wl.view, params(dev, chunk, 50000 + chunk * k, quality_flags()), aovs)
+        ms += s.gpu_ms
+        sub = _subset(rad, g)
+        rms.append(relmse(sub, ref) - noise)
+        acc = sub if acc is None else acc + sub
+    per_spp = float(np.mean(rms)) * chunk
+    ms_per_spp = ms / (chunks * chunk)
+    return {"ms": per_spp / RELMSE_TARGET * ms_per_spp, "measured_to_target": False,
+            "relmse_per_spp_mean": per_spp, "relmse_per_spp_median": float(np.median(rms)) * chunk,
+            "ms_per_spp": ms_per_spp, "spp_run": chunks * chunk, "gpu_ms_run": ms,
+            "relmse_cumulative": relmse(acc / chunks, ref) - noise}
+
+
+def cached_quality(dev, wl, g, batched: bool, bounces: int, rough: float, max_ms: float = 12000.0) -> dict:
+    """Radiance-cache form: a freshly initialised cache, CACHE_WARMUP_FRAMES 1-spp frames that only
+    train it, then progressive 1-spp frames (S2_FLAG_ACCUMULATE) until the relMSE against the FP64
+    image reaches 0.01 or `max_ms` of GPU time; the GPU time of every frame counts."""
+    import torch
+
+    from stratum2_b200 import _abi
+    from stratum2_b200.metrics import relmse
+    ref, noise = _ref_noise(g)
+    rad = torch.zeros((wl.height, wl.width, 4), dtype=torch.float32, device="cuda")
+    aovs = _abi.S2Aovs(rad.data_ptr(), None, None, None, None, None)
+    dev.cache_init()
+    ms, frames, rm, curve = 0.0, 0, float("inf"), []
+    while ms < max_ms:
+        acc = frames > CACHE_WARMUP_FRAMES
+        p = params(dev, 1, 70000 + frames, quality_flags() | _abi.FLAG_RADIANCE_CACHE | (_abi.FLAG_ACCUMULATE if acc else 0))
+        p.cache_bounces = bounces
+        p.cache_min_roughness = rough
         s = dev.render_views_device([wl.view], p, [aovs]) if batched else dev.render_device(wl.view, p, aovs)
-        total_ms += s.gpu_ms
-        sub = rad[y0::st, x0::st, :3].double().cpu().numpy()[:ref.shape[0], :ref.shape[1]]
-        n = spp // chunk + 1
-        spp += chunk
-        if cache_bounces:
-            rm = relmse(sub, ref) - noise
-        else:
-            chunk_rm.append(relmse(sub, ref) - noise)
-            acc = sub if acc is None else acc + sub
-            rm = relmse(acc / n, ref) - noise
-        if spp in (16, 64, 256, 1024, 4096) or rm <= RELMSE_TARGET:
-            curve.append([spp, round(total_ms, 1), round(rm, 5)])
-        if rm <= RELMSE_TARGET:
-            break
+        ms += s.gpu_ms
+        frames += 1
+        if frames <= CACHE_WARMUP_FRAMES:
+            continue
+        n = frames - CACHE_WARMUP_FRAMES
+        if n % 8 == 0 or n < 8:
+            rm = relmse(_subset(rad, g), ref) - noise
+            if n in (8, 32, 128, 512, 2048) or rm <= RELMSE_TARGET:
+                curve.append([n, round(ms, 1), round(rm, 5)])
+            if rm <= RELMSE_TARGET:
+                break
     reached = rm <= RELMSE_TARGET
-    if cache_bounces:
-        return {"ms": total_ms if reached else None, "measured_to_target": reached, "spp": spp, "gpu_ms_run": total_ms,
-                "relmse": rm, "curve_spp_ms_relmse": curve}
-    # expected time: relMSE of an unbiased mean falls as 1/spp from the mean single-chunk relMSE
-    per_chunk = float(np.mean(chunk_rm))
-    expected_ms = total_ms / spp * chunk * per_chunk / RELMSE_TARGET
-    return {"ms": total_ms if reached else expected_ms, "measured_to_target": reached, "spp": spp,
-            "gpu_ms_run": total_ms, "relmse": rm, "relmse_per_chunk_mean": per_chunk, "chunk_spp": chunk,
-            "expected_ms_from_chunk_variance": expected_ms, "curve_spp_ms_relmse": curve}
+    return {"ms": ms if reached else None, "measured_to_target": reached, "frames": frames, "gpu_ms_run": ms,
+            "ms_per_frame": ms / max(frames, 1), "relmse": rm, "curve_frames_ms_relmse": curve,
+            "cache_bounces": bounces, "min_roughness": rough, "entry_point": "s2_render_views" if batched else "s2_render"}
 
 
 def batched_line(dev, steps: int, spp: int = 8) -> dict:
@@ -622,14 +664,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the batched and time-to-relMSE measurements")
     ap.add_argument("--no-autotune", action="store_true", help="render with the default tuning")
-    ap.add_argument("--quality-spp", type=int, default=2048,
-                    help="sample budget of the time-to-relMSE runs (extrapolated beyond it)")
+    ap.add_argument("--quality-chunks", type=int, default=48,
+                    help="independent 64-spp renders behind the plain path tracer's time to relMSE 0.01")
+    ap.add_argument("--quality-only", action="store_true",
+                    help="run only the time-to-relMSE comparison on the learned-cache scene and print it")
     ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",
                     help="render one frame of the workload with SPP samples and exit (profiling)")
     ap.add_argument("--cache-kernels", type=int, default=0, metavar="STEPS",
                     help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
     ap.add_argument("--cached-frames", type=int, default=0, metavar="N",
-                    help="render N 1-spp frames of the workload in the radiance-cache form and exit (profiling)")
+                    help="render N 1-spp frames of the learned-cache scene in the 2-bounce radiance-cache form "
+                         "and exit (profiling)")
     ap.add_argument("--vcm-only", action="store_true",
                     help="run only the VCM renderer measurement on the many-lights frame and print it")
     ap.add_argument("--restir-only", action="store_true",
@@ -639,13 +684,14 @@ def main():
         from stratum2_b200 import Device, _abi
         from stratum2_b200.scenegen import terrain_scene
         dev = Device(0)
-        wl = terrain_scene()
+        wl = terrain_scene(area_lights=8)
         dev.upload_scene(wl.scene)
         dev.cache_init()
         out = []
         for k in range(args.cached_frames):
             p = params(dev, 1, 50000 + k, _abi.FLAG_RADIANCE_CACHE | (_abi.FLAG_ACCUMULATE if k else 0))
-            p.cache_bounces = 1
+            p.cache_bounces = 2
+            p.cache_min_roughness = CACHE_MIN_ROUGHNESS
             r = dev.render(wl.view, wl.width, wl.height, params=p)
             out.append({"gpu_ms": r.stats.gpu_ms, "launches": r.stats.kernel_launches,
                         "extension_rays": r.stats.extension_rays, "shadow_rays": r.stats.shadow_rays})
@@ -658,6 +704,10 @@ def main():
     if args.vcm_only:
         from stratum2_b200 import Device
         print(json.dumps(vcm_line(Device(0))))
+        return
+    if args.quality_only:
+        from stratum2_b200 import Device
+        print(json.dumps(quality_line(Device(0), args)))
         return
     if args.restir_only:
         from stratum2_b200 import Device

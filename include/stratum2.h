@@ -196,6 +196,16 @@ typedef struct S2View {
                                                   camera; no NEE, ReSTIR or cache; the radiance AOV
                                                   is written, the others are cleared to zero
                                                   (s2_render only) */
+#define S2_FLAG_ENV_FOOTPRINT_PDF   (1u << 19) /* importance-sample the environment by the largest
+                                                  luminance its bilinear reconstruction takes over each
+                                                  texel (tables built at s2_scene_upload) instead of
+                                                  the texel's own luminance, as the reference does
+                                                  (lights.hlsli:49-138); no counterpart in the
+                                                  reference.  Same expected image: the environment is
+                                                  evaluated bilinearly, so near a small bright source
+                                                  (a sun of one texel) the texel pdf leaves its
+                                                  interpolated halo to BSDF sampling, whose rare hits
+                                                  are fireflies; this pdf covers the halo */
 #define S2_FLAG_LIGHT_POWER_PICK    (1u << 16) /* pick emissive lights in proportion to their power
                                                   (emission luminance x area, from an alias table built
                                                   at s2_scene_upload) instead of uniformly as the
@@ -224,11 +234,12 @@ typedef struct S2RenderParams {
     float light_subpaths;            /* S2_FLAG_LIGHT_TRACE: light subpaths per sample pass =
                                         max(1, pixels x light_subpaths) (mLightSubpathCount, 0 = 1) */
     float cache_min_roughness;       /* S2_FLAG_RADIANCE_CACHE: path regularisation (no counterpart in
-                                        the reference).  Once a path has left a vertex of roughness >=
-                                        this value, every later vertex's roughness is raised to at least
-                                        it, so glossy reflections of small bright lights seen through a
-                                        rough bounce (caustics) are blurred instead of sampled as rare
-                                        fireflies.  Biased; 0 = off (default) */
+                                        the reference).  The roughness of every path vertex after the
+                                        first is raised to at least this value, so reflections of small
+                                        bright lights reached through a bounce (caustics, double glossy
+                                        reflections of the sun) are blurred instead of sampled as rare
+                                        fireflies; the first vertex is untouched.  Biased, as the cache
+                                        itself is; 0 = off (default) */
     uint32_t reserved;
 } S2RenderParams;
 
@@ -412,7 +423,8 @@ int  s2_cache_get_params(S2Context* ctx, float* weights, float* table);
 int  s2_cache_set_params(S2Context* ctx, const float* weights, const float* table);
 /* Evaluates the cache at n positions: positions and radiance are float4 per entry (xyz used). */
 int  s2_cache_query(S2Context* ctx, const float* positions, uint32_t n, float* radiance, int on_device);
-/* One optimiser step (Adam on the f32 masters, then refreshed f16 copies) on n records: float4
+/* One optimiser step (Adam on the f32 masters, then refreshed f16 copies; table entries no record
+ * touched keep their parameters and moments, as in lazy Adam) on n records: float4
  * positions and float4 target radiances.  Loss per record: sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / 3
  * with the denominator held constant; `loss` (may be NULL) receives its mean over the records. */
 int  s2_cache_train(S2Context* ctx, const float* positions, const float* targets, uint32_t n, float* loss,

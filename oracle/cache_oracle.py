@@ -18,18 +18,24 @@ def f16(x):
 def resolutions(base=16, top=2048, log2_table=19):
     b = np.exp((np.log(top) - np.log(base)) / (LEVELS - 1))
     res = np.floor(base * b ** np.arange(LEVELS) + 1e-9)
-    dense = (res + 1) ** 3 <= 2 ** log2_table
+    dense = 8 * ((res.astype(np.int64) + 2) // 2) ** 3 <= 2 ** log2_table
     return res, dense
 
 
 def corner_index(level, x, y, z, res, dense, log2_table):
-    mask = (1 << log2_table) - 1
+    """Table entry of grid vertex (x, y, z): 2x2x2 bricks of 8 consecutive entries, placed densely
+    or by the Instant-NGP spatial hash of the brick coordinates (s2_cache.cuh cache_index)."""
+    mask = np.uint64((1 << (log2_table - 3)) - 1)
     x, y, z = (np.asarray(v, np.uint64) for v in (x, y, z))
+    one = np.uint64(1)
+    bx, by, bz = x >> one, y >> one, z >> one
     if dense[level]:
-        n = np.uint64(int(res[level]) + 1)
-        return ((x + n * (y + n * z)) & np.uint64(mask)).astype(np.int64)
-    h = (x ^ ((y * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)) ^ ((z * np.uint64(805459861)) & np.uint64(0xFFFFFFFF)))
-    return (h & np.uint64(mask)).astype(np.int64)
+        n = np.uint64((int(res[level]) + 2) // 2)
+        b = (bx + n * (by + n * bz)) & mask
+    else:
+        b = (bx ^ ((by * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)) ^
+             ((bz * np.uint64(805459861)) & np.uint64(0xFFFFFFFF))) & mask
+    return ((b << np.uint64(3)) | (x & one) | ((y & one) << one) | ((z & one) << np.uint64(2))).astype(np.int64)
 
 
 def unit(pos, box_min, box_max):

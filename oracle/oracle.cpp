@@ -261,6 +261,7 @@ struct Scene {
     std::vector<uint32_t> light_map, inst_light_map;
     uint32_t env_addr = S2_NO_ENVIRONMENT;
     std::vector<Image<R>> images;
+    Image<R> env_fp;  // the environment image with its bilinear-footprint luminance pyramid
     int env_image = -1;
     R sphere[4];
     // flattened triangles + BVH2
@@ -390,6 +391,36 @@ struct Scene {
                         o.lum[l][t] = R(0.2126) * lv[l][4 * t] + R(0.7152) * lv[l][4 * t + 1] + R(0.0722) * lv[l][4 * t + 2];
                 }
                 env_image = (int)i;
+                // S2_FLAG_ENV_FOOTPRINT_PDF: level 0 weighs the largest value of the bilinear
+                // luminance over each texel's area (its centre, edge midpoints and corners, repeat
+                // addressing); coarser levels average 2x2 blocks
+                env_fp = o;
+                const int W = (int)o.lw[0], H = (int)o.lh[0];
+                auto L = [&](int x, int y) {
+                    x %= W; if (x < 0) x += W;
+                    y %= H; if (y < 0) y += H;
+                    return o.lum[0][(size_t)y * W + x];
+                };
+                for (int y = 0; y < H; ++y) for (int x = 0; x < W; ++x) {
+                    const R c = L(x, y);
+                    R w = c;
+                    for (int dd = -1; dd <= 1; dd += 2) {
+                        w = std::max(w, R(0.5) * (c + L(x + dd, y)));
+                        w = std::max(w, R(0.5) * (c + L(x, y + dd)));
+                        for (int e = -1; e <= 1; e += 2) w = std::max(w, R(0.25) * (c + L(x + dd, y) + L(x, y + e) + L(x + dd, y + e)));
+                    }
+                    env_fp.lum[0][(size_t)y * W + x] = w;
+                }
+                for (size_t l = 1; l < env_fp.lum.size(); ++l) {
+                    const uint32_t pw = o.lw[l - 1], ph = o.lh[l - 1];
+                    for (uint32_t y = 0; y < o.lh[l]; ++y) for (uint32_t x = 0; x < o.lw[l]; ++x) {
+                        const uint32_t x0 = std::min(2 * x, pw - 1), x1 = std::min(2 * x + 1, pw - 1);
+                        const uint32_t y0 = std::min(2 * y, ph - 1), y1 = std::min(2 * y + 1, ph - 1);
+                        const std::vector<R>& f = env_fp.lum[l - 1];
+                        env_fp.lum[l][(size_t)y * o.lw[l] + x] = R(0.25) * (f[(size_t)y0 * pw + x0] + f[(size_t)y0 * pw + x1] +
+                                                                            f[(size_t)y1 * pw + x0] + f[(size_t)y1 * pw + x1]);
+                    }
+                }
             }
         }
         // flatten triangles

@@ -603,12 +603,18 @@ template <class R> struct Tracer {
         if (img < s.images.size()) {
             R u, v; cart_to_uv(dir, u, v);
             e = e * s.images[img].sample(u, v);
-            pdfw = sample_texel_pdf(s.images[img], u, v) / (2 * PI<R>() * PI<R>() * std::sqrt(1 - dir.y * dir.y));
+            pdfw = sample_texel_pdf(env_samp(img), u, v) / (2 * PI<R>() * PI<R>() * std::sqrt(1 - dir.y * dir.y));
         } else {
             pdfw = 1 / (4 * PI<R>());
         }
         if (light_count() > 0) pdfw *= (R)p.env_prob;
         return e;
+    }
+
+    // the luminance tables that drive environment sampling: the image's own, or its bilinear
+    // footprint (S2_FLAG_ENV_FOOTPRINT_PDF, an extension of the reference's SampleTexel)
+    const Image<R>& env_samp(uint32_t img) const {
+        return (p.flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? s.env_fp : s.images[img];
     }
 
     struct Illum {
@@ -624,7 +630,7 @@ template <class R> struct Tracer {
                 const uint32_t img = s.u32(s.mat, s.env_addr + 12);
                 V3<R> dir; R pdf;
                 if (img < s.images.size()) {
-                    R u, v; sample_texel(s.images[img], rnd[0], rnd[1], u, v, pdf);
+                    R u, v; sample_texel(env_samp(img), rnd[0], rnd[1], u, v, pdf);
                     dir = uv_to_cart(u, v);
                     pdf /= (2 * PI<R>() * PI<R>() * std::sqrt(1 - pow2(dir.y)));
                 } else {
@@ -1000,6 +1006,23 @@ int oracle_trace(void* sp, const float* rays, uint32_t n, int anyhit, int precis
             t[i] = h.t; b1[i] = h.b1; b2[i] = h.b2;
             inst[i] = h.hit ? s->f.tid[h.tri].inst : 0xffffffffu; prim[i] = h.hit ? s->f.tid[h.tri].prim : 0xffffffffu;
         }
+    }
+    return 0;
+}
+
+// Environment radiance (rgb) and its light-sampling solid-angle pdf for n directions (3 doubles
+// each) under the flags of `rp` (FP64 scene): EvaluateEnvironment (lights.hlsli:143-164).
+int oracle_env_eval(void* sp, const S2RenderParams* rp, const double* dirs, uint32_t n, double* rgb, double* pdf) {
+    OracleScene* s = (OracleScene*)sp;
+    if (!s || !rp || !s->has_d) return -1;
+    orc::Params p{rp->min_path_length, rp->max_path_length, rp->spp, rp->frame_seed, rp->flags, 32u, rp->exposure,
+                  rp->environment_sample_probability > 0 ? rp->environment_sample_probability : 0.9f};
+    orc::Tracer<double> tr(s->d, p);
+    for (uint32_t i = 0; i < n; ++i) {
+        double pw = 0;
+        const orc::V3<double> e = tr.eval_env(orc::V3<double>(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]), pw);
+        rgb[3 * i] = e.x; rgb[3 * i + 1] = e.y; rgb[3 * i + 2] = e.z;
+        pdf[i] = pw;
     }
     return 0;
 }

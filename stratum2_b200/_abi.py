@@ -45,6 +45,7 @@ FLAG_RADIANCE_CACHE = 1 << 14
 FLAG_RESTIR_SCREEN = 1 << 15
 FLAG_LIGHT_POWER_PICK = 1 << 16
 FLAG_LIGHT_TRACE = 1 << 17
+FLAG_ENV_FOOTPRINT_PDF = 1 << 19
 FLAG_RESTIR_REUSE_VISIBILITY = 1 << 18
 SHADE_ORDER_MATERIAL = 0
 SHADE_ORDER_QUEUE = 1

@@ -177,9 +177,52 @@ void build_env_tables(S2Context* ctx, DevImage& di, const std::vector<float>& lu
     di.nested = (di.quad && di.pdf) ? 1u : 0u;
 }
 
+// Luminance pyramid and sampling tables of the environment's bilinear footprint
+// (S2_FLAG_ENV_FOOTPRINT_PDF): texel t of level 0 weighs the largest value the bilinear
+// reconstruction (repeat addressing, as sample_image) takes over t's area.  The reconstruction is
+// bilinear between texel centres, so that maximum is reached at a corner of one of the four
+// quarter-texel rectangles: t's centre, its four edge midpoints (the mean with a neighbour) and its
+// four corners (the mean of four texels).  Coarser levels average 2x2 blocks of the finer one, so
+// the hierarchical descent samples a texel in proportion to its level-0 weight.
+void build_env_footprint(S2Context* ctx, const DevImage& di, const std::vector<float>& lum, const DevImage* old_fp,
+                         DevImage& fp) {
+    fp = di;
+    const int W = (int)di.lw[0], H = (int)di.lh[0];
+    auto L = [&](int x, int y) {
+        x %= W; if (x < 0) x += W;
+        y %= H; if (y < 0) y += H;
+        return lum[(size_t)y * W + x];
+    };
+    std::vector<float> fl;
+    fl.reserve(lum.size());
+    for (int y = 0; y < H; ++y) for (int x = 0; x < W; ++x) {
+        const float c = L(x, y);
+        float w = c;
+        for (int d = -1; d <= 1; d += 2) {
+            w = std::max(w, 0.5f * (c + L(x + d, y)));
+            w = std::max(w, 0.5f * (c + L(x, y + d)));
+            for (int e = -1; e <= 1; e += 2) w = std::max(w, 0.25f * (c + L(x + d, y) + L(x, y + e) + L(x + d, y + e)));
+        }
+        fl.push_back(w);
+    }
+    for (uint32_t l = 1; l < di.levels; ++l) {
+        const uint32_t pw = di.lw[l - 1], ph = di.lh[l - 1], off = di.lum_offset[l - 1];
+        for (uint32_t y = 0; y < di.lh[l]; ++y) for (uint32_t x = 0; x < di.lw[l]; ++x) {
+            const uint32_t x0 = std::min(2 * x, pw - 1), x1 = std::min(2 * x + 1, pw - 1);
+            const uint32_t y0 = std::min(2 * y, ph - 1), y1 = std::min(2 * y + 1, ph - 1);
+            fl.push_back(0.25f * (fl[off + (size_t)y0 * pw + x0] + fl[off + (size_t)y0 * pw + x1] +
+                                  fl[off + (size_t)y1 * pw + x0] + fl[off + (size_t)y1 * pw + x1]));
+        }
+    }
+    fp.lum = put(ctx, fl.data(), fl.size(), old_fp ? old_fp->lum : nullptr);
+    build_env_tables(ctx, fp, fl, old_fp);
+}
+
 // Device copy of one image (float RGBA texels); an environment image also gets its luminance mip
-// pyramid and sampling tables.  `old`: the same image's current descriptor, overwritten in place.
-int build_image(S2Context* ctx, uint32_t i, const S2Image& im, bool env, const DevImage* old, DevImage& di) {
+// pyramid and sampling tables, and in `fp` the descriptor of its footprint tables.  `old` / `old_fp`:
+// the same image's current descriptors, overwritten in place.
+int build_image(S2Context* ctx, uint32_t i, const S2Image& im, bool env, const DevImage* old, DevImage& di,
+                const DevImage* old_fp = nullptr, DevImage* fp = nullptr) {
     if (!im.texels || im.width == 0 || im.height == 0 || im.channels < 1 || im.channels > 4)
         return set_error(ctx, S2_ERR_INVALID, "image " + std::to_string(i) + " is malformed");
     const size_t n = (size_t)im.width * im.height;
@@ -218,6 +261,7 @@ int build_image(S2Context* ctx, uint32_t i, const S2Image& im, bool env, const D
         }
         di.lum = put(ctx, lum.data(), lum.size(), old ? old->lum : nullptr);
         build_env_tables(ctx, di, lum, old);
+        if (fp) build_env_footprint(ctx, di, lum, old_fp, *fp);
     }
     return S2_OK;
 }
@@ -539,10 +583,11 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     ctx->images_host.assign(d->image_count, DevImage{});
     ctx->env_image = -1;
     ctx->image_channels.assign(d->image_count, 0);
+    ctx->env_fp_host = DevImage{};
     for (uint32_t i = 0; i < d->image_count; ++i) {
         const S2Image& im = d->images[i];
         DevImage di{};
-        S2_TRY(build_image(ctx, i, im, i == env_img, nullptr, di));
+        S2_TRY(build_image(ctx, i, im, i == env_img, nullptr, di, nullptr, &ctx->env_fp_host));
         if (i == env_img) ctx->env_image = (int)i;
         ctx->image_channels[i] = im.channels;
         ctx->images_host[i] = di;
@@ -550,6 +595,9 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     ctx->images_dev = upload(ctx, ctx->scene_bufs, ctx->images_host.data(), ctx->images_host.size());
     s.images = ctx->images_dev;
     s.image_count = d->image_count;
+    ctx->env_fp_dev = ctx->env_image >= 0 ? upload(ctx, ctx->scene_bufs, &ctx->env_fp_host, 1) : nullptr;
+    s.env_fp = ctx->env_fp_dev;
+    s.env_fp_on = 0;
     if (!ctx->last_error.empty() && ctx->last_error.find("cudaMalloc") != std::string::npos) return S2_ERR_OOM;
     S2_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "scene upload"));
     ctx->has_scene = true;
@@ -575,9 +623,13 @@ extern "C" int s2_update_image(S2Context* ctx, uint32_t index, const float* texe
         im.texels = texels;
     }
     DevImage di{};
-    S2_TRY(build_image(ctx, index, im, (int)index == ctx->env_image, &old, di));
+    const bool env = (int)index == ctx->env_image;
+    const DevImage old_fp = ctx->env_fp_host;
+    S2_TRY(build_image(ctx, index, im, env, &old, di, env ? &old_fp : nullptr, env ? &ctx->env_fp_host : nullptr));
     ctx->images_host[index] = di;
     cudaMemcpyAsync(ctx->images_dev + index, &ctx->images_host[index], sizeof(DevImage), cudaMemcpyHostToDevice, ctx->stream);
+    if (env && ctx->env_fp_dev)
+        cudaMemcpyAsync(ctx->env_fp_dev, &ctx->env_fp_host, sizeof(DevImage), cudaMemcpyHostToDevice, ctx->stream);
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "image update");
 }
 

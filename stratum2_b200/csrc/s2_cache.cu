@@ -42,7 +42,7 @@ namespace {
 __global__ void k_cache_pack(const float* __restrict__ w32, const float* __restrict__ t32, __half2* __restrict__ t16,
                              uint32_t entries, uint8_t* __restrict__ wimage) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < entries) t16[i] = __floats2half2_rn(t32[2 * i], t32[2 * i + 1]);
+    if (i < entries) t16[i] = __floats2half2_rn(t32[2 * i], t32[2 * i + 1]);  // entries = 0: weights only
     if (i < kCacheW1) {
         const uint32_t o = i / kCacheIn, k = i % kCacheIn;
         *(__half*)(wimage + kmaj_offset(o, k, kCacheIn)) = __float2half_rn(w32[i]);
@@ -77,10 +77,11 @@ float uniform(uint64_t& s, float lo, float hi) {
     return lo + (hi - lo) * (float)((splitmix(s) >> 40) * (1.0 / 16777216.0));
 }
 
-int repack(S2Context* ctx) {
+int repack(S2Context* ctx, bool table = true) {
     CacheState* c = ctx->cache;
-    const uint32_t n = std::max(c->table_entries, kCacheW2);
-    k_cache_pack<<<(n + 255) / 256, 256, 0, ctx->stream>>>(c->w32, c->t32, c->t16, c->table_entries, (uint8_t*)c->wimage);
+    const uint32_t entries = table ? c->table_entries : 0u;
+    const uint32_t n = std::max(entries, kCacheW2);
+    k_cache_pack<<<(n + 255) / 256, 256, 0, ctx->stream>>>(c->w32, c->t32, c->t16, entries, (uint8_t*)c->wimage);
     return check_cuda(ctx, cudaGetLastError(), "cache pack");
 }
 
@@ -174,8 +175,9 @@ extern "C" int s2_cache_set_params(S2Context* ctx, const float* weights, const f
                                                  (double)(kCacheLevels - 1)) : 1.0;
     for (uint32_t l = 0; l < kCacheLevels; ++l) {
         d.res[l] = (float)std::floor((double)c->prm.base_resolution * std::pow(b, (double)l) + 1e-9);
-        const double cells = std::pow((double)d.res[l] + 1.0, 3.0);
-        d.dense[l] = cells <= (double)(1u << c->prm.log2_table) ? 1u : 0u;
+        d.nbrick[l] = ((uint32_t)d.res[l] + 2u) / 2u;  // bricks of 2 vertices per axis over res + 1 vertices
+        const double entries = 8.0 * std::pow((double)d.nbrick[l], 3.0);
+        d.dense[l] = entries <= (double)(1u << c->prm.log2_table) ? 1u : 0u;
     }
     d.box_min = make_float3(c->prm.box_min[0], c->prm.box_min[1], c->prm.box_min[2]);
     d.box_inv_extent = make_float3(1.f / (c->prm.box_max[0] - c->prm.box_min[0]), 1.f / (c->prm.box_max[1] - c->prm.box_min[1]),
@@ -295,12 +297,12 @@ int cache_adam_device(S2Context* ctx, uint32_t n, const uint32_t* n_dev) {
                                                                        kCacheWeights, inv_n, n_dev, n, p.learning_rate, p.beta1,
                                                                        p.beta2, p.epsilon, c1, c2);
     const size_t nt = 2 * (size_t)c->table_entries;
-    k_cache_adam<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(c->t32, c->grad_t, c->adam_t, c->adam_t + nt, nt, inv_n,
-                                                                        n_dev, n, p.learning_rate, p.beta1, p.beta2, p.epsilon,
-                                                                        c1, c2);
+    k_cache_adam_table<<<(c->table_entries + 255) / 256, 256, 0, ctx->stream>>>(
+        (float2*)c->t32, (float2*)c->grad_t, (float2*)c->adam_t, (float2*)(c->adam_t + nt), c->t16, c->table_entries, inv_n,
+        n_dev, n, p.learning_rate, p.beta1, p.beta2, p.epsilon, c1, c2);
     int rc = check_cuda(ctx, cudaGetLastError(), "cache Adam launch");
     if (rc != S2_OK) return rc;
-    return repack(ctx);
+    return repack(ctx, false);  // the table's f16 copy was refreshed by the Adam pass
 }
 }  // namespace s2
 

@@ -47,7 +47,8 @@ struct CacheDev {
     const __half2* table;        // [levels][2^log2_table] feature pairs
     uint32_t log2_table;
     float res[kCacheLevels];     // grid resolution per level
-    uint32_t dense[kCacheLevels];// 1: level indexed densely ((res+1)^3 <= table size)
+    uint32_t dense[kCacheLevels];// 1: level indexed densely (all its bricks fit the table)
+    uint32_t nbrick[kCacheLevels];// bricks per axis of a dense level: ceil((res + 1) / 2)
     float3 box_min, box_inv_extent;
     const uint4* wimage;         // kWImageTrainBytes: W1, W2, W3 (padded), W2T, W1T in operand layout
     int* status;                 // bit 2: a tensor-core wait timed out
@@ -67,13 +68,21 @@ S2D float3 cache_unit(const CacheDev& c, float3 p) {
     return u;
 }
 
+// Table layout: the grid vertices of a level are grouped in 2 x 2 x 2 bricks of 8 consecutive
+// entries (32 bytes, one L2 sector), so the 8 corners of a cell touch 1 to 8 sectors (3.375 on
+// average) instead of 8.  Bricks are placed densely when they all fit the level's table, else by
+// the spatial hash of Instant-NGP (Mueller et al. 2022) applied to the brick coordinates.
 S2D uint32_t cache_index(const CacheDev& c, uint32_t level, uint32_t x, uint32_t y, uint32_t z) {
-    const uint32_t mask = (1u << c.log2_table) - 1u;
+    const uint32_t mask = (1u << (c.log2_table - 3u)) - 1u;
+    const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1;
+    uint32_t b;
     if (c.dense[level]) {
-        const uint32_t n = (uint32_t)c.res[level] + 1u;
-        return (x + n * (y + n * z)) & mask;
+        const uint32_t n = c.nbrick[level];
+        b = (bx + n * (by + n * bz)) & mask;
+    } else {
+        b = (bx ^ (by * 2654435761u) ^ (bz * 805459861u)) & mask;
     }
-    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & mask;
+    return (b << 3) | (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
 }
 
 // The 32 encoded features of one position (trilinear interpolation of the 8 corner entries per
@@ -598,6 +607,34 @@ __global__ void k_cache_adam(float* __restrict__ param, float* __restrict__ grad
     m[i] = mi;
     v[i] = vi;
     param[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Lazy Adam on the table (TensorFlow's LazyAdam semantics): an entry whose summed gradient is zero
+// this step (no record touched it) keeps its parameters and moments; touched entries take the Adam
+// step on their f32 masters, clear their gradient and refresh their f16 copy in the same pass, so
+// untouched entries cost an 8-byte gradient read.  One thread per entry (two features).
+__global__ void k_cache_adam_table(float2* __restrict__ param, float2* __restrict__ grad, float2* __restrict__ m,
+                                   float2* __restrict__ v, __half2* __restrict__ t16, uint32_t entries, float inv_n,
+                                   const uint32_t* __restrict__ n_dev, uint32_t n_cap, float lr, float b1, float b2,
+                                   float eps, float c1, float c2) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= entries) return;
+    const float2 g0 = grad[i];
+    if (g0.x == 0.f && g0.y == 0.f) return;
+    if (n_dev) inv_n = 1.f / (float)max(1u, min(*n_dev, n_cap));
+    grad[i] = make_float2(0.f, 0.f);
+    const float gx = g0.x * inv_n, gy = g0.y * inv_n;
+    float2 mi = m[i], vi = v[i], pi = param[i];
+    mi.x = b1 * mi.x + (1.f - b1) * gx;
+    mi.y = b1 * mi.y + (1.f - b1) * gy;
+    vi.x = b2 * vi.x + (1.f - b2) * gx * gx;
+    vi.y = b2 * vi.y + (1.f - b2) * gy * gy;
+    pi.x -= lr * (mi.x / c1) / (sqrtf(vi.x / c2) + eps);
+    pi.y -= lr * (mi.y / c1) / (sqrtf(vi.y / c2) + eps);
+    m[i] = mi;
+    v[i] = vi;
+    param[i] = pi;
+    t16[i] = __floats2half2_rn(pi.x, pi.y);
 }
 
 }  // namespace s2

@@ -50,6 +50,8 @@ struct S2Context {
     std::vector<DevImage> images_host;      // device-side descriptors, host copy
     std::vector<uint32_t> image_channels;   // channel count of each uploaded image
     DevImage* images_dev = nullptr;
+    DevImage env_fp_host{};                 // S2_FLAG_ENV_FOOTPRINT_PDF tables of the environment image
+    DevImage* env_fp_dev = nullptr;
     uint8_t** vbufs_dev = nullptr;
     int env_image = -1;
 

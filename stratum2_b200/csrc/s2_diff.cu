@@ -46,6 +46,7 @@ int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, Di
     std::memset(&A, 0, sizeof(A));
     A.scene = ctx->scene;
     A.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
+    A.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     A.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
     std::memcpy(A.proj, view->projection, sizeof(A.proj));
     A.imin[0] = view->image_min[0]; A.imin[1] = view->image_min[1];

@@ -108,6 +108,12 @@ S2D float sample_texel_pdf(const DevImage& im, float2 uv) {
 
 S2D bool has_env(const DevScene& s) { return s.env_address != 0xffffffffu; }
 
+// The descriptor whose luminance tables drive environment sampling and its pdf: the environment
+// image's own, or with S2_FLAG_ENV_FOOTPRINT_PDF the bilinear-footprint tables.
+S2D const DevImage& env_sampling_image(const DevScene& s, uint32_t img) {
+    return (s.env_fp_on && s.env_fp) ? *s.env_fp : s.images[img];
+}
+
 // EvaluateEnvironment (lights.hlsli:143-164): emission and its solid-angle pdf
 S2D float3 eval_env(const DevScene& s, float3 dir, float& pdfw) {
     pdfw = 0.f;
@@ -119,7 +125,7 @@ S2D float3 eval_env(const DevScene& s, float3 dir, float& pdfw) {
         const float2 uv = cartesian_to_spherical_uv(dir);
         const float4 t = sample_image(s.images[img], uv);
         e = e * f3(t.x, t.y, t.z);
-        pdfw = sample_texel_pdf(s.images[img], uv) / (2.f * S2_PI * S2_PI * sqrtf(1.f - dir.y * dir.y));
+        pdfw = sample_texel_pdf(env_sampling_image(s, img), uv) / (2.f * S2_PI * S2_PI * sqrtf(1.f - dir.y * dir.y));
     } else {
         pdfw = 1.f / (4.f * S2_PI);
     }
@@ -149,7 +155,7 @@ S2D Illum sample_illum(const DevScene& s, float4 rnd, float3 ref, bool shading_n
             float3 dir;
             float pdf;
             if (img < s.image_count) {
-                const float2 uv = sample_texel(s.images[img], rnd.x, rnd.y, pdf);
+                const float2 uv = sample_texel(env_sampling_image(s, img), rnd.x, rnd.y, pdf);
                 dir = spherical_uv_to_cartesian(uv);
                 pdf /= (2.f * S2_PI * S2_PI * sqrtf(1.f - pow2(dir.y)));
             } else {

@@ -168,6 +168,7 @@ extern "C" int s2_render_noalloc(S2Context* ctx, const S2View* view, const S2Ren
 
     P.scene = ctx->scene;
     P.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
+    P.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
     std::memcpy(P.proj, view->projection, sizeof(P.proj));
     P.imin[0] = view->image_min[0]; P.imin[1] = view->image_min[1];

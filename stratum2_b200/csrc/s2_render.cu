@@ -317,6 +317,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     std::memset(&P, 0, sizeof(P));
     P.scene = ctx->scene;
     P.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
+    P.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
     std::memcpy(P.proj, view->projection, sizeof(P.proj));
     P.imin[0] = view->image_min[0]; P.imin[1] = view->image_min[1];
@@ -803,6 +804,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     std::memset(&P, 0, sizeof(P));
     P.scene = ctx->scene;
     P.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
+    P.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
     P.min_len = prm->min_path_length;
     P.max_len = prm->max_path_length;

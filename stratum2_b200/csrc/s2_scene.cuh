@@ -66,6 +66,10 @@ struct DevScene {
     // images
     const DevImage* images;
     uint32_t image_count;
+    // S2_FLAG_ENV_FOOTPRINT_PDF: the environment image's descriptor with sampling tables built from
+    // the per-texel maximum of its bilinear luminance (same texels); env_fp_on is set per render call
+    const DevImage* env_fp;
+    uint32_t env_fp_on;
     float4 scene_sphere;
     // ray-coherence keys: the BVH root box as origin and 8 / extent per axis (zero: no BVH)
     float4 key_lo, key_scale;

@@ -374,11 +374,11 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                 const float isect_dist = half_round(h.x);
                 const float isect_pdfa = half_round(light_pdfa(s, inst, sd.area));
                 Mat m = load_material(s, sd.mat, sd.uv);
-                uint32_t rough_path = 0u;  // meta bit 10 of the continuation: cache-form regularisation
-                if (CACHE && P.cache_on && P.cache_rough > 0.f) {
-                    if ((meta & 0x400u) && m.roughness() < P.cache_rough)
-                        m.w[2] = (m.w[2] & ~0xff00u) | (pk8(P.cache_rough) << 8);
-                    if ((meta & 0x400u) || LAMBERT || m.roughness() >= P.cache_rough) rough_path = 0x400u;
+                // cache-form path regularisation: after the first bounce every vertex is at least
+                // cache_rough rough
+                if (CACHE && P.cache_on && P.cache_rough > 0.f && len >= 2) {
+                    const uint32_t floor8 = pk8(P.cache_rough);
+                    if (((m.w[2] >> 8) & 0xffu) < floor8) m.w[2] = (m.w[2] & ~0xff00u) | (floor8 << 8);
                 }
                 const float3 in = sd.to_local(-dir);
                 const float cos_in = fabsf(in.z);
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
                             n0 = make_float4(org.x, org.y, org.z, dir_pdf);
                             n1 = make_float4(nd.x, nd.y, nd.z, thr.x);
                             n2 = make_float4(thr.y, thr.z, __uint_as_float(slot),
-                                             __uint_as_float((meta & ~0xffu) | len | rough_path));
+                                             __uint_as_float((meta & ~0xffu) | len));
                             n3 = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
                         }
                     }

@@ -117,6 +117,7 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     A.scene.env_address = 0xffffffffu;  // black environment (see the header)
     A.scene.env_sample_prob = 0.f;
     A.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
+    A.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     std::memcpy(A.proj, view->projection, sizeof(A.proj));
     A.imin[0] = view->image_min[0]; A.imin[1] = view->image_min[1];
     A.imax[0] = view->image_max[0]; A.imax[1] = view->image_max[1];

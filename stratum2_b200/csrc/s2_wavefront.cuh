@@ -101,8 +101,8 @@ struct PTParams {
     // with a query {position, slot} + throughput; training paths (meta bit 9, one in train_mod)
     // record every vertex {position, slot}, throughput, accumulated radiance
     uint32_t cache_on, cache_len, train_mod;
-    // path regularisation of the cache form: after a vertex of roughness >= cache_rough, every later
-    // vertex's roughness is raised to at least cache_rough (meta bit 10 marks such paths); 0 = off
+    // path regularisation of the cache form: the roughness of every vertex after the first is raised
+    // to at least cache_rough; 0 = off
     float cache_rough;
     float4 *cq_pos, *cq_thr;
     uint32_t cq_cap;

@@ -34,6 +34,7 @@ def oracle() -> C.CDLL:
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_int]
         L.oracle_pcg4d.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        L.oracle_env_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         L.oracle_pack_normal.restype = C.c_uint32
         L.oracle_pack_normal.argtypes = [C.c_double, C.c_double, C.c_double]
         L.oracle_unpack_normal.argtypes = [C.c_uint32, C.c_void_p]
@@ -103,6 +104,15 @@ class OracleScene:
                                    inst.ctypes.data, prim.ctypes.data, b1.ctypes.data, b2.ctypes.data, threads)
         assert rc == 0
         return {"t": t, "instance": inst, "primitive": prim, "b1": b1, "b2": b2}
+
+    def env_eval(self, params, dirs: np.ndarray):
+        """Environment radiance (n, 3) and light-sampling solid-angle pdf (n,) of unit directions
+        (n, 3), FP64 scene."""
+        dirs = np.ascontiguousarray(dirs, np.float64)
+        n = dirs.shape[0]
+        rgb, pdf = np.zeros((n, 3)), np.zeros(n)
+        assert oracle().oracle_env_eval(self.h, C.byref(params), dirs.ctypes.data, n, rgb.ctypes.data, pdf.ctypes.data) == 0
+        return rgb, pdf
 
     def render(self, view, params, width: int, height: int, precision: int = 64, rect=None, stride: int = 1,
                threads: int = 0) -> dict:

@@ -169,7 +169,8 @@ def terrain(device):
     return wl, OracleScene(wl.scene, 1)
 
 
-@pytest.mark.parametrize("extra", [0, _abi.FLAG_REFERENCE_ENV_MIS, _abi.FLAG_SHADING_NORMALS_OFF])
+@pytest.mark.parametrize("extra", [0, _abi.FLAG_REFERENCE_ENV_MIS, _abi.FLAG_SHADING_NORMALS_OFF,
+                                   _abi.FLAG_ENV_FOOTPRINT_PDF])
 def test_terrain_disney_env_same_seed(device, terrain, extra):
     wl, osc = terrain
     device.upload_scene(wl.scene)
@@ -177,11 +178,14 @@ def test_terrain_disney_env_same_seed(device, terrain, extra):
     assert_same_seed(device, osc, wl, p, f"terrain flags{extra}")
 
 
-def test_terrain_converges_to_fp64_golden(device, terrain):
+@pytest.mark.parametrize("extra", [0, _abi.FLAG_ENV_FOOTPRINT_PDF])
+def test_terrain_converges_to_fp64_golden(device, terrain, extra):
+    """With the reference's texel pdf and with the footprint pdf (an unbiased change of the
+    environment's sampling density: the same expected image)."""
     wl, _ = terrain
     device.upload_scene(wl.scene)
     gold = np.load(GOLDEN / "terrain_64x36_fp64_131072spp.npz")
-    p = make_params(1, 1, 6, J)
+    p = make_params(1, 1, 6, J | extra)
     m, v = batches(device, wl, p, 16, 4096, seed0=0)  # 65536 spp in total
     floor = np.mean((v + gold["var_of_mean"]) / (gold["mean"] ** 2 + 1e-2))
     assert_converged(m, v, gold["mean"], gold["var_of_mean"], max(1e-3, 2 * floor), "terrain 65536 spp")
