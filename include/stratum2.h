@@ -318,6 +318,24 @@ int  s2_render_views(S2Context* ctx, const S2View* views, uint32_t view_count, c
 /* Defaults as in the reference (TestRenderer.cpp:38-43, VCM.cpp:39-40). */
 void s2_default_render_params(S2RenderParams* p);
 
+/* ---- device math check (diagnostic) ------------------------------------------------------
+ * Evaluates one of the device math functions of the path tracer on n entries, for checks against
+ * the reference's own shader functions (src/Shaders/common/rng.hlsli, common.hlsli,
+ * microfacet.hlsli).  Host arrays: `in` holds 8 doubles per entry, `out` receives 9 per entry
+ * (unsigned integers as exact doubles; float arguments are rounded to float first).
+ *   0 xxhash32 (u -> h)                    1 pcg (u -> h)
+ *   2 pcg4d (u4 -> u4)                     3 RandomSampler: first nextFloat() of state
+ *                                            (px, py, seed, offset) -> 4 floats
+ *   4 packNormal (xyz -> packed)           5 unpackNormal (packed -> xyz)
+ *   6 GTR1 (n.h, alpha)                    7 GTR2 anisotropic (h.xyz, ax, ay)
+ *   8 smith_masking_gtr2 (v.xyz, ax, ay)   9 smith_masking_gtr1 (v.xyz)
+ *  10 sample_visible_normals (in.xyz, ax, ay, u1, u2 -> h.xyz)
+ *  11 schlick_fresnel (F0, cos)           12 fresnel_dielectric (n.i, eta)
+ *  13 sampleConcentricDisc (u1, u2 -> xy) 14 sampleCosHemisphere (u1, u2 -> xyz)
+ *  15 sampleUniformSphere (u1, u2 -> xyz) 16 sampleUniformTriangle (u1, u2 -> b1, b2)
+ *  17 makeOrthonormal (n.xyz -> rows t, b, n) */
+int  s2_device_math(S2Context* ctx, int function_id, const double* in, uint32_t n, double* out);
+
 /* ---- allocation-free rendering ----------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate device memory while they
  * render (a host application that owns the GPU's memory budget and forbids cudaMalloc/cudaFree,

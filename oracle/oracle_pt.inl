@@ -1106,6 +1106,61 @@ int oracle_render(void* sp, const S2View* view, const S2RenderParams* rp, int pr
     return 0;
 }
 
+}  // extern "C"
+
+// ---- the oracle's restatements of the reference's shader math, one function at a time, with the
+// function ids and per-entry layouts of the reference build's ref_shader_math (oracle/ref_shader_math.cpp):
+// 8 input and 9 output doubles per entry.  precision 32: the FP32 instantiation, else FP64.
+template <class R> static void oracle_math_one(int fn, const double* a, double* o) {
+    using V = orc::V3<R>;
+    using T = orc::Tracer<R>;
+    auto f = [&](int i) { return (R)a[i]; };
+    auto u = [&](int i) { return (uint32_t)a[i]; };
+    auto put3 = [&](const V& v, int at) { o[at] = (double)v.x; o[at + 1] = (double)v.y; o[at + 2] = (double)v.z; };
+    switch (fn) {
+        case 0: o[0] = orc::xxhash32(u(0)); break;
+        case 1: o[0] = orc::pcg_hash(u(0)); break;
+        case 2: { const orc::U4 r = orc::pcg4d({u(0), u(1), u(2), u(3)}); o[0] = r.x; o[1] = r.y; o[2] = r.z; o[3] = r.w; break; }
+        case 3: {
+            orc::Rng rng(u(0), u(1), u(2), false);
+            rng.ctr = u(3);
+            float r[4]; rng.next_float(r);
+            for (int k = 0; k < 4; ++k) o[k] = r[k];
+            break;
+        }
+        case 4: o[0] = orc::pack_normal(V(f(0), f(1), f(2))); break;
+        case 5: put3(orc::unpack_normal<R>(u(0)), 0); break;
+        case 6: o[0] = (double)T::GTR1(f(0), f(1)); break;
+        case 7: o[0] = (double)T::GTR2(V(f(0), f(1), f(2)), f(3), f(4)); break;
+        case 8: o[0] = (double)T::smith_gtr2(V(f(0), f(1), f(2)), f(3), f(4)); break;
+        case 9: o[0] = (double)T::smith_gtr1(V(f(0), f(1), f(2))); break;
+        case 10: put3(T::sample_vndf(V(f(0), f(1), f(2)), f(3), f(4), f(5), f(6)), 0); break;
+        case 11: o[0] = (double)T::schlick(f(0), f(1)); break;
+        case 12: o[0] = (double)T::fresnel_dielectric(f(0), f(1)); break;
+        case 13: { R x, y; orc::sample_concentric_disc(f(0), f(1), x, y); o[0] = (double)x; o[1] = (double)y; break; }
+        case 14: put3(orc::sample_cos_hemisphere(f(0), f(1)), 0); break;
+        case 15: put3(orc::sample_uniform_sphere(f(0), f(1)), 0); break;
+        case 16: { const R q = std::sqrt(f(0)); o[0] = (double)(1 - q); o[1] = (double)(q * f(1)); break; }
+        case 17: {
+            const V n(f(0), f(1), f(2));
+            V t, b; orc::make_orthonormal(n, t, b);
+            put3(t, 0); put3(b, 3); put3(n, 6);
+            break;
+        }
+    }
+}
+
+extern "C" {
+
+int oracle_math(int fn, const double* in, uint32_t n, double* out, int precision) {
+    if (fn < 0 || fn > 17) return -1;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (precision == 32) oracle_math_one<float>(fn, in + 8 * (size_t)k, out + 9 * (size_t)k);
+        else oracle_math_one<double>(fn, in + 8 * (size_t)k, out + 9 * (size_t)k);
+    }
+    return 0;
+}
+
 // ---- unit-level entry points for known-answer tests (FP64)
 void oracle_pcg4d(const uint32_t* in, uint32_t* out, uint32_t n) {
     for (uint32_t i = 0; i < n; ++i) {

@@ -34,6 +34,7 @@ def oracle() -> C.CDLL:
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_int]
         L.oracle_pcg4d.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        L.oracle_math.argtypes = [C.c_int, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
         L.oracle_env_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         L.oracle_pack_normal.restype = C.c_uint32
         L.oracle_pack_normal.argtypes = [C.c_double, C.c_double, C.c_double]
@@ -44,6 +45,72 @@ def oracle() -> C.CDLL:
         L.oracle_bsdf_sample.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         _o = L
     return _o
+
+
+REF_SHADER = ROOT / "oracle" / "_ref" / "libref_shader.so"
+_rs = None
+
+# Function ids shared by oracle_math, ref_shader_math and s2_device_math; 8 input and 9 output
+# doubles per entry.
+MATH_FUNCTIONS = ["xxhash32", "pcg", "pcg4d", "next_float", "pack_normal", "unpack_normal", "gtr1", "gtr2",
+                  "smith_gtr2", "smith_gtr1", "vndf", "schlick", "fresnel_dielectric", "concentric_disc",
+                  "cos_hemisphere", "uniform_sphere", "uniform_triangle", "orthonormal"]
+MATH_IN, MATH_OUT = 8, 9
+
+
+def ref_shader() -> C.CDLL | None:
+    """The reference's shader math compiled as host C++ (oracle/build_oracle.py build_ref_shader)."""
+    global _rs
+    if _rs is None:
+        if not REF_SHADER.exists():
+            return None
+        L = C.CDLL(str(REF_SHADER))
+        L.ref_shader_math.argtypes = [C.c_int, C.c_void_p, C.c_uint32, C.c_void_p]
+        _rs = L
+    return _rs
+
+
+def math_inputs(fn: int, n: int, seed: int) -> np.ndarray:
+    """Seeded inputs (n, 8) in each function's domain."""
+    rng = np.random.default_rng(seed + 101 * fn)
+    a = np.zeros((n, MATH_IN))
+    name = MATH_FUNCTIONS[fn]
+    unit = rng.normal(size=(n, 3))
+    unit /= np.linalg.norm(unit, axis=1, keepdims=True)
+    u32 = lambda k: rng.integers(0, 2 ** 32, size=(n, k), dtype=np.uint64).astype(np.float64)
+    uni = lambda k: rng.uniform(0.0, 1.0, size=(n, k)).astype(np.float32).astype(np.float64)
+    if name in ("xxhash32", "pcg"):
+        a[:, :1] = u32(1)
+    elif name in ("pcg4d", "next_float"):
+        a[:, :4] = u32(4)
+    elif name == "pack_normal":
+        a[:, :3] = unit
+    elif name == "unpack_normal":
+        a[:, 0] = (rng.integers(0, 2 ** 16, n) | (rng.integers(0, 2 ** 16, n) << 16)).astype(np.float64)
+    elif name == "gtr1":
+        a[:, 0] = rng.uniform(0.0, 1.0, n)
+        a[:, 1] = rng.uniform(0.001, 0.99, n)
+    elif name in ("gtr2", "smith_gtr2"):
+        a[:, :3] = np.where(unit[:, 2:3] < 0, unit * [1, 1, -1], unit) if name == "gtr2" else unit
+        a[:, 3:5] = rng.uniform(0.01, 1.0, (n, 2))
+    elif name == "smith_gtr1":
+        a[:, :3] = unit
+    elif name == "vndf":
+        a[:, :3] = unit
+        a[:, 3:5] = rng.uniform(0.01, 1.0, (n, 2))
+        a[:, 5:7] = uni(2)
+    elif name == "schlick":
+        a[:, 0] = rng.uniform(0.0, 1.0, n)
+        a[:, 1] = rng.uniform(-0.2, 1.0, n)
+    elif name == "fresnel_dielectric":
+        a[:, 0] = rng.uniform(-1.0, 1.0, n)
+        a[:, 1] = rng.uniform(0.5, 2.5, n)
+    elif name in ("concentric_disc", "cos_hemisphere", "uniform_sphere", "uniform_triangle"):
+        a[:, :2] = uni(2)
+    elif name == "orthonormal":
+        a[:, :3] = unit
+        a[: n // 8, :3] = np.array([1.0, 1.0, 1.0]) / np.sqrt(3.0)  # the branch for N with equal components
+    return a
 
 
 def ref_compat() -> C.CDLL | None:

@@ -31,11 +31,39 @@ def test_library_exports_every_declared_symbol():
     assert set(declared_symbols()) <= exported
 
 
-def test_struct_sizes_match_header():
-    assert ctypes.sizeof(_abi.S2Ray) == 32
-    assert ctypes.sizeof(_abi.S2Hit) == 20
-    assert ctypes.sizeof(_abi.S2View) == 144
-    assert ctypes.sizeof(_abi.S2RenderParams) == 80
+def _ctypes_structs():
+    return {name: cls for name, cls in vars(_abi).items()
+            if isinstance(cls, type) and issubclass(cls, ctypes.Structure) and name.startswith("S2")}
+
+
+def test_every_header_struct_has_a_ctypes_mirror():
+    declared = set(re.findall(r"typedef struct (S2\w+) \{", HEADER.read_text()))
+    assert declared == set(_ctypes_structs())
+
+
+def test_struct_layouts_match_compiled_header(tmp_path):
+    """sizeof and offsetof of every field, compiled from include/stratum2.h by the C compiler, equal
+    the ctypes mirror's."""
+    structs = _ctypes_structs()
+    lines = ["#include <stddef.h>", "#include <stdio.h>", f'#include "{HEADER}"', "int main(void) {"]
+    for name, cls in sorted(structs.items()):
+        lines.append(f'    printf("{name} sizeof %zu\\n", sizeof({name}));')
+        for field in cls._fields_:
+            f = field[0]
+            lines.append(f'    printf("{name} {f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(src)], check=True)
+    got = {}
+    for row in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        struct, key, value = row.split()
+        got[(struct, key)] = int(value)
+    for name, cls in structs.items():
+        assert got[(name, "sizeof")] == ctypes.sizeof(cls), name
+        for field in cls._fields_:
+            assert got[(name, field[0])] == getattr(cls, field[0]).offset, (name, field[0])
 
 
 def test_calls_that_need_no_gpu():
@@ -58,3 +86,12 @@ def test_create_without_gpu_reports_an_error():
     h = ctypes.c_void_p()
     assert _abi.lib().s2_create(0, ctypes.byref(h)) == _abi.S2_ERR_CUDA
     assert not h.value
+
+
+def test_oracle_default_params_equal_the_library_defaults():
+    """The reference arm of bench.py fills its parameters with the oracle's restatement of the
+    reference's defaults (without loading the product library); they equal s2_default_render_params."""
+    from oracle_lib import default_render_params
+    lib_p = _abi.S2RenderParams()
+    _abi.lib().s2_default_render_params(lib_p)
+    assert bytes(default_render_params()) == bytes(lib_p)

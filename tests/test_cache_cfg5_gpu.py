@@ -6,11 +6,11 @@ frames) is pinned to the FP64 oracle image of the same scene (262,144 spp on a 6
 tests/golden/make_golden.py cfg5_1920x1080_subset30) by its relMSE, the oracle image's own noise
 subtracted.
 
-The 2-bounce form uses path regularisation (roughness raised to >= 0.35 after a rough vertex): the
-sun seen through a glossy second vertex from a rough first one is a caustic that the unbiased
-estimator samples as rare fireflies of ~7,000 (measured on B200: one such frame moves the
-progressive relMSE from 0.02 to 1.2 at frame 512).  The test also checks that the regularisation
-removes that tail: the largest per-frame subset value stays far below the sun's radiance."""
+The environment is sampled by its bilinear footprint (S2_FLAG_ENV_FOOTPRINT_PDF, same expected
+image): with the reference's texel pdf the sun's bilinear halo, one texel around a sun of one
+texel, is found only by BSDF sampling, and those rare length-3 hits of ~1,300 (measured on B200 and
+reproduced by the oracle on the same seeds) keep the 2-bounce form from converging.  The test also
+checks that no such tail is left: the largest value of every 16th frame on the subset stays far below it."""
 from pathlib import Path
 
 import numpy as np
@@ -31,7 +31,7 @@ def _params(seed, flags):
     _abi.lib().s2_default_render_params(p)
     p.spp, p.min_path_length, p.max_path_length, p.frame_seed, p.flags = 1, 3, 12, seed, flags
     p.cache_bounces = 2
-    p.cache_min_roughness = 0.35
+    p.flags |= _abi.FLAG_ENV_FOOTPRINT_PDF
     return p
 
 
@@ -65,4 +65,4 @@ def test_batched_two_bounce_cache_reaches_relmse_001_against_fp64(device):
     print("cfg5 2-bounce cached relMSE", err, "largest single-frame value of every 16th frame", peak)
     assert np.isfinite(sub).all()
     assert err < 0.01, err
-    assert peak < 1000.0, peak
+    assert peak < 500.0, peak
