@@ -166,7 +166,7 @@ def run_reference(args, rank: int, world: int):
     line = {"metric": "Mrays/s", "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene generator, no datasets)", "config": bench_config(world, wl.scene.triangle_count()),
+            "data": "synthetic (seeded scene generator, no datasets)", "config": bench_config(world, wl.scene.triangle_count),
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port",
                              "sample": f"pixel subset (stride {r['stride']}, {r['pixels']} pixels) x {SPP} spp per step"},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -286,7 +286,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, no datasets)",
-            "config": bench_config(world, wl.scene.triangle_count()),
+            "config": bench_config(world, wl.scene.triangle_count),
             "bvh8_nodes": int(dev.bvh_stats.node_count),
             "tuning": {"values": (tuning or {}).get("tuning", "defaults"), "autotune_trials": (tuning or {}).get("trials", 0)},
             "mpaths_per_s": paths / ms / 1e3,

@@ -318,6 +318,13 @@ int  s2_render_views(S2Context* ctx, const S2View* views, uint32_t view_count, c
 /* Defaults as in the reference (TestRenderer.cpp:38-43, VCM.cpp:39-40). */
 void s2_default_render_params(S2RenderParams* p);
 
+/* Failure-detection test (diagnostic; no counterpart in the reference): arms the next launch of the
+ * radiance cache's inference kernel (s2_cache_query, or the cache step of a render) to wait on its
+ * first-layer mbarrier without issuing that layer's MMA or commit -- an arrival that never comes --
+ * with each of its bounded waits limited to `polls` polls (1..2^20).  The launch gives up, frees
+ * its TMEM and returns; the call reports S2_ERR_TIMEOUT and the context stays usable.  One-shot. */
+int  s2_inject_wait_timeout(S2Context* ctx, uint32_t polls);
+
 /* ---- device math check (diagnostic) ------------------------------------------------------
  * Evaluates one of the device math functions of the path tracer on n entries, for checks against
  * the reference's own shader functions (src/Shaders/common/rng.hlsli, common.hlsli,

@@ -61,7 +61,7 @@ EXPORTED_SYMBOLS = [
     "s2_cache_train", "s2_cache_gradients", "s2_update_image", "s2_render_diff", "s2_render_adjoint",
     "s2_set_tuning", "s2_get_tuning", "s2_autotune",
     "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap", "s2_default_svgf_params", "s2_svgf_filter",
-    "s2_default_vcm_params", "s2_render_vcm", "s2_device_math",
+    "s2_default_vcm_params", "s2_render_vcm", "s2_device_math", "s2_inject_wait_timeout",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -226,6 +226,7 @@ def lib() -> C.CDLL:
     L.s2_destroy.argtypes = [C.c_void_p]
     L.s2_destroy.restype = None
     L.s2_device_math.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.c_void_p]
+    L.s2_inject_wait_timeout.argtypes = [C.c_void_p, C.c_uint32]
     L.s2_last_error.argtypes = [C.c_void_p]
     L.s2_last_error.restype = C.c_char_p
     L.s2_sync.argtypes = [C.c_void_p]

@@ -24,6 +24,7 @@ struct CacheState {
     float* grad_t = nullptr;         // table gradient accumulator
     float* loss = nullptr;           // summed per-record loss of the last pass
     uint64_t step = 0;
+    uint32_t inject_wait_polls = 0;  // armed by s2_inject_wait_timeout for the next inference launch
     CacheDev dev{};
     int sms = 148;
 };
@@ -216,13 +217,23 @@ void cache_prepare_device(S2Context* ctx) { set_infer_attributes(ctx); }
 
 // Path-tracer terminal vertices: accum[slot] += tput * cache(pos) for up to `cap` queries, the
 // count read from n_dev.
+// The device view for one inference launch: with a wait timeout armed (s2_inject_wait_timeout),
+// this launch carries it and the arming is used up.
+CacheDev infer_view(CacheState* c) {
+    CacheDev d = c->dev;
+    d.wait_test = c->inject_wait_polls;
+    c->inject_wait_polls = 0;
+    return d;
+}
+
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
                        float4* accum, unsigned long long* total_fx) {
     CacheState* c = ctx->cache;
     set_infer_attributes(ctx);
     const uint32_t tiles = (cap + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
-    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, cap, n_dev, nullptr, tput, accum, total_fx);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(infer_view(c), pos, cap, n_dev, nullptr, tput, accum,
+                                                                     total_fx);
     return check_cuda(ctx, cudaGetLastError(), "cache apply launch");
 }
 
@@ -233,10 +244,20 @@ int cache_infer_device(S2Context* ctx, const float4* pos, uint32_t n, float4* ou
     set_infer_attributes(ctx);
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     const uint32_t grid = std::min<uint32_t>(tiles, kInfCtasPerSm * (uint32_t)c->sms);
-    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(c->dev, pos, n, nullptr, out, nullptr, nullptr, nullptr);
+    k_cache_infer<<<grid, kInfThreads, kInfSmemBytes, ctx->stream>>>(infer_view(c), pos, n, nullptr, out, nullptr, nullptr,
+                                                                     nullptr);
     return check_cuda(ctx, cudaGetLastError(), "cache inference launch");
 }
 }  // namespace s2
+
+extern "C" int s2_inject_wait_timeout(S2Context* ctx, uint32_t polls) {
+    if (!ctx) return S2_ERR_INVALID;
+    if (!ctx->cache) return set_error(ctx, S2_ERR_NO_SCENE, "s2_inject_wait_timeout before s2_cache_init");
+    if (polls == 0 || polls > (1u << 20))
+        return set_error(ctx, S2_ERR_INVALID, "s2_inject_wait_timeout: polls must be in 1..2^20");
+    ctx->cache->inject_wait_polls = polls;
+    return S2_OK;
+}
 
 extern "C" int s2_cache_query(S2Context* ctx, const float* positions, uint32_t n, float* radiance, int on_device) {
     if (!ctx) return S2_ERR_INVALID;

@@ -52,6 +52,10 @@ struct CacheDev {
     float3 box_min, box_inv_extent;
     const uint4* wimage;         // kWImageTrainBytes: W1, W2, W3 (padded), W2T, W1T in operand layout
     int* status;                 // bit 2: a tensor-core wait timed out
+    // failure-detection test (s2_inject_wait_timeout): nonzero makes the inference kernel wait on
+    // its first-layer barrier without issuing that layer's MMA or commit -- an arrival that never
+    // comes -- polling at most this many times in each of its waits; 0 = off
+    uint32_t wait_test;
     // training
     float* grad_w;               // summed per-record gradients of the weights
     float* grad_t;               // summed per-record gradients of the table, [levels][entries][2]
@@ -212,10 +216,11 @@ __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_con
     const uint32_t s_x = smem_addr(smem + kInfSmemX), s_h = smem_addr(smem + kInfSmemH);
     uint32_t phase = 0;
     bool ok = true;
+    const uint32_t wait_limit = c.wait_test ? c.wait_test : kMbarWaitLimit;
     // MMA completion for the MLP warps (the others only take part in the block barriers)
     auto done = [&](bool issued) {
         if (!mlp) return;
-        const bool w = ok && issued && mbar_wait(&bar, phase);
+        const bool w = ok && issued && mbar_wait(&bar, phase, wait_limit);
         if (w) phase ^= 1u;
         ok = __all_sync(0xffffffffu, w);
     };
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_con
         const uint32_t q = tile * kCacheTile + t;  // MLP row of warps 0..3
         // layer 1: D[0:64) = X W1^T
         block_sync_tc();
-        if (t == 0 && ok) {
+        if (t == 0 && ok && !c.wait_test) {
             umma_gemm(tmem, s_x, s_w1, kCacheIn, kCacheHidden, false);
             umma_commit(&bar);
         }
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_con
         // a wait timed out: record it, give an MMA still in flight a bounded time to land, and
         // release TMEM only then
         if (t == 0) atomicOr(c.status, 4);
-        if (mlp) mbar_wait(&bar, phase);
+        if (mlp) mbar_wait(&bar, phase, wait_limit);
     }
     tc_fence_before_sync();
     __syncthreads();

@@ -61,7 +61,8 @@ S2D bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait for phase `parity` of `bar`: false after `limit` polls (each poll itself blocks
 // for a hardware-defined time slice), so a lost arrival cannot hang the GPU.
-S2D bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = 1u << 22) {
+constexpr uint32_t kMbarWaitLimit = 1u << 22;
+S2D bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kMbarWaitLimit) {
     for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;

@@ -5,6 +5,11 @@
 the per-channel error summed over RGB and pixels, divided by 3*W*H; MSE reported as its square
 root).  `relmse` is the relative mean squared error used for convergence targets:
 mean over pixels and RGB of (a - b)^2 / (b^2 + eps).
+
+Differences from the shader, where its result is undefined or inexact: a SMAPE channel that is 0
+in both images (0/0) contributes 0 here, where the shader's NaN makes the `(uint)` conversion of
+its whole wave's sum undefined; and the sums are exact floating point, where the shader adds
+wave sums truncated to integers after scaling by mQuantization.
 """
 from __future__ import annotations
 

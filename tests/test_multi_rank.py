@@ -61,3 +61,73 @@ def test_single_rank_is_identity():
     img = torch.ones(3)
     assert combine_images(img, 1) is img
     assert job_time_and_totals(5.0, [1.0, 2.0], 1) == (5.0, [1.0, 2.0])
+
+
+def _render_worker(rank, world, port, out):
+    """Each rank renders its own block of frame seeds of the same small frame with the CPU oracle
+    (the multi-GPU path's sample partition, with the oracle standing in for a GPU), and the images
+    are combined into rank 0."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle_lib import OracleScene, default_render_params
+        from stratum2_b200.scenegen import box_scene
+        wl = box_scene(seed=1, n_random=50, width=12, height=10)
+        spp = 4
+        p = default_render_params()
+        p.spp, p.min_path_length, p.max_path_length = spp, 2, 5
+        p.frame_seed = frame_seed(0, rank, world, spp)
+        r = OracleScene(wl.scene, 2).render(wl.view, p, wl.width, wl.height, precision=32, threads=1)
+        img = torch.from_numpy(r["mean"].copy())
+        combine_images(img, world, dist)
+        if rank == 0:
+            out[0] = img.numpy().tolist()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_gloo_ranks_render_sample_blocks_that_combine_to_one_render():
+    from oracle_lib import OracleScene, default_render_params
+    from stratum2_b200.scenegen import box_scene
+    world = 2
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_render_worker, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+    wl = box_scene(seed=1, n_random=50, width=12, height=10)
+    p = default_render_params()
+    p.spp, p.min_path_length, p.max_path_length, p.frame_seed = 4 * world, 2, 5, frame_seed(0, 0, world, 4)
+    ref = OracleScene(wl.scene, 2).render(wl.view, p, wl.width, wl.height, precision=32, threads=1)["mean"]
+    np.testing.assert_allclose(np.array(out[0]), ref, rtol=1e-12, atol=1e-12)
+
+
+def _dropout_worker(rank, world, port, out):
+    """Rank 1 leaves between steps, before the step's collective; rank 0 learns of it from the
+    collective's error (short process-group timeout), not by hanging."""
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    job_time_and_totals(1.0, [1.0], world, dist)  # step 0: both ranks
+    if rank == 1:
+        os._exit(0)  # leaves without its kernels or collectives in flight
+    try:
+        job_time_and_totals(1.0, [1.0], world, dist)  # step 1: the peer is gone
+        out[0] = "no error"
+    except Exception as e:  # noqa: BLE001 -- the failure is the point
+        out[0] = type(e).__name__
+
+
+@pytest.mark.timeout(120)
+def test_a_rank_leaving_between_steps_ends_the_next_collective_with_an_error():
+    world = 2
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    ctx = mp.start_processes(_dropout_worker, args=(world, port, out), nprocs=world, join=False, start_method="spawn")
+    for p in ctx.processes:
+        p.join(60)
+    assert all(not p.is_alive() for p in ctx.processes)
+    assert out.get(0) not in (None, "no error"), out.get(0)

@@ -41,9 +41,13 @@ def _oracle(fn, a, precision):
     return o
 
 
-def _close(name, got, ref, exact):
+def _close(name, got, ref, exact, device=False):
     if exact:
         np.testing.assert_array_equal(got, ref, err_msg=name)
+    elif device and name == "gtr1":
+        # (a^2 - 1) / log(a^2) is ill-conditioned as alpha -> 1: one ulp of the device's logf
+        # there is up to 2e-5 relative in the result
+        np.testing.assert_allclose(got, ref, rtol=1e-4, atol=0, err_msg=name)
     elif name in TRIG:
         np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5, err_msg=name)
     else:
@@ -85,4 +89,4 @@ def test_device_math_matches_reference_shader_math(device, fn):
     got = np.zeros((len(a), MATH_OUT))
     rc = _abi.lib().s2_device_math(device._h, fn, np.ascontiguousarray(a).ctypes.data, len(a), got.ctypes.data)
     assert rc == _abi.S2_OK, _abi.lib().s2_last_error(device._h)
-    _close(name, got, ref, name in INTEGER)
+    _close(name, got, ref, name in INTEGER, device=True)
