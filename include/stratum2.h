@@ -370,6 +370,8 @@ int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams*
 #define S2_SHADE_ORDER_QUEUE 1u
 #define S2_TRACE_ORDER_QUEUE 0u
 #define S2_TRACE_ORDER_COHERENT 1u
+#define S2_SHADE_RECORDS_ON 0u
+#define S2_SHADE_RECORDS_OFF 1u
 
 typedef struct S2Tuning {
     uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^26) */
@@ -382,7 +384,12 @@ typedef struct S2Tuning {
     uint32_t trace_order;         /* S2_TRACE_ORDER_QUEUE (0, default): trace continuation rays in queue
                                      order; S2_TRACE_ORDER_COHERENT (1): counting-sort them by origin cell
                                      and direction octant first.  Images are bit-identical either way. */
-    uint32_t reserved[2];
+    uint32_t shade_records;       /* S2_SHADE_RECORDS_ON (0, default): hits on meshes without texture
+                                     coordinates or normals read a 64-byte shading record baked per BVH
+                                     triangle at s2_build_bvh; S2_SHADE_RECORDS_OFF (1): gather through
+                                     the instance and vertex buffers as the reference does.  Images are
+                                     bit-identical either way. */
+    uint32_t reserved;
 } S2Tuning;
 
 int  s2_set_tuning(S2Context* ctx, const S2Tuning* tuning);

@@ -51,6 +51,8 @@ SHADE_ORDER_MATERIAL = 0
 SHADE_ORDER_QUEUE = 1
 TRACE_ORDER_QUEUE = 0
 TRACE_ORDER_COHERENT = 1
+SHADE_RECORDS_ON = 0
+SHADE_RECORDS_OFF = 1
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -151,7 +153,7 @@ class S2CacheParams(C.Structure):
 class S2Tuning(C.Structure):
     _fields_ = [("wave_paths", C.c_uint32), ("trav_tris_per_step", C.c_uint32), ("trav_vote8", C.c_uint32),
                 ("refill_min", C.c_uint32), ("shade_order", C.c_uint32), ("trace_order", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("shade_records", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 TEMPORAL_REPROJECT, TEMPORAL_CHECK_NORMAL, TEMPORAL_CHECK_DEPTH = 1 << 0, 1 << 1, 1 << 2

@@ -667,6 +667,7 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
         ctx->scene.key_lo = make_float4(root.p[0], root.p[1], root.p[2], 0.f);
         ctx->scene.key_scale = make_float4(8.f / sc[0], 8.f / sc[1], 8.f / sc[2], 0.f);
     }
+    S2_TRY(bake_shading_records(ctx, ctx->bvh_bufs));
     S2_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "BVH upload"));
     if (stats) {
         stats->node_count = out.nodes.size();

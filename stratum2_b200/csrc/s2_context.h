@@ -70,6 +70,8 @@ void free_bufs(std::vector<DevBuf>& bufs);
 void destroy_render_state(S2Context* ctx);
 void destroy_cache_state(S2Context* ctx);
 void destroy_post_state(S2Context* ctx);
+// baked shading records of the current BVH (s2_render.cu), allocated into `owner`
+int bake_shading_records(S2Context* ctx, std::vector<DevBuf>& owner);
 // radiance cache entry points used by the renderer (s2_cache.cu)
 int cache_apply_device(S2Context* ctx, const float4* pos, const float4* tput, uint32_t cap, const uint32_t* n_dev,
                        float4* accum, unsigned long long* total_fx = nullptr);

@@ -249,7 +249,45 @@ void launch_shade(const PTParams& P, uint32_t parity, const RenderState* st, cud
     else k_shade<L, R><<<R ? st->shade_blocks_rc : st->shade_blocks, 128, 0, s>>>(P, parity);
 }
 
+// One baked shading record per BVH triangle (make_shading_rec): triangles of mesh instances whose
+// vertex data has neither texture coordinates nor normals get make_shading's per-triangle terms,
+// evaluated here by make_shading itself; the others are marked invalid and keep the gather chain.
+__global__ void k_bake_shading(const __grid_constant__ DevScene s, float4* __restrict__ recs) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.tri_count) return;
+    float4* out = recs + 4 * (size_t)i;
+    out[3] = make_float4(0.f, 0.f, 0.f, 0.f);  // invalid unless baked below
+    const uint32_t inst = __float_as_uint(s.tris[3 * (size_t)i].w), prim = __float_as_uint(s.tris[3 * (size_t)i + 1].w);
+    const uint2 id = s.instances[inst];
+    if ((id.x & 0xfu) != S2_INSTANCE_TYPE_MESH) return;
+    const VInfo vi = load_vinfo(s, id.y & 0xffffu);
+    if (vi_texcoord_buffer(vi) < s.vbuf_count || vi_normal_buffer(vi) < s.vbuf_count) return;
+    const uint3 tri = load_triangle_indices(s.vbufs[vi_index_buffer(vi)], vi_index_offset(vi), vi_index_stride(vi), prim);
+    const uint8_t* pb = s.vbufs[vi_position_buffer(vi)];
+    const uint32_t po = vi_position_offset(vi), ps = vi_position_stride(vi);
+    const float3 v0 = load_f3(pb, po, ps, tri.x), v1 = load_f3(pb, po, ps, tri.y), v2 = load_f3(pb, po, ps, tri.z);
+    const float3 e1 = v1 - v0, e2 = v2 - v0;
+    const SD sd = make_shading(s, inst, prim, 0.f, 0.f, false);
+    out[0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(sd.mat));
+    out[1] = make_float4(e1.x, e1.y, e1.z, sd.area);
+    out[2] = make_float4(e2.x, e2.y, e2.z, __uint_as_float(sd.ng));
+    out[3] = make_float4(__uint_as_float(sd.tg), __uint_as_float(kShadeRecValid), 0.f, 0.f);
+}
+
 }  // namespace
+
+// Builds the baked shading records of the current BVH (called by s2_build_bvh).
+int bake_shading_records(S2Context* ctx, std::vector<DevBuf>& owner) {
+    ctx->scene.shade_recs = nullptr;
+    const uint32_t n = ctx->scene.tri_count;
+    if (n == 0) return S2_OK;
+    float4* recs = (float4*)dev_alloc(ctx, owner, sizeof(float4) * 4 * (size_t)n);
+    if (!recs) return set_error(ctx, S2_ERR_OOM, "shading record allocation failed");
+    k_bake_shading<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->scene, recs);
+    const int rc = check_cuda(ctx, cudaGetLastError(), "shading record bake");
+    if (rc == S2_OK) ctx->scene.shade_recs = recs;
+    return rc;
+}
 }  // namespace s2
 
 using namespace s2;
@@ -316,6 +354,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     PTParams P;
     std::memset(&P, 0, sizeof(P));
     P.scene = ctx->scene;
+    if (ctx->tuning.shade_records == S2_SHADE_RECORDS_OFF) P.scene.shade_recs = nullptr;
     P.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
     P.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
@@ -803,6 +842,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     PTParams P;
     std::memset(&P, 0, sizeof(P));
     P.scene = ctx->scene;
+    if (ctx->tuning.shade_records == S2_SHADE_RECORDS_OFF) P.scene.shade_recs = nullptr;
     P.scene.light_power_pick = (prm->flags & S2_FLAG_LIGHT_POWER_PICK) ? 1u : 0u;
     P.scene.env_fp_on = (prm->flags & S2_FLAG_ENV_FOOTPRINT_PDF) ? 1u : 0u;
     P.scene.env_sample_prob = prm->environment_sample_probability > 0.f ? prm->environment_sample_probability : 0.9f;
@@ -1061,9 +1101,10 @@ extern "C" int s2_set_tuning(S2Context* ctx, const S2Tuning* t) {
     if (!ctx) return S2_ERR_INVALID;
     if (!t) { std::memset(&ctx->tuning, 0, sizeof(ctx->tuning)); return S2_OK; }
     if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024) ||
-        t->shade_order > S2_SHADE_ORDER_QUEUE || t->trace_order > S2_TRACE_ORDER_COHERENT)
+        t->shade_order > S2_SHADE_ORDER_QUEUE || t->trace_order > S2_TRACE_ORDER_COHERENT ||
+        t->shade_records > S2_SHADE_RECORDS_OFF)
         return set_error(ctx, S2_ERR_INVALID, "tuning out of range (tris_per_step <= 32, vote8 <= 9, refill_min <= 32, "
-                                              "wave_paths 0 or >= 1024, shade_order and trace_order 0 or 1)");
+                                              "wave_paths 0 or >= 1024, shade_order, trace_order and shade_records 0 or 1)");
     ctx->tuning = *t;
     return S2_OK;
 }

@@ -73,6 +73,9 @@ struct DevScene {
     float4 scene_sphere;
     // ray-coherence keys: the BVH root box as origin and 8 / extent per axis (zero: no BVH)
     float4 key_lo, key_scale;
+    // baked shading records, four float4 per BVH triangle (k_bake_shading; null: none, or switched
+    // off by S2Tuning.shade_records)
+    const float4* shade_recs;
 };
 
 // Ray-coherence key: Morton code of the origin's cell in an 8^3 grid over the BVH root box

@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
             } else {
                 const float4 tr0 = s.tris[3 * (size_t)tri], tr1 = s.tris[3 * (size_t)tri + 1];
                 const uint32_t inst = __float_as_uint(tr0.w), prim = __float_as_uint(tr1.w);
-                SD sd = make_shading(s, inst, prim, h.z, h.w, sn);
+                SD sd = make_shading_rec(s, tri, inst, prim, h.z, h.w, sn);
                 if (!(P.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
                 const float isect_dist = half_round(h.x);
                 const float isect_pdfa = half_round(light_pdfa(s, inst, sd.area));

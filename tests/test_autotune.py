@@ -71,3 +71,30 @@ def test_queue_orders_keep_the_image_bitwise(device, flags):
     b, _ = device.render_views([wl.view], p)
     np.testing.assert_array_equal(a[0].radiance, b[0].radiance)
     device.set_tuning(None)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scene,flags", [("textured_box", _abi.FLAG_LAMBERTIAN), ("textured_box", 0),
+                                         ("terrain", 0), ("terrain", _abi.FLAG_RESTIR_DI)])
+def test_shading_records_keep_the_image_bitwise(device, scene, flags):
+    """The baked per-triangle shading records (S2Tuning.shade_records, on by default) hold
+    make_shading's own per-triangle terms: images and first-hit AOVs are bit-identical to the
+    gather through instance, vertex info, indices and positions, on meshes with texture
+    coordinates (not baked: the textured walls) and without (baked: spheres, terrain)."""
+    from stratum2_b200.scenegen import terrain_scene, textured_box_scene
+    wl = textured_box_scene(seed=4, width=48, height=48, spheres=3) if scene == "textured_box" else \
+        terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+    device.upload_scene(wl.scene)
+    p = device.default_params()
+    p.spp, p.min_path_length, p.max_path_length, p.flags, p.frame_seed = 8, 1, 6, flags | _abi.FLAG_PIXEL_JITTER, 17
+    p.restir_candidates = 4
+    off = _abi.S2Tuning()
+    off.shade_records = _abi.SHADE_RECORDS_OFF
+    device.set_tuning(off)
+    ref = device.render(wl.view, wl.width, wl.height, params=p)
+    device.set_tuning(None)
+    out = device.render(wl.view, wl.width, wl.height, params=p)
+    np.testing.assert_array_equal(out.radiance, ref.radiance)
+    np.testing.assert_array_equal(out.albedo, ref.albedo)
+    np.testing.assert_array_equal(out.visibility, ref.visibility)
+    np.testing.assert_array_equal(out.depth, ref.depth)

@@ -10,7 +10,8 @@ seeded inputs in each function's domain:
   float rounding (1e-6 relative, 2e-5 absolute for the trigonometric sampling maps) for the rest;
 * the oracle's FP64 build agrees within float tolerances (packing within one SNORM16 step);
 * the device functions (s2_device_math, GPU) equal the reference bit for bit for the integer
-  functions and the packing, and within float rounding for the rest.
+  functions and the packing, and within float rounding for the rest (1e-5 relative; 1e-4 for
+  GTR1, whose (a^2 - 1) / log(a^2) is ill-conditioned as alpha -> 1).
 """
 import ctypes as C
 
@@ -50,6 +51,9 @@ def _close(name, got, ref, exact, device=False):
         np.testing.assert_allclose(got, ref, rtol=1e-4, atol=0, err_msg=name)
     elif name in TRIG:
         np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5, err_msg=name)
+    elif device:
+        # the device's sqrtf / powf / division round within an ulp or two of the host's
+        np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-7, err_msg=name)
     else:
         np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7, err_msg=name)
 
