@@ -133,10 +133,12 @@ S2D Rng make_rng(uint32_t pixel_x, uint32_t pixel_y, uint32_t seed, bool pcg32) 
 // ---------------------------------------------------------------- normal packing
 // Octahedral map (src/Shaders/common/common.hlsli:5-22) stored as R16G16_SNORM
 // (D3DX_DXGIFormatConvert.inl: D3DX_FLOAT2_to_R16G16_SNORM / D3DX_R16G16_SNORM_to_FLOAT2).
+// D3DX_FLOAT_to_INT: a separate multiply and add (explicitly rounded, so no contraction into an
+// FMA changes the result with the surrounding code)
 S2D int snorm_from_float(float v) {
     if (isnan(v)) v = 0.f;
     v = fminf(fmaxf(v, -1.f), 1.f);
-    return (int)truncf(v * 32767.f + (v >= 0 ? 0.5f : -0.5f));
+    return (int)truncf(__fadd_rn(__fmul_rn(v, 32767.f), v >= 0 ? 0.5f : -0.5f));
 }
 S2D float float_from_snorm(int v) { return fmaxf((float)v / 32767.f, -1.f); }
 S2D uint32_t pack_normal(float3 v) {

