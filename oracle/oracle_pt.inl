@@ -5,7 +5,7 @@
 //
 // Deliberate differences from the reference shaders (each is a defect there):
 //  * environment NEE uses the sampled direction; the reference leaves
-//    IlluminationSampleRecord.mDirectionToLight unset for environment samples (lights.hlsli:413-423);
+//    IlluminationSampleRecord.mDirectionToLight unset for environment samples (lights.hlsli:234-244);
 //  * the MIS weight of a BSDF-sampled environment hit uses the environment's solid-angle pdf; the
 //    reference passes the light-tracing disc pdf 1/(pi R^2) (testrenderer.slang:1047-1050) unless
 //    S2_FLAG_REFERENCE_ENV_MIS is set;

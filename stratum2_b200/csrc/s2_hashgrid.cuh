@@ -1,7 +1,7 @@
 // World-space hash grid of ReSTIR DI reservoirs (src/Shaders/common/hashgrid.hlsli:14-119,
 // src/App/GpuHashGrid.cpp:17-111): cells keyed by the pcg hash of the quantized position with an
 // xxhash32 checksum and 32-step linear probing; items are appended with atomics, then a prefix sum
-// over the per-cell counters and a swizzle sort them by cell.  The renderer keeps two grids:
+// over the per-cell counters and a sort by (cell, record content) list them by cell.  The renderer keeps two grids:
 // the previous frame's (read) and the current frame's (appended to, built at the end of the call).
 #pragma once
 #include "s2_math.cuh"
@@ -76,18 +76,57 @@ S2D void hg_append(const HashGridDev& g, float3 pos, const ReservoirRecord& rec)
     g.data[idx] = rec;
 }
 
-// ComputeIndices (hashgrid.hlsli:101-108): one thread per cell
-__global__ void k_hg_compute_indices(HashGridDev g) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.cell_count) return;
-    g.indices[c] = atomicAdd(&g.other[1], g.cell_counters[c]);
+// Building the grid (the work of ComputeIndices and Swizzle, hashgrid.hlsli:101-119), so that the
+// order of the records inside a cell does not depend on the order of the atomic appends:
+//  * k_hg_scan: each cell's offset is the exclusive prefix sum of the cell counters in cell order
+//    (one block: per-thread runs of cells, then a block scan of the run totals), where the
+//    reference adds them with an atomic counter in arrival order;
+//  * k_hg_keys: a 64-bit key per appended record, its cell above a hash of its content, and
+//    unused slots in a cell past the last;
+//  * a radix sort of (key, record index) pairs (cub::DeviceRadixSort, in s2_render.cu) lists the
+//    records by cell, and inside a cell by content: data_indices[indices[c] + k] is the k-th
+//    record of cell c in an order fixed by the records themselves.
+constexpr uint32_t kHgScanThreads = 1024;
+__global__ void __launch_bounds__(kHgScanThreads) k_hg_scan(HashGridDev g) {
+    __shared__ uint32_t part[kHgScanThreads];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (g.cell_count + kHgScanThreads - 1) / kHgScanThreads;
+    const uint32_t c0 = t * per, c1 = min(c0 + per, g.cell_count);
+    uint32_t sum = 0;
+    for (uint32_t c = c0; c < c1; ++c) sum += g.cell_counters[c];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < kHgScanThreads; off <<= 1) {  // inclusive Hillis-Steele scan
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (uint32_t c = c0; c < c1; ++c) {
+        g.indices[c] = run;
+        run += g.cell_counters[c];
+    }
 }
 
-// Swizzle (hashgrid.hlsli:111-119): one thread per appended item
-__global__ void k_hg_swizzle(HashGridDev g) {
+S2D uint32_t hg_record_hash(const ReservoirRecord& r) {
+    uint32_t h = xxhash32(r.instance ^ 0x9e3779b9u);
+    h = xxhash32(h ^ r.primitive);
+    h = xxhash32(h ^ __float_as_uint(r.local_pos.x));
+    h = xxhash32(h ^ __float_as_uint(r.local_pos.y));
+    h = xxhash32(h ^ __float_as_uint(r.local_pos.z));
+    h = xxhash32(h ^ __float_as_uint(r.rnd.x));
+    h = xxhash32(h ^ __float_as_uint(r.rnd.y));
+    h = xxhash32(h ^ __float_as_uint(r.rnd.z));
+    h = xxhash32(h ^ __float_as_uint(r.rnd.w));
+    return xxhash32(h ^ __float_as_uint(r.W));
+}
+
+__global__ void k_hg_keys(HashGridDev g, unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.max_size) return;
     const uint32_t n = min(g.other[0], g.max_size);
-    if (i >= n) return;
-    const uint2 a = g.append_indices[i];
-    g.data_indices[g.indices[a.x] + a.y] = i;
+    vals[i] = i;
+    keys[i] = i < n ? (((unsigned long long)g.append_indices[i].x << 32) | hg_record_hash(g.data[i]))
+                    : (((unsigned long long)g.cell_count << 32) | 0xffffffffull);
 }

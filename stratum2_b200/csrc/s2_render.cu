@@ -6,6 +6,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "s2_context.h"
 #include "s2_shade_kernel.cuh"
 #include "s2_light_trace.cuh"
@@ -46,6 +48,12 @@ struct RenderState {
     struct Grid {
         std::vector<DevBuf> bufs;
         HashGridDev g{};
+        // build: sort keys in and out, record indices in, CUB temporary storage
+        unsigned long long *keys_in = nullptr, *keys_out = nullptr;
+        uint32_t* vals_in = nullptr;
+        void* sort_tmp = nullptr;
+        size_t sort_bytes = 0;
+        int end_bit = 64;
     } grid[2];
     uint32_t grid_cur = 0;
     bool grid_prev_valid = false;
@@ -221,6 +229,19 @@ int ensure_cache_queues(S2Context* ctx, RenderState* st, uint32_t cq, uint32_t t
     return S2_OK;
 }
 
+// Builds a grid after its appends (cell offsets by a scan, records sorted by cell and content);
+// returns the kernel launches issued.
+uint32_t build_grid(S2Context* ctx, RenderState::Grid& G, cudaStream_t s) {
+    const HashGridDev& g = G.g;
+    k_hg_scan<<<1, kHgScanThreads, 0, s>>>(g);
+    k_hg_keys<<<(g.max_size + 255) / 256, 256, 0, s>>>(g, G.keys_in, G.vals_in);
+    size_t bytes = G.sort_bytes;
+    cub::DeviceRadixSort::SortPairs(G.sort_tmp, bytes, G.keys_in, G.keys_out, G.vals_in, g.data_indices, (int)g.max_size, 0,
+                                    G.end_bit, s);
+    (void)ctx;
+    return 3;
+}
+
 // (Re)allocates one hash grid for `cells` cells and `size` records (GpuHashGrid::init,
 // src/App/GpuHashGrid.cpp:17-69).
 int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t size) {
@@ -235,8 +256,20 @@ int ensure_grid(S2Context* ctx, RenderState::Grid& G, uint32_t cells, uint32_t s
     g.data = alloc<ReservoirRecord>(ctx, G.bufs, size);
     g.indices = alloc<uint32_t>(ctx, G.bufs, cells);
     g.data_indices = alloc<uint32_t>(ctx, G.bufs, size);
+    G.keys_in = alloc<unsigned long long>(ctx, G.bufs, size);
+    G.keys_out = alloc<unsigned long long>(ctx, G.bufs, size);
+    G.vals_in = alloc<uint32_t>(ctx, G.bufs, size);
+    // keys: cell (bits 32 and up) above a 32-bit content hash; unused slots take cell `cells`, one
+    // past the last, so they sort last; the sort reads 32 + ceil(log2(cells + 1)) bits
+    int cell_bits = 1;
+    while (cell_bits < 32 && (1ull << cell_bits) <= cells) ++cell_bits;
+    G.end_bit = 32 + cell_bits;
+    G.sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, G.sort_bytes, G.keys_in, G.keys_out, G.vals_in, g.data_indices, (int)size, 0,
+                                    G.end_bit, ctx->stream);
+    G.sort_tmp = dev_alloc(ctx, G.bufs, std::max<size_t>(G.sort_bytes, 16));
     for (auto& b : G.bufs) if (!b.ptr) { free_bufs(G.bufs); return S2_ERR_OOM; }
-    if (G.bufs.size() != 7) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    if (G.bufs.size() != 11) { free_bufs(G.bufs); return S2_ERR_OOM; }
     g.cell_count = cells;
     g.max_size = size;
     G.g = g;
@@ -583,10 +616,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     }
     if (reuse) {
         // GpuHashGrid::build (GpuHashGrid.cpp:84-111), then this grid becomes the previous one
-        const HashGridDev& g = st->grid[st->grid_cur].g;
-        k_hg_compute_indices<<<(g.cell_count + 255) / 256, 256, 0, s>>>(g);
-        k_hg_swizzle<<<(g.max_size + 255) / 256, 256, 0, s>>>(g);
-        launches += 2;
+        launches += build_grid(ctx, st->grid[st->grid_cur], s);
         st->grid_cur ^= 1u;
         st->grid_prev_valid = true;
     }
@@ -1026,10 +1056,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (!*B->done_host) return set_error(ctx, S2_ERR_DEVICE, "batched render did not finish within its iteration bound");
     if (reuse) {
         // GpuHashGrid::build (GpuHashGrid.cpp:84-111), then this grid becomes the previous one
-        const HashGridDev& g = st->grid[st->grid_cur].g;
-        k_hg_compute_indices<<<(g.cell_count + 255) / 256, 256, 0, s>>>(g);
-        k_hg_swizzle<<<(g.max_size + 255) / 256, 256, 0, s>>>(g);
-        launches += 2;
+        launches += build_grid(ctx, st->grid[st->grid_cur], s);
         st->grid_cur ^= 1u;
         st->grid_prev_valid = true;
     }

@@ -1,9 +1,11 @@
 """ReSTIR DI reuse through the world-space hash grid on the GPU (S2_FLAG_RESTIR_REUSE,
 testrenderer.slang:608-726, hashgrid.hlsli:14-119).
 
-Reuse picks records in atomic append order, so a reuse render is not reproducible sample by
-sample; it is checked statistically:
-  * the first call of a sequence (no previous grid) is the RIS-only render, bit for bit;
+The grid build lists each cell's records in an order fixed by their content (a scan of the cell
+counters and a sort by cell and record hash, where the reference keeps the atomic append order), so
+reuse sequences are reproducible bit for bit; the estimator is checked statistically:
+  * the first call of a sequence (no previous grid) is the RIS-only render, bit for bit, and
+    repeating a sequence repeats its images;
   * a sequence of reuse frames converges to plain NEE (box: the FP64 golden image; many-lights
     terrain: a 16 x 4096 spp GPU NEE image) by the same z-test as the other convergence tests;
   * on the many-lights scene (256 emitters, power lognormal(0, 1), Lambertian, direct light only)
@@ -68,13 +70,22 @@ def z_check(m, v, ref, ref_var, tag):
     assert abs(z.mean()) < 0.15, f"{tag}: mean z {z.mean():.3f}"
 
 
+def test_reuse_sequences_are_reproducible(device, lights):
+    wl = lights
+    seqs = []
+    for _ in range(2):
+        device.upload_scene(wl.scene)  # a fresh render state: no previous grid
+        seqs.append(frames(device, wl, REUSE, 4, 300, 5))
+    np.testing.assert_array_equal(seqs[0], seqs[1])
+
+
 def test_first_reuse_call_is_ris_and_reuse_changes_later_calls(device, lights):
     wl = lights
     device.upload_scene(wl.scene)  # a fresh render state has no previous grid
     a = render(device, wl, params(1, REUSE | J, 4))
     b = render(device, wl, params(1, RIS | J, 4))
     np.testing.assert_array_equal(a.radiance, b.radiance)
-    assert a.stats.kernel_launches == b.stats.kernel_launches + 2  # grid build: indices + swizzle
+    assert a.stats.kernel_launches == b.stats.kernel_launches + 3  # grid build: scan, keys, sort
     render(device, wl, params(2, REUSE | J, 4))
     c = render(device, wl, params(3, REUSE | J, 4))
     d = render(device, wl, params(3, RIS | J, 4))
