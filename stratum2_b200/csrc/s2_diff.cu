@@ -38,7 +38,7 @@ int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, Di
     if (W <= 0 || H <= 0 || (int64_t)W * H > (1ll << 26)) return set_error(ctx, S2_ERR_INVALID, "invalid view extent");
     if (prm->spp == 0) return set_error(ctx, S2_ERR_INVALID, "spp must be >= 1");
     if ((uint64_t)W * H * prm->spp > 0xffffffffull)
-        return set_error(ctx, S2_ERR_INVALID, "pixels x spp must stay below 2^32 (one thread per path)");
+        return set_error(ctx, S2_ERR_INVALID, "pixels x spp must stay below 2^32 (32-bit path ids)");
     if (prm->max_path_length > 255) return set_error(ctx, S2_ERR_INVALID, "max_path_length must be <= 255");
     if (prm->flags & kDiffUnsupported)
         return set_error(ctx, S2_ERR_UNSUPPORTED, "differentiable rendering supports plain NEE path tracing only "
@@ -63,12 +63,77 @@ int check_args(S2Context* ctx, const S2View* view, const S2RenderParams* prm, Di
     return S2_OK;
 }
 
-template <bool ADJ>
-void launch(const DiffArgs& A, cudaStream_t s) {
-    const uint32_t blocks = (uint32_t)(((uint64_t)A.pixels * A.spp + 127) / 128);
-    if (A.flags & S2_FLAG_LAMBERTIAN) dk::k_diff<true, ADJ><<<blocks, 128, 0, s>>>(A);
-    else dk::k_diff<false, ADJ><<<blocks, 128, 0, s>>>(A);
-    if (!ADJ) dk::k_diff_resolve<<<(A.pixels + 255) / 256, 256, 0, s>>>(A);
+// Wavefront buffers of one call: paths are rendered in waves of at most kDiffWave.
+constexpr uint32_t kDiffWave = 1u << 23;
+
+struct DiffWave {
+    dk::PTParams P;
+    dk::DiffQueues Q;
+    uint32_t cap = 0;
+    int ext_blocks = 0, shade_blocks = 0;
+};
+
+int alloc_wave(S2Context* ctx, std::vector<DevBuf>& tmp, const DiffArgs& A, DiffWave& w) {
+    const uint64_t total = (uint64_t)A.pixels * A.spp;
+    w.cap = (uint32_t)std::min<uint64_t>(total, kDiffWave);
+    std::memset(&w.P, 0, sizeof(w.P));
+    w.P.scene = A.scene;
+    if (ctx->tuning.shade_records == S2_SHADE_RECORDS_OFF) w.P.scene.shade_recs = nullptr;
+    w.P.flags = A.flags;
+    w.P.trav.tris_per_step = ctx->tuning.trav_tris_per_step;
+    w.P.trav.vote8 = ctx->tuning.trav_vote8;
+    w.P.refill_min = ctx->tuning.refill_min;
+    w.P.status = A.status;
+    for (int k = 0; k < 2; ++k) {
+        // positional: the four 16-byte streams of a path queue (the namespace rename above also
+        // renames the queue's third member)
+        float4* a = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+        float4* b = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+        float4* c = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+        uint4* d = (uint4*)dev_alloc(ctx, tmp, sizeof(uint4) * (size_t)w.cap);
+        w.Q.L[k] = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+        if (!a || !b || !c || !d || !w.Q.L[k]) return S2_ERR_OOM;
+        w.P.q[k] = dk::PathQueue{a, b, c, d};
+    }
+    w.P.hits = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+    w.P.counters = (uint32_t*)dev_alloc(ctx, tmp, sizeof(uint32_t) * dk::C_COUNT);
+    w.P.stats = (unsigned long long*)dev_alloc(ctx, tmp, sizeof(unsigned long long) * dk::S_COUNT);
+    if (!w.P.hits || !w.P.counters || !w.P.stats) return S2_ERR_OOM;
+    int sms = 148, b = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dk::k_extend<false>, dk::kTravBlock, 0);
+    w.ext_blocks = std::max(1, b) * sms;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (A.flags & S2_FLAG_LAMBERTIAN) ? dk::k_diff_shade<true> : dk::k_diff_shade<false>,
+                                                  128, 0);
+    w.shade_blocks = std::max(1, b) * sms;
+    return S2_OK;
+}
+
+// Renders every path in waves (adj: the second replay, path_l holding each path's radiance).
+// Returns the kernel launches issued.
+uint64_t launch(const DiffArgs& A, DiffWave& w, bool adj, cudaStream_t s) {
+    const uint64_t total = (uint64_t)A.pixels * A.spp;
+    const uint32_t bounces = std::max(1u, A.max_len);
+    uint64_t launches = 0;
+    for (uint64_t base = 0; base < total; base += w.cap) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(w.cap, total - base);
+        cudaMemsetAsync(w.P.counters, 0, sizeof(uint32_t) * dk::C_COUNT, s);
+        dk::k_diff_gen<<<(n + 255) / 256, 256, 0, s>>>(A, w.P, w.Q, (uint32_t)base, n, adj ? 1 : 0);
+        launches += 1;
+        for (uint32_t b = 0; b < bounces; ++b) {
+            const uint32_t parity = b & 1u;
+            dk::k_diff_bounce<<<1, 32, 0, s>>>(A, w.P, parity);
+            dk::k_extend<false><<<w.ext_blocks, dk::kTravBlock, 0, s>>>(w.P, parity);
+            if (A.flags & S2_FLAG_LAMBERTIAN) dk::k_diff_shade<true><<<w.shade_blocks, 128, 0, s>>>(A, w.P, w.Q, parity, adj ? 1 : 0);
+            else dk::k_diff_shade<false><<<w.shade_blocks, 128, 0, s>>>(A, w.P, w.Q, parity, adj ? 1 : 0);
+            launches += 3;
+        }
+    }
+    if (!adj) {
+        dk::k_diff_resolve<<<(A.pixels + 255) / 256, 256, 0, s>>>(A);
+        launches += 1;
+    }
+    return launches;
 }
 
 int finish(S2Context* ctx, std::vector<DevBuf>& tmp, unsigned long long* rays_dev, float ms_unused, S2RenderStats* st,
@@ -111,14 +176,16 @@ extern "C" int s2_render_diff(S2Context* ctx, const S2View* view, const S2Render
     A.image = out_on_host ? (float4*)dev_alloc(ctx, tmp, sizeof(float4) * A.pixels) : (float4*)radiance;
     A.path_l = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)A.pixels * A.spp);
     if (!A.rays || !A.image || !A.path_l) { free_bufs(tmp); return S2_ERR_OOM; }
+    DiffWave w;
+    if (alloc_wave(ctx, tmp, A, w) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "differentiable render queues"); }
     cudaMemsetAsync(A.rays, 0, 2 * sizeof(unsigned long long), ctx->stream);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaEventRecord(ctx->ev0, ctx->stream);
-    launch<false>(A, ctx->stream);
+    const uint64_t launches = launch(A, w, false, ctx->stream);
     rc = check_cuda(ctx, cudaGetLastError(), "differentiable render launch");
     if (rc != S2_OK) { cudaStreamSynchronize(ctx->stream); free_bufs(tmp); return rc; }
     if (out_on_host) cudaMemcpyAsync(radiance, A.image, sizeof(float4) * A.pixels, cudaMemcpyDeviceToHost, ctx->stream);
-    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, 2);
+    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, launches);
 }
 
 extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2RenderParams* prm, const float* d_radiance,
@@ -141,14 +208,20 @@ extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2Ren
     A.grad = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * std::max<size_t>(1, off[ni]));
     A.grad_offset = (const uint32_t*)dev_alloc(ctx, tmp, sizeof(uint32_t) * (ni + 1));
     A.d_image = on_host ? (const float4*)dev_alloc(ctx, tmp, sizeof(float4) * A.pixels) : (const float4*)d_radiance;
-    if (!A.rays || !A.grad || !A.grad_offset || !A.d_image) { free_bufs(tmp); return S2_ERR_OOM; }
+    A.path_l = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)A.pixels * A.spp);
+    A.image = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * A.pixels);
+    if (!A.rays || !A.grad || !A.grad_offset || !A.d_image || !A.path_l || !A.image) { free_bufs(tmp); return S2_ERR_OOM; }
+    DiffWave w;
+    if (alloc_wave(ctx, tmp, A, w) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "adjoint render queues"); }
     cudaMemcpyAsync((void*)A.grad_offset, off.data(), sizeof(uint32_t) * (ni + 1), cudaMemcpyHostToDevice, ctx->stream);
     if (on_host) cudaMemcpyAsync((void*)A.d_image, d_radiance, sizeof(float4) * A.pixels, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemsetAsync(A.grad, 0, sizeof(float4) * std::max<size_t>(1, off[ni]), ctx->stream);
     cudaMemsetAsync(A.rays, 0, 2 * sizeof(unsigned long long), ctx->stream);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaEventRecord(ctx->ev0, ctx->stream);
-    launch<true>(A, ctx->stream);
+    // first replay: every path's radiance into path_l; second replay: the texel gradients
+    uint64_t launches = launch(A, w, false, ctx->stream);
+    launches += launch(A, w, true, ctx->stream);
     rc = check_cuda(ctx, cudaGetLastError(), "adjoint render launch");
     if (rc != S2_OK) { cudaStreamSynchronize(ctx->stream); free_bufs(tmp); return rc; }
     for (uint32_t k = 0; k < ni; ++k) {
@@ -157,5 +230,5 @@ extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2Ren
         cudaMemcpyAsync(d_images[k], A.grad + off[k], bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                         ctx->stream);
     }
-    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, 1);
+    return finish(ctx, tmp, A.rays, 0.f, stats_out, (uint64_t)A.pixels * A.spp, launches);
 }

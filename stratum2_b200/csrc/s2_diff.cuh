@@ -1,6 +1,7 @@
 // Differentiable rendering by adjoint path replay (no counterpart in the reference): the same
 // unidirectional path tracer with NEE + MIS as the wavefront renderer (same random-number stream,
-// path-length gates, MIS and Russian roulette), evaluated per path by one thread, with textured
+// path-length gates, MIS and Russian roulette), in wavefront form over the renderer's own queues
+// and closest-hit kernel (one thread per queued path in the shading step), with textured
 // material parameters kept in f32 (no 8-bit requantisation, so the image is differentiable in the
 // texels).  The adjoint replays every path from its seed twice (Vicini et al. 2021, path replay
 // backpropagation): the first replay gives the path's radiance L, the second walks the path again
@@ -186,139 +187,132 @@ S2D void material_grads(const DiffArgs& A, const MatF& m, float3 in, float3 out,
     }
 }
 
-// One path of pixel (px, py), sample `sample`.  adj = false: returns the path's radiance.
-// adj = true: replays the same path and adds the texel gradients for the image adjoint `delta`,
-// with `ltot` the radiance the first replay returned.  Not inlined, so both replays run the same
-// machine code and take the same decisions.
+// The work at one path vertex, after the closest-hit query of the ray (org, dir): increments len,
+// adds the vertex's emission and NEE to L, and samples the continuation (org, dir, thr, dir_pdf
+// updated; returns false when the path ends).  adj = true (the second replay): adds the texel
+// gradients for the image adjoint `delta`, with `ltot` the path's radiance from the first replay.
+// Not inlined, and the adjoint is a run-time argument, so both replays run the same machine code
+// and take the same decisions.
 template <bool LAMBERT>
-__device__ __noinline__ float3 diff_path(const DiffArgs& A, uint32_t px, uint32_t py, uint32_t sample, bool adj, float3 ltot,
-                                         float3 delta, uint2* smem_stack, uint32_t lane_stride, uint32_t& ext_rays,
-                                         uint32_t& shadow_rays, bool& overflow) {
+__device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, uint32_t& len, float3& org, float3& dir,
+                                         float3& thr, float3& L, float& dir_pdf, Rng& rng, bool adj, float3 ltot, float3 delta,
+                                         uint2* smem_stack, uint32_t lane_stride, uint32_t& shadow_rays, bool& overflow) {
     const DevScene& s = A.scene;
     const bool nee = !(A.flags & S2F_NO_NEE), sn = !(A.flags & S2F_NO_SN);
     const SceneAlphaTest alpha{&s, !(A.flags & S2F_NO_ALPHA)};
-    Rng rng = make_rng(px, py, A.frame_seed + sample, (A.flags & S2F_PCG32) != 0);
-    float ox = 0.5f, oy = 0.5f;
-    if (A.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
-    float3 dir = camera_dir(A.proj, A.imin, A.imax, A.cam, px, py, ox, oy);
-    float3 org = f3(A.cam[3], A.cam[7], A.cam[11]);
-    float3 thr = f3(1.f);
-    float3 L = f3(0.f);
-    float dir_pdf = 0.f;
-    uint32_t len = 0;
     TravCounters ctr{0, 0};
-    while (true) {
-        TravHit h;
-        ext_rays++;
-        if (!traverse<false, false>(make_trav_ray(org, dir, 0.f), S2_INF, s.nodes, s.tris, smem_stack, lane_stride, h, ctr, alpha))
-            overflow = true;
-        len++;
-        if (h.tri == 0xffffffffu) {
-            // environment (TraceRay, testrenderer.slang:1036-1054)
-            float env_pdf = 0.f;
-            const float3 le = eval_env(s, dir, env_pdf);
-            const float3 e = len >= A.min_len ? thr * le : f3(0.f);
-            if (any_pos(e)) {
-                float w = 1.f;
-                if (len > 1 && nee && dir_pdf > 0.f) {
-                    const float lp = (A.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;
-                    w = mis_w(dir_pdf, lp);
-                }
-                if (w > 0.f) {
-                    L = L + e * w;
-                    if (adj) env_grad(A, dir, delta * thr * w);
-                }
+    len++;
+    if (h.tri == 0xffffffffu) {
+        // environment (TraceRay, testrenderer.slang:1036-1054)
+        float env_pdf = 0.f;
+        const float3 le = eval_env(s, dir, env_pdf);
+        const float3 e = len >= A.min_len ? thr * le : f3(0.f);
+        if (any_pos(e)) {
+            float w = 1.f;
+            if (len > 1 && nee && dir_pdf > 0.f) {
+                const float lp = (A.flags & S2F_REF_ENV_MIS) ? (S2_INV_PI / pow2(s.scene_sphere.w)) : env_pdf;
+                w = mis_w(dir_pdf, lp);
             }
-            break;
-        }
-        SD sd = make_shading(s, h.instance, h.primitive, h.b1, h.b2, sn);
-        if (!(A.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
-        const float isect_dist = half_round(h.t);
-        const float isect_pdfa = half_round(light_pdfa(s, h.instance, sd.area));
-        Taps tb, tr;
-        float3 base_rec;
-        float rough_rec;
-        const MatF m = load_material_f(s, sd.mat, sd.uv, tb, tr, base_rec, rough_rec);
-        const float3 in = sd.to_local(-dir);
-        const float cos_in = fabsf(in.z);
-        if (in.z > 0.f) {
-            const float3 e = thr * m.emission();
-            if (any_pos(e) && len >= A.min_len) {
-                float w = 1.f;
-                if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
-                if (w > 0.f) L = L + e * w;
+            if (w > 0.f) {
+                L = L + e * w;
+                if (adj) env_grad(A, dir, delta * thr * w);
             }
         }
-        if (!(len < A.max_len && any_pos(m.base()))) break;
-        const bool sing = mat_singular<LAMBERT>(m);
-        const float cp = (A.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
-        // NEE (ConnectToLight, testrenderer.slang:751-779), same stream use as the wavefront shade
-        if (!sing && nee) {
-            if (len + 1 < A.min_len) {
-                rng.skip();
-            } else {
-                const float4 x = rng.next_float();
-                const Illum r = sample_illum(s, x, sd.pos, sn);
-                if (!(all_nonpos(r.radiance) || r.pdf <= 0.f)) {
-                    const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
-                    const float dpw = r.pdf * AtoW;
-                    const float3 out = sd.to_local(r.dir);
-                    float3 f; float fwd, rev;
-                    bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
-                    f = f * sd.snc(in, out);
-                    fwd *= cp;
-                    const float3 contrib = thr * r.radiance * f / dpw;
-                    const float w = mis_w(r.pdf, fwd / AtoW);
-                    if (w > 0.f && !all_nonpos(contrib)) {
-                        TravHit sh;
-                        shadow_rays++;
-                        if (!traverse<true, false>(make_trav_ray(ray_offset(sd.pos, sd.gn, r.dir), r.dir, 0.f),
-                                                   adjust_distance(r.dist), s.nodes, s.tris, smem_stack, lane_stride, sh, ctr, alpha))
-                            overflow = true;
-                        if (sh.tri == 0xffffffffu) {
-                            L = L + f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
-                            if (adj) {
-                                const float k = w / dpw;
-                                material_grads<LAMBERT>(A, m, in, out, delta * thr * r.radiance * k, tb, tr, base_rec, rough_rec);
-                                if (!r.finite) env_grad(A, r.dir, delta * thr * f * k);
-                            }
+        return false;
+    }
+    SD sd = make_shading(s, h.instance, h.primitive, h.b1, h.b2, sn);
+    if (!(A.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(s, sd);
+    const float isect_dist = half_round(h.t);
+    const float isect_pdfa = half_round(light_pdfa(s, h.instance, sd.area));
+    Taps tb, tr;
+    float3 base_rec;
+    float rough_rec;
+    const MatF m = load_material_f(s, sd.mat, sd.uv, tb, tr, base_rec, rough_rec);
+    const float3 in = sd.to_local(-dir);
+    const float cos_in = fabsf(in.z);
+    if (in.z > 0.f) {
+        const float3 e = thr * m.emission();
+        if (any_pos(e) && len >= A.min_len) {
+            float w = 1.f;
+            if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
+            if (w > 0.f) L = L + e * w;
+        }
+    }
+    if (!(len < A.max_len && any_pos(m.base()))) return false;
+    const bool sing = mat_singular<LAMBERT>(m);
+    const float cp = (A.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
+    // NEE (ConnectToLight, testrenderer.slang:751-779), same stream use as the wavefront shade;
+    // the shadow ray is traced here (first hit), so the vertex's gradient terms can follow it
+    if (!sing && nee) {
+        if (len + 1 < A.min_len) {
+            rng.skip();
+        } else {
+            const float4 x = rng.next_float();
+            const Illum r = sample_illum(s, x, sd.pos, sn);
+            if (!(all_nonpos(r.radiance) || r.pdf <= 0.f)) {
+                const float AtoW = r.finite ? pow2(r.dist) / r.cos_light : 1.f;
+                const float dpw = r.pdf * AtoW;
+                const float3 out = sd.to_local(r.dir);
+                float3 f; float fwd, rev;
+                bsdf_eval<LAMBERT>(m, in, out, f, fwd, rev);
+                f = f * sd.snc(in, out);
+                fwd *= cp;
+                const float3 contrib = thr * r.radiance * f / dpw;
+                const float w = mis_w(r.pdf, fwd / AtoW);
+                if (w > 0.f && !all_nonpos(contrib)) {
+                    TravHit sh;
+                    shadow_rays++;
+                    if (!traverse<true, false>(make_trav_ray(ray_offset(sd.pos, sd.gn, r.dir), r.dir, 0.f),
+                                               adjust_distance(r.dist), s.nodes, s.tris, smem_stack, lane_stride, sh, ctr, alpha))
+                        overflow = true;
+                    if (sh.tri == 0xffffffffu) {
+                        L = L + f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
+                        if (adj) {
+                            const float k = w / dpw;
+                            material_grads<LAMBERT>(A, m, in, out, delta * thr * r.radiance * k, tb, tr, base_rec, rough_rec);
+                            if (!r.finite) env_grad(A, r.dir, delta * thr * f * k);
                         }
                     }
                 }
             }
         }
-        if (!(A.flags & S2F_NO_RR)) {
-            const float4 u = rng.next_float();
-            if (u.x > fminf(1.f, cp)) break;
-        }
-        const float4 rnd = rng.next_float();
-        float3 sdir, refl;
-        float fwd, rev, rough;
-        bsdf_sample<LAMBERT>(m, in, rnd, sdir, refl, fwd, rev, rough);
-        if (adj) {
-            // every later contribution carries refl / fwd: d/dtheta = (L - L_so_far) * d refl / refl
-            const float3 after = ltot - L;
-            const float3 y = f3(refl.x > 0.f ? delta.x * after.x / refl.x : 0.f, refl.y > 0.f ? delta.y * after.y / refl.y : 0.f,
-                                refl.z > 0.f ? delta.z * after.z / refl.z : 0.f);
-            if (any_pos(f3(fabsf(y.x), fabsf(y.y), fabsf(y.z)))) material_grads<LAMBERT>(A, m, in, sdir, y, tb, tr, base_rec, rough_rec);
-        }
-        const float cpm = (A.flags & S2F_NO_RR) ? 1.f : cp;
-        fwd *= cpm;
-        thr = thr * refl / fwd;
-        dir_pdf = (rough == 0.f || sing) ? 0.f : half_round(fwd);
-        thr = thr * sd.snc(in, sdir);
-        const float3 wd = sd.to_world(sdir);
-        org = ray_offset(sd.pos, sd.gn, wd);
-        dir = unpack_normal(pack_normal(wd));
-        if (any_nan(thr) || !any_pos(thr)) break;
     }
-    return L;
+    if (!(A.flags & S2F_NO_RR)) {
+        const float4 u = rng.next_float();
+        if (u.x > fminf(1.f, cp)) return false;
+    }
+    const float4 rnd = rng.next_float();
+    float3 sdir, refl;
+    float fwd, rev, rough;
+    bsdf_sample<LAMBERT>(m, in, rnd, sdir, refl, fwd, rev, rough);
+    if (adj) {
+        // every later contribution carries refl / fwd: d/dtheta = (L - L_so_far) * d refl / refl
+        const float3 after = ltot - L;
+        const float3 y = f3(refl.x > 0.f ? delta.x * after.x / refl.x : 0.f, refl.y > 0.f ? delta.y * after.y / refl.y : 0.f,
+                            refl.z > 0.f ? delta.z * after.z / refl.z : 0.f);
+        if (any_pos(f3(fabsf(y.x), fabsf(y.y), fabsf(y.z)))) material_grads<LAMBERT>(A, m, in, sdir, y, tb, tr, base_rec, rough_rec);
+    }
+    const float cpm = (A.flags & S2F_NO_RR) ? 1.f : cp;
+    fwd *= cpm;
+    thr = thr * refl / fwd;
+    dir_pdf = (rough == 0.f || sing) ? 0.f : half_round(fwd);
+    thr = thr * sd.snc(in, sdir);
+    const float3 wd = sd.to_world(sdir);
+    org = ray_offset(sd.pos, sd.gn, wd);
+    dir = unpack_normal(pack_normal(wd));
+    return !(any_nan(thr) || !any_pos(thr));
 }
 
-// One thread per path (sample-major: a warp takes 32 neighbouring pixels of one sample, so its
-// lanes start in phase).  Forward (ADJ = false): path_l[path] = the path's radiance, summed per
-// pixel by k_diff_resolve.  Adjoint: the thread replays its path twice, the second time adding the
-// texel gradients of sum(d_image * image).
+// Wavefront form: the paths' state lives in the wavefront renderer's queues (s0: origin, dir pdf;
+// s1: direction, throughput x; s2: throughput yz, path id, path length; s3: random state) plus one
+// stream of the radiance gathered so far; every bounce is the renderer's own closest-hit kernel
+// (k_extend) and k_diff_shade, which runs diff_vertex for each queued path and appends the
+// survivors to the other queue.  Path p (sample-major: p = sample x pixels + pixel) writes its
+// radiance to path_l[p] when it ends; the adjoint's second replay reads it there as `ltot`.
+struct DiffQueues {
+    float4* L[2];       // radiance gathered so far, by queue parity
+};
+
 S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow) {
     // warp sums of the ray counts, one 64-bit atomic pair per warp
     for (int o = 16; o > 0; o >>= 1) { ext += __shfl_xor_sync(0xffffffffu, ext, o); shd += __shfl_xor_sync(0xffffffffu, shd, o); }
@@ -326,27 +320,105 @@ S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow
     if (overflow) atomicOr(A.status, 1);
 }
 
-template <bool LAMBERT, bool ADJ>
-__global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs A) {
-    __shared__ uint2 stack[S2_STACK_SMEM * 128];
-    const uint32_t path = blockIdx.x * 128u + threadIdx.x;
-    const uint32_t n = A.pixels * A.spp;
-    uint32_t ext = 0, shd = 0;
-    bool overflow = false;
-    if (path < n) {
-        const uint32_t k = path / A.pixels, pix = path - k * A.pixels;
-        const uint32_t px = pix % A.width, py = pix / A.width;
-        const float3 l = diff_path<LAMBERT>(A, px, py, k, false, f3(0.f), f3(0.f), stack + threadIdx.x, 128u, ext, shd, overflow);
-        if (ADJ) {
+// Camera paths base .. base + n - 1 into queue 0 (the adjoint skips paths of pixels whose adjoint
+// is zero, as its replay adds nothing).
+__global__ void k_diff_gen(const __grid_constant__ DiffArgs A, PTParams P, DiffQueues Q, uint32_t base, uint32_t n, int adj) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    uint32_t path = 0, px = 0, py = 0, k = 0;
+    if (i < n) {
+        path = base + i;
+        k = path / A.pixels;
+        const uint32_t pix = path - k * A.pixels;
+        px = pix % A.width; py = pix / A.width;
+        want = true;
+        if (adj) {
             const float4 d = A.d_image[pix];
-            const float3 delta = f3(d.x, d.y, d.z) * A.out_scale;
-            if (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f)
-                diff_path<LAMBERT>(A, px, py, k, true, l, delta, stack + threadIdx.x, 128u, ext, shd, overflow);
-        } else {
-            A.path_l[path] = make_float4(l.x, l.y, l.z, 0.f);
+            want = d.x != 0.f || d.y != 0.f || d.z != 0.f;
         }
     }
-    diff_count(A, ext, shd, overflow);
+    const uint32_t q = warp_append(&P.counters[C_QUEUE0], want);
+    if (!want) return;
+    Rng rng = make_rng(px, py, A.frame_seed + k, (A.flags & S2F_PCG32) != 0);
+    float ox = 0.5f, oy = 0.5f;
+    if (A.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
+    const float3 dir = camera_dir(A.proj, A.imin, A.imax, A.cam, px, py, ox, oy);
+    const PathQueue& Qo = P.q[0];
+    Qo.s0[q] = make_float4(A.cam[3], A.cam[7], A.cam[11], 0.f);
+    Qo.s1[q] = make_float4(dir.x, dir.y, dir.z, 1.f);
+    Qo.s2[q] = make_float4(1.f, 1.f, __uint_as_float(path), __uint_as_float(0u));
+    Qo.s3[q] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+    Q.L[0][q] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Counters before a bounce: the queue about to be traced counts as extension rays; the other
+// queue and the traversal work counter restart.
+__global__ void k_diff_bounce(const __grid_constant__ DiffArgs A, PTParams P, uint32_t parity) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    atomicAdd(A.rays, (unsigned long long)P.counters[parity]);
+    P.counters[1 - parity] = 0;
+    P.counters[C_WORK_EXT] = 0;
+}
+
+template <bool LAMBERT>
+__global__ void __launch_bounds__(128) k_diff_shade(const __grid_constant__ DiffArgs A, const __grid_constant__ PTParams P,
+                                                    DiffQueues Q, uint32_t parity, int adj) {
+    __shared__ uint2 stack[S2_STACK_SMEM * 128];
+    const uint32_t count = P.counters[parity];
+    const PathQueue qi = P.q[parity], qo = P.q[1 - parity];
+    const uint32_t rounded = (count + 31u) & ~31u;
+    uint32_t shd = 0;
+    bool overflow = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
+        bool alive = false;
+        float4 n0, n1, n2, nl;
+        uint4 n3;
+        if (i < count) {
+            const float4 a = qi.s0[i], b = qi.s1[i], c = qi.s2[i], l4 = Q.L[parity][i];
+            const uint4 rs = qi.s3[i];
+            const float4 hv = P.hits[i];
+            float3 org = f3(a.x, a.y, a.z), dir = f3(b.x, b.y, b.z), thr = f3(b.w, c.x, c.y), L = f3(l4.x, l4.y, l4.z);
+            float dir_pdf = a.w;
+            const uint32_t path = __float_as_uint(c.z);
+            uint32_t len = __float_as_uint(c.w);
+            Rng rng;
+            rng.px = rs.x; rng.py = rs.y; rng.seed = rs.z; rng.ctr = rs.w; rng.pcg32 = (A.flags & S2F_PCG32) != 0;
+            TravHit h;
+            h.t = hv.x;
+            h.tri = __float_as_uint(hv.y);
+            h.b1 = hv.z; h.b2 = hv.w;
+            h.instance = h.primitive = 0xffffffffu;
+            if (h.tri != 0xffffffffu) {
+                const float4 t0 = P.scene.tris[3 * (size_t)h.tri], t1 = P.scene.tris[3 * (size_t)h.tri + 1];
+                h.instance = __float_as_uint(t0.w);
+                h.primitive = __float_as_uint(t1.w);
+            }
+            float3 ltot = f3(0.f), delta = f3(0.f);
+            if (adj) {
+                const uint32_t pix = path % A.pixels;
+                const float4 lt = A.path_l[path], d = A.d_image[pix];
+                ltot = f3(lt.x, lt.y, lt.z);
+                delta = f3(d.x, d.y, d.z) * A.out_scale;
+            }
+            alive = diff_vertex<LAMBERT>(A, h, len, org, dir, thr, L, dir_pdf, rng, adj != 0, ltot, delta,
+                                         stack + threadIdx.x, 128u, shd, overflow);
+            if (alive) {
+                n0 = make_float4(org.x, org.y, org.z, dir_pdf);
+                n1 = make_float4(dir.x, dir.y, dir.z, thr.x);
+                n2 = make_float4(thr.y, thr.z, __uint_as_float(path), __uint_as_float(len));
+                n3 = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
+                nl = make_float4(L.x, L.y, L.z, 0.f);
+            } else if (!adj) {
+                A.path_l[path] = make_float4(L.x, L.y, L.z, 0.f);
+            }
+        }
+        const uint32_t o = warp_append(&P.counters[1 - parity], alive);
+        if (alive) {
+            qo.s0[o] = n0; qo.s1[o] = n1; qo.s2[o] = n2; qo.s3[o] = n3;
+            Q.L[1 - parity][o] = nl;
+        }
+    }
+    diff_count(A, 0u, shd, overflow);
 }
 
 // image[pixel] = sum of the pixel's path radiances in sample order * 2^exposure / spp.
