@@ -627,6 +627,8 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
         rays += st.extension_rays + st.shadow_rays
     last_restir = rad[..., :3].double().cpu().numpy()
     restir_ms = ms / frames
+    ris_1 = dev.render_device(views[-1], prm(4000, _abi.FLAG_RESTIR_DI), aov).gpu_ms  # RIS alone, no reuse
+    relmse_ris_1 = rad[..., :3].double().cpu().numpy()
     nee_1 = min(dev.render_device(views[-1], prm(5000 + k, 0), aov).gpu_ms for k in range(3))
     relmse_nee_1 = rad[..., :3].double().cpu().numpy()
     spp_eq = max(1, int(round(restir_ms / nee_1)))
@@ -636,6 +638,7 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
     dev.render_device(views[-1], prm(7000, 0, ref_spp), aov)
     ref = rad[..., :3].double().cpu().numpy()
     relmse_nee_1 = metrics.relmse(relmse_nee_1, ref)
+    relmse_ris_1 = metrics.relmse(relmse_ris_1, ref)
     return {"workload": "cfg2 terrain + 100k emissive triangles (power lognormal(0,2)), 32-frame Catmull-Rom camera "
                         "loop, 1920x1080, 1 spp per frame, direct illumination at the primary vertex",
             "restir": "32 RIS candidates, screen-space reuse: 1 temporal + 5 spatial neighbours within 30 px, M-cap 20",
@@ -645,6 +648,7 @@ def restir_line(dev, frames: int = 32, ref_spp: int = 1024) -> dict:
             "relmse_restir_last_frame": metrics.relmse(last_restir, ref),
             "relmse_nee_equal_time": metrics.relmse(last_nee, ref),
             "relmse_nee_1spp": relmse_nee_1,
+            "ris_1spp_ms": ris_1, "relmse_ris_1spp_no_reuse": relmse_ris_1,
             "reference": f"plain NEE, {ref_spp} spp, last view (GPU, power-proportional pick)"}
 
 
@@ -677,6 +681,8 @@ def main():
                          "and exit (profiling)")
     ap.add_argument("--vcm-only", action="store_true",
                     help="run only the VCM renderer measurement on the many-lights frame and print it")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the differentiable forward and adjoint measurement and print it")
     ap.add_argument("--restir-only", action="store_true",
                     help="run only the many-lights ReSTIR DI versus equal-time NEE comparison and print it")
     args = ap.parse_args()
@@ -708,6 +714,10 @@ def main():
     if args.quality_only:
         from stratum2_b200 import Device
         print(json.dumps(quality_line(Device(0), args)))
+        return
+    if args.adjoint_only:
+        from stratum2_b200 import Device
+        print(json.dumps(adjoint_line(Device(0))))
         return
     if args.restir_only:
         from stratum2_b200 import Device
