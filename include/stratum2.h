@@ -406,6 +406,23 @@ int  s2_autotune(S2Context* ctx, const S2View* view, const S2RenderParams* param
  * The alpha-test flags baked into the BVH at s2_build_bvh are not recomputed. */
 int  s2_update_image(S2Context* ctx, uint32_t index, const float* texels, int on_device);
 
+/* Texture repack of a glTF metallic-roughness material on the device: the reference's from_gltf_pbr
+ * pass (src/Shaders/kernels/convert_material.slang:33-69, dispatched by makeMetallicRoughnessMaterial,
+ * src/App/Scene.cpp:195-208, for the textures load_gltf.cpp:92-128 passes it).  Sources are RGBA8
+ * texels of one width x height (NULL = absent, read as 1): the base colour (sRGB rgb, linear alpha),
+ * the metallic-roughness texture (linear; metallic b, roughness g) and the emission (sRGB rgb); at
+ * least one is required.  Per texel the PackedMaterialData of those values is written as the four
+ * packed words' images, float4 each (byte / 255): packed[0] base colour + specular 1, packed[1]
+ * emission / its largest channel + sheen 1, packed[2] metallic, roughness, anisotropic 1,
+ * subsurface 1, packed[3] clearcoat, clearcoat gloss, transmission and eta all 1.  alpha_mask (may
+ * be NULL; needs the base colour) receives the base colour's alpha as one float per texel, and
+ * *min_alpha the smallest 8-bit alpha below 255 (255 when every texel is opaque or there is no base
+ * colour).  on_device: all pointers but min_alpha are device pointers (sources 4-byte, packed
+ * images 16-byte aligned); else host pointers. */
+int  s2_repack_metallic_roughness(S2Context* ctx, uint32_t width, uint32_t height, const uint8_t* base_rgba8,
+                                  const uint8_t* metallic_roughness_rgba8, const uint8_t* emission_rgba8,
+                                  float* const* packed, float* alpha_mask, uint32_t* min_alpha, int on_device);
+
 /* ---------------------------------------------------------------- differentiable rendering
  * No counterpart in the reference.  The same path tracer as s2_render (NEE + MIS, Russian
  * roulette, path-length gates, the same random numbers per pixel and sample) with textured material

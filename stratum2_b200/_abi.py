@@ -64,6 +64,7 @@ EXPORTED_SYMBOLS = [
     "s2_set_tuning", "s2_get_tuning", "s2_autotune",
     "s2_default_temporal_params", "s2_temporal_accumulate", "s2_tonemap", "s2_default_svgf_params", "s2_svgf_filter",
     "s2_default_vcm_params", "s2_render_vcm", "s2_device_math", "s2_inject_wait_timeout",
+    "s2_repack_metallic_roughness",
 ]
 
 CACHE_WEIGHTS = 6336
@@ -245,6 +246,8 @@ def lib() -> C.CDLL:
     L.s2_default_render_params.argtypes = [P(S2RenderParams)]
     L.s2_default_render_params.restype = None
     L.s2_update_image.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+    L.s2_repack_metallic_roughness.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_int]
     L.s2_set_tuning.argtypes = [C.c_void_p, P(S2Tuning)]
     L.s2_default_temporal_params.restype = None
     L.s2_default_temporal_params.argtypes = [P(S2TemporalParams)]

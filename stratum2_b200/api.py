@@ -290,6 +290,27 @@ class Device:
         a = np.ascontiguousarray(texels, np.float32)
         self._check(self._lib.s2_update_image(self._h, index, a.ctypes.data, 0))
 
+    def repack_metallic_roughness(self, base=None, metallic_roughness=None, emission=None):
+        """Texture repack of a glTF metallic-roughness material on the GPU
+        (s2_repack_metallic_roughness): uint8 RGBA8 sources of one (h, w) extent, None for an absent
+        one -> (the four packed images as float32 (h, w, 4), the base colour's alpha as float32 (h, w)
+        or None without a base colour, the smallest 8-bit alpha below 255)."""
+        src = [None if t is None else np.ascontiguousarray(t, np.uint8) for t in (base, metallic_roughness, emission)]
+        shapes = {t.shape for t in src if t is not None}
+        if not shapes:
+            raise ValueError("at least one source texture is required")
+        if len(shapes) != 1 or len(next(iter(shapes))) != 3 or next(iter(shapes))[2] != 4:
+            raise ValueError(f"sources must be RGBA8 arrays of one extent, got {sorted(shapes)}")
+        h, w, _ = next(iter(shapes))
+        imgs = [np.empty((h, w, 4), np.float32) for _ in range(4)]
+        alpha = np.empty((h, w), np.float32) if base is not None else None
+        ptrs = (C.c_void_p * 4)(*[im.ctypes.data for im in imgs])
+        min_alpha = C.c_uint32(0)
+        self._check(self._lib.s2_repack_metallic_roughness(
+            self._h, w, h, *[None if t is None else t.ctypes.data for t in src], ptrs,
+            None if alpha is None else alpha.ctypes.data, C.byref(min_alpha), 0))
+        return imgs, alpha, int(min_alpha.value)
+
     def render_diff(self, view, width: int, height: int, params: _abi.S2RenderParams):
         """Image of the differentiable renderer (f32 materials): (H, W, 4) float32 and statistics."""
         out = np.zeros((height, width, 4), np.float32)

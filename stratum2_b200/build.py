@@ -19,7 +19,7 @@ LIB = PKG / "libstratum2_b200.so"
 BUILD = PKG / "_build"
 
 CUDA_SOURCES = ["s2_api.cu", "s2_render.cu", "s2_noalloc.cu", "s2_cache.cu", "s2_diff.cu", "s2_post.cu", "s2_vcm.cu",
-                "s2_math_check.cu"]
+                "s2_math_check.cu", "s2_repack.cu"]
 CXX_SOURCES = ["s2_bvh_build.cpp"]
 
 NVCC_FLAGS = [

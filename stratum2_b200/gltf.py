@@ -9,10 +9,12 @@ reference's loader does it (src/App/loaders/load_gltf.cpp:12-315):
   pbrMetallicRoughness factors, emissiveFactor x KHR_materials_emissive_strength,
   KHR_materials_ior (default 1.5), KHR_materials_transmission, then KHR_materials_clearcoat and
   KHR_materials_specular (load_gltf.cpp:92-128); the normal texture is the bump image (strength 1);
-* textures: PNG (the decoder below; JPEG is not supported and raises), base colour and emission
-  decoded as sRGB, the others linear; repacked per texel into the four packed-material images as
-  the reference's from_gltf_pbr pass does (convert_material.slang:33-69), with the base colour's
-  alpha as the alpha mask;
+* textures: PNG (the decoder below, 8-bit) and JPEG (Pillow's decoder: the reference decodes with
+  stb_image through tinygltf, whose JPEG IDCT and chroma upsampling may differ from libjpeg's by one
+  8-bit step), expanded to RGBA8; repacked per texel into the four packed-material images on the
+  GPU (Device.repack_metallic_roughness, the reference's from_gltf_pbr pass,
+  convert_material.slang:33-69), which decodes the base colour and emission as sRGB, with the base
+  colour's alpha as the alpha mask;
 * cameras: perspective cameras become views (make_view) at their node's position and rotation.
 """
 from __future__ import annotations
@@ -34,11 +36,15 @@ _NCOMP = {"SCALAR": 1, "VEC2": 2, "VEC3": 3, "VEC4": 4, "MAT4": 16}
 
 
 # ------------------------------------------------------------------------------ PNG
-def decode_png(data: bytes) -> np.ndarray:
-    """8-bit PNG (grey, RGB, palette, grey + alpha, RGBA; no interlace) -> float32 (h, w, 4) in
-    [0, 1], alpha 1 where the image has none."""
-    if data[:8] != b"\x89PNG\r\n\x1a\n":
-        raise ValueError("not a PNG image (JPEG textures are not supported)")
+PNG_MAGIC = b"\x89PNG\r\n\x1a\n"
+JPEG_MAGIC = b"\xff\xd8\xff"
+
+
+def decode_png_rgba8(data: bytes) -> np.ndarray:
+    """8-bit PNG (grey, RGB, palette, grey + alpha, RGBA; no interlace) -> uint8 (h, w, 4), grey
+    broadcast to RGB, alpha 255 where the image has none."""
+    if data[:8] != PNG_MAGIC:
+        raise ValueError("not a PNG image")
     pos, idat, plte, trns = 8, b"", None, None
     w = h = depth = ctype = interlace = None
     while pos < len(data):
@@ -100,42 +106,32 @@ def decode_png(data: bytes) -> np.ndarray:
         rgba[..., 3] = px[..., 1]
     else:
         rgba[..., :ch] = px
-    return rgba.astype(np.float32) / 255.0
+    return rgba
 
 
-def srgb_to_linear(c):
-    """srgbToRgb (compat/common.h:81-86): the sRGB decode a Vulkan sRGB texture applies."""
-    c = np.asarray(c, np.float64)
-    return np.where(c <= 0.04045, c / 12.92, ((c + 0.055) / 1.055) ** 2.4)
+def decode_png(data: bytes) -> np.ndarray:
+    """decode_png_rgba8 as float32 in [0, 1]."""
+    return decode_png_rgba8(data).astype(np.float32) / np.float32(255.0)
 
 
-# ------------------------------------------------------------------------------ texture repack
-def repack_metallic_roughness(base=None, mr=None, emission=None):
-    """from_gltf_pbr (convert_material.slang:33-69): per-texel PackedMaterialData of the textures
-    (base colour rgba linear, metallic-roughness rgba, emission rgb linear; any may be None, all
-    present ones share the first one's size), stored as the four packed words' RGBA8 images.
-    Returns (images[4] as float32 (h, w, 4), alpha (h, w) or None, min alpha 0..255)."""
-    ref = next(t for t in (base, mr, emission) if t is not None)
-    h, w = ref.shape[:2]
-    one = np.ones((h, w, 4), np.float32)
-    d = base if base is not None else one
-    m = mr if mr is not None else one
-    e = emission[..., :3] if emission is not None else one[..., :3]
-    q = lambda v: np.floor(np.clip(v, 0, 1) * 255 + 0.5).astype(np.uint8)  # PackedMaterialData's UNORM8
-    img0 = np.stack([q(d[..., 0]), q(d[..., 1]), q(d[..., 2]), q(np.ones((h, w)))], -1)           # base, specular 1
-    emax = e.max(-1, keepdims=True)
-    en = np.where(emax > 0, e / np.where(emax > 0, emax, 1), 0)                                       # setEmission: colour / max
-    img1 = np.concatenate([q(en), q(np.ones((h, w, 1)))], -1)                                         # emission, sheen 1
-    img2 = np.stack([q(m[..., 2]), q(m[..., 1]), q(np.ones((h, w))), q(np.ones((h, w)))], -1)      # metallic, roughness
-    img3 = np.stack([q(np.ones((h, w)))] * 4, -1)                                                   # clearcoat.. eta: 1
-    alpha, min_alpha = None, 255
-    if base is not None:
-        alpha = base[..., 3].astype(np.float32)
-        below = alpha < 1
-        if below.any():
-            min_alpha = int(np.floor(np.clip(alpha[below], 0, 1) * 255 + 0.5).min())
-    imgs = [im.astype(np.float32) / 255.0 for im in (img0, img1, img2, img3)]
-    return imgs, alpha, min_alpha
+def decode_jpeg_rgba8(data: bytes) -> np.ndarray:
+    """Baseline or progressive JPEG (grey, YCbCr, CMYK) -> uint8 (h, w, 4), alpha 255."""
+    import io
+
+    from PIL import Image
+    with Image.open(io.BytesIO(data)) as im:
+        if im.format != "JPEG":
+            raise ValueError("not a JPEG image")
+        return np.asarray(im.convert("RGBA"), np.uint8).copy()
+
+
+def decode_image_rgba8(data: bytes) -> np.ndarray:
+    """A glTF image (PNG or JPEG, by its signature) -> uint8 (h, w, 4)."""
+    if data[:8] == PNG_MAGIC:
+        return decode_png_rgba8(data)
+    if data[:3] == JPEG_MAGIC:
+        return decode_jpeg_rgba8(data)
+    raise ValueError("unsupported image format (PNG and JPEG are supported)")
 
 
 # ------------------------------------------------------------------------------ loader
@@ -157,8 +153,13 @@ def _trs_matrix(node) -> np.ndarray:
     return m
 
 
-def load_gltf(path, width: int = 640, height: int = 480) -> GltfScene:
+def load_gltf(path, width: int = 640, height: int = 480, device=None, repack=None) -> GltfScene:
+    """Loads a .gltf or .glb file.  Textured materials are repacked on the GPU through `device`
+    (a Device); `repack` replaces that call (same signature and result as
+    Device.repack_metallic_roughness).  A textured material with neither raises ValueError."""
     path = Path(path)
+    if repack is None and device is not None:
+        repack = device.repack_metallic_roughness
     raw = path.read_bytes()
     bin_chunk = None
     if raw[:4] == b"glTF":
@@ -209,11 +210,12 @@ def load_gltf(path, width: int = 640, height: int = 480) -> GltfScene:
 
     image_cache = {}
 
-    def texture(tex_info, srgb):
+    def texture(tex_info):
+        """The texture's image as decoded RGBA8 (the sRGB decode is the repack's)."""
         if tex_info is None:
             return None
         t = doc["textures"][tex_info["index"]]
-        key = (t["source"], srgb)
+        key = t["source"]
         if key not in image_cache:
             im = doc["images"][t["source"]]
             if "bufferView" in im:
@@ -222,10 +224,7 @@ def load_gltf(path, width: int = 640, height: int = 480) -> GltfScene:
                 data = base64.b64decode(im["uri"].split(",", 1)[1])
             else:
                 data = (path.parent / im["uri"]).read_bytes()
-            px = decode_png(bytes(data))
-            if srgb:
-                px = np.concatenate([srgb_to_linear(px[..., :3]).astype(np.float32), px[..., 3:]], -1)
-            image_cache[key] = px
+            image_cache[key] = decode_image_rgba8(bytes(data))
         return image_cache[key]
 
     s = Scene()
@@ -250,11 +249,16 @@ def load_gltf(path, width: int = 640, height: int = 480) -> GltfScene:
                 m.specular = 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]
             elif "specularFactor" in sp:
                 m.specular = sp["specularFactor"]
-        base_t = texture(pbr.get("baseColorTexture"), True)
-        mr_t = texture(pbr.get("metallicRoughnessTexture"), False)
-        em_t = texture(gm.get("emissiveTexture"), True)
-        if base_t is not None or mr_t is not None or em_t is not None:
-            imgs, alpha, min_alpha = repack_metallic_roughness(base_t, mr_t, em_t)
+        base_t = texture(pbr.get("baseColorTexture"))
+        mr_t = texture(pbr.get("metallicRoughnessTexture"))
+        em_t = texture(gm.get("emissiveTexture"))
+        present = [t for t in (base_t, mr_t, em_t) if t is not None]
+        if present:
+            if repack is None:
+                raise ValueError("textured glTF materials are repacked on the GPU: pass device=")
+            if len({t.shape for t in present}) != 1:
+                raise ValueError("the textures of one material must share one extent")
+            imgs, alpha, min_alpha = repack(base_t, mr_t, em_t)
             ids = [s.add_image(imgs[0]), s.add_image(imgs[1]) if em_t is not None else _abi.NO_IMAGE,
                    s.add_image(imgs[2]) if mr_t is not None else _abi.NO_IMAGE, _abi.NO_IMAGE]
             m.images = tuple(ids)
@@ -262,7 +266,7 @@ def load_gltf(path, width: int = 640, height: int = 480) -> GltfScene:
                 m.alpha_mask = s.add_image(alpha)
         nt = gm.get("normalTexture")
         if nt is not None:
-            m.bump_image = s.add_image(texture(nt, False)[..., :3])
+            m.bump_image = s.add_image(texture(nt)[..., :3].astype(np.float32) / np.float32(255.0))
             m.bump_strength = 1.0
             m.bump_channels = 3
         mat_addr.append(s.add_material(m))

@@ -1,19 +1,28 @@
 """glTF ingest (stratum2_b200/gltf.py): a document written here (two meshes under a node
 hierarchy, materials with factors, extensions and PNG textures, a camera) loads the same from
 .gltf with data URIs and from .glb; transforms, materials, the per-texel texture repack
-(from_gltf_pbr, convert_material.slang:33-69) and the PNG decoder (every row filter) are checked
-against direct computations.  CPU only."""
+(from_gltf_pbr, convert_material.slang:33-69, through the oracle's restatement standing in for the
+GPU repack) and the PNG and JPEG decoders are checked against direct computations.  CPU only; the
+GPU repack and a glTF render are compared with the oracle in tests/test_gltf_gpu.py."""
 import base64
+import io
 import json
 import struct
+import sys
 import zlib
+from pathlib import Path
 
 import numpy as np
 import pytest
 
 from stratum2_b200 import _abi
-from stratum2_b200.gltf import decode_png, load_gltf, repack_metallic_roughness, srgb_to_linear
+from stratum2_b200.gltf import decode_image_rgba8, decode_png, load_gltf
 from stratum2_b200.scene import Material, rotation_from_quaternion
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+from gltf_oracle import repack_metallic_roughness, srgb_to_linear  # noqa: E402
+
+REPACK = repack_metallic_roughness
 
 
 def png_encode(px: np.ndarray, filters=(0, 1, 2, 3, 4)) -> bytes:
@@ -135,7 +144,7 @@ def test_gltf_and_glb_load_the_same_scene(tmp_path):
     doc, data, base_px, mr_px, quad, tri = _document(np.random.default_rng(0))
     (tmp_path / "s.gltf").write_text(json.dumps(doc))
     _write_glb(doc, data, tmp_path / "s.glb")
-    a, b = load_gltf(tmp_path / "s.gltf"), load_gltf(tmp_path / "s.glb")
+    a, b = load_gltf(tmp_path / "s.gltf", repack=REPACK), load_gltf(tmp_path / "s.glb", repack=REPACK)
     assert a.instances == b.instances == 2
     assert bytes(a.scene.material_data) == bytes(b.scene.material_data)
     for x, y in zip(a.scene.vertex_buffers + a.scene.images + a.scene.transforms,
@@ -146,7 +155,7 @@ def test_gltf_and_glb_load_the_same_scene(tmp_path):
 def test_gltf_transforms_materials_and_repack(tmp_path):
     doc, data, base_px, mr_px, quad, tri = _document(np.random.default_rng(0))
     (tmp_path / "s.gltf").write_text(json.dumps(doc))
-    g = load_gltf(tmp_path / "s.gltf", width=64, height=48)
+    g = load_gltf(tmp_path / "s.gltf", width=64, height=48, repack=REPACK)
     s = g.scene
     # parent TRS x child matrix; second mesh under the parent alone
     parent = np.eye(4)
@@ -183,12 +192,16 @@ def test_gltf_transforms_materials_and_repack(tmp_path):
 
 
 def test_repack_per_texel_packing():
+    """The oracle's repack of every texel equals Material.packed_words (pinned to the reference's
+    PackedMaterialData setters) of the texel's sRGB-decoded values."""
     rng = np.random.default_rng(3)
-    base = rng.uniform(0, 1, (3, 5, 4)).astype(np.float32)
-    emis = rng.uniform(0, 2, (3, 5, 3)).astype(np.float32)
+    base = rng.integers(0, 256, (3, 5, 4), dtype=np.uint8)
+    emis = rng.integers(0, 256, (3, 5, 4), dtype=np.uint8)
+    emis[0, 0, :3] = 0  # black emission: 0/0 saturates to 0
     imgs, _, _ = repack_metallic_roughness(base, None, emis)
     for y, x in ((0, 0), (2, 4), (1, 3)):
-        m = Material(base_color=tuple(base[y, x, :3]), emission=tuple(emis[y, x]), specular=1.0, sheen=1.0)
+        m = Material(base_color=tuple(srgb_to_linear(base[y, x, :3] / 255.0)),
+                     emission=tuple(srgb_to_linear(emis[y, x, :3] / 255.0)), specular=1.0, sheen=1.0)
         w, _ = m.packed_words()
         got0 = np.round(imgs[0][y, x] * 255).astype(int)
         got1 = np.round(imgs[1][y, x] * 255).astype(int)
@@ -196,18 +209,47 @@ def test_repack_per_texel_packing():
         assert list(got1) == [(w[1] >> (8 * k)) & 0xFF for k in range(4)]
 
 
-@pytest.mark.gpu
-def test_gltf_scene_renders(device, tmp_path):
-    """The loaded scene (packed buffers, textures, alpha mask) uploads, builds and renders; the
-    camera looks down onto the front faces (a back-face hit of a non-transmissive Disney material
-    samples a direction with zero pdf, which the renderer counts as a NaN path)."""
-    doc, data, *_ = _document(np.random.default_rng(0))
+def test_textured_material_needs_the_gpu_repack(tmp_path):
+    doc, *_ = _document(np.random.default_rng(0))
     (tmp_path / "s.gltf").write_text(json.dumps(doc))
-    g = load_gltf(tmp_path / "s.gltf", width=64, height=48)
-    g.scene.set_environment((1.0, 1.0, 1.0))
-    device.upload_scene(g.scene)
-    r = device.render(g.views[0], 64, 48, spp=16, min_path_length=0, max_path_length=4, flags=_abi.FLAG_PIXEL_JITTER)
-    assert np.isfinite(r.radiance).all() and r.radiance[..., :3].max() > 0
-    assert r.stats.nan_count == 0
-    hit = r.ids32[..., 0] != 0xFFFFFFFF
-    assert hit.any()
+    with pytest.raises(ValueError, match="repacked on the GPU"):
+        load_gltf(tmp_path / "s.gltf")
+
+
+def _jpeg(px: np.ndarray, quality: int = 95) -> bytes:
+    from PIL import Image
+    buf = io.BytesIO()
+    Image.fromarray(px).save(buf, format="JPEG", quality=quality, subsampling=0)
+    return buf.getvalue()
+
+
+def test_jpeg_and_png_decode_by_signature():
+    yy, xx = np.mgrid[0:24, 0:40]
+    px = np.stack([xx * 6, yy * 10, (xx + yy) * 4], -1).astype(np.uint8)  # smooth: small JPEG error
+    j = decode_image_rgba8(_jpeg(px))
+    assert j.shape == (24, 40, 4) and j.dtype == np.uint8 and (j[..., 3] == 255).all()
+    assert np.abs(j[..., :3].astype(int) - px).max() <= 6
+    rgba = np.concatenate([px, np.full((24, 40, 1), 200, np.uint8)], -1)
+    np.testing.assert_array_equal(decode_image_rgba8(png_encode(rgba)), rgba)
+    with pytest.raises(ValueError, match="unsupported image format"):
+        decode_image_rgba8(b"GIF89a" + b"\0" * 32)
+
+
+def test_gltf_with_a_jpeg_texture(tmp_path):
+    """A JPEG base-colour texture goes through the same repack as a PNG one: the repack's input is
+    the decoded RGBA8."""
+    doc, data, base_px, *_ = _document(np.random.default_rng(0))
+    smooth = np.repeat(np.repeat(base_px[:1, :1, :3], 4, 0), 4, 1)  # one colour: JPEG keeps it within a step
+    doc["images"][0]["uri"] = "data:image/jpeg;base64," + base64.b64encode(_jpeg(smooth)).decode()
+    (tmp_path / "s.gltf").write_text(json.dumps(doc))
+    seen = []
+
+    def spy(*a):
+        seen.append(a)
+        return REPACK(*a)
+
+    g = load_gltf(tmp_path / "s.gltf", repack=spy)
+    base_in = seen[0][0]
+    assert base_in.shape == (4, 4, 4) and (base_in[..., 3] == 255).all()
+    assert np.abs(base_in[..., :3].astype(int) - smooth).max() <= 2
+    assert g.scene.materials[0].alpha_mask == _abi.NO_IMAGE  # JPEG has no alpha
