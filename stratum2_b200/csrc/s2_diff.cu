@@ -70,13 +70,28 @@ struct DiffWave {
     dk::PTParams P;
     dk::DiffQueues Q;
     uint32_t cap = 0;
-    int ext_blocks = 0, shade_blocks = 0;
+    int ext_blocks = 0, shade_blocks = 0, occ_blocks = 0, grad_blocks = 0;
 };
 
-int alloc_wave(S2Context* ctx, std::vector<DevBuf>& tmp, const DiffArgs& A, DiffWave& w) {
+// adjoint: also the visibility words of every path and the gradient records of one bounce
+int alloc_wave(S2Context* ctx, std::vector<DevBuf>& tmp, const DiffArgs& A, DiffWave& w, bool adjoint) {
     const uint64_t total = (uint64_t)A.pixels * A.spp;
     w.cap = (uint32_t)std::min<uint64_t>(total, kDiffWave);
     std::memset(&w.P, 0, sizeof(w.P));
+    std::memset(&w.Q, 0, sizeof(w.Q));
+    w.Q.paths = (uint32_t)total;
+    w.P.sh_o = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+    w.P.sh_d = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+    w.P.sh_c = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+    w.Q.gcount = (uint32_t*)dev_alloc(ctx, tmp, sizeof(uint32_t));
+    if (!w.P.sh_o || !w.P.sh_d || !w.P.sh_c || !w.Q.gcount) return S2_ERR_OOM;
+    if (adjoint) {
+        // at most three records per vertex: an environment hit, or NEE (material + environment)
+        // and the continuation
+        w.Q.vis = (uint32_t*)dev_alloc(ctx, tmp, sizeof(uint32_t) * total * ((A.max_len + 31u) >> 5));
+        w.Q.grec = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * 9 * (size_t)w.cap);
+        if (!w.Q.vis || !w.Q.grec) return S2_ERR_OOM;
+    }
     w.P.scene = A.scene;
     if (ctx->tuning.shade_records == S2_SHADE_RECORDS_OFF) w.P.scene.shade_recs = nullptr;
     w.P.flags = A.flags;
@@ -91,8 +106,8 @@ int alloc_wave(S2Context* ctx, std::vector<DevBuf>& tmp, const DiffArgs& A, Diff
         float4* b = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
         float4* c = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
         uint4* d = (uint4*)dev_alloc(ctx, tmp, sizeof(uint4) * (size_t)w.cap);
-        w.Q.L[k] = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
-        if (!a || !b || !c || !d || !w.Q.L[k]) return S2_ERR_OOM;
+        if (adjoint) w.Q.L[k] = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
+        if (!a || !b || !c || !d || (adjoint && !w.Q.L[k])) return S2_ERR_OOM;
         w.P.q[k] = dk::PathQueue{a, b, c, d};
     }
     w.P.hits = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)w.cap);
@@ -106,6 +121,11 @@ int alloc_wave(S2Context* ctx, std::vector<DevBuf>& tmp, const DiffArgs& A, Diff
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (A.flags & S2_FLAG_LAMBERTIAN) ? dk::k_diff_shade<true> : dk::k_diff_shade<false>,
                                                   128, 0);
     w.shade_blocks = std::max(1, b) * sms;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dk::k_diff_occlude, dk::kTravBlock, 0);
+    w.occ_blocks = std::max(1, b) * sms;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (A.flags & S2_FLAG_LAMBERTIAN) ? dk::k_diff_grads<true> : dk::k_diff_grads<false>,
+                                                  128, 0);
+    w.grad_blocks = std::max(1, b) * sms;
     return S2_OK;
 }
 
@@ -120,13 +140,18 @@ uint64_t launch(const DiffArgs& A, DiffWave& w, bool adj, cudaStream_t s) {
         cudaMemsetAsync(w.P.counters, 0, sizeof(uint32_t) * dk::C_COUNT, s);
         dk::k_diff_gen<<<(n + 255) / 256, 256, 0, s>>>(A, w.P, w.Q, (uint32_t)base, n, adj ? 1 : 0);
         launches += 1;
+        const bool lambert = (A.flags & S2_FLAG_LAMBERTIAN) != 0;
         for (uint32_t b = 0; b < bounces; ++b) {
             const uint32_t parity = b & 1u;
-            dk::k_diff_bounce<<<1, 32, 0, s>>>(A, w.P, parity);
+            dk::k_diff_bounce<<<1, 32, 0, s>>>(A, w.P, w.Q, parity);
             dk::k_extend<false><<<w.ext_blocks, dk::kTravBlock, 0, s>>>(w.P, parity);
-            if (A.flags & S2_FLAG_LAMBERTIAN) dk::k_diff_shade<true><<<w.shade_blocks, 128, 0, s>>>(A, w.P, w.Q, parity, adj ? 1 : 0);
+            if (lambert) dk::k_diff_shade<true><<<w.shade_blocks, 128, 0, s>>>(A, w.P, w.Q, parity, adj ? 1 : 0);
             else dk::k_diff_shade<false><<<w.shade_blocks, 128, 0, s>>>(A, w.P, w.Q, parity, adj ? 1 : 0);
-            launches += 3;
+            // the forward traces the bounce's shadow rays; the adjoint replay pushes its gradients
+            if (!adj) dk::k_diff_occlude<<<w.occ_blocks, dk::kTravBlock, 0, s>>>(A, w.P, w.Q);
+            else if (lambert) dk::k_diff_grads<true><<<w.grad_blocks, 128, 0, s>>>(A, w.Q);
+            else dk::k_diff_grads<false><<<w.grad_blocks, 128, 0, s>>>(A, w.Q);
+            launches += 4;
         }
     }
     if (!adj) {
@@ -177,7 +202,7 @@ extern "C" int s2_render_diff(S2Context* ctx, const S2View* view, const S2Render
     A.path_l = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * (size_t)A.pixels * A.spp);
     if (!A.rays || !A.image || !A.path_l) { free_bufs(tmp); return S2_ERR_OOM; }
     DiffWave w;
-    if (alloc_wave(ctx, tmp, A, w) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "differentiable render queues"); }
+    if (alloc_wave(ctx, tmp, A, w, false) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "differentiable render queues"); }
     cudaMemsetAsync(A.rays, 0, 2 * sizeof(unsigned long long), ctx->stream);
     cudaMemsetAsync(ctx->status_dev, 0, sizeof(int), ctx->stream);
     cudaEventRecord(ctx->ev0, ctx->stream);
@@ -212,7 +237,7 @@ extern "C" int s2_render_adjoint(S2Context* ctx, const S2View* view, const S2Ren
     A.image = (float4*)dev_alloc(ctx, tmp, sizeof(float4) * A.pixels);
     if (!A.rays || !A.grad || !A.grad_offset || !A.d_image || !A.path_l || !A.image) { free_bufs(tmp); return S2_ERR_OOM; }
     DiffWave w;
-    if (alloc_wave(ctx, tmp, A, w) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "adjoint render queues"); }
+    if (alloc_wave(ctx, tmp, A, w, true) != S2_OK) { free_bufs(tmp); return set_error(ctx, S2_ERR_OOM, "adjoint render queues"); }
     cudaMemcpyAsync((void*)A.grad_offset, off.data(), sizeof(uint32_t) * (ni + 1), cudaMemcpyHostToDevice, ctx->stream);
     if (on_host) cudaMemcpyAsync((void*)A.d_image, d_radiance, sizeof(float4) * A.pixels, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemsetAsync(A.grad, 0, sizeof(float4) * std::max<size_t>(1, off[ni]), ctx->stream);

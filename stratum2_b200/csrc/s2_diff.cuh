@@ -187,20 +187,60 @@ S2D void material_grads(const DiffArgs& A, const MatF& m, float3 in, float3 out,
     }
 }
 
+// Wavefront state beside the renderer's queues (PTParams.q): the adjoint replay's running radiance
+// (moved with its path, by queue parity), the NEE visibility the first replay found, and the
+// gradient records the adjoint replay appends for k_diff_grads.
+struct DiffQueues {
+    float4* L[2];           // adjoint replay: radiance gathered so far, by queue parity
+    uint32_t* vis;          // bit (len - 1) & 31 of word (len - 1) >> 5 of path p: vis[word * paths + p]
+    uint32_t paths;         // pixels x spp
+    float4* grec;           // gradient records, 3 float4 each (see push_grad)
+    uint32_t* gcount;       // records appended this bounce
+};
+
+// Slot in a queue for the calling lane, one atomic per group of converged lanes (opportunistic
+// warp aggregation; valid in divergent code).
+S2D uint32_t append_active(uint32_t* counter) {
+    const uint32_t mask = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Gradient record: {in.xyz, uv.x}, {out.xyz, uv.y}, {y.xyz, material address} for the BSDF value at
+// (in, out) of the material at uv weighted by y; material address 0xffffffff: environment texels in
+// direction in, weighted by y.
+S2D void push_grad(const DiffQueues& Q, uint32_t mat, float2 uv, float3 in, float3 out, float3 y) {
+    const uint32_t k = append_active(Q.gcount);
+    float4* r = Q.grec + 3 * (size_t)k;
+    r[0] = make_float4(in.x, in.y, in.z, uv.x);
+    r[1] = make_float4(out.x, out.y, out.z, uv.y);
+    r[2] = make_float4(y.x, y.y, y.z, __uint_as_float(mat));
+}
+S2D void push_env_grad(const DiffQueues& Q, float3 dir, float3 y) {
+    push_grad(Q, 0xffffffffu, make_float2(0.f, 0.f), dir, f3(0.f), y);
+}
+
+S2D float3 add_rn(float3 a, float3 b) { return f3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+
 // The work at one path vertex, after the closest-hit query of the ray (org, dir): increments len,
-// adds the vertex's emission and NEE to L, and samples the continuation (org, dir, thr, dir_pdf
-// updated; returns false when the path ends).  adj = true (the second replay): adds the texel
-// gradients for the image adjoint `delta`, with `ltot` the path's radiance from the first replay.
-// Not inlined, and the adjoint is a run-time argument, so both replays run the same machine code
-// and take the same decisions.
+// adds the vertex's emission to L, makes the NEE estimate and samples the continuation (org, dir,
+// thr, dir_pdf updated; returns false when the path ends).  adj = false (the forward): the NEE
+// shadow ray goes to the renderer's shadow queue, whose k_diff_occlude adds its contribution to
+// the path's radiance and records the visibility.  adj = true (the adjoint replay): the visibility
+// comes from the forward's record, the contribution is added to L here, and the vertex's gradient
+// terms for the image adjoint `delta` (ltot: the path's radiance from the forward) go to the
+// gradient queue.  Not inlined, and the adjoint is a run-time argument, so both replays run the
+// same machine code and take the same decisions.
 template <bool LAMBERT>
-__device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, uint32_t& len, float3& org, float3& dir,
-                                         float3& thr, float3& L, float& dir_pdf, Rng& rng, bool adj, float3 ltot, float3 delta,
-                                         uint2* smem_stack, uint32_t lane_stride, uint32_t& shadow_rays, bool& overflow) {
+__device__ __noinline__ bool diff_vertex(const DiffArgs& A, const PTParams& P, const DiffQueues& Q, const TravHit& h,
+                                         uint32_t path, uint32_t& len, float3& org, float3& dir, float3& thr, float3& L,
+                                         float& dir_pdf, Rng& rng, bool adj, float3 ltot, float3 delta, uint32_t& shadow_rays) {
     const DevScene& s = A.scene;
     const bool nee = !(A.flags & S2F_NO_NEE), sn = !(A.flags & S2F_NO_SN);
-    const SceneAlphaTest alpha{&s, !(A.flags & S2F_NO_ALPHA)};
-    TravCounters ctr{0, 0};
     len++;
     if (h.tri == 0xffffffffu) {
         // environment (TraceRay, testrenderer.slang:1036-1054)
@@ -214,8 +254,8 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
                 w = mis_w(dir_pdf, lp);
             }
             if (w > 0.f) {
-                L = L + e * w;
-                if (adj) env_grad(A, dir, delta * thr * w);
+                L = add_rn(L, e * w);
+                if (adj) push_env_grad(Q, dir, delta * thr * w);
             }
         }
         return false;
@@ -228,6 +268,7 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
     float3 base_rec;
     float rough_rec;
     const MatF m = load_material_f(s, sd.mat, sd.uv, tb, tr, base_rec, rough_rec);
+    const bool textured = tb.img != 0xffffffffu || tr.img != 0xffffffffu;  // else no texel has a gradient
     const float3 in = sd.to_local(-dir);
     const float cos_in = fabsf(in.z);
     if (in.z > 0.f) {
@@ -235,14 +276,13 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
         if (any_pos(e) && len >= A.min_len) {
             float w = 1.f;
             if (len > 1 && nee && dir_pdf > 0.f) w = mis_w(dir_pdf * (cos_in / pow2(isect_dist)), isect_pdfa);
-            if (w > 0.f) L = L + e * w;
+            if (w > 0.f) L = add_rn(L, e * w);
         }
     }
     if (!(len < A.max_len && any_pos(m.base()))) return false;
     const bool sing = mat_singular<LAMBERT>(m);
     const float cp = (A.flags & S2F_NO_RR) ? 1.f : cont_prob(m);
-    // NEE (ConnectToLight, testrenderer.slang:751-779), same stream use as the wavefront shade;
-    // the shadow ray is traced here (first hit), so the vertex's gradient terms can follow it
+    // NEE (ConnectToLight, testrenderer.slang:751-779), same stream use as the wavefront shade
     if (!sing && nee) {
         if (len + 1 < A.min_len) {
             rng.skip();
@@ -260,18 +300,19 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
                 const float3 contrib = thr * r.radiance * f / dpw;
                 const float w = mis_w(r.pdf, fwd / AtoW);
                 if (w > 0.f && !all_nonpos(contrib)) {
-                    TravHit sh;
-                    shadow_rays++;
-                    if (!traverse<true, false>(make_trav_ray(ray_offset(sd.pos, sd.gn, r.dir), r.dir, 0.f),
-                                               adjust_distance(r.dist), s.nodes, s.tris, smem_stack, lane_stride, sh, ctr, alpha))
-                        overflow = true;
-                    if (sh.tri == 0xffffffffu) {
-                        L = L + f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
-                        if (adj) {
-                            const float k = w / dpw;
-                            material_grads<LAMBERT>(A, m, in, out, delta * thr * r.radiance * k, tb, tr, base_rec, rough_rec);
-                            if (!r.finite) env_grad(A, r.dir, delta * thr * f * k);
-                        }
+                    const float3 c = f3(fmaxf(contrib.x * w, 0.f), fmaxf(contrib.y * w, 0.f), fmaxf(contrib.z * w, 0.f));
+                    if (!adj) {
+                        const float3 o = ray_offset(sd.pos, sd.gn, r.dir);
+                        const uint32_t q = append_active(&P.counters[C_SHADOW]);
+                        P.sh_o[q] = make_float4(o.x, o.y, o.z, adjust_distance(r.dist));
+                        P.sh_d[q] = make_float4(r.dir.x, r.dir.y, r.dir.z, __uint_as_float(path));
+                        P.sh_c[q] = make_float4(c.x, c.y, c.z, __uint_as_float(len));
+                        shadow_rays++;
+                    } else if (Q.vis[(size_t)((len - 1) >> 5) * Q.paths + path] & (1u << ((len - 1) & 31u))) {
+                        L = add_rn(L, c);
+                        const float k = w / dpw;
+                        if (textured) push_grad(Q, sd.mat, sd.uv, in, out, delta * thr * r.radiance * k);
+                        if (!r.finite) push_env_grad(Q, r.dir, delta * thr * f * k);
                     }
                 }
             }
@@ -290,7 +331,8 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
         const float3 after = ltot - L;
         const float3 y = f3(refl.x > 0.f ? delta.x * after.x / refl.x : 0.f, refl.y > 0.f ? delta.y * after.y / refl.y : 0.f,
                             refl.z > 0.f ? delta.z * after.z / refl.z : 0.f);
-        if (any_pos(f3(fabsf(y.x), fabsf(y.y), fabsf(y.z)))) material_grads<LAMBERT>(A, m, in, sdir, y, tb, tr, base_rec, rough_rec);
+        if (textured && any_pos(f3(fabsf(y.x), fabsf(y.y), fabsf(y.z))))
+            push_grad(Q, sd.mat, sd.uv, in, sdir, y);
     }
     const float cpm = (A.flags & S2F_NO_RR) ? 1.f : cp;
     fwd *= cpm;
@@ -303,16 +345,6 @@ __device__ __noinline__ bool diff_vertex(const DiffArgs& A, const TravHit& h, ui
     return !(any_nan(thr) || !any_pos(thr));
 }
 
-// Wavefront form: the paths' state lives in the wavefront renderer's queues (s0: origin, dir pdf;
-// s1: direction, throughput x; s2: throughput yz, path id, path length; s3: random state) plus one
-// stream of the radiance gathered so far; every bounce is the renderer's own closest-hit kernel
-// (k_extend) and k_diff_shade, which runs diff_vertex for each queued path and appends the
-// survivors to the other queue.  Path p (sample-major: p = sample x pixels + pixel) writes its
-// radiance to path_l[p] when it ends; the adjoint's second replay reads it there as `ltot`.
-struct DiffQueues {
-    float4* L[2];       // radiance gathered so far, by queue parity
-};
-
 S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow) {
     // warp sums of the ray counts, one 64-bit atomic pair per warp
     for (int o = 16; o > 0; o >>= 1) { ext += __shfl_xor_sync(0xffffffffu, ext, o); shd += __shfl_xor_sync(0xffffffffu, shd, o); }
@@ -320,8 +352,9 @@ S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow
     if (overflow) atomicOr(A.status, 1);
 }
 
-// Camera paths base .. base + n - 1 into queue 0 (the adjoint skips paths of pixels whose adjoint
-// is zero, as its replay adds nothing).
+// Camera paths base .. base + n - 1 into queue 0.  The forward zeroes each path's radiance in
+// path_l and its visibility words; the adjoint skips paths of pixels whose adjoint is zero, as
+// their replay adds nothing.
 __global__ void k_diff_gen(const __grid_constant__ DiffArgs A, PTParams P, DiffQueues Q, uint32_t base, uint32_t n, int adj) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool want = false;
@@ -335,6 +368,10 @@ __global__ void k_diff_gen(const __grid_constant__ DiffArgs A, PTParams P, DiffQ
         if (adj) {
             const float4 d = A.d_image[pix];
             want = d.x != 0.f || d.y != 0.f || d.z != 0.f;
+        } else {
+            A.path_l[path] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (Q.vis)
+                for (uint32_t w = 0; w < (A.max_len + 31u) >> 5; ++w) Q.vis[(size_t)w * Q.paths + path] = 0u;
         }
     }
     const uint32_t q = warp_append(&P.counters[C_QUEUE0], want);
@@ -348,38 +385,40 @@ __global__ void k_diff_gen(const __grid_constant__ DiffArgs A, PTParams P, DiffQ
     Qo.s1[q] = make_float4(dir.x, dir.y, dir.z, 1.f);
     Qo.s2[q] = make_float4(1.f, 1.f, __uint_as_float(path), __uint_as_float(0u));
     Qo.s3[q] = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
-    Q.L[0][q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (adj) Q.L[0][q] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Counters before a bounce: the queue about to be traced counts as extension rays; the other
-// queue and the traversal work counter restart.
-__global__ void k_diff_bounce(const __grid_constant__ DiffArgs A, PTParams P, uint32_t parity) {
+// queue, the shadow queue, the gradient records and the traversal work counters restart.
+__global__ void k_diff_bounce(const __grid_constant__ DiffArgs A, PTParams P, DiffQueues Q, uint32_t parity) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     atomicAdd(A.rays, (unsigned long long)P.counters[parity]);
     P.counters[1 - parity] = 0;
+    P.counters[C_SHADOW] = 0;
     P.counters[C_WORK_EXT] = 0;
+    P.counters[C_WORK_OCC] = 0;
+    *Q.gcount = 0;
 }
 
 template <bool LAMBERT>
-__global__ void __launch_bounds__(128) k_diff_shade(const __grid_constant__ DiffArgs A, const __grid_constant__ PTParams P,
+__global__ void __launch_bounds__(128, 8) k_diff_shade(const __grid_constant__ DiffArgs A, const __grid_constant__ PTParams P,
                                                     DiffQueues Q, uint32_t parity, int adj) {
-    __shared__ uint2 stack[S2_STACK_SMEM * 128];
     const uint32_t count = P.counters[parity];
     const PathQueue qi = P.q[parity], qo = P.q[1 - parity];
     const uint32_t rounded = (count + 31u) & ~31u;
     uint32_t shd = 0;
-    bool overflow = false;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
         bool alive = false;
         float4 n0, n1, n2, nl;
         uint4 n3;
         if (i < count) {
-            const float4 a = qi.s0[i], b = qi.s1[i], c = qi.s2[i], l4 = Q.L[parity][i];
+            const float4 a = qi.s0[i], b = qi.s1[i], c = qi.s2[i];
             const uint4 rs = qi.s3[i];
             const float4 hv = P.hits[i];
+            const uint32_t path = __float_as_uint(c.z);
+            const float4 l4 = adj ? Q.L[parity][i] : A.path_l[path];
             float3 org = f3(a.x, a.y, a.z), dir = f3(b.x, b.y, b.z), thr = f3(b.w, c.x, c.y), L = f3(l4.x, l4.y, l4.z);
             float dir_pdf = a.w;
-            const uint32_t path = __float_as_uint(c.z);
             uint32_t len = __float_as_uint(c.w);
             Rng rng;
             rng.px = rs.x; rng.py = rs.y; rng.seed = rs.z; rng.ctr = rs.w; rng.pcg32 = (A.flags & S2F_PCG32) != 0;
@@ -400,25 +439,62 @@ __global__ void __launch_bounds__(128) k_diff_shade(const __grid_constant__ Diff
                 ltot = f3(lt.x, lt.y, lt.z);
                 delta = f3(d.x, d.y, d.z) * A.out_scale;
             }
-            alive = diff_vertex<LAMBERT>(A, h, len, org, dir, thr, L, dir_pdf, rng, adj != 0, ltot, delta,
-                                         stack + threadIdx.x, 128u, shd, overflow);
+            alive = diff_vertex<LAMBERT>(A, P, Q, h, path, len, org, dir, thr, L, dir_pdf, rng, adj != 0, ltot, delta, shd);
+            if (!adj) A.path_l[path] = make_float4(L.x, L.y, L.z, 0.f);
             if (alive) {
                 n0 = make_float4(org.x, org.y, org.z, dir_pdf);
                 n1 = make_float4(dir.x, dir.y, dir.z, thr.x);
                 n2 = make_float4(thr.y, thr.z, __uint_as_float(path), __uint_as_float(len));
                 n3 = make_uint4(rng.px, rng.py, rng.seed, rng.ctr);
                 nl = make_float4(L.x, L.y, L.z, 0.f);
-            } else if (!adj) {
-                A.path_l[path] = make_float4(L.x, L.y, L.z, 0.f);
             }
         }
         const uint32_t o = warp_append(&P.counters[1 - parity], alive);
         if (alive) {
             qo.s0[o] = n0; qo.s1[o] = n1; qo.s2[o] = n2; qo.s3[o] = n3;
-            Q.L[1 - parity][o] = nl;
+            if (adj) Q.L[1 - parity][o] = nl;
         }
     }
-    diff_count(A, 0u, shd, overflow);
+    diff_count(A, 0u, shd, false);
+}
+
+// The forward's shadow rays, on the renderer's persistent any-hit loop: an unoccluded ray adds its
+// contribution to its path's radiance (one shadow ray per path and bounce, so no other thread
+// touches the path meanwhile) and, for the adjoint, sets its visibility bit.
+__global__ void __launch_bounds__(kTravBlock) k_diff_occlude(const __grid_constant__ DiffArgs A, const __grid_constant__ PTParams P,
+                                                            DiffQueues Q) {
+    occlude_queue<false>(P, [&](uint32_t ray) {
+        const float4 cc = P.sh_c[ray];
+        const uint32_t path = __float_as_uint(P.sh_d[ray].w);
+        const float4 l = A.path_l[path];
+        A.path_l[path] = make_float4(__fadd_rn(l.x, cc.x), __fadd_rn(l.y, cc.y), __fadd_rn(l.z, cc.z), 0.f);
+        if (Q.vis) {
+            const uint32_t j = __float_as_uint(cc.w) - 1u;
+            Q.vis[(size_t)(j >> 5) * Q.paths + path] |= 1u << (j & 31u);
+        }
+    });
+}
+
+// The adjoint replay's gradient records of one bounce: the BSDF partials of the record's material
+// (reloaded from its address and uv) pushed to the texels, or the environment texels' gradient.
+template <bool LAMBERT>
+__global__ void __launch_bounds__(128) k_diff_grads(const __grid_constant__ DiffArgs A, DiffQueues Q) {
+    const uint32_t count = *Q.gcount;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4* r = Q.grec + 3 * (size_t)i;
+        const float4 r0 = r[0], r1 = r[1], r2 = r[2];
+        const uint32_t mat = __float_as_uint(r2.w);
+        const float3 y = f3(r2.x, r2.y, r2.z);
+        if (mat == 0xffffffffu) {
+            env_grad(A, f3(r0.x, r0.y, r0.z), y);
+            continue;
+        }
+        Taps tb, tr;
+        float3 base_rec;
+        float rough_rec;
+        const MatF m = load_material_f(A.scene, mat, make_float2(r0.w, r1.w), tb, tr, base_rec, rough_rec);
+        material_grads<LAMBERT>(A, m, f3(r0.x, r0.y, r0.z), f3(r1.x, r1.y, r1.z), y, tb, tr, base_rec, rough_rec);
+    }
 }
 
 // image[pixel] = sum of the pixel's path radiances in sample order * 2^exposure / spp.

@@ -429,10 +429,10 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
     if (COUNT) add_fetches(P.stats, S_EXT_NODES, c);
 }
 
-// ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
-// ray belongs to one accumulator slot and adds its contribution when unoccluded.
-template <bool COUNT>
-__global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ PTParams P) {
+// The persistent any-hit loop over the shadow queue (sh_o: origin + t_max, sh_d: direction): warps
+// refill lanes from the work counter; `on_visible(ray)` runs for every unoccluded ray.
+template <bool COUNT, class OnVisible>
+S2D void occlude_queue(const PTParams& P, const OnVisible& on_visible) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[C_SHADOW];
@@ -458,15 +458,22 @@ __global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ 
                       : trav_step_pp<true, false>(r, st, P.scene.nodes, P.scene.tris, stack + threadIdx.x, kTravBlock, lstack, h, c,
                                                   tri_step, P.trav.tris_per_step, alpha)) {
                 if (!st.ok) atomicOr(P.status, 1);
-                if (h.tri == 0xffffffffu) {
-                    const float4 cc = P.sh_c[ray];
-                    add_contrib(P, __float_as_uint(P.sh_d[ray].w), f3(cc.x, cc.y, cc.z));
-                }
+                if (h.tri == 0xffffffffu) on_visible(ray);
                 ray = kNoRay;
             }
         }
     }
     if (COUNT) add_fetches(P.stats, S_SH_NODES, c);
+}
+
+// ProcessShadowRays (testrenderer.slang:1147-1166) without the fixed-point atomics: each shadow
+// ray belongs to one accumulator slot (sh_d.w) and adds its contribution (sh_c) when unoccluded.
+template <bool COUNT>
+__global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ PTParams P) {
+    occlude_queue<COUNT>(P, [&](uint32_t ray) {
+        const float4 cc = P.sh_c[ray];
+        add_contrib(P, __float_as_uint(P.sh_d[ray].w), f3(cc.x, cc.y, cc.z));
+    });
 }
 
 // ---------------------------------------------------------------- accumulation
