@@ -216,3 +216,39 @@ def test_batched_screen_reuse_matches_single_view_sequence(device):
     m, ms = both[:, 0].mean(0), single.mean(0)
     assert abs(m.sum() / ms.sum() - 1) < 1e-3, (m.sum(), ms.sum())
     assert np.mean(np.abs(m - ms)) < 1e-3 * np.mean(ms), np.mean(np.abs(m - ms)) / np.mean(ms)
+
+
+def test_batched_screen_reuse_of_different_views_matches_each_single_view(device):
+    """Two views that differ in camera and extent (64x64 and 48x32) in one batched call: each view
+    keeps its own reservoirs (its slice of the per-pixel records), so over 4 sequences of 32 calls
+    each view's mean image equals its own s2_render sequence's with the same seeds, within the
+    accumulation-order tolerance of the identical-view test."""
+    from stratum2_b200.scene import make_view
+    wl = box_scene(seed=1, width=64, height=64)
+    device.upload_scene(wl.scene)
+    rot = np.array([[0.9659258, 0.0, 0.258819], [0.0, 1.0, 0.0], [-0.258819, 0.0, 0.9659258]])
+    other = make_view((0.6, 0.1, 2.6), 48, 32, 45.0, rot)
+    views = [wl.view, other]
+    extents = [(64, 64), (48, 32)]
+
+    def single(view, wh, seed0):
+        w, h = wh
+        device.render(view, w, h, params=params(1, RIS | J | LAM, minl=2, maxl=5))
+        return np.mean([device.render(view, w, h, params=params(seed0 + k, SCREEN | J | LAM, minl=2, maxl=5))
+                        .radiance[..., :3].astype(np.float64) for k in range(32)], axis=0)
+
+    singles = [[], []]
+    batched = [[], []]
+    for b in range(4):
+        seed0 = 50000 + 128 * b
+        for v in range(2):
+            singles[v].append(single(views[v], extents[v], seed0))
+        device.render_views(views, params(1, RIS | J | LAM, minl=2, maxl=5))
+        calls = [device.render_views(views, params(seed0 + k, SCREEN | J | LAM, minl=2, maxl=5))[0] for k in range(32)]
+        for v in range(2):
+            batched[v].append(np.mean([c[v].radiance[..., :3].astype(np.float64) for c in calls], axis=0))
+    for v in range(2):
+        m, ms = np.mean(batched[v], axis=0), np.mean(singles[v], axis=0)
+        assert m.shape == (extents[v][1], extents[v][0], 3)
+        assert abs(m.sum() / ms.sum() - 1) < 1e-3, (v, m.sum(), ms.sum())
+        assert np.mean(np.abs(m - ms)) < 1e-3 * np.mean(ms), (v, np.mean(np.abs(m - ms)) / np.mean(ms))
