@@ -77,12 +77,20 @@ class ClockSampler:
         self.proc = None
 
     def start(self):
+        """Starts sampling and waits (up to 5 s) for the first sample, so that the samples cover the
+        timed region that follows even when it lasts well under a second."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            if Path(self.file.name).stat().st_size > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self) -> dict | None:
         if self.proc is None:

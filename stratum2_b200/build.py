@@ -25,6 +25,7 @@ CXX_SOURCES = ["s2_bvh_build.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
+    "-prec-div=false", "-prec-sqrt=false",  # approximate / and sqrtf; exact paths use __fdiv_rn etc.
     "-Xcompiler", "-fPIC,-O3,-ffp-contract=off,-fopenmp",
     "--expt-relaxed-constexpr",
     "-Xptxas", "-v",

@@ -10,12 +10,13 @@ S2D float pow5(float x) { const float x2 = x * x; return x2 * x2 * x; }
 // microfacet.hlsli:22-27
 S2D float schlick1(float F0, float c) { return F0 + (1.f - F0) * pow5(fmaxf(1.f - c, 0.f)); }
 S2D float3 schlick3(float3 F0, float c) { const float k = pow5(fmaxf(1.f - c, 0.f)); return F0 + (f3(1.f) - F0) * k; }
-// microfacet.hlsli:42-62
+// microfacet.hlsli:42-62; IEEE-rounded division and square root (the reflectance ratios cancel
+// near Brewster's angle, where an approximate quotient loses relative accuracy)
 S2D float fresnel_dielectric(float ndi, float eta) {
-    const float ndt2 = 1.f - (1.f - ndi * ndi) / (eta * eta);
+    const float ndt2 = 1.f - __fdiv_rn(1.f - ndi * ndi, eta * eta);
     if (ndt2 < 0.f) return 1.f;
-    const float ndt = sqrtf(ndt2), ni = fabsf(ndi);
-    const float rs = (ni - eta * ndt) / (ni + eta * ndt), rp = (eta * ni - ndt) / (eta * ni + ndt);
+    const float ndt = __fsqrt_rn(ndt2), ni = fabsf(ndi);
+    const float rs = __fdiv_rn(ni - eta * ndt, ni + eta * ndt), rp = __fdiv_rn(eta * ni - ndt, eta * ni + ndt);
     return (rs * rs + rp * rp) * 0.5f;
 }
 // microfacet.hlsli:64-81

@@ -140,9 +140,15 @@ S2D int snorm_from_float(float v) {
     v = fminf(fmaxf(v, -1.f), 1.f);
     return (int)truncf(__fadd_rn(__fmul_rn(v, 32767.f), v >= 0 ? 0.5f : -0.5f));
 }
-S2D float float_from_snorm(int v) { return fmaxf((float)v / 32767.f, -1.f); }
+// The packing divides and normalises with IEEE-rounded intrinsics: ray directions go through this
+// quantisation, so it stays exact whatever the compiler's division and square-root settings.
+S2D float float_from_snorm(int v) { return fmaxf(__fdiv_rn((float)v, 32767.f), -1.f); }
+S2D float3 normalize_ieee(float3 a) {
+    const float l = __fsqrt_rn(dot(a, a));
+    return f3(__fdiv_rn(a.x, l), __fdiv_rn(a.y, l), __fdiv_rn(a.z, l));
+}
 S2D uint32_t pack_normal(float3 v) {
-    const float inv = 1.f / (fabsf(v.x) + fabsf(v.y) + fabsf(v.z));
+    const float inv = __fdiv_rn(1.f, fabsf(v.x) + fabsf(v.y) + fabsf(v.z));
     float px = v.x * inv, py = v.y * inv;
     if (v.z <= 0) {
         const float ox = (1.f - fabsf(py)) * (px >= 0 ? 1.f : -1.f);
@@ -160,7 +166,7 @@ S2D float3 unpack_normal(uint32_t p) {
         const float oy = (1.f - fabsf(v.x)) * (v.y >= 0 ? 1.f : -1.f);
         v.x = ox; v.y = oy;
     }
-    return normalize(v);
+    return normalize_ieee(v);
 }
 
 // makeOrthonormal (common.hlsli:24-34): rows t, b, n

@@ -46,7 +46,7 @@ struct RepackArgs {
 // setX's quantisation followed by D3DX_R8G8B8A8_UNORM_to_FLOAT4's byte / 255 (IEEE division)
 __device__ __forceinline__ float unorm8(double v) {
     v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
-    return (float)floor(v * 255.0 + 0.5) / 255.f;
+    return __fdiv_rn((float)floor(v * 255.0 + 0.5), 255.f);
 }
 
 __global__ void __launch_bounds__(kRepackBlock) k_repack_gltf_pbr(const RepackArgs A) {
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kRepackBlock) k_repack_gltf_pbr(const RepackAr
         const uchar4 d = A.base ? A.base[t] : make_uchar4(255, 255, 255, 255);
         A.out0[t] = make_float4(unorm8(lin[d.x]), unorm8(lin[d.y]), unorm8(lin[d.z]), one);
         if (A.base) {
-            if (A.alpha) A.alpha[t] = d.w / 255.f;
+            if (A.alpha) A.alpha[t] = __fdiv_rn((float)d.w, 255.f);
             if (d.w < 255u) amin = min(amin, (uint32_t)d.w);  // floor(saturate(a) * 255 + 0.5) of a = w / 255
         }
         double er = 1.0, eg = 1.0, eb = 1.0;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kRepackBlock) k_repack_gltf_pbr(const RepackAr
         A.out1[t] = emax > 0.0 ? make_float4(unorm8(er / emax), unorm8(eg / emax), unorm8(eb / emax), one)
                                : make_float4(0.f, 0.f, 0.f, one);  // 0/0 saturates to 0
         const uchar4 m = A.mr ? A.mr[t] : make_uchar4(255, 255, 255, 255);
-        A.out2[t] = make_float4(m.z / 255.f, m.y / 255.f, one, one);
+        A.out2[t] = make_float4(__fdiv_rn((float)m.z, 255.f), __fdiv_rn((float)m.y, 255.f), one, one);
         A.out3[t] = make_float4(one, one, one, one);
     }
     if (A.min_alpha) {

@@ -38,7 +38,9 @@ def test_cache_beyond_max_length_is_the_plain_render(device, terrain):
     p.cache_bounces = 10
     p.cache_train_paths = 512
     cached = device.render(wl.view, wl.width, wl.height, params=p)
-    np.testing.assert_allclose(cached.radiance, plain.radiance, rtol=1e-5, atol=1e-7)
+    # the same estimator in another instantiation of the shade kernel: its floating-point
+    # contractions and approximate quotients may round differently in the last bits
+    np.testing.assert_allclose(cached.radiance, plain.radiance, rtol=1e-4, atol=1e-7)
     w_after, _ = device.cache_get_params()
     device.cache_init()
     w0, _ = device.cache_get_params()

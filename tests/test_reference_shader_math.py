@@ -49,10 +49,15 @@ def _close(name, got, ref, exact, device=False):
         # (a^2 - 1) / log(a^2) is ill-conditioned as alpha -> 1: one ulp of the device's logf
         # there is up to 2e-5 relative in the result
         np.testing.assert_allclose(got, ref, rtol=1e-4, atol=0, err_msg=name)
+    elif device and name == "vndf":
+        # the renderer is compiled with approximate division and square root (two ulp each); the
+        # visible-normal map is ill-conditioned for grazing directions, where that moves the sampled
+        # half vector by up to a few 1e-5
+        np.testing.assert_allclose(got, ref, rtol=0, atol=5e-5, err_msg=name)
     elif name in TRIG:
         np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5, err_msg=name)
     elif device:
-        # the device's sqrtf / powf / division round within an ulp or two of the host's
+        # the device's sqrtf / powf / division (approximate: two ulp) round near the host's
         np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-7, err_msg=name)
     else:
         np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7, err_msg=name)

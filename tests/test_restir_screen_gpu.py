@@ -46,11 +46,23 @@ def img(device, view, wl, p):
     return device.render(view, wl.width, wl.height, params=p).radiance[..., :3].astype(np.float64)
 
 
-def z_check(m, v, ref, ref_var, tag):
+def z_check(m, v, ref, ref_var, tag, mean_z=True):
     z = (m - ref) / np.sqrt(v + ref_var + (1e-5 * np.abs(ref) + 1e-9) ** 2)
     frac = np.mean(np.abs(z) > 5)
     assert frac <= 2e-3, f"{tag}: {frac:.4%} of pixel channels with |z| > 5"
-    assert abs(z.mean()) < 0.15, f"{tag}: mean z {z.mean():.3f}"
+    if mean_z:
+        assert abs(z.mean()) < 0.15, f"{tag}: mean z {z.mean():.3f}"
+
+
+def total_check(seq_means, ref, ref_var, tag, bound=4.0):
+    """Bias test on the image total: the sequences' totals are independent (one per sequence),
+    where the pixels of one sequence are not (spatial reuse shares reservoirs between neighbours,
+    so an image-wide mean of per-pixel z scores measured -0.15 to +0.29 between seed sets of an
+    unbiased estimator)."""
+    totals = seq_means[..., :3].sum(axis=(1, 2, 3))
+    ref_total, ref_total_var = ref[..., :3].sum(), ref_var[..., :3].sum()
+    t = (totals.mean() - ref_total) / np.sqrt(totals.var(ddof=1) / len(totals) + ref_total_var)
+    assert abs(t) < bound, f"{tag}: image total {totals.mean():.6g} against {ref_total:.6g} (t = {t:.2f})"
 
 
 @pytest.fixture(scope="module")
@@ -86,7 +98,8 @@ def test_box_screen_reuse_converges_to_fp64_golden(device):
         means.append(np.mean([img(device, wl.view, wl, params(30000 + 256 * b + k, SCREEN | J | LAM, minl=2, maxl=5))
                               for k in range(256)], axis=0))
     means = np.stack(means)
-    z_check(means.mean(0), means.var(0, ddof=1) / 16, gold["mean"], gold["var_of_mean"], "box screen reuse")
+    z_check(means.mean(0), means.var(0, ddof=1) / 16, gold["mean"], gold["var_of_mean"], "box screen reuse", mean_z=False)
+    total_check(means, gold["mean"], gold["var_of_mean"], "box screen reuse")
 
 
 def test_many_lights_moving_camera_unbiased_and_lower_error(device, lights):
