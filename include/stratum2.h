@@ -372,6 +372,8 @@ int  s2_render_noalloc(S2Context* ctx, const S2View* view, const S2RenderParams*
 #define S2_TRACE_ORDER_COHERENT 1u
 #define S2_SHADE_RECORDS_ON 0u
 #define S2_SHADE_RECORDS_OFF 1u
+#define S2_SHADOW_MERGE_ON    0u
+#define S2_SHADOW_MERGE_OFF   1u
 
 typedef struct S2Tuning {
     uint32_t wave_paths;          /* paths per wave when S2RenderParams.wave_paths is 0 (0 = 2^26) */
@@ -389,12 +391,17 @@ typedef struct S2Tuning {
                                      triangle at s2_build_bvh; S2_SHADE_RECORDS_OFF (1): gather through
                                      the instance and vertex buffers as the reference does.  Images are
                                      bit-identical either way. */
-    uint32_t reserved;
+    uint32_t shadow_merge;        /* S2_SHADOW_MERGE_ON (0, default): a bounce's shadow rays are traced by
+                                     the next bounce's traversal launch, after its closest hits (one
+                                     persistent launch for both queues; not with the radiance cache);
+                                     S2_SHADOW_MERGE_OFF (1): a separate any-hit launch after every shade.
+                                     Images are bit-identical either way. */
 } S2Tuning;
 
 int  s2_set_tuning(S2Context* ctx, const S2Tuning* tuning);
 int  s2_get_tuning(S2Context* ctx, S2Tuning* tuning);
-/* Coordinate search over wave size, triangle batch, vote, refill threshold and shading order: every candidate
+/* Coordinate search over wave size, triangle batch, vote, refill threshold, shading order, trace order and
+ * shadow merging: every candidate
  * renders `params` (its spp; frame seeds advance per trial) and the highest ray throughput wins.
  * The result is applied to `ctx` and written to `out` (may be NULL); `trials_out` (may be NULL)
  * receives the number of timed renders. */

@@ -53,6 +53,8 @@ TRACE_ORDER_QUEUE = 0
 TRACE_ORDER_COHERENT = 1
 SHADE_RECORDS_ON = 0
 SHADE_RECORDS_OFF = 1
+SHADOW_MERGE_ON = 0
+SHADOW_MERGE_OFF = 1
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -154,7 +156,7 @@ class S2CacheParams(C.Structure):
 class S2Tuning(C.Structure):
     _fields_ = [("wave_paths", C.c_uint32), ("trav_tris_per_step", C.c_uint32), ("trav_vote8", C.c_uint32),
                 ("refill_min", C.c_uint32), ("shade_order", C.c_uint32), ("trace_order", C.c_uint32),
-                ("shade_records", C.c_uint32), ("reserved", C.c_uint32)]
+                ("shade_records", C.c_uint32), ("shadow_merge", C.c_uint32)]
 
 
 TEMPORAL_REPROJECT, TEMPORAL_CHECK_NORMAL, TEMPORAL_CHECK_DEPTH = 1 << 0, 1 << 1, 1 << 2

@@ -1,7 +1,9 @@
 """Autotuner front end: runs s2_autotune (a coordinate search over the wavefront renderer's wave
 size, traversal triangle batch, triangle-step vote and lane-refill threshold, timed on the caller's
-own scene, view and render parameters; and whether to shade in material-sorted or queue order) and keeps the results in a JSON file keyed by GPU and
-workload, so later runs of the same workload apply them without searching."""
+own scene, view and render parameters; whether to shade in material-sorted or queue order, to
+sort continuation rays, and to trace each bounce's shadow rays in the next bounce's traversal
+launch) and keeps the results in a JSON file keyed by GPU and workload, so later runs of the same
+workload apply them without searching."""
 from __future__ import annotations
 
 import json
@@ -10,7 +12,7 @@ from pathlib import Path
 
 from . import _abi
 
-FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min", "shade_order", "trace_order")
+FIELDS = ("wave_paths", "trav_tris_per_step", "trav_vote8", "refill_min", "shade_order", "trace_order", "shadow_merge")
 
 
 def default_path() -> Path:

@@ -463,7 +463,8 @@ __global__ void __launch_bounds__(128, 8) k_diff_shade(const __grid_constant__ D
 // touches the path meanwhile) and, for the adjoint, sets its visibility bit.
 __global__ void __launch_bounds__(kTravBlock) k_diff_occlude(const __grid_constant__ DiffArgs A, const __grid_constant__ PTParams P,
                                                             DiffQueues Q) {
-    occlude_queue<false>(P, [&](uint32_t ray) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    occlude_queue<false>(P, C_SHADOW, stack, [&](uint32_t ray) {
         const float4 cc = P.sh_c[ray];
         const uint32_t path = __float_as_uint(P.sh_d[ray].w);
         const float4 l = A.path_l[path];

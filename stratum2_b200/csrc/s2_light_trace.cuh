@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(128) k_light_shade(PTParams P, uint32_t parity
         }
         const uint32_t qo_i = warp_append(&P.counters[1 - parity], alive);
         if (alive) { qo.s0[qo_i] = n0; qo.s1[qo_i] = n1; qo.s2[qo_i] = n2; qo.s3[qo_i] = n3; }
-        const uint32_t si = warp_append(&P.counters[C_SHADOW], shadow);
+        const uint32_t si = warp_append(&P.counters[sh_counter(P)], shadow);
         if (shadow) {
             P.sh_o[si] = make_float4(so_o.x, so_o.y, so_o.z, so_t);
             P.sh_d[si] = make_float4(so_d.x, so_d.y, so_d.z, __uint_as_float(so_pix));

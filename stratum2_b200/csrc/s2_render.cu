@@ -570,20 +570,32 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
         k_wave_finish<<<1, 32, 0, s>>>(P);
         launches += 1;
     }
+    // shadow rays of bounce b traced by bounce b + 1's k_trace (S2Tuning::shadow_merge; the cache's
+    // terminal contributions must land after the NEE of the same vertex, so not with the cache)
+    const bool merge = !cache && ctx->tuning.shadow_merge != S2_SHADOW_MERGE_OFF;
+    P.sh_merge = merge ? 1u : 0u;
     for (uint32_t done = 0; !light_trace && done < prm->spp; done += slots) {
         P.wave_base_sample = done;
         P.wave_samples = std::min(slots, prm->spp - done);
         const uint32_t n = P.wave_samples * pixels;
         if (cache) P.train_mod = std::max(1u, n / train_paths);
+        P.sh_parity = 0;
         k_raygen<<<(n + 255) / 256, 256, 0, s>>>(P);
         for (uint32_t b = 0; b < prm->max_path_length; ++b) {
             const uint32_t parity = b & 1u;
+            const uint32_t sh_prev = sh_counter(P);  // the previous bounce's shadow rays
+            P.sh_parity = merge ? (b & 1u) : 0u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
             P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
             if (P.ray_sorted) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(0);
-            if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
-            else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            if (merge && b > 0) {
+                if (count) k_trace<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
+                else k_trace<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
+            } else {
+                if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+                else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            }
             ev_end();
             if (sort) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(1);
@@ -596,11 +608,22 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
                 if (rc != S2_OK) return rc;
                 launches += 1;
             }
+            if (!merge) {
+                ev_begin(2);
+                if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+                else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+                ev_end();
+                launches += 1;
+            }
+            launches += 3;
+        }
+        if (merge) {  // the last bounce's shadow rays
+            k_occlude_setup<<<1, 32, 0, s>>>(P);
             ev_begin(2);
             if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
             else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
             ev_end();
-            launches += 4;
+            launches += 2;
         }
         if (cache) {
             // training: per-vertex targets from the finished training paths, one optimiser step
@@ -1127,9 +1150,10 @@ extern "C" int s2_set_tuning(S2Context* ctx, const S2Tuning* t) {
     if (!t) { std::memset(&ctx->tuning, 0, sizeof(ctx->tuning)); return S2_OK; }
     if (t->trav_tris_per_step > 32 || t->trav_vote8 > 9 || t->refill_min > 32 || (t->wave_paths && t->wave_paths < 1024) ||
         t->shade_order > S2_SHADE_ORDER_QUEUE || t->trace_order > S2_TRACE_ORDER_COHERENT ||
-        t->shade_records > S2_SHADE_RECORDS_OFF)
+        t->shade_records > S2_SHADE_RECORDS_OFF || t->shadow_merge > S2_SHADOW_MERGE_OFF)
         return set_error(ctx, S2_ERR_INVALID, "tuning out of range (tris_per_step <= 32, vote8 <= 9, refill_min <= 32, "
-                                              "wave_paths 0 or >= 1024, shade_order, trace_order and shade_records 0 or 1)");
+                                              "wave_paths 0 or >= 1024, shade_order, trace_order, shade_records and "
+                                              "shadow_merge 0 or 1)");
     ctx->tuning = *t;
     return S2_OK;
 }
@@ -1175,15 +1199,17 @@ extern "C" int s2_autotune(S2Context* ctx, const S2View* view, const S2RenderPar
     const uint32_t refills[] = {4, 8, 12, 16};
     const uint32_t sorts[] = {S2_SHADE_ORDER_MATERIAL, S2_SHADE_ORDER_QUEUE};
     const uint32_t traces[] = {S2_TRACE_ORDER_QUEUE, S2_TRACE_ORDER_COHERENT};
+    const uint32_t merges[] = {S2_SHADOW_MERGE_ON, S2_SHADOW_MERGE_OFF};
     for (int pass = 0; pass < 2; ++pass) {
-        for (int knob = 0; knob < 6; ++knob) {
+        for (int knob = 0; knob < 7; ++knob) {
             const uint32_t* vals = knob == 0 ? waves : knob == 1 ? tris : knob == 2 ? votes : knob == 3 ? refills
-                                 : knob == 4 ? sorts : traces;
+                                 : knob == 4 ? sorts : knob == 5 ? traces : merges;
             const int nv = knob == 0 ? 5 : knob == 1 ? 4 : knob == 2 ? 5 : knob == 3 ? 4 : 2;
             for (int v = 0; v < nv; ++v) {
                 S2Tuning t = best;
                 uint32_t* field = knob == 0 ? &t.wave_paths : knob == 1 ? &t.trav_tris_per_step
-                                : knob == 2 ? &t.trav_vote8 : knob == 3 ? &t.refill_min : knob == 4 ? &t.shade_order : &t.trace_order;
+                                : knob == 2 ? &t.trav_vote8 : knob == 3 ? &t.refill_min : knob == 4 ? &t.shade_order
+                                : knob == 5 ? &t.trace_order : &t.shadow_merge;
                 if (*field == vals[v]) continue;
                 *field = vals[v];
                 ctx->tuning = t;

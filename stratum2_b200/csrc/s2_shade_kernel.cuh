@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(128, kShadeMinBlocks<RESTIR, CACHE>) k_shade(P
             qo.s0[qi_out] = n0; qo.s1[qi_out] = n1; qo.s2[qi_out] = n2; qo.s3[qi_out] = n3;
             if (P.ray_sort_on) P.sort_keys[qi_out] = ray_key(s, f3(n0.x, n0.y, n0.z), f3(n1.x, n1.y, n1.z));
         }
-        const uint32_t si = warp_append(&P.counters[C_SHADOW], shadow);
+        const uint32_t si = warp_append(&P.counters[sh_counter(P)], shadow);
         if (shadow) {
             P.sh_o[si] = make_float4(so.o.x, so.o.y, so.o.z, so.tmax);
             P.sh_d[si] = make_float4(so.d.x, so.d.y, so.d.z, __uint_as_float(slot));

@@ -27,6 +27,7 @@ enum Counter : uint32_t {
     C_WORK_OCC = 4,
     C_CACHEQ = 5,   // radiance-cache queries appended this bounce
     C_TRAIN = 6,    // radiance-cache training vertices appended this wave
+    C_SHADOW1 = 7,  // shadow rays of odd bounces when shadow tracing is merged into the next trace
     C_COUNT = 8
 };
 enum Stat : uint32_t { S_EXT = 0, S_SHADOW = 1, S_NAN = 2, S_EXT_NODES = 3, S_EXT_TRIS = 4, S_SH_NODES = 5, S_SH_TRIS = 6, S_COUNT = 8 };
@@ -126,7 +127,13 @@ struct PTParams {
     uint32_t* sort_keys;
     uint32_t* sort_perm;
     uint32_t* sort_hist;   // kSortBuckets counters / offsets
+    // shadow rays traced by the next bounce's k_trace (S2Tuning::shadow_merge): the shade kernel
+    // counts its shadow rays in C_SHADOW1 when sh_parity is 1, so that the previous bounce's count
+    // stays readable while they are traced; sh_merge tells k_bounce_setup which count to retire
+    uint32_t sh_parity, sh_merge;
 };
+
+__host__ __device__ __forceinline__ uint32_t sh_counter(const PTParams& P) { return P.sh_parity ? C_SHADOW1 : C_SHADOW; }
 
 constexpr uint32_t kSortBuckets = 4096;  // k_sort_scan: 1024 threads x 4 buckets
 
@@ -204,6 +211,7 @@ __global__ void k_raygen(PTParams P) {
         P.counters[C_QUEUE0] = n;
         P.counters[C_QUEUE1] = 0;
         P.counters[C_SHADOW] = 0;
+        P.counters[C_SHADOW1] = 0;
         P.counters[C_WORK_EXT] = 0;
         P.counters[C_WORK_OCC] = 0;
         P.counters[C_CACHEQ] = 0;
@@ -247,20 +255,30 @@ __global__ void k_raygen(PTParams P) {
 }
 
 // ---------------------------------------------------------------- per-bounce bookkeeping
+// Counters before a bounce.  The previous bounce's shadow rays are retired into the statistics:
+// already traced, or (sh_merge) about to be traced by this bounce's k_trace from their own count,
+// while this bounce's shade appends to the other one.
 __global__ void k_bounce_setup(PTParams P, uint32_t parity, int first) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (!first) P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    const uint32_t cur = sh_counter(P), prev = P.sh_merge ? (cur == C_SHADOW ? C_SHADOW1 : C_SHADOW) : cur;
+    if (!first) P.stats[S_SHADOW] += P.counters[prev];
     P.stats[S_EXT] += P.counters[parity];
     P.counters[1 - parity] = 0;
-    P.counters[C_SHADOW] = 0;
+    P.counters[cur] = 0;
     P.counters[C_WORK_EXT] = 0;
     P.counters[C_WORK_OCC] = 0;
     P.counters[C_CACHEQ] = 0;
 }
+// Before the trailing k_occlude of a wave whose shadow tracing was merged into k_trace.
+__global__ void k_occlude_setup(PTParams P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    P.counters[C_WORK_OCC] = 0;
+}
 __global__ void k_wave_finish(PTParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    P.stats[S_SHADOW] += P.counters[sh_counter(P)];
     P.counters[C_SHADOW] = 0;
+    P.counters[C_SHADOW1] = 0;
 }
 
 // ---------------------------------------------------------------- batched streaming mode
@@ -387,9 +405,9 @@ S2D uint32_t refill(uint32_t* work, uint32_t count, uint32_t item, bool& exhaust
 }
 
 // Closest hit of the live path queue.  Hit record: {t, triangle record index, b1, b2}.
+// `stack`: the block's shared-memory traversal stacks (S2_STACK_SMEM entries per thread).
 template <bool COUNT>
-__global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ PTParams P, uint32_t parity) {
-    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+S2D void extend_queue(const PTParams& P, uint32_t parity, uint2* stack) {
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
     const uint32_t count = P.counters[parity];
     const PathQueue q = P.q[parity];
@@ -429,13 +447,19 @@ __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ P
     if (COUNT) add_fetches(P.stats, S_EXT_NODES, c);
 }
 
+template <bool COUNT>
+__global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ PTParams P, uint32_t parity) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    extend_queue<COUNT>(P, parity, stack);
+}
+
 // The persistent any-hit loop over the shadow queue (sh_o: origin + t_max, sh_d: direction): warps
 // refill lanes from the work counter; `on_visible(ray)` runs for every unoccluded ray.
+// `count_idx`: the counter holding the queue's length; `stack` as in extend_queue.
 template <bool COUNT, class OnVisible>
-S2D void occlude_queue(const PTParams& P, const OnVisible& on_visible) {
-    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+S2D void occlude_queue(const PTParams& P, uint32_t count_idx, uint2* stack, const OnVisible& on_visible) {
     uint2 lstack[S2_STACK_DEPTH - S2_STACK_SMEM];
-    const uint32_t count = P.counters[C_SHADOW];
+    const uint32_t count = P.counters[count_idx];
     TravCounters c{0, 0};
     TravRay r;
     TravState st;
@@ -470,7 +494,22 @@ S2D void occlude_queue(const PTParams& P, const OnVisible& on_visible) {
 // ray belongs to one accumulator slot (sh_d.w) and adds its contribution (sh_c) when unoccluded.
 template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_occlude(const __grid_constant__ PTParams P) {
-    occlude_queue<COUNT>(P, [&](uint32_t ray) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    occlude_queue<COUNT>(P, sh_counter(P), stack, [&](uint32_t ray) {
+        const float4 cc = P.sh_c[ray];
+        add_contrib(P, __float_as_uint(P.sh_d[ray].w), f3(cc.x, cc.y, cc.z));
+    });
+}
+
+// One bounce's closest hits followed by the previous bounce's shadow rays (count in counter
+// `sh_prev`), in one persistent launch: a warp whose extension work has run out takes shadow rays
+// while other warps finish their long extension rays, so the two launches' tails overlap.  The
+// contributions reach the accumulators before the next shade, as with a separate k_occlude.
+template <bool COUNT>
+__global__ void __launch_bounds__(kTravBlock, 9) k_trace(const __grid_constant__ PTParams P, uint32_t parity, uint32_t sh_prev) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    extend_queue<COUNT>(P, parity, stack);
+    occlude_queue<COUNT>(P, sh_prev, stack, [&](uint32_t ray) {
         const float4 cc = P.sh_c[ray];
         add_contrib(P, __float_as_uint(P.sh_d[ray].w), f3(cc.x, cc.y, cc.z));
     });

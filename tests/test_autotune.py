@@ -98,3 +98,33 @@ def test_shading_records_keep_the_image_bitwise(device, scene, flags):
     np.testing.assert_array_equal(out.albedo, ref.albedo)
     np.testing.assert_array_equal(out.visibility, ref.visibility)
     np.testing.assert_array_equal(out.depth, ref.depth)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags", [_abi.FLAG_LAMBERTIAN, 0, _abi.FLAG_RESTIR_DI])
+def test_shadow_merge_keeps_the_image_bitwise(device, flags):
+    """Tracing a bounce's shadow rays in the next bounce's traversal launch (S2Tuning.shadow_merge,
+    on by default) instead of a launch of their own changes when they are traced, not what they
+    add: every contribution still reaches its accumulator slot before the next shade, so images,
+    AOVs and ray counts are bit-identical, in one wave and in several."""
+    from stratum2_b200.scenegen import terrain_scene
+    wl = terrain_scene(seed=2, grid=128, spheres=8, sphere_level=2, width=64, height=36, tiles=2, area_lights=2)
+    device.upload_scene(wl.scene)
+    p = device.default_params()
+    p.spp, p.min_path_length, p.max_path_length, p.flags, p.frame_seed = 8, 1, 7, flags | _abi.FLAG_PIXEL_JITTER, 23
+    p.restir_candidates = 4
+    for wave in (0, 4096):
+        off = _abi.S2Tuning()
+        off.wave_paths, off.shadow_merge = wave, _abi.SHADOW_MERGE_OFF
+        device.set_tuning(off)
+        ref = device.render(wl.view, wl.width, wl.height, params=p)
+        on = _abi.S2Tuning()
+        on.wave_paths = wave
+        device.set_tuning(on)
+        out = device.render(wl.view, wl.width, wl.height, params=p)
+        np.testing.assert_array_equal(out.radiance, ref.radiance)
+        np.testing.assert_array_equal(out.albedo, ref.albedo)
+        assert out.stats.extension_rays == ref.stats.extension_rays
+        assert out.stats.shadow_rays == ref.stats.shadow_rays > 0
+        assert out.stats.kernel_launches < ref.stats.kernel_launches
+    device.set_tuning(None)
