@@ -37,6 +37,7 @@ WORKLOAD = ("terrain 1024^2 grid (2.09M tris) + 64 icospheres (1.31M tris), GLTF
 # fetch + one 48-byte record per triangle fetch, with the fetch counts of the sequential
 # nearest-first BVH8 walk (the counting run).  NODE_PAYLOAD is the node's 80 bytes of content.
 NODE_BYTES, NODE_PAYLOAD, TRI_BYTES, RAY_BYTES, HIT_BYTES = 128, 80, 48, 32, 16
+SHADOW_RAY_BYTES = 64  # shadow-ray record read: origin + t_max, direction + slot, contribution
 # Algorithmic bytes of shading: a path's 64-byte state read, the 64-byte material record, 3 x (4-byte
 # index + 32 bytes of position/normal/uv), the 64-byte state written for a continuation ray, and a
 # 48-byte shadow-ray record per NEE sample.
@@ -262,23 +263,39 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     payload_per_ray = RAY_BYTES + HIT_BYTES + NODE_PAYLOAD * n_node + TRI_BYTES * n_tri
     rays_per_launch = ext_rays / max(ext_launches, 1)
     avg_launch_s = ext_ms / 1e3 / max(ext_launches, 1)
-    achieved = bytes_per_ray * rays_per_launch / avg_launch_s / 1e9
+    # with shadow merging (the default) the timed traversal launches also trace the previous
+    # bounce's shadow rays (the last bounce casts none: NEE needs a vertex below the maximum length)
+    merged = dev.get_tuning().shadow_merge == _abi.SHADOW_MERGE_ON
+    n_sh_node = cnt.shadow_node_fetches / max(cnt.shadow_rays, 1)
+    n_sh_tri = cnt.shadow_tri_fetches / max(cnt.shadow_rays, 1)
+    sh_bytes_per_ray = SHADOW_RAY_BYTES + NODE_BYTES * n_sh_node + TRI_BYTES * n_sh_tri
+    sh_rays = sum(s.shadow_rays for s in stats) if merged else 0
+    launch_bytes = (bytes_per_ray * ext_rays + sh_bytes_per_ray * sh_rays) / max(ext_launches, 1)
+    achieved = launch_bytes / avg_launch_s / 1e9
     pk = peaks()
-    dominant = max([("k_extend", ext_ms), ("k_shade", sh_ms), ("k_occlude", oc_ms)], key=lambda x: x[1])[0]
-    roof = {"kernel": "k_extend", "dominant_kernel": dominant, "bound": "hbm", "achieved": achieved,
+    trace_name = "k_trace (closest hits + the previous bounce's shadow rays)" if merged else "k_extend"
+    dominant = max([(trace_name, ext_ms), ("k_shade", sh_ms), ("k_occlude", oc_ms)], key=lambda x: x[1])[0]
+    roof = {"kernel": trace_name, "dominant_kernel": dominant, "bound": "hbm", "achieved": achieved,
             "peak": pk["hbm_gbs"], "peak_source": pk["source"] + " copy bandwidth", "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"],
             "traffic": None,
             "traffic_note": "DRAM bytes are not measurable inside the timed run; the ncu figures per launch are "
                             "in profiles/k_extend_terrain.md",
-            "algorithmic_bytes_per_launch": bytes_per_ray * rays_per_launch,
+            "algorithmic_bytes_per_launch": launch_bytes,
             "bytes_per_ray": bytes_per_ray,
-            "byte_model": "32 ray + 16 hit + 128 per node fetch + 48 per triangle fetch; fetch counts of the "
+            "shadow_bytes_per_ray": sh_bytes_per_ray if merged else None,
+            "byte_model": "extension ray: 32 ray + 16 hit + 128 per node fetch + 48 per triangle fetch; shadow ray "
+                          "(merged launches): 64 record + 128 per node + 48 per triangle fetch; fetch counts of the "
                           "sequential nearest-first BVH8 walk (equal to the CPU BVH8 walker's)",
-            "frac_node_payload_80B": achieved * payload_per_ray / bytes_per_ray / pk["hbm_gbs"],
+            "frac_node_payload_80B": (achieved * payload_per_ray / bytes_per_ray / pk["hbm_gbs"]) if not merged else None,
             "node_fetches_per_ray": n_node,
             "tri_fetches_per_ray": n_tri,
-            "avg_launch_ms": avg_launch_s * 1e3}
+            "shadow_node_fetches_per_ray": n_sh_node,
+            "avg_launch_ms": avg_launch_s * 1e3,
+            "reading": "the byte model counts every node and triangle fetch as a line from HBM; a fraction near "
+                       "or above 1 means most fetches are served from L1/L2 (the camera rays of one pixel's "
+                       "samples traverse together), and the kernel's measured limit is instruction issue "
+                       "(profiles/k_extend_terrain.md)"}
     # shading: the measurement plan's byte model per shaded path vertex (state in, hit, material
     # record, three indices + attributes), per continuation (state out) and per shadow ray record
     sh_launches = sum(s.shade_launches for s in stats)
@@ -298,7 +315,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "bvh8_nodes": int(dev.bvh_stats.node_count),
             "tuning": {"values": (tuning or {}).get("tuning", "defaults"), "autotune_trials": (tuning or {}).get("trials", 0)},
             "mpaths_per_s": paths / ms / 1e3,
-            "kernel_ms_per_step": {"k_extend": ext_ms / args.steps, "k_shade": sh_ms / args.steps,
+            "kernel_ms_per_step": {("k_trace" if merged else "k_extend"): ext_ms / args.steps, "k_shade": sh_ms / args.steps,
                                    "k_occlude": oc_ms / args.steps},
             "gpu_launches": int(sum(s.kernel_launches for s in stats)),
             "roofline": roof,
@@ -682,6 +699,9 @@ def main():
                     help="run only the time-to-relMSE comparison on the learned-cache scene and print it")
     ap.add_argument("--single-frame", type=int, default=0, metavar="SPP",
                     help="render one frame of the workload with SPP samples and exit (profiling)")
+    ap.add_argument("--frame-size", default="", metavar="WxH",
+                    help="with --single-frame: the frame's extent (default: the workload's 1920x1080); "
+                         "the same scene and camera, for small profiling captures")
     ap.add_argument("--cache-kernels", type=int, default=0, metavar="STEPS",
                     help="run the radiance-cache inference and training kernels STEPS times and exit (profiling)")
     ap.add_argument("--cached-frames", type=int, default=0, metavar="N",
@@ -735,7 +755,8 @@ def main():
         from stratum2_b200 import Device
         from stratum2_b200.scenegen import terrain_scene
         dev = Device(0)
-        wl = terrain_scene()
+        w, h = (int(v) for v in args.frame_size.split("x")) if args.frame_size else (1920, 1080)
+        wl = terrain_scene(width=w, height=h)
         dev.upload_scene(wl.scene)
         r = dev.render(wl.view, wl.width, wl.height, params=params(dev, args.single_frame, 0))
         print(json.dumps({"gpu_ms": r.stats.gpu_ms, "extension_rays": r.stats.extension_rays,

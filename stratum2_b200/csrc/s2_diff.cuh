@@ -111,7 +111,7 @@ struct DiffArgs {
     uint32_t min_len, max_len, flags, frame_seed;
     float out_scale;                  // 2^exposure / spp
     float4* image;                    // forward: mean radiance * 2^exposure per pixel
-    float4* path_l;                   // forward: radiance of every path, [sample][pixel]
+    float4* path_l;                   // forward: radiance of every path, [pixel][sample]
     const float4* d_image;            // adjoint: dLoss / d image
     float4* grad;                     // adjoint: texel gradients of every image, concatenated
     const uint32_t* grad_offset;      // first texel of image k in `grad`
@@ -352,17 +352,19 @@ S2D void diff_count(const DiffArgs& A, uint32_t ext, uint32_t shd, bool overflow
     if (overflow) atomicOr(A.status, 1);
 }
 
-// Camera paths base .. base + n - 1 into queue 0.  The forward zeroes each path's radiance in
-// path_l and its visibility words; the adjoint skips paths of pixels whose adjoint is zero, as
-// their replay adds nothing.
+// Camera paths base .. base + n - 1 into queue 0.  Path ids run over pixels (row-major), then
+// samples (path = pixel x spp + sample), so a warp takes the samples of one or a few neighbouring
+// pixels, their camera rays traverse together and a pixel's radiances are contiguous in path_l.
+// The forward zeroes each path's radiance in path_l and its visibility words; the adjoint skips
+// paths of pixels whose adjoint is zero, as their replay adds nothing.
 __global__ void k_diff_gen(const __grid_constant__ DiffArgs A, PTParams P, DiffQueues Q, uint32_t base, uint32_t n, int adj) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool want = false;
     uint32_t path = 0, px = 0, py = 0, k = 0;
     if (i < n) {
         path = base + i;
-        k = path / A.pixels;
-        const uint32_t pix = path - k * A.pixels;
+        const uint32_t pix = path / A.spp;
+        k = path - pix * A.spp;
         px = pix % A.width; py = pix / A.width;
         want = true;
         if (adj) {
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(128, 8) k_diff_shade(const __grid_constant__ D
             }
             float3 ltot = f3(0.f), delta = f3(0.f);
             if (adj) {
-                const uint32_t pix = path % A.pixels;
+                const uint32_t pix = path / A.spp;
                 const float4 lt = A.path_l[path], d = A.d_image[pix];
                 ltot = f3(lt.x, lt.y, lt.z);
                 delta = f3(d.x, d.y, d.z) * A.out_scale;
@@ -504,7 +506,7 @@ __global__ void k_diff_resolve(const __grid_constant__ DiffArgs A) {
     if (pix >= A.pixels) return;
     float3 sum = f3(0.f);
     for (uint32_t k = 0; k < A.spp; ++k) {
-        const float4 l = A.path_l[(size_t)k * A.pixels + pix];
+        const float4 l = A.path_l[(size_t)pix * A.spp + k];
         sum = sum + f3(l.x, l.y, l.z);
     }
     A.image[pix] = make_float4(sum.x * A.out_scale, sum.y * A.out_scale, sum.z * A.out_scale, 1.f);

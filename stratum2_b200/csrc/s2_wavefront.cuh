@@ -218,14 +218,14 @@ __global__ void k_raygen(PTParams P) {
         P.counters[C_TRAIN] = 0;
     }
     if (i >= n) return;
-    // Queue order: image row, then sample, then column.  All samples of a row are traced together,
-    // so the BVH region under a few rows stays in L2 instead of every sample sweeping the whole
-    // image (and the whole visible BVH) again; a warp still takes 32 neighbouring pixels.  The
-    // accumulator slot keeps the sample-major layout that k_reduce sums.
-    const uint32_t row_rays = P.wave_samples * P.width;
-    const uint32_t py = i / row_rays, rem = i - py * row_rays;
-    const uint32_t k = rem / P.width, px = rem - k * P.width;
-    const uint32_t slot = k * P.pixels + py * P.width + px;
+    // Queue order: pixel (row-major), then sample.  A warp takes 32 samples of one pixel (or, with
+    // fewer samples per wave, the samples of neighbouring pixels): camera rays through one pixel
+    // visit nearly the same BVH nodes, so the warp's lanes step through the traversal together,
+    // and the pixels in flight at any time cover a few image rows, whose BVH region stays in L2.
+    // The accumulator slot keeps the sample-major layout that k_reduce sums.
+    const uint32_t pix = i / P.wave_samples, k = i - pix * P.wave_samples;
+    const uint32_t py = pix / P.width, px = pix - py * P.width;
+    const uint32_t slot = k * P.pixels + pix;
     const uint32_t sample = P.wave_base_sample + k;
     Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
     float ox = 0.5f, oy = 0.5f;
@@ -333,13 +333,11 @@ S2D void regen_one(const PTParams& P, uint32_t parity, uint32_t fill, uint32_t i
     while (v + 1 < P.nviews && P.views[v + 1].path_offset <= id) ++v;
     const ViewEntry& V = P.views[v];
     const unsigned long long local = id - V.path_offset;
-    // path order inside a view: image row, then sample, then column (as k_raygen), so the samples
-    // of a row are traced together and the BVH under a few rows stays in L2
-    const unsigned long long row_paths = (unsigned long long)P.view_spp * V.width;
-    const uint32_t py = (uint32_t)(local / row_paths);
-    const uint32_t rem = (uint32_t)(local - (unsigned long long)py * row_paths);
-    const uint32_t sample = rem / V.width, px = rem - sample * V.width;
-    const uint32_t pix = py * V.width + px;
+    // path order inside a view: pixel (row-major), then sample (as k_raygen): a warp takes the
+    // samples of one or a few neighbouring pixels, whose camera rays traverse nearly the same nodes
+    const uint32_t pix = (uint32_t)(local / P.view_spp);
+    const uint32_t sample = (uint32_t)(local - (unsigned long long)pix * P.view_spp);
+    const uint32_t py = pix / V.width, px = pix - py * V.width;
     Rng rng = make_rng(px, py, P.frame_seed + sample, (P.flags & S2F_PCG32) != 0);
     float ox = 0.5f, oy = 0.5f;
     if (P.flags & S2F_JITTER) { const float4 f = rng.next_float(); ox = f.x; oy = f.y; }
