@@ -140,7 +140,7 @@ S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint
     const uint32_t xn0 = nx ? xhi0 : xlo0, xn1 = nx ? xhi1 : xlo1, xf0 = nx ? xlo0 : xhi0, xf1 = nx ? xlo1 : xhi1;
     const uint32_t yn0 = ny ? yhi0 : ylo0, yn1 = ny ? yhi1 : ylo1, yf0 = ny ? ylo0 : yhi0, yf1 = ny ? ylo1 : yhi1;
     const uint32_t zn0 = nz ? zhi0 : zlo0, zn1 = nz ? zhi1 : zlo1, zf0 = nz ? zlo0 : zhi0, zf1 = nz ? zlo1 : zhi1;
-    hits = 0; trimask = 0;
+    uint32_t m = 0;  // children whose box the ray segment overlaps, in slot order
 #pragma unroll
     for (uint32_t s = 0; s < 8; ++s) {
         const uint32_t w = s < 4 ? 0 : 1, i = s & 3;
@@ -153,15 +153,22 @@ S2D void intersect_node(const TravRay& r, const uint4* __restrict__ nodes4, uint
         // min(tf, tmax) * c == min(tf * c, tmax * c): the padding also covers tmax
         const float tn = max3f(tnx, tny, fmaxf(tnz, r.tmin));
         const float tf = min3f(tfx, tfy, fminf(tfz, tmax)) * 1.0000004f;
-        if (tn <= tf) {
-            if ((imask >> s) & 1u) {
-                hits |= 1u << (s ^ r.oct);
-            } else {
-                const uint32_t meta = extract_byte(w ? meta_hi : meta_lo, i);
-                const uint32_t cnt = meta >> 5, off = meta & 31u;
-                trimask |= ((1u << cnt) - 1u) << off;
-            }
-        }
+        if (tn <= tf) m |= 1u << s;
+    }
+    // internal children: bit s ^ oct (the octant order), by three conditional swaps of bit groups
+    uint32_t h = m & imask;
+    if (r.oct & 1u) h = ((h & 0x55u) << 1) | ((h >> 1) & 0x55u);
+    if (r.oct & 2u) h = ((h & 0x33u) << 2) | ((h >> 2) & 0x33u);
+    if (r.oct & 4u) h = ((h & 0x0fu) << 4) | ((h >> 4) & 0x0fu);
+    hits = h;
+    // leaf children: their triangle ranges (usually one or two per node)
+    trimask = 0;
+    uint32_t leaf = m & ~imask & 0xffu;
+    while (leaf) {
+        const uint32_t s = __ffs(leaf) - 1;
+        leaf &= leaf - 1;
+        const uint32_t meta = extract_byte(s < 4 ? meta_lo : meta_hi, s & 3u);
+        trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
     }
 }
 
