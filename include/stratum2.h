@@ -604,6 +604,15 @@ int  s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2Tonemap
                                                       debug_camera_vertices / debug_light_vertices */
 #define S2_VCM_FLAG_DEBUG_UNWEIGHTED    (1u << 2)  /* with DEBUG_PATHS and not gDebugPathWeights: every
                                                       MIS weight 1 */
+#define S2_VCM_FLAG_DI_RIS              (1u << 3)  /* gDIReservoirFlags eRIS: the direct illumination of
+                                                      camera vertices resamples di_candidates light
+                                                      samples by lum(Le) |cos| G and traces one shadow
+                                                      ray for the chosen one (vcm.slang:343-366) */
+#define S2_VCM_FLAG_DI_REUSE            (1u << 4)  /* with DI_RIS, eReuse: each camera vertex also
+                                                      resamples a reservoir of the previous iteration
+                                                      (or call) found in a world-space hash grid near it
+                                                      and stores its own (vcm.slang:296-340, 368-386);
+                                                      not with PPM or light tracing */
 
 typedef struct S2VcmParams {
     uint32_t algorithm;              /* S2_VCM_PATH_TRACE .. S2_VCM_VCM (default S2_VCM_BPT, VCM.hpp:66) */
@@ -621,7 +630,10 @@ typedef struct S2VcmParams {
     float exposure;                  /* output x 2^exposure */
     uint16_t debug_camera_vertices;  /* mDebugPathLengths (compat/vcm.h:49-55) */
     uint16_t debug_light_vertices;
-    uint32_t reserved[3];
+    uint32_t di_candidates;          /* mDIReservoirSampleCount (default 32, VCM.cpp:33), 1..1024 */
+    float di_max_m;                  /* mDIReservoirMaxM (default 3, VCM.cpp:34): stored M is capped
+                                        at di_max_m x di_candidates */
+    uint32_t reserved;
 } S2VcmParams;
 
 void s2_default_vcm_params(S2VcmParams* p);

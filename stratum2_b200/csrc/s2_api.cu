@@ -300,6 +300,7 @@ extern "C" void s2_destroy(S2Context* ctx) {
     destroy_render_state(ctx);
     destroy_cache_state(ctx);
     destroy_post_state(ctx);
+    destroy_vcm_state(ctx);
     free_bufs(ctx->scene_bufs);
     free_bufs(ctx->bvh_bufs);
     if (ctx->status_dev) cudaFree(ctx->status_dev);
@@ -346,6 +347,7 @@ extern "C" int s2_scene_upload(S2Context* ctx, const S2SceneDesc* d) {
     free_bufs(ctx->bvh_bufs);
     ctx->has_scene = ctx->has_bvh = false;
     destroy_render_state(ctx);
+    destroy_vcm_state(ctx);  // stored reservoirs name the old scene's instances
     ctx->scene = DevScene{};
     const uint32_t ni = d->instance_count;
 

@@ -20,6 +20,7 @@ struct DevBuf {
 struct RenderState;  // wavefront queues and accumulators (s2_render.cu)
 struct CacheState;   // learned radiance cache parameters and optimiser state (s2_cache.cu)
 struct PostState;    // temporal-accumulation history and tonemap scratch (s2_post.cu)
+struct VcmState;     // the VCM renderer's direct-illumination reservoir grids (s2_vcm.cu)
 
 struct HostImage {
     uint32_t w = 0, h = 0;
@@ -58,6 +59,7 @@ struct S2Context {
     s2::RenderState* render = nullptr;
     s2::CacheState* cache = nullptr;
     s2::PostState* post = nullptr;
+    s2::VcmState* vcm = nullptr;
     S2Tuning tuning{};                      // wavefront renderer tuning (zeros = defaults)
     int* status_dev = nullptr;              // device status word (stack/queue overflow, timeouts)
 };
@@ -70,6 +72,7 @@ void free_bufs(std::vector<DevBuf>& bufs);
 void destroy_render_state(S2Context* ctx);
 void destroy_cache_state(S2Context* ctx);
 void destroy_post_state(S2Context* ctx);
+void destroy_vcm_state(S2Context* ctx);
 // baked shading records of the current BVH (s2_render.cu), allocated into `owner`
 int bake_shading_records(S2Context* ctx, std::vector<DevBuf>& owner);
 // radiance cache entry points used by the renderer (s2_cache.cu)

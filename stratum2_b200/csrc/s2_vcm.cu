@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "s2_context.h"
@@ -31,7 +32,8 @@ namespace {
 
 constexpr uint32_t kVcmRenderFlags = S2_FLAG_LAMBERTIAN | S2_FLAG_PCG32 | S2_FLAG_NO_RR | S2_FLAG_SHADING_NORMALS_OFF |
                                      S2_FLAG_ALPHA_TEST_OFF | S2_FLAG_NORMAL_MAPS_OFF | S2_FLAG_LIGHT_POWER_PICK;
-constexpr uint32_t kVcmOwnFlags = S2_VCM_FLAG_LIGHT_VERTEX_CACHE | S2_VCM_FLAG_DEBUG_PATHS | S2_VCM_FLAG_DEBUG_UNWEIGHTED;
+constexpr uint32_t kVcmOwnFlags = S2_VCM_FLAG_LIGHT_VERTEX_CACHE | S2_VCM_FLAG_DEBUG_PATHS | S2_VCM_FLAG_DEBUG_UNWEIGHTED |
+                                   S2_VCM_FLAG_DI_RIS | S2_VCM_FLAG_DI_REUSE;
 
 void invert_affine(const float* m, float* out) {
     // inverse of a row-major 3x4 rigid (or scaled) transform
@@ -49,6 +51,61 @@ void invert_affine(const float* m, float* out) {
     }
 }
 
+// The world-space grids of the direct-illumination reservoirs (GpuHashGrid, src/App/GpuHashGrid.cpp:
+// 17-111, as the path tracer's reuse grids): appended to by one iteration's camera pass, read by
+// the next one's.
+struct DiGrid {
+    std::vector<DevBuf> bufs;
+    HashGridDev g{};
+    unsigned long long *keys_in = nullptr, *keys_out = nullptr;
+    uint32_t* vals_in = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    int end_bit = 64;
+};
+
+int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size) {
+    if (G.g.checksums && G.g.cell_count == cells && G.g.max_size >= size) return S2_OK;
+    free_bufs(G.bufs);
+    G.g = HashGridDev{};
+    HashGridDev g{};
+    auto al = [&](size_t bytes) { return dev_alloc(ctx, G.bufs, bytes); };
+    g.checksums = (uint32_t*)al(sizeof(uint32_t) * cells);
+    g.cell_counters = (uint32_t*)al(sizeof(uint32_t) * cells);
+    g.other = (uint32_t*)al(sizeof(uint32_t) * 4);
+    g.append_indices = (uint2*)al(sizeof(uint2) * size);
+    g.data = (ReservoirRecord*)al(sizeof(ReservoirRecord) * size);
+    g.indices = (uint32_t*)al(sizeof(uint32_t) * cells);
+    g.data_indices = (uint32_t*)al(sizeof(uint32_t) * size);
+    G.keys_in = (unsigned long long*)al(sizeof(unsigned long long) * size);
+    G.keys_out = (unsigned long long*)al(sizeof(unsigned long long) * size);
+    G.vals_in = (uint32_t*)al(sizeof(uint32_t) * size);
+    int cell_bits = 1;  // keys: cell above a 32-bit content hash (unused slots take cell `cells`)
+    while (cell_bits < 32 && (1ull << cell_bits) <= cells) ++cell_bits;
+    G.end_bit = 32 + cell_bits;
+    G.sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, G.sort_bytes, G.keys_in, G.keys_out, G.vals_in, g.data_indices, (int)size, 0,
+                                    G.end_bit, ctx->stream);
+    G.sort_tmp = al(std::max<size_t>(G.sort_bytes, 16));
+    for (auto& b : G.bufs) if (!b.ptr) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    if (G.bufs.size() != 11) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    g.cell_count = cells;
+    g.max_size = size;
+    G.g = g;
+    return S2_OK;
+}
+
+// Cell offsets by a scan, records sorted by (cell, content); returns the launches issued.
+uint32_t build_di_grid(const DiGrid& G, cudaStream_t s) {
+    const HashGridDev& g = G.g;
+    k_hg_scan<<<1, kHgScanThreads, 0, s>>>(g);
+    k_hg_keys<<<(g.max_size + 255) / 256, 256, 0, s>>>(g, G.keys_in, G.vals_in);
+    size_t bytes = G.sort_bytes;
+    cub::DeviceRadixSort::SortPairs(G.sort_tmp, bytes, G.keys_in, G.keys_out, G.vals_in, g.data_indices, (int)g.max_size, 0,
+                                    G.end_bit, s);
+    return 3;
+}
+
 template <bool LAMBERT>
 void launch_light(const vk::VcmArgs& A, cudaStream_t s) {
     const uint32_t blocks = std::min<uint32_t>((A.n_light + 127) / 128, 148u * 8u);
@@ -61,6 +118,22 @@ void launch_camera(const vk::VcmArgs& A, cudaStream_t s) {
 
 }  // namespace
 
+namespace s2 {
+// Kept in the context between calls: the reservoir grids of the last iteration, so that a call's
+// first iteration reuses the previous call's reservoirs (the reference's frame-to-frame reuse).
+struct VcmState {
+    DiGrid grid[2];
+    uint32_t cur = 0;
+    bool prev_valid = false;
+};
+void destroy_vcm_state(S2Context* ctx) {
+    if (!ctx || !ctx->vcm) return;
+    for (auto& g : ctx->vcm->grid) free_bufs(g.bufs);
+    delete ctx->vcm;
+    ctx->vcm = nullptr;
+}
+}  // namespace s2
+
 extern "C" void s2_default_vcm_params(S2VcmParams* p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
@@ -72,6 +145,8 @@ extern "C" void s2_default_vcm_params(S2VcmParams* p) {
     p->light_path_fraction = 1.f;                    // VCM.hpp:67
     p->merge_radius_factor = 0.025f;                 // VCM.hpp:59-60
     p->merge_radius_alpha = 0.01f;
+    p->di_candidates = 32;                           // VCM.cpp:33-34
+    p->di_max_m = 3.f;
 }
 
 extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmParams* prm, const S2Aovs* out, int out_on_host,
@@ -93,6 +168,15 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     if (lvc && algo != S2_VCM_BPT) return set_error(ctx, S2_ERR_UNSUPPORTED, "the light vertex cache serves BPT only");
     if (!(prm->light_path_fraction > 0.f) || !std::isfinite(prm->light_path_fraction))
         return set_error(ctx, S2_ERR_INVALID, "light_path_fraction must be finite and > 0");
+    const bool di_ris = (prm->vcm_flags & S2_VCM_FLAG_DI_RIS) != 0;
+    if ((prm->vcm_flags & S2_VCM_FLAG_DI_REUSE) && !di_ris) return set_error(ctx, S2_ERR_INVALID, "DI_REUSE needs DI_RIS");
+    if (di_ris && (prm->di_candidates < 1 || prm->di_candidates > 1024))
+        return set_error(ctx, S2_ERR_INVALID, "di_candidates must be in 1..1024");
+    // the camera vertices' direct illumination exists in path tracing, BPT and VCM only
+    const bool di_reuse = (prm->vcm_flags & S2_VCM_FLAG_DI_REUSE) && algo != S2_VCM_PPM && algo != S2_VCM_LIGHT_TRACE &&
+                          algo != S2_VCM_BPM;
+    if (di_reuse && !(prm->di_max_m > 0.f && std::isfinite(prm->di_max_m)))
+        return set_error(ctx, S2_ERR_INVALID, "di_max_m must be finite and > 0");
     const bool use_vc = algo == S2_VCM_BPT || algo == S2_VCM_VCM;
     const bool use_vm = algo == S2_VCM_PPM || algo == S2_VCM_BPM || algo == S2_VCM_VCM;
     const float R = ctx->scene.scene_sphere.w;
@@ -139,6 +223,29 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     A.debug_light = prm->debug_light_vertices;
     A.lv_slots = slots;
     A.status = ctx->status_dev;
+    A.di_ris = di_ris ? 1u : 0u;
+    A.di_reuse = di_reuse ? 1u : 0u;
+    A.di_m = prm->di_candidates;
+    A.di_max_m = prm->di_max_m;
+    s2::VcmState* vs = nullptr;
+    if (di_reuse) {
+        if (!ctx->vcm) ctx->vcm = new (std::nothrow) s2::VcmState();
+        vs = ctx->vcm;
+        if (!vs) return set_error(ctx, S2_ERR_OOM, "VCM state allocation failed");
+        // VCM.cpp:26, 490-499: 100,000 cells of at least 0.1, one record per camera vertex
+        const uint32_t cells = 100000u;
+        const uint32_t size = (uint32_t)std::min<uint64_t>((uint64_t)pixels * std::max(1u, prm->max_path_length - 1), 1u << 24);
+        for (auto& g : vs->grid) {
+            const int rc0 = ensure_di_grid(ctx, g, cells, size);
+            if (rc0 != S2_OK) { vs->prev_valid = false; return set_error(ctx, rc0, "reservoir grid allocation failed"); }
+            g.g.min_cell_size = 0.1f;
+            g.g.cell_pixel_radius = 0.f;
+            g.g.camera_position = make_float3(view->camera_to_world[3], view->camera_to_world[7], view->camera_to_world[11]);
+            g.g.distance_scale = 0.f;  // tan(0): cells of the minimum size everywhere
+        }
+    } else if (ctx->vcm) {
+        ctx->vcm->prev_valid = false;  // a call without reuse drops the grids (VCM.cpp:231-235)
+    }
 
     std::vector<DevBuf> tmp;
     auto fail = [&](int code, const char* msg) { cudaStreamSynchronize(s); free_bufs(tmp); return set_error(ctx, code, msg); };
@@ -237,8 +344,24 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
             }
         }
         if (!A.light_trace_only) {
+            DiGrid* cur = nullptr;
+            if (di_reuse) {
+                cur = &vs->grid[vs->cur];
+                const HashGridDev& g = cur->g;
+                cudaMemsetAsync(g.checksums, 0, sizeof(uint32_t) * g.cell_count, s);  // GpuHashGrid::clear
+                cudaMemsetAsync(g.cell_counters, 0, sizeof(uint32_t) * g.cell_count, s);
+                cudaMemsetAsync(g.other, 0, sizeof(uint32_t) * 4, s);
+                A.di_cur = g;
+                A.di_prev = vs->grid[vs->cur ^ 1].g;
+                A.di_prev_valid = vs->prev_valid ? 1u : 0u;
+            }
             if (lam) launch_camera<true>(A, s); else launch_camera<false>(A, s);
             launches += 1;
+            if (cur) {  // this iteration's reservoirs become the next one's previous grid
+                launches += build_di_grid(*cur, s);
+                vs->cur ^= 1u;
+                vs->prev_valid = true;
+            }
         }
     }
     if (rad) {

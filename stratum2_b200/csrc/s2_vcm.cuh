@@ -64,6 +64,11 @@ struct VcmArgs {
     uint32_t write_aovs;
     unsigned long long* counts;    // [0] extension rays, [1] shadow rays, [2] NaN paths
     int* status;                   // bit 0: traversal stack overflow
+    // direct-illumination reservoirs (S2_VCM_FLAG_DI_RIS / _DI_REUSE): candidates, M cap, and the
+    // world-space grids of this iteration's reservoirs (appended) and the previous one's (read)
+    uint32_t di_ris, di_reuse, di_m, di_prev_valid;
+    float di_max_m;
+    HashGridDev di_cur, di_prev;
 };
 
 // Mis() (compat/vcm.h:9-11): power heuristic with exponent 2.
@@ -397,6 +402,114 @@ S2D float3 vcm_merge(const VcmArgs& A, const Mat& m, const SD& sd, float3 in, fl
     return sum;
 }
 
+// ---------------------------------------------------------------- direct-illumination reservoirs
+// ReservoirStateDI (vcm.slang:251-340): resampled light samples with the target pdf
+// lum(Le) |n_s . w| G, no BSDF.  A sample is its four random numbers; `r` receives it evaluated at
+// (pos, ns).  GetTargetPdf<true> also traces the sample's visibility from (pos, gn).
+S2D float vcm_di_target(const VcmArgs& A, VcmTrace& T, float3 pos, float3 ns, float3 gn, float4 x, bool sn, bool vis,
+                        Illum& r) {
+    r = sample_illum(A.scene, x, pos, sn);
+    if (!(r.pdf > 0.f) || !any_pos(r.radiance)) return 0.f;
+    const float g = r.finite ? r.cos_light / (r.dist * r.dist) : 1.f;
+    const float t = luminance(r.radiance) * fabsf(dot(ns, r.dir)) * g;
+    if (vis && t > 0.f && !vcm_visible(A, T, ray_offset(pos, gn, r.dir), r.dir, r.dist * 0.99f)) return 0.f;
+    return t;
+}
+
+struct VcmReservoir {
+    float4 rnd;      // the selected sample
+    Illum r;         // it, evaluated at the camera vertex
+    float phat;      // its target pdf (0 when occluded)
+    float wsum;      // total resampling weight
+    float M;
+    S2D float iw() const { return phat > 0.f ? wsum / phat : 0.f; }  // mIntegrationWeight
+};
+
+// Reuse (vcm.slang:296-340): resamples the stored reservoir q into `res` with the pairwise MIS
+// weights over the two domains' visibility-aware target pdfs.
+S2D void vcm_di_reuse(const VcmArgs& A, VcmTrace& T, const SD& sd, const ReservoirRecord& q, VcmReservoir& res, Rng& rng,
+                      bool sn) {
+    if (!(q.M > 0.f)) return;
+    const SD sdq = make_shading_local(A.scene, q.instance, q.primitive, q.local_pos, sn);
+    Illum tmp, nr;
+    const float phat_i_old = vcm_di_target(A, T, sdq.pos, sdq.n, sdq.gn, res.rnd, sn, true, tmp);  // current sample, q's domain
+    const float phat_new = vcm_di_target(A, T, sd.pos, sd.n, sd.gn, q.rnd, sn, true, nr);           // q's sample, this domain
+    const float a0 = res.phat * res.M, b0 = phat_i_old * q.M;
+    const float a1 = q.target_pdf * q.M, b1 = phat_new * res.M;
+    const float m0 = a0 + b0 > 0.f ? a0 / (a0 + b0) : 0.f;
+    const float m1 = a1 + b1 > 0.f ? a1 / (a1 + b1) : 0.f;
+    const float iw0 = res.iw();
+    res.M += q.M;
+    const float w0 = m0 * res.phat * iw0;
+    const float w1 = m1 * phat_new * q.W;
+    res.wsum = w0 + w1;
+    if (rng.next_float().x * res.wsum <= w1) {
+        res.rnd = q.rnd;
+        res.phat = phat_new;
+        res.r = nr;
+    }
+}
+
+// SampleDirectIlluminationReservoir (vcm.slang:343-390): di_m candidates, the chosen one's shadow
+// ray, optionally the reuse of a previous reservoir found near the vertex, and the store of this
+// one (whatever its weight, see below).  Returns the reservoir (integration weight iw(); its
+// sample in r).
+S2D VcmReservoir vcm_di_reservoir(const VcmArgs& A, VcmTrace& T, const SD& sd, uint32_t inst, uint32_t prim, Rng& rng,
+                                  bool sn) {
+    VcmReservoir res;
+    res.rnd = make_float4(0.f, 0.f, 0.f, 0.f);
+    res.phat = 0.f; res.wsum = 0.f; res.M = (float)A.di_m;
+    res.r.radiance = f3(0.f); res.r.pdf = 0.f; res.r.dir = f3(0.f); res.r.dist = 0.f; res.r.cos_light = 0.f; res.r.finite = true;
+    for (uint32_t c = 0; c < A.di_m; ++c) {  // ProcessSample
+        const float4 x = rng.next_float();
+        const float u = rng.next_float().x;
+        Illum r;
+        const float phat = vcm_di_target(A, T, sd.pos, sd.n, sd.gn, x, sn, false, r);
+        if (!(phat > 0.f)) continue;
+        const float wi = phat / (r.pdf * res.M);
+        res.wsum += wi;
+        if (u * res.wsum <= wi) { res.rnd = x; res.phat = phat; res.r = r; }
+    }
+    if (res.phat > 0.f && !vcm_visible(A, T, ray_offset(sd.pos, sd.gn, res.r.dir), res.r.dir, res.r.dist * 0.99f))
+        res.phat = 0.f;
+    if (A.di_reuse) {
+        if (A.di_prev_valid) {
+            const float4 j = rng.next_float();
+            float3 t, b;
+            make_orthonormal(sd.gn, t, b);
+            const float csz = hg_cell_size(A.di_prev, sd.pos);
+            const float3 qp = sd.pos + (t * (j.x * 2.f - 1.f) + b * (j.y * 2.f - 1.f)) * csz;
+            const uint32_t cell = hg_find_cell<false>(A.di_prev, qp, hg_cell_size(A.di_prev, qp));
+            if (cell != 0xffffffffu) {
+                const uint32_t count = A.di_prev.cell_counters[cell];
+                if (count > 0) {
+                    const uint32_t off = A.di_prev.indices[cell];
+                    const ReservoirRecord q = A.di_prev.data[A.di_prev.data_indices[off + rng.next().x % count]];
+                    vcm_di_reuse(A, T, sd, q, res, rng, sn);
+                }
+            }
+        }
+        // Every reservoir is stored, also those of integration weight 0 (no candidate, or the chosen
+        // one occluded).  The reference appends only positive weights (vcm.slang:370), which makes
+        // the reused population conditional on success: its expected weight is then 1 / P(W > 0)
+        // too large, and on the box scene the image came out 3.9 % too bright.
+        {
+            ReservoirRecord rec;
+            rec.local_pos = xform_point(A.scene.inv_transforms + 3 * (size_t)inst, sd.pos);
+            rec.instance = inst;
+            rec.primitive = prim;
+            rec.rnd = res.rnd;
+            rec.target_pdf = res.phat;
+            rec.W = res.iw();
+            rec.M = fminf(res.M, A.di_max_m * (float)A.di_m);
+            rec.local_dir_in = f3(0.f);
+            rec.pad = 0.f;
+            hg_append(A.di_cur, sd.pos, rec);
+        }
+    }
+    return res;
+}
+
 template <bool LAMBERT>
 __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmArgs A) {
     __shared__ uint2 stack[S2_STACK_SMEM * 128];
@@ -484,8 +597,19 @@ __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmA
             if (!sing) {
                 // DirectIllumination (vcm.slang:396-475): MIS of tech. rep. eqs. 37, 44-45
                 if ((A.use_vc || A.path_trace_only) && p.len + 1 >= A.min_len) {
-                    const Illum r = sample_illum(s, rng.next_float(), sd.pos, sn);
-                    if (any_pos(r.radiance) && r.pdf > 0.f && vcm_pass(A, p.len + 1, 1)) {
+                    // the light sample: resampled (visibility traced inside) or one sample (its
+                    // shadow ray below); iw: its contribution weight per unit area
+                    Illum r;
+                    float iw;
+                    if (A.di_ris) {
+                        const VcmReservoir res = vcm_di_reservoir(A, T, sd, h.instance, h.primitive, rng, sn);
+                        r = res.r;
+                        iw = res.iw();
+                    } else {
+                        r = sample_illum(s, rng.next_float(), sd.pos, sn);
+                        iw = r.pdf > 0.f ? 1.f / r.pdf : 0.f;
+                    }
+                    if (any_pos(r.radiance) && r.pdf > 0.f && iw > 0.f && vcm_pass(A, p.len + 1, 1)) {
                         const float direct_pdfw = r.pdf * r.dist * r.dist / r.cos_light;
                         const float emission_pdfw = r.pdf * cos_hemisphere_pdfw(r.cos_light);
                         const float3 out = sd.to_local(r.dir);
@@ -503,8 +627,11 @@ __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmA
                                                        (A.vm_weight + p.dvcm + p.dvc * vmis(bsdf_rev));
                                 w = vcm_w(A, 1.f / (w_light + 1.f + w_camera));
                             }
-                            const float3 contrib = r.radiance * f * (w / direct_pdfw);
-                            if (any_pos(contrib) && vcm_visible(A, T, ray_offset(sd.pos, sd.gn, r.dir), r.dir, r.dist * 0.99f))
+                            // 1 / direct_pdfw without resampling; iw G with it (vcm.slang:390, 463)
+                            const float g = r.cos_light / (r.dist * r.dist);
+                            const float3 contrib = r.radiance * f * (A.di_ris ? w * iw * g : w / direct_pdfw);
+                            if (any_pos(contrib) &&
+                                (A.di_ris || vcm_visible(A, T, ray_offset(sd.pos, sd.gn, r.dir), r.dir, r.dist * 0.99f)))
                                 L = L + p.thr * contrib;
                         }
                     }

@@ -8,6 +8,10 @@ vcm.slang:880-1238, SmallVCM's techniques with the dVCM / dVC / dVM MIS quantiti
   the paths of its length that path tracing renders: every technique's pdf and throughput
   bookkeeping is checked without MIS.
 * Merging is consistent: BPM, VCM and PPM approach the golden image as the merge radius shrinks.
+* Direct illumination by resampled reservoirs (the reference's gDIReservoirFlags eRIS and eReuse,
+  vcm.slang:251-390) leaves these images unchanged in expectation: path tracing and BPT with it,
+  with and without the reuse of the previous iteration's reservoirs through the hash grid, converge
+  to the same golden image.
 """
 from pathlib import Path
 
@@ -23,8 +27,10 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 W = H = 64
 
 
-def vparams(algo, iters, seed, vcm_flags=0, fraction=1.0, radius=0.025, first=0, lengths=(2, 5)):
+def vparams(algo, iters, seed, vcm_flags=0, fraction=1.0, radius=0.025, first=0, lengths=(2, 5), di_m=None):
     p = Device.default_vcm_params()
+    if di_m is not None:
+        p.di_candidates = di_m
     p.algorithm, p.iterations, p.frame_seed = algo, iters, seed
     p.min_path_length, p.max_path_length = lengths
     p.flags = _abi.FLAG_LAMBERTIAN
@@ -153,3 +159,48 @@ def test_vcm_reproducible_aovs_and_argument_checks(device, box):
     with pytest.raises(_abi.S2Error) as e:
         device.render_vcm(wl.view, W, H, p)
     assert e.value.code == _abi.S2_ERR_INVALID
+
+
+@pytest.mark.parametrize("algo,vcm_flags", [
+    (_abi.VCM_PATH_TRACE, _abi.VCM_FLAG_DI_RIS),
+    (_abi.VCM_BPT, _abi.VCM_FLAG_DI_RIS),
+    (_abi.VCM_PATH_TRACE, _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
+    (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
+])
+def test_di_reservoirs_converge_to_golden(device, box, algo, vcm_flags):
+    """Resampled direct illumination (8 candidates per camera vertex), with and without reuse, is
+    unbiased: the image converges to the FP64 golden.  With reuse, neighbouring pixels share
+    reservoirs, so the bias check is on the image total (one value per independent batch) and the
+    per-pixel z-test only bounds the outliers."""
+    wl, ref, ref_v = box
+    device.upload_scene(wl.scene)
+    device.render_vcm(wl.view, W, H, vparams(algo, 1, 1))  # a call without reuse drops old reservoirs
+    img = batches(device, wl.view, 16, 256, 5000 + 100000 * algo + 7 * vcm_flags, algo=algo, vcm_flags=vcm_flags, di_m=8)
+    z, rel = zstats(img, ref, ref_v)
+    assert np.mean(np.abs(z) > 5) <= 2e-3, f"{np.mean(np.abs(z) > 5):.4%} of pixel channels with |z| > 5"
+    totals = img.sum(axis=(1, 2, 3))
+    t = (totals.mean() - ref.sum()) / np.sqrt(totals.var(ddof=1) / len(totals) + ref_v.sum())
+    assert abs(t) < 4.0, (t, rel)
+    if not vcm_flags & _abi.VCM_FLAG_DI_REUSE:
+        assert abs(z.mean()) < 0.15, z.mean()
+
+
+def test_di_reservoirs_reproducible_and_argument_checks(device, box):
+    """Reservoir sequences reproduce bit for bit (the grid is built by a sort on cell and record
+    content), reuse changes the image, and the flags are checked."""
+    wl, _, _ = box
+    device.upload_scene(wl.scene)
+    fl = _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE
+    seqs = []
+    for _ in range(2):
+        device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 1, 1))  # drops the grids
+        seqs.append(np.stack([device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 40 + 2 * k, vcm_flags=fl)).radiance
+                              for k in range(3)]))
+    np.testing.assert_array_equal(seqs[0], seqs[1])
+    ris = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 44, vcm_flags=_abi.VCM_FLAG_DI_RIS)).radiance
+    assert not np.array_equal(seqs[0][2], ris)  # the third call reused the second's reservoirs
+    for bad in (vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_REUSE),
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_RIS, di_m=0)):
+        with pytest.raises(_abi.S2Error) as e:
+            device.render_vcm(wl.view, W, H, bad)
+        assert e.value.code == _abi.S2_ERR_INVALID
