@@ -1,5 +1,5 @@
 """World-size-2 gloo ranks on CPU: the sample partition and the image/timing combination used by
-bench.py's multi-GPU path (no GPU needed)."""
+bench.py's multi-GPU path, and the view partition of the batched form (no GPU needed)."""
 import os
 import socket
 
@@ -9,7 +9,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from stratum2_b200.multi import combine_images, frame_seed, job_time_and_totals
+from stratum2_b200.multi import combine_images, frame_seed, gather_views, job_time_and_totals, partition_views
 
 
 def _free_port():
@@ -131,3 +131,67 @@ def test_a_rank_leaving_between_steps_ends_the_next_collective_with_an_error():
         p.join(60)
     assert all(not p.is_alive() for p in ctx.processes)
     assert out.get(0) not in (None, "no error"), out.get(0)
+
+
+def test_view_partition_balances_pixels_and_covers_every_view():
+    counts = [1920 * 1080, 256 * 256, 640 * 480, 1280 * 720, 300 * 200, 800 * 800, 512 * 512]
+    for world in (1, 2, 3, 4, 8):
+        parts = partition_views(counts, world)
+        assert sorted(v for p in parts for v in p) == list(range(len(counts)))
+        loads = [sum(counts[v] for v in p) for p in parts]
+        # greedy largest-first: no rank exceeds the mean load by more than the largest view
+        assert max(loads) <= sum(counts) / world + max(counts)
+        assert parts == partition_views(counts, world)  # every rank computes the same partition
+    assert partition_views(counts, 2)[0][0] == 0 and len(partition_views([5], 3)[2]) == 0
+
+
+_VIEWS = [(12, 10, (0.0, 0.0, 3.0)), (8, 6, (0.3, 0.1, 2.8)), (10, 10, (-0.2, 0.0, 3.1)), (6, 4, (0.0, 0.4, 2.6))]
+
+
+def _view_worker(rank, world, port, out):
+    """Each rank renders its share of four views of different extents with the CPU oracle (the
+    batched form's view partition, the oracle standing in for a GPU); rank 0 gathers all views."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle_lib import OracleScene, default_render_params
+        from stratum2_b200.scene import make_view
+        from stratum2_b200.scenegen import box_scene
+        wl = box_scene(seed=1, n_random=50, width=12, height=10)
+        osc = OracleScene(wl.scene, 2)
+        p = default_render_params()
+        p.spp, p.min_path_length, p.max_path_length, p.frame_seed = 2, 2, 5, 5
+        parts = partition_views([w * h for w, h, _ in _VIEWS], world)
+        local = {}
+        for v in parts[rank]:
+            w, h, pos = _VIEWS[v]
+            r = osc.render(make_view(pos, w, h, 40.0), p, w, h, precision=32, threads=1)
+            local[v] = torch.from_numpy(r["mean"].astype(np.float32))
+        imgs = gather_views(local, [(h, w, 3) for w, h, _ in _VIEWS], parts, dist)
+        if rank == 0:
+            out[0] = [im.numpy().tolist() for im in imgs]
+        else:
+            out[rank] = imgs is None
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_gloo_ranks_render_their_views_and_gather_them():
+    from oracle_lib import OracleScene, default_render_params
+    from stratum2_b200.scene import make_view
+    from stratum2_b200.scenegen import box_scene
+    world = 2
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_view_worker, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+    assert out[1] is True
+    wl = box_scene(seed=1, n_random=50, width=12, height=10)
+    osc = OracleScene(wl.scene, 2)
+    p = default_render_params()
+    p.spp, p.min_path_length, p.max_path_length, p.frame_seed = 2, 2, 5, 5
+    for v, (w, h, pos) in enumerate(_VIEWS):
+        ref = osc.render(make_view(pos, w, h, 40.0), p, w, h, precision=32, threads=1)["mean"].astype(np.float32)
+        np.testing.assert_array_equal(np.array(out[0][v], dtype=np.float32), ref)
