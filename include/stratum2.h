@@ -108,8 +108,13 @@ typedef struct S2BvhParams {
     uint32_t max_leaf_size;   /* triangles per BVH8 leaf slot, 1..3 (default 3) */
     uint32_t sah_bins;        /* binned-SAH bins (default 32) */
     uint32_t threads;         /* host build threads (0 = all) */
-    uint32_t reserved;
+    uint32_t collapse;        /* S2_BVH_COLLAPSE_SAH (0, default): the binary tree is collapsed into
+                                 8-wide nodes by a cost-optimal dynamic program over the surface-area
+                                 cost; S2_BVH_COLLAPSE_GREEDY (1): by repeatedly opening the child of
+                                 largest area */
 } S2BvhParams;
+#define S2_BVH_COLLAPSE_SAH    0u
+#define S2_BVH_COLLAPSE_GREEDY 1u
 
 typedef struct S2BvhStats {
     uint64_t node_count, triangle_count, leaf_slot_count;

@@ -55,6 +55,8 @@ SHADE_RECORDS_ON = 0
 SHADE_RECORDS_OFF = 1
 SHADOW_MERGE_ON = 0
 SHADOW_MERGE_OFF = 1
+BVH_COLLAPSE_SAH = 0
+BVH_COLLAPSE_GREEDY = 1
 
 # every symbol include/stratum2.h declares
 EXPORTED_SYMBOLS = [
@@ -105,7 +107,7 @@ class S2SceneDesc(C.Structure):
 
 class S2BvhParams(C.Structure):
     _fields_ = [("max_leaf_size", C.c_uint32), ("sah_bins", C.c_uint32), ("threads", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("collapse", C.c_uint32)]
 
 
 class S2BvhStats(C.Structure):

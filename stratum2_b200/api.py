@@ -73,12 +73,12 @@ class Device:
         if rc != _abi.S2_OK:
             raise S2Error(rc, self._lib.s2_last_error(self._h).decode())
 
-    def upload_scene(self, scene, build: bool = True, max_leaf_size: int = 3):
+    def upload_scene(self, scene, build: bool = True, max_leaf_size: int = 3, collapse: int = _abi.BVH_COLLAPSE_SAH):
         self.scene = scene
         d = scene.desc()
         self._check(self._lib.s2_scene_upload(self._h, C.byref(d)))
         if build:
-            p = _abi.S2BvhParams(max_leaf_size=max_leaf_size, sah_bins=32, threads=0)
+            p = _abi.S2BvhParams(max_leaf_size=max_leaf_size, sah_bins=32, threads=0, collapse=collapse)
             st = _abi.S2BvhStats()
             self._check(self._lib.s2_build_bvh(self._h, C.byref(p), C.byref(st)))
             self.bvh_stats = st

@@ -648,6 +648,8 @@ extern "C" int s2_build_bvh(S2Context* ctx, const S2BvhParams* params, S2BvhStat
         if (params->max_leaf_size) bp.max_leaf_size = params->max_leaf_size;
         if (params->sah_bins) bp.sah_bins = params->sah_bins;
         bp.threads = params->threads;
+        if (params->collapse > S2_BVH_COLLAPSE_GREEDY) return set_error(ctx, S2_ERR_INVALID, "unknown BVH collapse mode");
+        bp.collapse = params->collapse;
     }
     BuildOutput out;
     std::string err;

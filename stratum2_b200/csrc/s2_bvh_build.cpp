@@ -1,6 +1,8 @@
-// Host BVH8 builder: binned-SAH binary BVH, greedy collapse to 8-wide nodes, octant-ordered
-// slots and conservative 8-bit quantized child boxes.  Replaces the driver-side
-// vkCmdBuildAccelerationStructuresKHR build of the reference (src/App/Scene.cpp:17-55).
+// Host BVH8 builder: binned-SAH binary BVH, collapse to 8-wide nodes (cost-optimal by dynamic
+// programming over the binary tree, in the manner of Ylitie, Karras and Laine, HPG 2017, or greedy
+// by largest child area), octant-ordered slots and conservative 8-bit quantized child boxes.
+// Replaces the driver-side vkCmdBuildAccelerationStructuresKHR build of the reference
+// (src/App/Scene.cpp:17-55).
 #include "s2_bvh_build.h"
 
 #include <algorithm>
@@ -152,45 +154,121 @@ inline void quantize(const float p, const int e, const float clo, const float ch
     qhi = (uint8_t)hi;
 }
 
+// Cost-optimal collapse (SAH over 8-wide nodes): for every binary node n and slot budget k = 1..8,
+// F[n][k] is the least cost of representing n's subtree in at most k slots of its parent's
+// 8-wide node, each slot a leaf (at most max_leaf triangles) or an 8-wide node of its own:
+//   F[n][1] = min(leaf: A(n) c_tri count(n),  node: A(n) c_node + D[n][8])
+//   D[n][j] = min over 1 <= k < j of F[left][k] + F[right][j - k]   (n opened over j slots)
+//   F[n][k] = min(F[n][k - 1], D[n][k])
+// with A the surface area; the decisions are kept so the 8-wide nodes can be read back.  The
+// constants weigh an 8-child box test against one triangle test (about 3.5 : 1 in instructions).
+constexpr float kCostNode = 1.0f, kCostTri = 0.3f;
+enum : uint8_t { kSlotLeaf = 0xfe, kSlotNode = 0xff };  // else: opened, left takes that many slots
+
+struct CollapsePlan {
+    std::vector<float> cost;     // F[n][k - 1], 8 per binary node
+    std::vector<uint8_t> how;    // decision per (n, k)
+    std::vector<uint8_t> open8;  // D[n][8]'s split: slots of the left child when n is an 8-wide node
+
+    void build(const Builder& b, uint32_t nodes, uint32_t max_leaf) {
+        cost.assign((size_t)nodes * 8, std::numeric_limits<float>::infinity());
+        how.assign((size_t)nodes * 8, kSlotNode);
+        open8.assign(nodes, 4);
+        // binary children have higher indices than their parent: reverse index order is post-order
+        for (int64_t n = (int64_t)nodes - 1; n >= 0; --n) {
+            const BNode& bn = b.nodes[n];
+            const double a = bn.box.area();
+            float* F = &cost[8 * (size_t)n];
+            uint8_t* H = &how[8 * (size_t)n];
+            const double leaf = bn.count <= max_leaf ? a * kCostTri * bn.count : std::numeric_limits<double>::infinity();
+            if (bn.leaf()) {
+                for (int k = 0; k < 8; ++k) { F[k] = (float)leaf; H[k] = kSlotLeaf; }
+                continue;
+            }
+            const float* L = &cost[8 * (size_t)bn.left];
+            const float* R = &cost[8 * (size_t)bn.right];
+            double D[9];
+            uint8_t split[9];
+            for (int j = 2; j <= 8; ++j) {
+                D[j] = std::numeric_limits<double>::infinity();
+                split[j] = 1;
+                for (int k = 1; k < j; ++k) {
+                    const double c = (double)L[k - 1] + (double)R[j - k - 1];
+                    if (c < D[j]) { D[j] = c; split[j] = (uint8_t)k; }
+                }
+            }
+            open8[n] = split[8];
+            const double node = a * kCostNode + D[8];
+            F[0] = (float)std::min(leaf, node);
+            H[0] = leaf <= node ? kSlotLeaf : kSlotNode;
+            for (int k = 2; k <= 8; ++k) {
+                if (D[k] < F[k - 2]) { F[k - 1] = (float)D[k]; H[k - 1] = split[k]; }
+                else { F[k - 1] = F[k - 2]; H[k - 1] = H[k - 2]; }
+            }
+        }
+    }
+
+    // The slots of binary node n given k slots: appends (binary node, is_leaf) pairs.
+    void slots(const Builder& b, uint32_t n, int k, uint32_t* ch, bool* leaf, int& nc) const {
+        const uint8_t h = how[8 * (size_t)n + (k - 1)];
+        if (h == kSlotLeaf || h == kSlotNode) {
+            ch[nc] = n; leaf[nc] = h == kSlotLeaf; nc++;
+            return;
+        }
+        const BNode& bn = b.nodes[n];
+        slots(b, (uint32_t)bn.left, h, ch, leaf, nc);
+        slots(b, (uint32_t)bn.right, k - h, ch, leaf, nc);
+    }
+};
+
 struct Collapser {
     Builder& b;
     std::vector<S2BvhNode>& out_nodes;
     std::vector<S2TriRecord>& out_tris;
+    const CollapsePlan* plan;     // null: greedy collapse
     uint32_t max_depth = 0;
     uint64_t leaf_slots = 0;
     double sah = 0;
 
-    Collapser(Builder& bb, std::vector<S2BvhNode>& n, std::vector<S2TriRecord>& t)
-        : b(bb), out_nodes(n), out_tris(t) {}
+    Collapser(Builder& bb, std::vector<S2BvhNode>& n, std::vector<S2TriRecord>& t, const CollapsePlan* p)
+        : b(bb), out_nodes(n), out_tris(t), plan(p) {}
 
     // Fill node `ni` from binary node `bn`.
     void fill(uint32_t ni, uint32_t bn, uint32_t depth) {
         max_depth = std::max(max_depth, depth);
         const BNode& root = b.nodes[bn];
-        // gather up to 8 children by expanding the largest-area internal child
         uint32_t ch[8]; int nc = 0;
-        if (root.leaf()) { ch[nc++] = bn; }
-        else { ch[nc++] = (uint32_t)root.left; ch[nc++] = (uint32_t)root.right; }
-        while (nc < 8) {
-            int best = -1; double ba = -1;
-            for (int i = 0; i < nc; ++i) {
-                const BNode& c = b.nodes[ch[i]];
-                if (c.leaf()) continue;
-                double a = c.box.area();
-                if (a > ba) { ba = a; best = i; }
-            }
-            if (best < 0) break;
-            const BNode& c = b.nodes[ch[best]];
-            ch[best] = (uint32_t)c.left;
-            ch[nc++] = (uint32_t)c.right;
-        }
-        // a child subtree with <= max_leaf triangles becomes a leaf slot
         bool is_leaf[8];
         int n_internal = 0;
-        for (int i = 0; i < nc; ++i) {
-            const BNode& c = b.nodes[ch[i]];
-            is_leaf[i] = c.leaf() || c.count <= b.prm.max_leaf_size;
-            if (!is_leaf[i]) n_internal++;
+        if (plan && !root.leaf()) {
+            // the cost-optimal slots of bn opened over 8 slots (D[bn][8] and its decisions)
+            const int kleft = plan->open8[bn];
+            plan->slots(b, (uint32_t)root.left, kleft, ch, is_leaf, nc);
+            plan->slots(b, (uint32_t)root.right, 8 - kleft, ch, is_leaf, nc);
+            for (int i = 0; i < nc; ++i) if (!is_leaf[i]) n_internal++;
+        } else {
+            // greedy: expand the largest-area internal child until 8 children
+            if (root.leaf()) { ch[nc++] = bn; }
+            else { ch[nc++] = (uint32_t)root.left; ch[nc++] = (uint32_t)root.right; }
+            while (nc < 8) {
+                int best = -1; double ba = -1;
+                for (int i = 0; i < nc; ++i) {
+                    const BNode& c = b.nodes[ch[i]];
+                    if (c.leaf()) continue;
+                    double a = c.box.area();
+                    if (a > ba) { ba = a; best = i; }
+                }
+                if (best < 0) break;
+                const BNode& c = b.nodes[ch[best]];
+                ch[best] = (uint32_t)c.left;
+                ch[nc++] = (uint32_t)c.right;
+            }
+            // a child subtree with <= max_leaf triangles becomes a leaf slot
+            for (int i = 0; i < nc; ++i) {
+                const BNode& c = b.nodes[ch[i]];
+                is_leaf[i] = c.leaf() || c.count <= b.prm.max_leaf_size;
+                if (!is_leaf[i]) n_internal++;
+            }
         }
         // octant slot assignment: slot s gets the child nearest along direction octant s
         const BNode& nb = b.nodes[bn];
@@ -324,7 +402,10 @@ int build_bvh8(const BuildInput& in, const BuildParams& prm_in, BuildOutput& out
     out.nodes.reserve(n / 2 + 16);
     out.tris.reserve(n);
     out.nodes.resize(1);
-    Collapser c(b, out.nodes, out.tris);
+    CollapsePlan plan;
+    const bool optimal = prm.collapse == 0;
+    if (optimal) plan.build(b, b.node_count.load(), prm.max_leaf_size);
+    Collapser c(b, out.nodes, out.tris, optimal ? &plan : nullptr);
     c.fill(0, 0, 1);
     if (c.max_depth > S2_STACK_DEPTH) {
         err = "BVH depth " + std::to_string(c.max_depth) + " exceeds traversal stack depth";

@@ -22,6 +22,7 @@ struct BuildParams {
     uint32_t max_leaf_size = 3;
     uint32_t sah_bins = 32;
     uint32_t threads = 0;
+    uint32_t collapse = 0;  // S2_BVH_COLLAPSE_SAH (0): cost-optimal collapse; S2_BVH_COLLAPSE_GREEDY (1)
 };
 
 struct BuildOutput {
