@@ -124,3 +124,24 @@ def test_counted_trace_matches_cpu_bvh8_walker(device, scene_case):
             np.testing.assert_array_equal(h["t"].view(np.uint32), oh[:, 0])
             np.testing.assert_array_equal(h["b1"].view(np.uint32), oh[:, 3])
             np.testing.assert_array_equal(h["b2"].view(np.uint32), oh[:, 4])
+
+
+@pytest.mark.parametrize("name", ["box", "terrain"])
+def test_collapse_modes_give_the_same_hits(device, name):
+    """The cost-optimal and the greedy collapse build different 8-wide trees over the same binary
+    tree; hits (bit-exact against the FP32 replica, which does not depend on the tree) and first
+    hits are the same with either, and the cost-optimal tree visits fewer nodes per ray."""
+    from stratum2_b200 import _abi
+    wl = dict(_scenes())[name]
+    rays = np.concatenate([camera_rays(wl.view, wl.width, wl.height), random_rays(50_000, seed=21)])
+    out = {}
+    for col in (_abi.BVH_COLLAPSE_SAH, _abi.BVH_COLLAPSE_GREEDY):
+        device.upload_scene(wl.scene, collapse=col)
+        h, cnt = device.trace(rays, counted=True)
+        out[col] = (h, cnt[:, 0].mean(), device.bvh_stats.node_count, device.trace(rays, anyhit=True)["instance"] != INV)
+    a, b = out[_abi.BVH_COLLAPSE_SAH], out[_abi.BVH_COLLAPSE_GREEDY]
+    for k in ("instance", "primitive", "t", "b1", "b2"):
+        np.testing.assert_array_equal(a[0][k], b[0][k])
+    np.testing.assert_array_equal(a[3], b[3])
+    assert a[1] <= b[1] * 1.01 and a[2] < b[2], (a[1], b[1], a[2], b[2])
+    device.upload_scene(wl.scene)
