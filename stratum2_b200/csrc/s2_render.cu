@@ -1020,12 +1020,24 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     const bool count = (prm->flags & S2_FLAG_COUNT_FETCHES) != 0;
     int apply_rc = S2_OK;
     // one graph = two iterations (parity 0 and 1) of setup, regeneration, extend, [material sort,]
-    // shade, [radiance-cache inference for the terminal vertices,] occlude
+    // shade, [radiance-cache inference for the terminal vertices,] occlude; with shadow merging
+    // (not with the cache) each iteration's k_trace also traces the previous iteration's shadow
+    // rays, whose count sits in the other parity's counter.  The iteration whose setup finds no
+    // path left still traces the last shadow rays before the host sees it done.
+    const bool merge = !cache && ctx->tuning.shadow_merge != S2_SHADOW_MERGE_OFF;
+    P.sh_merge = merge ? 1u : 0u;
     auto iteration = [&](uint32_t parity, int first) {
+        P.sh_parity = merge ? parity : 0u;
+        const uint32_t sh_prev = parity ? C_SHADOW : C_SHADOW1;  // counter of parity 1 - parity
         k_stream_setup<<<1, 32, 0, s>>>(P, parity, first);
         k_regen<<<std::min<uint32_t>((capacity + 255) / 256, 148u * 16u), 256, 0, s>>>(P, parity);
-        if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
-        else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+        if (merge && !first) {
+            if (count) k_trace<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
+            else k_trace<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
+        } else {
+            if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+            else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
+        }
         if (sort) launch_sort(P, parity, st->sort_blocks, s);
         if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
         else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
@@ -1033,8 +1045,10 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
             const int r = cache_apply_device(ctx, st->cq_pos, st->cq_thr, st->cq_cap, B->counters + C_CACHEQ, nullptr, B->total_fx);
             if (r != S2_OK) apply_rc = r;
         }
-        if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
-        else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+        if (!merge) {
+            if (count) k_occlude<true><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+            else k_occlude<false><<<st->occ_blocks, kTravBlock, 0, s>>>(P);
+        }
     };
     cudaEventRecord(ctx->ev0, s);
     iteration(0, 1);  // first iteration outside the graph (it skips the shadow accounting)
@@ -1048,7 +1062,7 @@ extern "C" int s2_render_views(S2Context* ctx, const S2View* views, uint32_t nvi
     if (rc == S2_OK) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
     if (rc != S2_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
     if (apply_rc != S2_OK) { cudaGraphExecDestroy(exec); cudaGraphDestroy(graph); return apply_rc; }
-    const uint64_t per_iter = (sort ? 8 : 5) + (cache ? 1 : 0);
+    const uint64_t per_iter = (sort ? 8 : 5) + (cache ? 1 : 0) - (merge ? 1 : 0);
     uint64_t launches = per_iter;
     // replay until the device reports every path finished; the check trails one group behind so
     // the host never waits on the group it just queued

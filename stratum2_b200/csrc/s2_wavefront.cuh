@@ -288,7 +288,9 @@ __global__ void k_wave_finish(PTParams P) {
 __global__ void k_stream_setup(PTParams P, uint32_t parity, int first) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long* ss = P.stream_state;
-    if (!first) P.stats[S_SHADOW] += P.counters[C_SHADOW];
+    // the previous iteration's shadow rays are retired as in k_bounce_setup
+    const uint32_t cur = sh_counter(P), prev = P.sh_merge ? (cur == C_SHADOW ? C_SHADOW1 : C_SHADOW) : cur;
+    if (!first) P.stats[S_SHADOW] += P.counters[prev];
     const uint32_t live = P.counters[parity];
     const unsigned long long left = P.total_paths - ss[0];
     const uint32_t fill = (uint32_t)min((unsigned long long)(P.capacity - live), left);
@@ -299,7 +301,7 @@ __global__ void k_stream_setup(PTParams P, uint32_t parity, int first) {
     P.counters[parity] = live + fill;
     P.stats[S_EXT] += live + fill;
     P.counters[1 - parity] = 0;
-    P.counters[C_SHADOW] = 0;
+    P.counters[cur] = 0;
     P.counters[C_WORK_EXT] = 0;
     P.counters[C_WORK_OCC] = 0;
     P.counters[C_CACHEQ] = 0;

@@ -127,4 +127,14 @@ def test_shadow_merge_keeps_the_image_bitwise(device, flags):
         assert out.stats.extension_rays == ref.stats.extension_rays
         assert out.stats.shadow_rays == ref.stats.shadow_rays > 0
         assert out.stats.kernel_launches < ref.stats.kernel_launches
+    # the batched streaming form: fixed-point pixel totals, so also bit-identical
+    off = _abi.S2Tuning()
+    off.shadow_merge = _abi.SHADOW_MERGE_OFF
+    device.set_tuning(off)
+    a, sa = device.render_views([wl.view, wl.view], p)
+    device.set_tuning(None)
+    b, sb = device.render_views([wl.view, wl.view], p)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.radiance, y.radiance)
+    assert sa.shadow_rays == sb.shadow_rays > 0 and sa.extension_rays == sb.extension_rays
     device.set_tuning(None)
