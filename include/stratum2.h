@@ -613,6 +613,12 @@ int  s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2Tonemap
                                                       camera vertices resamples di_candidates light
                                                       samples by lum(Le) |cos| G and traces one shadow
                                                       ray for the chosen one (vcm.slang:343-366) */
+#define S2_VCM_FLAG_LVC_RIS             (1u << 5)  /* with LIGHT_VERTEX_CACHE, gLVCReservoirFlags eRIS:
+                                                      each camera vertex resamples lvc_candidates
+                                                      random cached light vertices by the luminance
+                                                      of their connection and traces one shadow ray
+                                                      (vcm.slang:568-736; the reuse of these
+                                                      reservoirs is not built) */
 #define S2_VCM_FLAG_DI_REUSE            (1u << 4)  /* with DI_RIS, eReuse: each camera vertex also
                                                       resamples a reservoir of the previous iteration
                                                       (or call) found in a world-space hash grid near it
@@ -638,7 +644,7 @@ typedef struct S2VcmParams {
     uint32_t di_candidates;          /* mDIReservoirSampleCount (default 32, VCM.cpp:33), 1..1024 */
     float di_max_m;                  /* mDIReservoirMaxM (default 3, VCM.cpp:34): stored M is capped
                                         at di_max_m x di_candidates */
-    uint32_t reserved;
+    uint32_t lvc_candidates;         /* mLVCReservoirSampleCount (default 8, VCM.cpp:35), 1..1024 */
 } S2VcmParams;
 
 void s2_default_vcm_params(S2VcmParams* p);

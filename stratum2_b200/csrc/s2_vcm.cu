@@ -33,7 +33,7 @@ namespace {
 constexpr uint32_t kVcmRenderFlags = S2_FLAG_LAMBERTIAN | S2_FLAG_PCG32 | S2_FLAG_NO_RR | S2_FLAG_SHADING_NORMALS_OFF |
                                      S2_FLAG_ALPHA_TEST_OFF | S2_FLAG_NORMAL_MAPS_OFF | S2_FLAG_LIGHT_POWER_PICK;
 constexpr uint32_t kVcmOwnFlags = S2_VCM_FLAG_LIGHT_VERTEX_CACHE | S2_VCM_FLAG_DEBUG_PATHS | S2_VCM_FLAG_DEBUG_UNWEIGHTED |
-                                   S2_VCM_FLAG_DI_RIS | S2_VCM_FLAG_DI_REUSE;
+                                   S2_VCM_FLAG_DI_RIS | S2_VCM_FLAG_DI_REUSE | S2_VCM_FLAG_LVC_RIS;
 
 void invert_affine(const float* m, float* out) {
     // inverse of a row-major 3x4 rigid (or scaled) transform
@@ -145,8 +145,9 @@ extern "C" void s2_default_vcm_params(S2VcmParams* p) {
     p->light_path_fraction = 1.f;                    // VCM.hpp:67
     p->merge_radius_factor = 0.025f;                 // VCM.hpp:59-60
     p->merge_radius_alpha = 0.01f;
-    p->di_candidates = 32;                           // VCM.cpp:33-34
+    p->di_candidates = 32;                           // VCM.cpp:33-35
     p->di_max_m = 3.f;
+    p->lvc_candidates = 8;
 }
 
 extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmParams* prm, const S2Aovs* out, int out_on_host,
@@ -168,6 +169,11 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     if (lvc && algo != S2_VCM_BPT) return set_error(ctx, S2_ERR_UNSUPPORTED, "the light vertex cache serves BPT only");
     if (!(prm->light_path_fraction > 0.f) || !std::isfinite(prm->light_path_fraction))
         return set_error(ctx, S2_ERR_INVALID, "light_path_fraction must be finite and > 0");
+    const bool lvc_ris = (prm->vcm_flags & S2_VCM_FLAG_LVC_RIS) != 0;
+    if (lvc_ris && !(prm->vcm_flags & S2_VCM_FLAG_LIGHT_VERTEX_CACHE))
+        return set_error(ctx, S2_ERR_INVALID, "LVC_RIS needs LIGHT_VERTEX_CACHE");
+    if (lvc_ris && (prm->lvc_candidates < 1 || prm->lvc_candidates > 1024))
+        return set_error(ctx, S2_ERR_INVALID, "lvc_candidates must be in 1..1024");
     const bool di_ris = (prm->vcm_flags & S2_VCM_FLAG_DI_RIS) != 0;
     if ((prm->vcm_flags & S2_VCM_FLAG_DI_REUSE) && !di_ris) return set_error(ctx, S2_ERR_INVALID, "DI_REUSE needs DI_RIS");
     if (di_ris && (prm->di_candidates < 1 || prm->di_candidates > 1024))
@@ -227,6 +233,7 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     A.di_reuse = di_reuse ? 1u : 0u;
     A.di_m = prm->di_candidates;
     A.di_max_m = prm->di_max_m;
+    A.lvc_m = lvc_ris ? prm->lvc_candidates : 0u;
     s2::VcmState* vs = nullptr;
     if (di_reuse) {
         if (!ctx->vcm) ctx->vcm = new (std::nothrow) s2::VcmState();

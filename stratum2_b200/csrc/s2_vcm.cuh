@@ -3,7 +3,7 @@
 // transport simulation with vertex connection and merging", tech. rep. eqs. 31-55).  One thread per
 // light subpath, then one per camera path, both on the shared BVH8 traversal:
 //   * light pass (GenerateLightPaths, vcm.slang:1145-1219): emission sample, random walk with the
-//     adjoint BSDF, every non-singular vertex stored (64-byte LightVertex) and connected to the camera;
+//     adjoint BSDF, every non-singular vertex stored (80-byte LightVertex) and connected to the camera;
 //   * grid build: the stored vertices sorted by the hash of their merge cell (cells 2r wide, so a
 //     query visits the 2x2x2 cells around it);
 //   * camera pass (GenerateCameraPaths, vcm.slang:880-1009): per vertex the emission hit, direct
@@ -22,12 +22,13 @@ namespace s2 {
 enum : uint32_t { VCM_PT = 0, VCM_LT = 1, VCM_PPM = 2, VCM_BPM = 3, VCM_BPT = 4, VCM_VCM = 5 };
 
 // One stored light-subpath vertex (PackedVcmVertex, compat/vcm.h:75-85, with the hit kept as
-// barycentrics so make_shading rebuilds the same shading frame): 64 bytes.
+// barycentrics so make_shading rebuilds the same shading frame): 80 bytes.
 struct LightVertex {
     float4 a;  // position, continuation probability of its material
     float4 b;  // throughput, dVCM
     float4 c;  // dVC, dVM, packed world direction toward the previous vertex (bits), path length (bits)
     uint4 d;   // instance, primitive, barycentrics b1, b2 (bits)
+    float4 e;  // the subpath's area-measure pdf up to this vertex (mPathPdfA), unused x 3
 };
 
 struct VcmArgs {
@@ -69,6 +70,7 @@ struct VcmArgs {
     uint32_t di_ris, di_reuse, di_m, di_prev_valid;
     float di_max_m;
     HashGridDev di_cur, di_prev;
+    uint32_t lvc_m;                // light-vertex-cache reservoirs (S2_VCM_FLAG_LVC_RIS): candidates, 0 = off
 };
 
 // Mis() (compat/vcm.h:9-11): power heuristic with exponent 2.
@@ -121,6 +123,7 @@ struct SubPath {
     float fwd_pdfw;   // BSDF pdf of the last scattering (infinite after a singular one)
     uint32_t len;
     bool specular;    // every scattering so far was singular
+    float pdfa;       // light subpaths: the path's pdf in area measure (mPathPdfA, vcm.slang:114, 1025, 1193)
 };
 
 // SampleScattering<Adjoint> (vcm.slang:67-113): Russian roulette, BSDF sampling and the MIS updates
@@ -151,6 +154,7 @@ S2D bool vcm_scatter(const VcmArgs& A, const Mat& m, const SD& sd, float3 in, bo
         p.fwd_pdfw = dir_pdf;
     }
     p.thr = p.thr * refl / dir_pdf;
+    p.pdfa *= dir_pdf;
     if (any_nan(p.thr) || !any_pos(p.thr)) return false;
     dir = sd.to_world(sdir);
     return true;
@@ -223,6 +227,7 @@ __global__ void __launch_bounds__(128) k_vcm_light(const __grid_constant__ VcmAr
         p.fwd_pdfw = 0.f;
         p.len = 1;
         p.specular = true;
+        p.pdfa = emission_pdfw;
         uint32_t stored = 0;
         while (true) {
             const TravHit h = vcm_closest(A, T, org, dir);
@@ -238,6 +243,7 @@ __global__ void __launch_bounds__(128) k_vcm_light(const __grid_constant__ VcmAr
             p.dvcm /= vmis(cos_in);
             p.dvc /= vmis(cos_in);
             p.dvm /= vmis(cos_in);
+            p.pdfa *= cos_in / (h.t * h.t);
             const bool sing = mat_singular<LAMBERT>(m);
             if (!sing) {
                 if ((A.use_vc || A.use_vm) && p.len < A.max_len) {  // StoreLightVertex (vcm.slang:1112-1140)
@@ -246,6 +252,7 @@ __global__ void __launch_bounds__(128) k_vcm_light(const __grid_constant__ VcmAr
                     v.b = make_float4(p.thr.x, p.thr.y, p.thr.z, p.dvcm);
                     v.c = make_float4(p.dvc, p.dvm, __uint_as_float(pack_normal(-dir)), __uint_as_float(p.len));
                     v.d = make_uint4(h.instance, h.primitive, __float_as_uint(h.b1), __float_as_uint(h.b2));
+                    v.e = make_float4(p.pdfa, 0.f, 0.f, 0.f);
                     A.lv[(size_t)stored * A.n_light + i] = v;
                     stored++;
                 }
@@ -308,10 +315,10 @@ __global__ void k_vcm_ranges(const __grid_constant__ VcmArgs A, const uint32_t* 
 
 // ---------------------------------------------------------------- camera pass
 // ConnectVertices (vcm.slang:484-558): camera vertex to light vertex with the MIS weights of tech.
-// rep. eqs. 37, 40-41; the visibility ray is traced here.
+// rep. eqs. 37, 40-41; the visibility ray is traced here unless `vis` is false.
 template <bool LAMBERT>
 S2D float3 vcm_connect(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp, const SubPath& p,
-                       const LightVertex& v) {
+                       const LightVertex& v, bool vis = true) {
     const DevScene& s = A.scene;
     const bool sn = !(A.flags & S2F_NO_SN);
     const float3 lpos = f3(v.a.x, v.a.y, v.a.z);
@@ -343,8 +350,44 @@ S2D float3 vcm_connect(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd
     const float w = vcm_w(A, 1.f / (w_light + 1.f + w_camera));
     const float3 contrib = fc * fl * (w / dist2);
     if (!any_pos(contrib)) return f3(0.f);
-    if (!vcm_visible(A, T, ray_offset(sd.pos, sd.gn, d), d, dist * 0.99f)) return f3(0.f);  // AdjustDistance
+    if (vis && !vcm_visible(A, T, ray_offset(sd.pos, sd.gn, d), d, dist * 0.99f)) return f3(0.f);  // AdjustDistance
     return contrib;
+}
+
+// ConnectToLVCReservoir without reuse (vcm.slang:568-627, 681-696, 728-736): lvc_m cached light
+// vertices picked at random, resampled by the target lum(throughput x pathPdfA x connection) with
+// source pdf pathPdfA (the discrete pick's 1 / count cancels in the estimate), one shadow ray for
+// the chosen one.  Returns the contribution to add with the camera throughput, already scaled by
+// cached vertices / light subpaths.
+template <bool LAMBERT>
+S2D float3 vcm_connect_lvc_ris(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp,
+                               const SubPath& p, uint32_t total, Rng& rng) {
+    float wsum = 0.f, phat_sel = 0.f;
+    float3 c_sel = f3(0.f);
+    LightVertex v_sel;
+    const float M = (float)A.lvc_m;
+    for (uint32_t i = 0; i < A.lvc_m; ++i) {
+        const LightVertex v = A.lv[A.lvc_list[rng.next().x % total]];
+        const float u = rng.next_float().x;
+        const uint32_t vlen = __float_as_uint(v.c.w);
+        const uint32_t full = vlen + 1 + p.len;
+        if (full < A.min_len || full > A.max_len || !vcm_pass(A, p.len + 1, vlen + 1)) continue;
+        const float pdfa = v.e.x;
+        if (!(pdfa > 0.f)) continue;
+        const float3 c = f3(v.b.x, v.b.y, v.b.z) * pdfa * vcm_connect<LAMBERT>(A, T, m, sd, in, cp, p, v, false);
+        const float phat = luminance(c);
+        if (!(phat > 0.f)) continue;
+        const float wi = phat / (pdfa * M);
+        wsum += wi;
+        if (u * wsum <= wi) { phat_sel = phat; c_sel = c; v_sel = v; }
+    }
+    if (!(phat_sel > 0.f)) return f3(0.f);
+    const float3 lpos = f3(v_sel.a.x, v_sel.a.y, v_sel.a.z);
+    float3 d = lpos - sd.pos;
+    const float dist = length(d);
+    d = d / dist;
+    if (!vcm_visible(A, T, ray_offset(sd.pos, sd.gn, d), d, dist * 0.99f)) return f3(0.f);
+    return c_sel * ((wsum / phat_sel) * ((float)total / (float)A.n_light));
 }
 
 // ProcessVertex (vcm.slang:842-875): merging with one light vertex, MIS of tech. rep. eqs. 37-39.
@@ -637,7 +680,10 @@ __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmA
                     }
                 }
                 if (!A.path_trace_only) {
-                    if (A.use_vc && A.lvc && A.lvc_total) {
+                    if (A.use_vc && A.lvc && A.lvc_total && A.lvc_m) {
+                        const uint32_t total = *A.lvc_total;
+                        if (total > 0) L = L + p.thr * vcm_connect_lvc_ris<LAMBERT>(A, T, m, sd, in, cp, p, total, rng);
+                    } else if (A.use_vc && A.lvc && A.lvc_total) {
                         // ConnectToLVC (vcm.slang:732-753): one random cached vertex, weighted by the
                         // cached vertex count over the light subpath count
                         const uint32_t total = *A.lvc_total;

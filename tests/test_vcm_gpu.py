@@ -9,9 +9,10 @@ vcm.slang:880-1238, SmallVCM's techniques with the dVCM / dVC / dVM MIS quantiti
   bookkeeping is checked without MIS.
 * Merging is consistent: BPM, VCM and PPM approach the golden image as the merge radius shrinks.
 * Direct illumination by resampled reservoirs (the reference's gDIReservoirFlags eRIS and eReuse,
-  vcm.slang:251-390) leaves these images unchanged in expectation: path tracing and BPT with it,
-  with and without the reuse of the previous iteration's reservoirs through the hash grid, converge
-  to the same golden image.
+  vcm.slang:251-390) and the resampled light-vertex-cache connection (gLVCReservoirFlags eRIS,
+  vcm.slang:568-736) leave these images unchanged in expectation: path tracing and BPT with them,
+  with and without the reuse of the previous iteration's DI reservoirs through the hash grid,
+  converge to the same golden image.
 """
 from pathlib import Path
 
@@ -162,6 +163,8 @@ def test_vcm_reproducible_aovs_and_argument_checks(device, box):
 
 
 @pytest.mark.parametrize("algo,vcm_flags", [
+    (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS),
+    (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_DI_RIS),
     (_abi.VCM_PATH_TRACE, _abi.VCM_FLAG_DI_RIS),
     (_abi.VCM_BPT, _abi.VCM_FLAG_DI_RIS),
     (_abi.VCM_PATH_TRACE, _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
@@ -200,7 +203,8 @@ def test_di_reservoirs_reproducible_and_argument_checks(device, box):
     ris = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 44, vcm_flags=_abi.VCM_FLAG_DI_RIS)).radiance
     assert not np.array_equal(seqs[0][2], ris)  # the third call reused the second's reservoirs
     for bad in (vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_REUSE),
-                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_RIS, di_m=0)):
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_RIS, di_m=0),
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_LVC_RIS)):
         with pytest.raises(_abi.S2Error) as e:
             device.render_vcm(wl.view, W, H, bad)
         assert e.value.code == _abi.S2_ERR_INVALID
