@@ -34,6 +34,7 @@ struct RenderState {
     float4* aov_depth = nullptr;
     float2* aov_prev_uv = nullptr;
     uint2* aov_ids = nullptr;
+    uint32_t* hint_tri = nullptr;  // per pixel: the centre ray's triangle (k_pixel_hint)
     uint32_t* counters = nullptr;
     unsigned long long* stats = nullptr;
     uint64_t accumulated_spp = 0;
@@ -133,10 +134,11 @@ int ensure_state(S2Context* ctx, uint32_t width, uint32_t height, uint32_t capac
         st->aov_depth = alloc<float4>(ctx, st->pixel_bufs, pixels);
         st->aov_prev_uv = alloc<float2>(ctx, st->pixel_bufs, pixels);
         st->aov_ids = alloc<uint2>(ctx, st->pixel_bufs, pixels);
+        st->hint_tri = alloc<uint32_t>(ctx, st->pixel_bufs, pixels);
         st->counters = alloc<uint32_t>(ctx, st->pixel_bufs, C_COUNT);
         st->stats = alloc<unsigned long long>(ctx, st->pixel_bufs, S_COUNT);
         if (!st->total || !st->out_radiance || !st->aov_albedo || !st->aov_vis || !st->aov_depth || !st->aov_prev_uv ||
-            !st->aov_ids || !st->counters || !st->stats) {
+            !st->aov_ids || !st->hint_tri || !st->counters || !st->stats) {
             free_bufs(st->pixel_bufs);
             st->pixels = 0;
             return S2_ERR_OOM;
@@ -574,6 +576,13 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
     // terminal contributions must land after the NEE of the same vertex, so not with the cache)
     const bool merge = !cache && ctx->tuning.shadow_merge != S2_SHADOW_MERGE_OFF;
     P.sh_merge = merge ? 1u : 0u;
+    // frames of 8 or more samples per pixel: every camera ray first tests the triangle its pixel's
+    // centre ray hits (one traversal per pixel, once per call), so it starts with a tight t_max
+    const bool hint = !light_trace && prm->spp >= 8;
+    if (hint) {
+        k_pixel_hint<<<(pixels + kTravBlock - 1) / kTravBlock, kTravBlock, 0, s>>>(P, st->hint_tri);
+        launches += 1;
+    }
     for (uint32_t done = 0; !light_trace && done < prm->spp; done += slots) {
         P.wave_base_sample = done;
         P.wave_samples = std::min(slots, prm->spp - done);
@@ -589,6 +598,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
             if (P.ray_sorted) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(0);
+            P.hint_tri = hint && b == 0 ? st->hint_tri : nullptr;
             if (merge && b > 0) {
                 if (count) k_trace<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
                 else k_trace<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity, sh_prev);
@@ -596,6 +606,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
                 if (count) k_extend<true><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
                 else k_extend<false><<<st->ext_blocks, kTravBlock, 0, s>>>(P, parity);
             }
+            P.hint_tri = nullptr;
             ev_end();
             if (sort) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(1);

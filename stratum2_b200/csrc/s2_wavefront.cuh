@@ -127,6 +127,9 @@ struct PTParams {
     uint32_t* sort_keys;
     uint32_t* sort_perm;
     uint32_t* sort_hist;   // kSortBuckets counters / offsets
+    // camera launches of frames with several samples per pixel: the triangle hit by each pixel's
+    // centre ray (k_pixel_hint), tested first so that the traversal starts with a tight t_max
+    const uint32_t* hint_tri;
     // shadow rays traced by the next bounce's k_trace (S2Tuning::shadow_merge): the shade kernel
     // counts its shadow rays in C_SHADOW1 when sh_parity is 1, so that the previous bounce's count
     // stays readable while they are traced; sh_merge tells k_bounce_setup which count to retire
@@ -426,6 +429,23 @@ S2D void extend_queue(const PTParams& P, uint32_t parity, uint2* stack) {
             const float4 a = q.s0[ray], b = q.s1[ray];
             r = make_trav_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), 0.f);
             trav_begin(st, h, S2_INF);
+            if (P.hint_tri) {
+                // the pixel centre's triangle as a first candidate: a hit there becomes the closest
+                // hit so far, exactly as if the traversal had found it first (hits are resolved by
+                // distance, then by the lowest instance and primitive, in any visiting order)
+                const uint32_t ti = P.hint_tri[__float_as_uint(q.s2[ray].z) % P.pixels];
+                if (ti != 0xffffffffu) {
+                    const float4 t0 = __ldg(P.scene.tris + 3 * (size_t)ti), t1 = __ldg(P.scene.tris + 3 * (size_t)ti + 1);
+                    const float4 t2 = __ldg(P.scene.tris + 3 * (size_t)ti + 2);
+                    float t, b1, b2;
+                    if (COUNT) c.tris++;
+                    if (!(__float_as_uint(t2.w) & S2_TRI_ALPHA_TESTED) &&
+                        intersect_triangle(r, ld3(t0), ld3(t1), ld3(t2), h.t, t, b1, b2)) {
+                        h.t = t; h.tri = ti; h.instance = __float_as_uint(t0.w); h.primitive = __float_as_uint(t1.w);
+                        h.b1 = b1; h.b2 = b2;
+                    }
+                }
+            }
         }
         // counting runs take the sequential nearest-first walk, the order the CPU BVH8 walker
         // restates.  The postponed-triangle order visits the same nodes: a lane tests its pending
@@ -451,6 +471,22 @@ template <bool COUNT>
 __global__ void __launch_bounds__(kTravBlock) k_extend(const __grid_constant__ PTParams P, uint32_t parity) {
     __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
     extend_queue<COUNT>(P, parity, stack);
+}
+
+// The closest-hit triangle record (or none) of every pixel's centre ray, for the camera launch's
+// first candidate.  One thread per pixel.
+__global__ void __launch_bounds__(kTravBlock) k_pixel_hint(const __grid_constant__ PTParams P, uint32_t* __restrict__ hint) {
+    __shared__ uint2 stack[S2_STACK_SMEM * kTravBlock];
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= P.pixels) return;
+    const uint32_t px = pix % P.width, py = pix / P.width;
+    const float3 d = camera_dir(P.proj, P.imin, P.imax, P.cam, px, py, 0.5f, 0.5f);
+    TravHit h;
+    TravCounters c{0, 0};
+    const SceneAlphaTest alpha{&P.scene, !(P.flags & S2F_NO_ALPHA)};
+    traverse<false, false>(make_trav_ray(f3(P.cam[3], P.cam[7], P.cam[11]), d, 0.f), S2_INF, P.scene.nodes, P.scene.tris,
+                           stack + threadIdx.x, kTravBlock, h, c, alpha);
+    hint[pix] = h.tri;
 }
 
 // The persistent any-hit loop over the shadow queue (sh_o: origin + t_max, sh_d: direction): warps
