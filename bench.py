@@ -587,7 +587,7 @@ def vcm_line(dev, iterations: int = 3) -> dict:
     segments (the VCM renderer's default), one light subpath per pixel, power-proportional light
     pick.  Device time per iteration (a light pass and a camera pass) and rays traced per second,
     for path tracing, BPT with the light vertex cache (the reference's default algorithm), the same
-    with the DI and light-vertex-cache reservoirs (32 and 8 candidates, DI reuse), BPT connecting to
+    with the DI and light-vertex-cache reservoirs (32 and 8 candidates, both reused), BPT connecting to
     whole light subpaths, and VCM."""
     from stratum2_b200 import _abi
     from stratum2_b200.scenegen import terrain_scene
@@ -600,7 +600,8 @@ def vcm_line(dev, iterations: int = 3) -> dict:
     for name, algo, fl in (("path_trace", _abi.VCM_PATH_TRACE, 0),
                            ("bpt_light_vertex_cache", _abi.VCM_BPT, lvc),
                            ("bpt_light_vertex_cache_reservoirs", _abi.VCM_BPT,
-                            lvc | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
+                            lvc | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_LVC_REUSE | _abi.VCM_FLAG_DI_RIS |
+                            _abi.VCM_FLAG_DI_REUSE),
                            ("bpt", _abi.VCM_BPT, 0), ("vcm", _abi.VCM_VCM, 0)):
         p = dev.default_vcm_params()
         p.algorithm, p.vcm_flags, p.iterations = algo, fl, 1

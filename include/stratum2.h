@@ -617,8 +617,12 @@ int  s2_tonemap(S2Context* ctx, uint32_t width, uint32_t height, const S2Tonemap
                                                       each camera vertex resamples lvc_candidates
                                                       random cached light vertices by the luminance
                                                       of their connection and traces one shadow ray
-                                                      (vcm.slang:568-736; the reuse of these
-                                                      reservoirs is not built) */
+                                                      (vcm.slang:568-736) */
+#define S2_VCM_FLAG_LVC_REUSE           (1u << 6)  /* with LVC_RIS, eReuse: each camera vertex also
+                                                      resamples an LVC reservoir of the previous
+                                                      iteration (or call) found in a world-space hash
+                                                      grid near it, and stores its own with the light
+                                                      vertex by value (vcm.slang:633-726) */
 #define S2_VCM_FLAG_DI_REUSE            (1u << 4)  /* with DI_RIS, eReuse: each camera vertex also
                                                       resamples a reservoir of the previous iteration
                                                       (or call) found in a world-space hash grid near it
@@ -645,6 +649,8 @@ typedef struct S2VcmParams {
     float di_max_m;                  /* mDIReservoirMaxM (default 3, VCM.cpp:34): stored M is capped
                                         at di_max_m x di_candidates */
     uint32_t lvc_candidates;         /* mLVCReservoirSampleCount (default 8, VCM.cpp:35), 1..1024 */
+    float lvc_max_m;                 /* mLVCReservoirMaxM (default 3, VCM.cpp:36): stored M is capped
+                                        at lvc_max_m x lvc_candidates */
 } S2VcmParams;
 
 void s2_default_vcm_params(S2VcmParams* p);

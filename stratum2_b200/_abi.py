@@ -191,7 +191,7 @@ class S2TonemapParams(C.Structure):
 # vertex connection and merging (S2_VCM_*)
 VCM_PATH_TRACE, VCM_LIGHT_TRACE, VCM_PPM, VCM_BPM, VCM_BPT, VCM_VCM = range(6)
 VCM_FLAG_LIGHT_VERTEX_CACHE, VCM_FLAG_DEBUG_PATHS, VCM_FLAG_DEBUG_UNWEIGHTED = 1 << 0, 1 << 1, 1 << 2
-VCM_FLAG_DI_RIS, VCM_FLAG_DI_REUSE, VCM_FLAG_LVC_RIS = 1 << 3, 1 << 4, 1 << 5
+VCM_FLAG_DI_RIS, VCM_FLAG_DI_REUSE, VCM_FLAG_LVC_RIS, VCM_FLAG_LVC_REUSE = 1 << 3, 1 << 4, 1 << 5, 1 << 6
 
 
 class S2VcmParams(C.Structure):
@@ -200,7 +200,8 @@ class S2VcmParams(C.Structure):
                 ("flags", C.c_uint32), ("vcm_flags", C.c_uint32), ("light_path_fraction", C.c_float),
                 ("merge_radius_factor", C.c_float), ("merge_radius_alpha", C.c_float), ("exposure", C.c_float),
                 ("debug_camera_vertices", C.c_uint16), ("debug_light_vertices", C.c_uint16),
-                ("di_candidates", C.c_uint32), ("di_max_m", C.c_float), ("lvc_candidates", C.c_uint32)]
+                ("di_candidates", C.c_uint32), ("di_max_m", C.c_float), ("lvc_candidates", C.c_uint32),
+                ("lvc_max_m", C.c_float)]
 
 
 class S2RenderStats(C.Structure):
@@ -215,7 +216,7 @@ class S2RenderStats(C.Structure):
 assert C.sizeof(S2Ray) == 32 and C.sizeof(S2Hit) == 20
 assert C.sizeof(S2RenderParams) == 80
 assert C.sizeof(S2CacheParams) == 80
-assert C.sizeof(S2VcmParams) == 64
+assert C.sizeof(S2VcmParams) == 68
 
 _lib = None
 

@@ -65,15 +65,17 @@ S2D uint32_t hg_find_cell(const HashGridDev& g, float3 pos, float cell_size) {
     return 0xffffffffu;
 }
 
-// Append (hashgrid.hlsli:77-97)
-S2D void hg_append(const HashGridDev& g, float3 pos, const ReservoirRecord& rec) {
+// Append (hashgrid.hlsli:77-97): returns the record's data index, 0xffffffff when the grid is full
+// (grids with a wider payload store it in their own array at that index).
+S2D uint32_t hg_append(const HashGridDev& g, float3 pos, const ReservoirRecord& rec) {
     const uint32_t cell = hg_find_cell<true>(g, pos, hg_cell_size(g, pos));
-    if (cell == 0xffffffffu) return;
+    if (cell == 0xffffffffu) return 0xffffffffu;
     const uint32_t idx = atomicAdd(&g.other[0], 1u);
-    if (idx >= g.max_size) return;
+    if (idx >= g.max_size) return 0xffffffffu;
     const uint32_t in_cell = atomicAdd(&g.cell_counters[cell], 1u);
     g.append_indices[idx] = make_uint2(cell, in_cell);
     g.data[idx] = rec;
+    return idx;
 }
 
 // Building the grid (the work of ComputeIndices and Swizzle, hashgrid.hlsli:101-119), so that the

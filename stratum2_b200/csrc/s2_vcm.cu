@@ -33,7 +33,8 @@ namespace {
 constexpr uint32_t kVcmRenderFlags = S2_FLAG_LAMBERTIAN | S2_FLAG_PCG32 | S2_FLAG_NO_RR | S2_FLAG_SHADING_NORMALS_OFF |
                                      S2_FLAG_ALPHA_TEST_OFF | S2_FLAG_NORMAL_MAPS_OFF | S2_FLAG_LIGHT_POWER_PICK;
 constexpr uint32_t kVcmOwnFlags = S2_VCM_FLAG_LIGHT_VERTEX_CACHE | S2_VCM_FLAG_DEBUG_PATHS | S2_VCM_FLAG_DEBUG_UNWEIGHTED |
-                                   S2_VCM_FLAG_DI_RIS | S2_VCM_FLAG_DI_REUSE | S2_VCM_FLAG_LVC_RIS;
+                                   S2_VCM_FLAG_DI_RIS | S2_VCM_FLAG_DI_REUSE | S2_VCM_FLAG_LVC_RIS |
+                                   S2_VCM_FLAG_LVC_REUSE;
 
 void invert_affine(const float* m, float* out) {
     // inverse of a row-major 3x4 rigid (or scaled) transform
@@ -51,12 +52,15 @@ void invert_affine(const float* m, float* out) {
     }
 }
 
-// The world-space grids of the direct-illumination reservoirs (GpuHashGrid, src/App/GpuHashGrid.cpp:
-// 17-111, as the path tracer's reuse grids): appended to by one iteration's camera pass, read by
-// the next one's.
+// The world-space grids of the direct-illumination and light-vertex-cache reservoirs (GpuHashGrid,
+// src/App/GpuHashGrid.cpp:17-111, as the path tracer's reuse grids): appended to by one iteration's
+// camera pass, read by the next one's.  An LVC grid keeps its 128-byte records in `wide`, at the
+// data index of each record's sort key.
 struct DiGrid {
     std::vector<DevBuf> bufs;
     HashGridDev g{};
+    void* wide = nullptr;
+    size_t wide_bytes = 0;
     unsigned long long *keys_in = nullptr, *keys_out = nullptr;
     uint32_t* vals_in = nullptr;
     void* sort_tmp = nullptr;
@@ -64,10 +68,12 @@ struct DiGrid {
     int end_bit = 64;
 };
 
-int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size) {
-    if (G.g.checksums && G.g.cell_count == cells && G.g.max_size >= size) return S2_OK;
+int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size, size_t wide_bytes = 0) {
+    if (G.g.checksums && G.g.cell_count == cells && G.g.max_size >= size && G.wide_bytes == wide_bytes) return S2_OK;
     free_bufs(G.bufs);
     G.g = HashGridDev{};
+    G.wide = nullptr;
+    G.wide_bytes = 0;
     HashGridDev g{};
     auto al = [&](size_t bytes) { return dev_alloc(ctx, G.bufs, bytes); };
     g.checksums = (uint32_t*)al(sizeof(uint32_t) * cells);
@@ -87,8 +93,10 @@ int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size) {
     cub::DeviceRadixSort::SortPairs(nullptr, G.sort_bytes, G.keys_in, G.keys_out, G.vals_in, g.data_indices, (int)size, 0,
                                     G.end_bit, ctx->stream);
     G.sort_tmp = al(std::max<size_t>(G.sort_bytes, 16));
+    if (wide_bytes) G.wide = al(wide_bytes * size);
     for (auto& b : G.bufs) if (!b.ptr) { free_bufs(G.bufs); return S2_ERR_OOM; }
-    if (G.bufs.size() != 11) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    if (G.bufs.size() != (wide_bytes ? 12u : 11u)) { free_bufs(G.bufs); return S2_ERR_OOM; }
+    G.wide_bytes = wide_bytes;
     g.cell_count = cells;
     g.max_size = size;
     G.g = g;
@@ -113,7 +121,8 @@ void launch_light(const vk::VcmArgs& A, cudaStream_t s) {
 }
 template <bool LAMBERT>
 void launch_camera(const vk::VcmArgs& A, cudaStream_t s) {
-    vk::k_vcm_camera<LAMBERT><<<(A.pixels + 127) / 128, 128, 0, s>>>(A);
+    if (A.lvc_m) vk::k_vcm_camera<LAMBERT, true><<<(A.pixels + 127) / 128, 128, 0, s>>>(A);
+    else vk::k_vcm_camera<LAMBERT, false><<<(A.pixels + 127) / 128, 128, 0, s>>>(A);
 }
 
 }  // namespace
@@ -125,10 +134,14 @@ struct VcmState {
     DiGrid grid[2];
     uint32_t cur = 0;
     bool prev_valid = false;
+    DiGrid lvc_grid[2];  // the light-vertex-cache reservoirs, likewise
+    uint32_t lvc_cur = 0;
+    bool lvc_prev_valid = false;
 };
 void destroy_vcm_state(S2Context* ctx) {
     if (!ctx || !ctx->vcm) return;
     for (auto& g : ctx->vcm->grid) free_bufs(g.bufs);
+    for (auto& g : ctx->vcm->lvc_grid) free_bufs(g.bufs);
     delete ctx->vcm;
     ctx->vcm = nullptr;
 }
@@ -148,6 +161,7 @@ extern "C" void s2_default_vcm_params(S2VcmParams* p) {
     p->di_candidates = 32;                           // VCM.cpp:33-35
     p->di_max_m = 3.f;
     p->lvc_candidates = 8;
+    p->lvc_max_m = 3.f;
 }
 
 extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmParams* prm, const S2Aovs* out, int out_on_host,
@@ -174,6 +188,10 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
         return set_error(ctx, S2_ERR_INVALID, "LVC_RIS needs LIGHT_VERTEX_CACHE");
     if (lvc_ris && (prm->lvc_candidates < 1 || prm->lvc_candidates > 1024))
         return set_error(ctx, S2_ERR_INVALID, "lvc_candidates must be in 1..1024");
+    const bool lvc_reuse = (prm->vcm_flags & S2_VCM_FLAG_LVC_REUSE) != 0;
+    if (lvc_reuse && !lvc_ris) return set_error(ctx, S2_ERR_INVALID, "LVC_REUSE needs LVC_RIS");
+    if (lvc_reuse && !(prm->lvc_max_m > 0.f && std::isfinite(prm->lvc_max_m)))
+        return set_error(ctx, S2_ERR_INVALID, "lvc_max_m must be finite and > 0");
     const bool di_ris = (prm->vcm_flags & S2_VCM_FLAG_DI_RIS) != 0;
     if ((prm->vcm_flags & S2_VCM_FLAG_DI_REUSE) && !di_ris) return set_error(ctx, S2_ERR_INVALID, "DI_REUSE needs DI_RIS");
     if (di_ris && (prm->di_candidates < 1 || prm->di_candidates > 1024))
@@ -234,11 +252,30 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
     A.di_m = prm->di_candidates;
     A.di_max_m = prm->di_max_m;
     A.lvc_m = lvc_ris ? prm->lvc_candidates : 0u;
+    A.lvc_reuse = lvc_reuse ? 1u : 0u;
+    A.lvc_max_m = prm->lvc_max_m;
     s2::VcmState* vs = nullptr;
-    if (di_reuse) {
+    if (di_reuse || lvc_reuse) {
         if (!ctx->vcm) ctx->vcm = new (std::nothrow) s2::VcmState();
         vs = ctx->vcm;
         if (!vs) return set_error(ctx, S2_ERR_OOM, "VCM state allocation failed");
+    }
+    if (lvc_reuse) {
+        // VCM.cpp:27, 491-500: as the DI grid, one record per camera vertex
+        const uint32_t cells = 100000u;
+        const uint32_t size = (uint32_t)std::min<uint64_t>((uint64_t)pixels * std::max(1u, prm->max_path_length - 1), 1u << 24);
+        for (auto& g : vs->lvc_grid) {
+            const int rc0 = ensure_di_grid(ctx, g, cells, size, sizeof(vk::LvcRecord));
+            if (rc0 != S2_OK) { vs->lvc_prev_valid = false; return set_error(ctx, rc0, "LVC reservoir grid allocation failed"); }
+            g.g.min_cell_size = 0.1f;
+            g.g.cell_pixel_radius = 0.f;
+            g.g.camera_position = make_float3(view->camera_to_world[3], view->camera_to_world[7], view->camera_to_world[11]);
+            g.g.distance_scale = 0.f;
+        }
+    } else if (ctx->vcm) {
+        ctx->vcm->lvc_prev_valid = false;  // a call without LVC reuse drops its grids
+    }
+    if (di_reuse) {
         // VCM.cpp:26, 490-499: 100,000 cells of at least 0.1, one record per camera vertex
         const uint32_t cells = 100000u;
         const uint32_t size = (uint32_t)std::min<uint64_t>((uint64_t)pixels * std::max(1u, prm->max_path_length - 1), 1u << 24);
@@ -362,12 +399,31 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
                 A.di_prev = vs->grid[vs->cur ^ 1].g;
                 A.di_prev_valid = vs->prev_valid ? 1u : 0u;
             }
+            DiGrid* lcur = nullptr;
+            if (lvc_reuse) {
+                lcur = &vs->lvc_grid[vs->lvc_cur];
+                const HashGridDev& g = lcur->g;
+                cudaMemsetAsync(g.checksums, 0, sizeof(uint32_t) * g.cell_count, s);
+                cudaMemsetAsync(g.cell_counters, 0, sizeof(uint32_t) * g.cell_count, s);
+                cudaMemsetAsync(g.other, 0, sizeof(uint32_t) * 4, s);
+                A.lvc_cur = g;
+                A.lvc_cur_rec = (vk::LvcRecord*)lcur->wide;
+                const DiGrid& prev = vs->lvc_grid[vs->lvc_cur ^ 1];
+                A.lvc_prev = prev.g;
+                A.lvc_prev_rec = (const vk::LvcRecord*)prev.wide;
+                A.lvc_prev_valid = vs->lvc_prev_valid ? 1u : 0u;
+            }
             if (lam) launch_camera<true>(A, s); else launch_camera<false>(A, s);
             launches += 1;
             if (cur) {  // this iteration's reservoirs become the next one's previous grid
                 launches += build_di_grid(*cur, s);
                 vs->cur ^= 1u;
                 vs->prev_valid = true;
+            }
+            if (lcur) {
+                launches += build_di_grid(*lcur, s);
+                vs->lvc_cur ^= 1u;
+                vs->lvc_prev_valid = true;
             }
         }
     }

@@ -31,6 +31,25 @@ struct LightVertex {
     float4 e;  // the subpath's area-measure pdf up to this vertex (mPathPdfA), unused x 3
 };
 
+// One stored light-vertex-cache reservoir (LVCReservoir, compat/vcm.h:92-101): the selected light
+// vertex by value (the cache is rebuilt every iteration), the camera vertex it was resampled at (on
+// its triangle, with the MIS quantities its connections use) and the reservoir's M, integration
+// weight and target pdf.  128 bytes.  A reservoir without a sample keeps a zero-throughput vertex.
+struct LvcRecord {
+    LightVertex lv;
+    float3 local_pos;     // camera vertex, object space of its instance
+    uint32_t instance;
+    uint32_t primitive;
+    uint32_t in_dir;      // packed world direction toward the previous camera vertex
+    uint32_t len;         // camera vertices so far
+    float dvcm;
+    float dvc;
+    float M;
+    float W;
+    float phat;
+};
+static_assert(sizeof(LvcRecord) == 128, "LvcRecord is two 64-byte lines");
+
 struct VcmArgs {
     DevScene scene;
     float proj[8];
@@ -71,6 +90,13 @@ struct VcmArgs {
     float di_max_m;
     HashGridDev di_cur, di_prev;
     uint32_t lvc_m;                // light-vertex-cache reservoirs (S2_VCM_FLAG_LVC_RIS): candidates, 0 = off
+    // their reuse (S2_VCM_FLAG_LVC_REUSE): M cap, this iteration's grid (appended; records in
+    // lvc_cur_rec at the grid's data index) and the previous one's (read)
+    uint32_t lvc_reuse, lvc_prev_valid;
+    float lvc_max_m;
+    HashGridDev lvc_cur, lvc_prev;
+    LvcRecord* lvc_cur_rec;
+    const LvcRecord* lvc_prev_rec;
 };
 
 // Mis() (compat/vcm.h:9-11): power heuristic with exponent 2.
@@ -354,39 +380,151 @@ S2D float3 vcm_connect(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd
     return contrib;
 }
 
-// ConnectToLVCReservoir without reuse (vcm.slang:568-627, 681-696, 728-736): lvc_m cached light
-// vertices picked at random, resampled by the target lum(throughput x pathPdfA x connection) with
-// source pdf pathPdfA (the discrete pick's 1 / count cancels in the estimate), one shadow ray for
-// the chosen one.  Returns the contribution to add with the camera throughput, already scaled by
-// cached vertices / light subpaths.
+// GetTargetPdf (vcm.slang:584-608): lum(throughput x pathPdfA x connection) of light vertex v at the
+// camera vertex (sd, in, p), 0 outside the path-length range; `c` receives that weighted
+// connection.  With `vis` the connection's visibility is traced too, and an occluded one gives 0.
 template <bool LAMBERT>
-S2D float3 vcm_connect_lvc_ris(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp,
-                               const SubPath& p, uint32_t total, Rng& rng) {
+S2D float vcm_lvc_target(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp, const SubPath& p,
+                         const LightVertex& v, bool vis, float3& c) {
+    c = f3(0.f);
+    const uint32_t vlen = __float_as_uint(v.c.w);
+    const uint32_t full = vlen + 1 + p.len;
+    if (full < A.min_len || full > A.max_len || !vcm_pass(A, p.len + 1, vlen + 1)) return 0.f;
+    const float pdfa = v.e.x;
+    const float3 thr = f3(v.b.x, v.b.y, v.b.z);
+    if (!(pdfa > 0.f) || !any_pos(thr)) return 0.f;
+    c = thr * pdfa * vcm_connect<LAMBERT>(A, T, m, sd, in, cp, p, v, vis);
+    return luminance(c);
+}
+
+// The same target, visibility included, at the camera vertex of a stored reservoir (rebuilt from
+// its triangle, as Reuse does with PackedVcmVertex, vcm.slang:647-653).
+template <bool LAMBERT>
+S2D float vcm_lvc_target_at(const VcmArgs& A, VcmTrace& T, const LvcRecord& q, const LightVertex& v, bool sn) {
+    SD sdq = make_shading_local(A.scene, q.instance, q.primitive, q.local_pos, sn);
+    const Mat mq = load_material(A.scene, sdq.mat, sdq.uv);
+    if (!(A.flags & S2F_NO_NORMAL_MAPS)) apply_normal_map(A.scene, sdq);
+    const float3 inq = sdq.to_local(unpack_normal(q.in_dir));
+    const float cpq = (A.flags & S2F_NO_RR) ? 1.f : cont_prob(mq);
+    SubPath pq;
+    pq.thr = f3(1.f);
+    pq.dvcm = q.dvcm; pq.dvc = q.dvc; pq.dvm = 0.f;
+    pq.fwd_pdfw = 0.f;
+    pq.len = q.len;
+    pq.specular = false;
+    pq.pdfa = 0.f;
+    float3 c;
+    return vcm_lvc_target<LAMBERT>(A, T, mq, sdq, inq, cpq, pq, v, true, c);
+}
+
+// The reuse and the store of ConnectToLVCReservoir (vcm.slang:697-726): updates the reservoir
+// (wsum, phat_sel, c_sel, v_sel) in place.
+template <bool LAMBERT>
+S2D void vcm_lvc_reuse(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp, const SubPath& p,
+                       const TravHit& h, float3 dir, Rng& rng, float& wsum, float& phat_sel, float3& c_sel,
+                       LightVertex& v_sel) {
+    const bool sn = !(A.flags & S2F_NO_SN);
+    const uint32_t inst = h.instance, prim = h.primitive;
+    const float M = (float)A.lvc_m;
+    float Mres = M;
+    if (A.lvc_prev_valid) {
+        const float4 j = rng.next_float();
+        float3 t, b;
+        make_orthonormal(sd.gn, t, b);
+        const float csz = hg_cell_size(A.lvc_prev, sd.pos);
+        const float3 qp = sd.pos + (t * (j.x * 2.f - 1.f) + b * (j.y * 2.f - 1.f)) * csz;
+        const uint32_t cell = hg_find_cell<false>(A.lvc_prev, qp, hg_cell_size(A.lvc_prev, qp));
+        if (cell != 0xffffffffu) {
+            const uint32_t count = A.lvc_prev.cell_counters[cell];
+            if (count > 0) {
+                const uint32_t off = A.lvc_prev.indices[cell];
+                const LvcRecord q = A.lvc_prev_rec[A.lvc_prev.data_indices[off + rng.next().x % count]];
+                const float u = rng.next_float().x;
+                if (q.M > 0.f) {
+                    // target pdfs: q's sample here, and the current sample in q's domain
+                    float3 c_new = f3(0.f);
+                    const float phat_new = q.W > 0.f && q.phat > 0.f
+                                               ? vcm_lvc_target<LAMBERT>(A, T, m, sd, in, cp, p, q.lv, true, c_new) : 0.f;
+                    const float phat_i_old = phat_sel > 0.f ? vcm_lvc_target_at<LAMBERT>(A, T, q, v_sel, sn) : 0.f;
+                    const float a0 = phat_sel * Mres, b0 = phat_i_old * q.M;
+                    const float a1 = q.phat * q.M, b1 = phat_new * Mres;
+                    const float m0 = a0 + b0 > 0.f ? a0 / (a0 + b0) : 0.f;
+                    const float m1 = a1 + b1 > 0.f ? a1 / (a1 + b1) : 0.f;
+                    const float iw0 = phat_sel > 0.f ? wsum / phat_sel : 0.f;
+                    Mres += q.M;
+                    const float w0 = m0 * phat_sel * iw0;
+                    const float w1 = m1 * phat_new * q.W;
+                    wsum = w0 + w1;
+                    if (u * wsum <= w1) { v_sel = q.lv; phat_sel = phat_new; c_sel = c_new; }
+                }
+            }
+        }
+    }
+    LvcRecord rec;
+    rec.lv = v_sel;
+    rec.local_pos = xform_point(A.scene.inv_transforms + 3 * (size_t)inst, sd.pos);
+    rec.instance = inst;
+    rec.primitive = prim;
+    rec.in_dir = pack_normal(-dir);
+    rec.len = p.len;
+    rec.dvcm = p.dvcm;
+    rec.dvc = p.dvc;
+    rec.M = fminf(Mres, A.lvc_max_m * M);
+    rec.W = phat_sel > 0.f ? wsum / phat_sel : 0.f;
+    rec.phat = phat_sel;
+    ReservoirRecord key;  // what the grid build sorts a cell's records by
+    key.local_pos = rec.local_pos;
+    key.instance = inst;
+    key.rnd = make_float4(v_sel.a.x, v_sel.a.y, v_sel.a.z, v_sel.b.x);
+    key.target_pdf = rec.phat;
+    key.W = rec.W;
+    key.M = rec.M;
+    key.primitive = prim;
+    key.local_dir_in = f3(0.f);
+    key.pad = 0.f;
+    const uint32_t idx = hg_append(A.lvc_cur, sd.pos, key);
+    if (idx != 0xffffffffu) A.lvc_cur_rec[idx] = rec;
+}
+
+// ConnectToLVCReservoir (vcm.slang:568-736): lvc_m cached light vertices picked at random,
+// resampled by the target above with source pdf pathPdfA (the discrete pick's 1 / count cancels in
+// the estimate), one shadow ray for the chosen one.  With reuse (S2_VCM_FLAG_LVC_REUSE) a reservoir
+// of the previous iteration found in the hash grid near the vertex is resampled in with the
+// pairwise MIS weights of Reuse (vcm.slang:633-678), and this vertex's reservoir is stored for the
+// next iteration: every one, also those of weight 0, as with the direct-illumination reservoirs (a
+// population of successes only would be conditional on success and too bright).  Returns the
+// contribution to add with the camera throughput, already scaled by cached vertices / light
+// subpaths.  (h, dir): the camera vertex's hit and the ray that reached it.  Out of line: inlined,
+// the reservoir state spills in the camera kernel.
+template <bool LAMBERT>
+__device__ __noinline__ float3 vcm_connect_lvc_ris(const VcmArgs& A, VcmTrace& T, const Mat& m, const SD& sd, float3 in, float cp,
+                               const SubPath& p, uint32_t total, const TravHit& h, float3 dir, Rng& rng) {
     float wsum = 0.f, phat_sel = 0.f;
     float3 c_sel = f3(0.f);
     LightVertex v_sel;
+    v_sel.a = v_sel.b = v_sel.c = v_sel.e = make_float4(0.f, 0.f, 0.f, 0.f);
+    v_sel.d = make_uint4(0u, 0u, 0u, 0u);
     const float M = (float)A.lvc_m;
     for (uint32_t i = 0; i < A.lvc_m; ++i) {
         const LightVertex v = A.lv[A.lvc_list[rng.next().x % total]];
         const float u = rng.next_float().x;
-        const uint32_t vlen = __float_as_uint(v.c.w);
-        const uint32_t full = vlen + 1 + p.len;
-        if (full < A.min_len || full > A.max_len || !vcm_pass(A, p.len + 1, vlen + 1)) continue;
-        const float pdfa = v.e.x;
-        if (!(pdfa > 0.f)) continue;
-        const float3 c = f3(v.b.x, v.b.y, v.b.z) * pdfa * vcm_connect<LAMBERT>(A, T, m, sd, in, cp, p, v, false);
-        const float phat = luminance(c);
+        float3 c;
+        const float phat = vcm_lvc_target<LAMBERT>(A, T, m, sd, in, cp, p, v, false, c);
         if (!(phat > 0.f)) continue;
-        const float wi = phat / (pdfa * M);
+        const float wi = phat / (v.e.x * M);
         wsum += wi;
         if (u * wsum <= wi) { phat_sel = phat; c_sel = c; v_sel = v; }
     }
+    if (phat_sel > 0.f) {
+        const float3 lpos = f3(v_sel.a.x, v_sel.a.y, v_sel.a.z);
+        float3 d = lpos - sd.pos;
+        const float dist = length(d);
+        d = d / dist;
+        if (!vcm_visible(A, T, ray_offset(sd.pos, sd.gn, d), d, dist * 0.99f)) phat_sel = 0.f;
+    }
+    if (A.lvc_reuse)
+        vcm_lvc_reuse<LAMBERT>(A, T, m, sd, in, cp, p, h, dir, rng, wsum, phat_sel, c_sel, v_sel);
     if (!(phat_sel > 0.f)) return f3(0.f);
-    const float3 lpos = f3(v_sel.a.x, v_sel.a.y, v_sel.a.z);
-    float3 d = lpos - sd.pos;
-    const float dist = length(d);
-    d = d / dist;
-    if (!vcm_visible(A, T, ray_offset(sd.pos, sd.gn, d), d, dist * 0.99f)) return f3(0.f);
     return c_sel * ((wsum / phat_sel) * ((float)total / (float)A.n_light));
 }
 
@@ -553,7 +691,9 @@ S2D VcmReservoir vcm_di_reservoir(const VcmArgs& A, VcmTrace& T, const SD& sd, u
     return res;
 }
 
-template <bool LAMBERT>
+// LVC_RIS: the variant for the light-vertex-cache reservoirs (lvc_m > 0), compiled apart so that
+// the other techniques' code keeps its registers.
+template <bool LAMBERT, bool LVC_RIS>
 __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmArgs A) {
     __shared__ uint2 stack[S2_STACK_SMEM * 128];
     VcmTrace T{stack + threadIdx.x, 128u, 0u, 0u, false, {0, 0}};
@@ -680,9 +820,10 @@ __global__ void __launch_bounds__(128) k_vcm_camera(const __grid_constant__ VcmA
                     }
                 }
                 if (!A.path_trace_only) {
-                    if (A.use_vc && A.lvc && A.lvc_total && A.lvc_m) {
+                    if (LVC_RIS && A.use_vc && A.lvc && A.lvc_total) {
                         const uint32_t total = *A.lvc_total;
-                        if (total > 0) L = L + p.thr * vcm_connect_lvc_ris<LAMBERT>(A, T, m, sd, in, cp, p, total, rng);
+                        if (total > 0)
+                            L = L + p.thr * vcm_connect_lvc_ris<LAMBERT>(A, T, m, sd, in, cp, p, total, h, dir, rng);
                     } else if (A.use_vc && A.lvc && A.lvc_total) {
                         // ConnectToLVC (vcm.slang:732-753): one random cached vertex, weighted by the
                         // cached vertex count over the light subpath count

@@ -9,9 +9,9 @@ vcm.slang:880-1238, SmallVCM's techniques with the dVCM / dVC / dVM MIS quantiti
   bookkeeping is checked without MIS.
 * Merging is consistent: BPM, VCM and PPM approach the golden image as the merge radius shrinks.
 * Direct illumination by resampled reservoirs (the reference's gDIReservoirFlags eRIS and eReuse,
-  vcm.slang:251-390) and the resampled light-vertex-cache connection (gLVCReservoirFlags eRIS,
-  vcm.slang:568-736) leave these images unchanged in expectation: path tracing and BPT with them,
-  with and without the reuse of the previous iteration's DI reservoirs through the hash grid,
+  vcm.slang:251-390) and the resampled light-vertex-cache connection (gLVCReservoirFlags eRIS and
+  eReuse, vcm.slang:568-736) leave these images unchanged in expectation: path tracing and BPT with
+  them, with and without the reuse of the previous iteration's reservoirs through the hash grids,
   converge to the same golden image.
 """
 from pathlib import Path
@@ -28,10 +28,13 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 W = H = 64
 
 
-def vparams(algo, iters, seed, vcm_flags=0, fraction=1.0, radius=0.025, first=0, lengths=(2, 5), di_m=None):
+def vparams(algo, iters, seed, vcm_flags=0, fraction=1.0, radius=0.025, first=0, lengths=(2, 5), di_m=None,
+            lvc_max_m=None):
     p = Device.default_vcm_params()
     if di_m is not None:
         p.di_candidates = di_m
+    if lvc_max_m is not None:
+        p.lvc_max_m = lvc_max_m
     p.algorithm, p.iterations, p.frame_seed = algo, iters, seed
     p.min_path_length, p.max_path_length = lengths
     p.flags = _abi.FLAG_LAMBERTIAN
@@ -169,12 +172,15 @@ def test_vcm_reproducible_aovs_and_argument_checks(device, box):
     (_abi.VCM_BPT, _abi.VCM_FLAG_DI_RIS),
     (_abi.VCM_PATH_TRACE, _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
     (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
+    (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_LVC_REUSE),
+    (_abi.VCM_BPT, _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_LVC_REUSE |
+     _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE),
 ])
 def test_di_reservoirs_converge_to_golden(device, box, algo, vcm_flags):
-    """Resampled direct illumination (8 candidates per camera vertex), with and without reuse, is
-    unbiased: the image converges to the FP64 golden.  With reuse, neighbouring pixels share
-    reservoirs, so the bias check is on the image total (one value per independent batch) and the
-    per-pixel z-test only bounds the outliers."""
+    """Resampled direct illumination (8 candidates per camera vertex) and resampled light-vertex-cache
+    connections, with and without reuse, are unbiased: the image converges to the FP64 golden.  With
+    reuse, neighbouring pixels share reservoirs, so the bias check is on the image total (one value
+    per independent batch) and the per-pixel z-test only bounds the outliers."""
     wl, ref, ref_v = box
     device.upload_scene(wl.scene)
     device.render_vcm(wl.view, W, H, vparams(algo, 1, 1))  # a call without reuse drops old reservoirs
@@ -184,7 +190,7 @@ def test_di_reservoirs_converge_to_golden(device, box, algo, vcm_flags):
     totals = img.sum(axis=(1, 2, 3))
     t = (totals.mean() - ref.sum()) / np.sqrt(totals.var(ddof=1) / len(totals) + ref_v.sum())
     assert abs(t) < 4.0, (t, rel)
-    if not vcm_flags & _abi.VCM_FLAG_DI_REUSE:
+    if not vcm_flags & (_abi.VCM_FLAG_DI_REUSE | _abi.VCM_FLAG_LVC_REUSE):
         assert abs(z.mean()) < 0.15, z.mean()
 
 
@@ -202,9 +208,35 @@ def test_di_reservoirs_reproducible_and_argument_checks(device, box):
     np.testing.assert_array_equal(seqs[0], seqs[1])
     ris = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 44, vcm_flags=_abi.VCM_FLAG_DI_RIS)).radiance
     assert not np.array_equal(seqs[0][2], ris)  # the third call reused the second's reservoirs
+    lvc = _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS
     for bad in (vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_REUSE),
                 vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_DI_RIS, di_m=0),
-                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_LVC_RIS)):
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_LVC_RIS),
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=_abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_REUSE),
+                vparams(_abi.VCM_BPT, 1, 0, vcm_flags=lvc | _abi.VCM_FLAG_LVC_REUSE, lvc_max_m=0.0)):
         with pytest.raises(_abi.S2Error) as e:
             device.render_vcm(wl.view, W, H, bad)
         assert e.value.code == _abi.S2_ERR_INVALID
+
+
+def test_lvc_reservoir_reuse_reproducible(device, box):
+    """LVC reservoir sequences reproduce bit for bit, a call reuses the previous call's reservoirs
+    (its image differs from resampling alone), and a call without reuse drops them."""
+    wl, _, _ = box
+    device.upload_scene(wl.scene)
+    lvc = _abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS
+    fl = lvc | _abi.VCM_FLAG_LVC_REUSE
+    seqs = []
+    for _ in range(2):
+        device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 1, 1))  # drops the grids
+        seqs.append(np.stack([device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 60 + 2 * k, vcm_flags=fl)).radiance
+                              for k in range(3)]))
+    np.testing.assert_array_equal(seqs[0], seqs[1])
+    assert np.all(np.isfinite(seqs[0]))
+    ris = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 64, vcm_flags=lvc)).radiance
+    assert not np.array_equal(seqs[0][2], ris)  # the third call reused the second's reservoirs
+    # after a call without reuse the first reuse call has no history: its first iteration resamples
+    # alone, so it differs from the same call made with the history of a reuse call
+    device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 1, 1))
+    fresh = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 60, vcm_flags=fl)).radiance
+    np.testing.assert_array_equal(fresh, seqs[0][0])
