@@ -114,9 +114,19 @@ S2D void cache_encode(const CacheDev& c, float3 p, __half2 out[kCacheLevels]) {
     }
 }
 
-// Levels l0 .. l0+3 of the encoding of one position (see cache_encode).
+// One corner entry (f16x2 bits) of a 16-byte quad: the 2 x 2 entries of one z layer of a brick.
+S2D uint32_t cache_quad_entry(uint4 q, uint32_t xb, uint32_t yb) {
+    const uint32_t lo = xb ? q.y : q.x, hi = xb ? q.w : q.z;
+    return yb ? hi : lo;
+}
+
+// Levels l0 .. l0+3 of the encoding of one position: the values of cache_encode, gathered by quads.
+// A z layer of the cell's 2 x 2 x 2 corners lies in 1, 2 or 4 quads (whether x0 and y0 are odd),
+// so a level issues 4.5 16-byte loads on average instead of eight 4-byte ones; the corners are
+// picked from the quads by selects and summed in cache_encode's order.
 S2D void cache_encode4(const CacheDev& c, float3 p, uint32_t l0, __half2 out[4]) {
     const float3 u = cache_unit(c, p);
+    const uint32_t mask = (1u << (c.log2_table - 3u)) - 1u;
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j) {
         const uint32_t l = l0 + j;
@@ -125,15 +135,42 @@ S2D void cache_encode4(const CacheDev& c, float3 p, uint32_t l0, __half2 out[4])
         const float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
         const float wx = fx - ix, wy = fy - iy, wz = fz - iz;
         const uint32_t x0 = (uint32_t)ix, y0 = (uint32_t)iy, z0 = (uint32_t)iz;
-        const __half2* tab = c.table + ((size_t)l << c.log2_table);
+        const uint32_t ox = x0 & 1u, oy = y0 & 1u, oz = z0 & 1u;
+        const uint32_t bx = x0 >> 1, by = y0 >> 1, bz = z0 >> 1;
+        const uint4* tq = (const uint4*)(c.table + ((size_t)l << c.log2_table));
+        // brick index = combine(x term, y term, z term) & mask, as in cache_index
+        const bool dense = c.dense[l] != 0;
+        const uint32_t n = c.nbrick[l];
+        const uint32_t tx0 = bx, tx1 = bx + ox;
+        const uint32_t ty0 = dense ? n * by : by * 2654435761u, ty1 = dense ? n * (by + oy) : (by + oy) * 2654435761u;
+        const uint32_t tz0 = dense ? n * n * bz : bz * 805459861u, tz1 = dense ? n * n * (bz + oz) : (bz + oz) * 805459861u;
         float a0 = 0.f, a1 = 0.f;
 #pragma unroll
-        for (uint32_t k = 0; k < 8; ++k) {
-            const uint32_t dx = k & 1u, dy = (k >> 1) & 1u, dz = k >> 2;
-            const float w = (dx ? wx : 1.f - wx) * (dy ? wy : 1.f - wy) * (dz ? wz : 1.f - wz);
-            const float2 f = __half22float2(__ldg(tab + cache_index(c, l, x0 + dx, y0 + dy, z0 + dz)));
-            a0 += w * f.x;
-            a1 += w * f.y;
+        for (uint32_t dz = 0; dz < 2; ++dz) {
+            const uint32_t tz = dz ? tz1 : tz0, zb = oz ^ dz;
+            const uint32_t b00 = (dense ? tx0 + ty0 + tz : tx0 ^ ty0 ^ tz) & mask;
+            const uint32_t b10 = (dense ? tx1 + ty0 + tz : tx1 ^ ty0 ^ tz) & mask;
+            const uint32_t b01 = (dense ? tx0 + ty1 + tz : tx0 ^ ty1 ^ tz) & mask;
+            const uint32_t b11 = (dense ? tx1 + ty1 + tz : tx1 ^ ty1 ^ tz) & mask;
+            const uint4 q00 = __ldg(tq + ((b00 << 1) | zb));
+            uint4 q10 = q00, q01 = q00, q11 = q00;
+            if (ox) q10 = __ldg(tq + ((b10 << 1) | zb));
+            if (oy) q01 = __ldg(tq + ((b01 << 1) | zb));
+            if (ox & oy) q11 = __ldg(tq + ((b11 << 1) | zb));
+            else q11 = ox ? q10 : q01;
+            const float wz_ = dz ? wz : 1.f - wz;
+#pragma unroll
+            for (uint32_t k = 0; k < 4; ++k) {
+                const uint32_t dx = k & 1u, dy = k >> 1;
+                const uint4 q = dx ? (dy ? q11 : q10) : (dy ? q01 : q00);
+                const uint32_t h = cache_quad_entry(q, ox ^ dx, oy ^ dy);
+                const float w = (dx ? wx : 1.f - wx) * (dy ? wy : 1.f - wy) * wz_;
+                __half2 hv;
+                *(uint32_t*)&hv = h;
+                const float2 f = __half22float2(hv);
+                a0 += w * f.x;
+                a1 += w * f.y;
+            }
         }
         out[j] = __floats2half2_rn(a0, a1);
     }
@@ -151,10 +188,13 @@ constexpr uint32_t kInfSmemW = 0;
 constexpr uint32_t kInfSmemX = kWImageBytes;                         // 128 x 32 f16
 constexpr uint32_t kInfSmemH = kInfSmemX + kCacheTile * kCacheIn * 2; // 128 x 64 f16
 constexpr uint32_t kInfSmemBytes = kInfSmemH + kCacheTile * kCacheHidden * 2;
-// Inference CTA: 512 threads; four threads encode one query (four levels = one 16-byte operand
-// chunk each, so four times the table gathers in flight), the first warpgroup runs the MLP.
-constexpr uint32_t kInfThreads = 512;
-constexpr uint32_t kInfCtasPerSm = 1;
+// Inference CTA: 256 threads; two threads encode one query (eight levels = two 16-byte operand
+// chunks each), the first warpgroup runs the MLP.  Two CTAs per SM: the MLP chain of one (three
+// dependent MMAs, 12 of 16 warps idle) overlaps the table gathers of the other.
+constexpr uint32_t kInfThreads = 256;
+constexpr uint32_t kInfCtasPerSm = 2;
+constexpr uint32_t kInfParts = kInfThreads / kCacheTile;  // threads per query
+static_assert(kInfParts * kCacheTile == kInfThreads && 4 % kInfParts == 0, "whole operand chunks per thread");
 
 // Writes 8 f16 values (one 16-byte chunk) of row r, chunk q of a K-major tile.
 S2D void store_chunk(uint8_t* tile, uint32_t r, uint32_t q, uint32_t K, const __half2 h[4]) {
@@ -185,8 +225,8 @@ S2D void tmem_relu_to_tile(uint32_t tlane, uint32_t col, uint8_t* dst, uint32_t 
 // (the path tracer's terminal vertices) the result is instead added to the path's accumulator:
 // accum[slot] += tput[i] * max(y, 0), slot in pos[i].w, or with `total_fx` (the batched renderer)
 // to the pixel's fixed-point totals.  n_dev (optional) caps n with a device count.
-// Persistent: grid-stride over tiles of 128 queries; 128 threads; kInfSmemBytes dynamic smem.
-__global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
+// Persistent: grid-stride over tiles of 128 queries; kInfThreads threads; kInfSmemBytes dynamic smem.
+__global__ void __launch_bounds__(kInfThreads, kInfCtasPerSm) k_cache_infer(const __grid_constant__ CacheDev c, const float4* __restrict__ pos,
                                                                 uint32_t n, const uint32_t* __restrict__ n_dev,
                                                                 float4* __restrict__ out, const float4* __restrict__ tput,
                                                                 float4* __restrict__ accum,
@@ -227,17 +267,22 @@ __global__ void __launch_bounds__(kInfThreads, 1) k_cache_infer(const __grid_con
     const uint32_t tiles = (n + kCacheTile - 1) / kCacheTile;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         {
-            // encode: thread t takes query row t / 4, levels 4 * (t % 4) .. +3 (one operand chunk)
-            const uint32_t row = t >> 2, part = t & 3u, q = tile * kCacheTile + row;
-            __half2 f[4];
-            if (q < n) {
-                const float4 p = pos[q];
-                cache_encode4(c, f3(p.x, p.y, p.z), 4u * part, f);
-            } else {
+            // encode: thread t takes query row t / kInfParts and the operand chunks (four levels
+            // each) part, part + kInfParts, ... of it
+            const uint32_t row = t / kInfParts, part = t % kInfParts, q = tile * kCacheTile + row;
+            float3 p = f3(0.f);
+            if (q < n) { const float4 p4 = pos[q]; p = f3(p4.x, p4.y, p4.z); }
 #pragma unroll
-                for (uint32_t j = 0; j < 4; ++j) f[j] = __floats2half2_rn(0.f, 0.f);
+            for (uint32_t ch = part; ch < 4; ch += kInfParts) {
+                __half2 f[4];
+                if (q < n) {
+                    cache_encode4(c, p, 4u * ch, f);
+                } else {
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; ++j) f[j] = __floats2half2_rn(0.f, 0.f);
+                }
+                store_chunk(smem + kInfSmemX, row, ch, kCacheIn, f);
             }
-            store_chunk(smem + kInfSmemX, row, part, kCacheIn, f);
         }
         const uint32_t q = tile * kCacheTile + t;  // MLP row of warps 0..3
         // layer 1: D[0:64) = X W1^T
