@@ -596,6 +596,9 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             P.sh_parity = merge ? (b & 1u) : 0u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
             P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
+            // camera paths are queued pixel by pixel: a warp's samples share a pixel and nearly
+            // always its material, so the material sort starts with the first bounce
+            P.sort_on = sort && b > 0;
             if (P.ray_sorted) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(0);
             P.hint_tri = hint && b == 0 ? st->hint_tri : nullptr;
@@ -608,7 +611,7 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             }
             P.hint_tri = nullptr;
             ev_end();
-            if (sort) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
+            if (P.sort_on) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(1);
             if (lam) { if (restir) launch_shade<true, true>(P, parity, st, s); else launch_shade<true, false>(P, parity, st, s); }
             else { if (restir) launch_shade<false, true>(P, parity, st, s); else launch_shade<false, false>(P, parity, st, s); }
