@@ -596,9 +596,11 @@ extern "C" int s2_render(S2Context* ctx, const S2View* view, const S2RenderParam
             P.sh_parity = merge ? (b & 1u) : 0u;
             k_bounce_setup<<<1, 32, 0, s>>>(P, parity, b == 0);
             P.ray_sorted = ray_sort && b > 0;  // camera rays come in pixel-tile order
-            // camera paths are queued pixel by pixel: a warp's samples share a pixel and nearly
-            // always its material, so the material sort starts with the first bounce
-            P.sort_on = sort && b > 0;
+            // camera paths are queued pixel by pixel: with 32 or more samples per pixel in the wave
+            // a warp's camera paths share a pixel and nearly always its material, so the material
+            // sort starts with the first bounce (with fewer, a warp spans several pixels and the
+            // camera bounce is sorted too)
+            P.sort_on = sort && (b > 0 || P.wave_samples < 32);
             if (P.ray_sorted) { launch_sort(P, parity, st->sort_blocks, s); launches += 3; }
             ev_begin(0);
             P.hint_tri = hint && b == 0 ? st->hint_tri : nullptr;
