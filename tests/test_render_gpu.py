@@ -19,7 +19,7 @@ z = (gpu - oracle) / sqrt(var_gpu + var_oracle) with var_gpu from the 16 batches
 (box) or twice the noise floor the two estimators' variances predict (terrain: sun and glossy spheres
 give a high relative per-sample variance).  The parity terrain uses a sun of radiance 50 over a
 5 degree cone: the benchmark's 5e3 sun over 0.5 degrees makes per-pixel estimates heavy-tailed
-(rare sun reflections), which no z-test at these sample counts can judge.
+(rare sun reflections), which no z-test at these sample counts can assess.
 """
 from pathlib import Path
 

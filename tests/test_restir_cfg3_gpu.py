@@ -7,7 +7,7 @@ of 1920x1080 (same camera and scene; the reference image below needs 65,536 spp 
 The camera plays the workload's closed Catmull-Rom loop (16 views) over and over, reusing across
 frames; the frames rendered at the loop's last view average to plain NEE there (a 16 x 4096 spp NEE
 image of that view): over 24 independent batches of 48 loops, the image total agrees by a z-test,
-and so does RIS alone (frames without reuse, the control).  A per-pixel z-test is no judge here:
+and so does RIS alone (frames without reuse, the control).  A per-pixel z-test cannot decide here:
 emitters 2-8 cm above the terrain make single-pixel estimates so heavy tailed that RIS alone, which
 is unbiased by construction, fails it at this sample count exactly as the reuse does (measured on
 B200: 1.9 % vs 2.1 % of pixel channels beyond |z| = 5, mean z -0.55 vs -0.56, image totals +0.3 %
