@@ -68,8 +68,10 @@ struct DiGrid {
     int end_bit = 64;
 };
 
-int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size, size_t wide_bytes = 0) {
+// `fresh` (optional) is set when the grid was (re)allocated: its buffers then hold no reservoirs.
+int ensure_di_grid(S2Context* ctx, DiGrid& G, uint32_t cells, uint32_t size, size_t wide_bytes = 0, bool* fresh = nullptr) {
     if (G.g.checksums && G.g.cell_count == cells && G.g.max_size >= size && G.wide_bytes == wide_bytes) return S2_OK;
+    if (fresh) *fresh = true;
     free_bufs(G.bufs);
     G.g = HashGridDev{};
     G.wide = nullptr;
@@ -264,8 +266,13 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
         // VCM.cpp:27, 491-500: as the DI grid, one record per camera vertex
         const uint32_t cells = 100000u;
         const uint32_t size = (uint32_t)std::min<uint64_t>((uint64_t)pixels * std::max(1u, prm->max_path_length - 1), 1u << 24);
-        for (auto& g : vs->lvc_grid) {
-            const int rc0 = ensure_di_grid(ctx, g, cells, size, sizeof(vk::LvcRecord));
+        // a grid reallocated for a larger call holds no reservoirs: if it is the one the first
+        // iteration would read, there is no history
+        for (uint32_t k = 0; k < 2; ++k) {
+            DiGrid& g = vs->lvc_grid[k];
+            bool fresh = false;
+            const int rc0 = ensure_di_grid(ctx, g, cells, size, sizeof(vk::LvcRecord), &fresh);
+            if (fresh && k != vs->lvc_cur) vs->lvc_prev_valid = false;
             if (rc0 != S2_OK) { vs->lvc_prev_valid = false; return set_error(ctx, rc0, "LVC reservoir grid allocation failed"); }
             g.g.min_cell_size = 0.1f;
             g.g.cell_pixel_radius = 0.f;
@@ -279,8 +286,11 @@ extern "C" int s2_render_vcm(S2Context* ctx, const S2View* view, const S2VcmPara
         // VCM.cpp:26, 490-499: 100,000 cells of at least 0.1, one record per camera vertex
         const uint32_t cells = 100000u;
         const uint32_t size = (uint32_t)std::min<uint64_t>((uint64_t)pixels * std::max(1u, prm->max_path_length - 1), 1u << 24);
-        for (auto& g : vs->grid) {
-            const int rc0 = ensure_di_grid(ctx, g, cells, size);
+        for (uint32_t k = 0; k < 2; ++k) {  // as for the LVC grids above
+            DiGrid& g = vs->grid[k];
+            bool fresh = false;
+            const int rc0 = ensure_di_grid(ctx, g, cells, size, 0, &fresh);
+            if (fresh && k != vs->cur) vs->prev_valid = false;
             if (rc0 != S2_OK) { vs->prev_valid = false; return set_error(ctx, rc0, "reservoir grid allocation failed"); }
             g.g.min_cell_size = 0.1f;
             g.g.cell_pixel_radius = 0.f;

@@ -240,3 +240,21 @@ def test_lvc_reservoir_reuse_reproducible(device, box):
     device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 1, 1))
     fresh = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 60, vcm_flags=fl)).radiance
     np.testing.assert_array_equal(fresh, seqs[0][0])
+
+
+def test_reservoir_grids_grown_for_a_larger_view_carry_no_history(device, box):
+    """A call that needs larger reservoir grids than the previous one (here a 64x64 view after a
+    32x32 one) reallocates them, so the reservoirs of the smaller call are gone: its first
+    iteration must resample without history, exactly as after a call without reuse."""
+    from stratum2_b200.scene import make_view
+    wl, _, _ = box
+    device.upload_scene(wl.scene)
+    small = make_view((0.0, 0.0, 3.0), 32, 32, 40.0)
+    fl = (_abi.VCM_FLAG_LIGHT_VERTEX_CACHE | _abi.VCM_FLAG_LVC_RIS | _abi.VCM_FLAG_LVC_REUSE |
+          _abi.VCM_FLAG_DI_RIS | _abi.VCM_FLAG_DI_REUSE)
+    device.render_vcm(small, 32, 32, vparams(_abi.VCM_BPT, 2, 70, vcm_flags=fl, di_m=8))  # grids sized for 32x32
+    grown = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 80, vcm_flags=fl, di_m=8)).radiance
+    device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 1, 1))  # drops the grids
+    fresh = device.render_vcm(wl.view, W, H, vparams(_abi.VCM_BPT, 2, 80, vcm_flags=fl, di_m=8)).radiance
+    assert np.all(np.isfinite(grown))
+    np.testing.assert_array_equal(grown, fresh)
